@@ -1,0 +1,368 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 force-and-integrate step (one JSON line on rank 0).
+
+Workload (default): the bead-spring polymer melt of the headline metric —
+400 chains x 100 beads (40,000 beads, 3 types), tabulated harmonic bond,
+angle (112 deg) and 3-fold torsion, six Lorentz-Berthelot LJ tables to a
+1.0 nm cutoff (list 1.2 nm, rebuilt every 10 steps), Berendsen NVT at 500 K,
+dt 1 fs; seeded synthetic input written in the reference's file formats.
+A step is one loop body of NEW_LOOP.F90 (SHIFT, list rebuild when due,
+nonbonded + bonded forces, MOVE, Berendsen scaling).
+
+Legs:
+  value      device time (CUDA events on the library's stream) of K steps
+             replayed as CUDA graphs, state resident in HBM, L2 flushed
+             before each step (a 256 MiB write, outside the timed interval);
+  e2e        wall time through the C ABI with host buffers: ibg_set_state
+             from pinned host arrays, K x ibg_step with its observables read
+             back each step, ibg_get_state at the end;
+  fp64_plain the same K steps on the plain FP64 path (comparison path);
+  roofline   nonbonded kernel, the dominant launch: algorithmic bytes per
+             launch (16 B position + 4 B per listed pair, per particle) over its
+             event-timed average duration, against the measured HBM copy peak;
+  cpu_baseline  the oracle (C++ restatement of the reference, OpenMP) on this
+             host's cores over a bounded sample of the same workload.
+
+--impl reference times that CPU restatement alone (the reference itself is
+Fortran and no Fortran compiler is available).
+Multi-GPU (torchrun): one independent replica per GPU, weak scaling, timing =
+max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "melt40k": "bead-spring melt: 400 chains x 100 beads (40,000), 3 types, bond/angle/torsion tables, "
+               "6 LJ tables rc 1.0 nm, list 1.2 nm every 10 steps, NVT 500 K, dt 1 fs",
+    "fluid4k": "single-type LJ fluid: 4,000 beads, rho 8/nm^3, rc 1.2 nm, list 1.4 nm every 10 steps, NVE, dt 10 fs",
+    "melt2m": "CG melt: 10,000 chains x 200 beads (2,000,000), 4 types, bond/angle tables, 10 LJ tables "
+              "rc 1.4 nm, list 1.6 nm every 10 steps, NVT 300 K, dt 10 fs",
+}
+
+
+def make_workload(name: str, directory: str):
+    from ibisco_b200 import synth
+
+    if name == "melt40k":
+        spec = synth.config2(nchains=400, nper=100, seed=2)
+    elif name == "fluid4k":
+        spec = synth.config1(n=4000, seed=1)
+    elif name == "melt2m":
+        spec = synth.config4()
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    synth.write_system(spec, directory)
+    return spec
+
+
+class Clocks:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            p = [x.strip() for x in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for k, n in enumerate(names):
+                if p[5 + k].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_summary: str):
+    """Per-launch DRAM bytes of the nonbonded kernel from the committed ncu
+    summary (a 'dram_bytes_per_launch: <n>' line), scaled later to this run."""
+    p = os.path.join(ROOT, "profiles", kernel_summary)
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"dram_bytes_per_particle:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+def cpu_baseline(directory: str, n_particles: int, budget_s: float = 20.0, max_steps: int = 40):
+    """Oracle (OpenMP) on this host's cores: init, one warm-up step, then steps
+    until the time budget is used."""
+    from oracle import oracle as orc
+
+    threads = os.cpu_count() or 1
+    o = orc.Oracle(directory, threads=threads)
+    o.init(0)
+    o.step(1, 0)
+    t0 = time.perf_counter()
+    k = 0
+    while k < max_steps:
+        o.step(2 + k, 0)
+        k += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": n_particles * k / dt, "unit": "atom-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{k} steps of the full {n_particles}-particle workload after 1 warm-up step "
+                      f"({dt:.1f} s, REAL*4 restatement of the reference, OpenMP {threads} threads)"}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def reduce_max(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def run_reference(args, world, rank, pg):
+    if rank != 0:
+        return
+    with tempfile.TemporaryDirectory() as d:
+        make_workload(args.workload, d)
+        from oracle import oracle as orc
+
+        threads = os.cpu_count() or 1
+        o = orc.Oracle(d, threads=threads)
+        n = o.info["NATOMS"]
+        o.init(0)
+        for k in range(args.warmup):
+            o.step(1 + k, 0)
+        # bounded sample: stop early if the projected time exceeds ~150 s
+        t0 = time.perf_counter()
+        done = 0
+        for k in range(args.steps):
+            o.step(1 + args.warmup + k, 0)
+            done += 1
+            el = time.perf_counter() - t0
+            if el / done * args.steps > 150.0 and done >= 3:
+                break
+        el = time.perf_counter() - t0
+        value = n * done / el
+        line = {"impl": "reference", "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s",
+                "n_gpus": world, "steps": done, "warmup": args.warmup, "ms_per_step": 1000 * el / done,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
+                                                "particles": n},
+                "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": threads, "kind": "port",
+                                 "sample": f"{done} of {args.steps} requested steps (C++ REAL*4 restatement of the "
+                                           f"reference, OpenMP {threads} threads; no Fortran compiler here)"},
+                "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+
+
+def run_b200(args, world, rank, local, pg):
+    import ctypes
+
+    from ibisco_b200 import native
+
+    native.lib()
+    native.lib().ibg_set_device(local)
+    with tempfile.TemporaryDirectory() as d:
+        make_workload(args.workload, d)
+        setup = native.Setup(d)
+        s0, v0, b0 = setup.initial_state()
+        n = s0.shape[0]
+        nitems = len(setup.array("ITYPE"))
+        dt_ps = float(open(os.path.join(d, "control")).read().split("time_step")[1].split()[0])
+        prec = native.IBG_PREC_FP64_PLAIN if args.precision == "fp64" else native.IBG_PREC_FP32_FIXED
+        g = native.System(setup, prec)
+        g.set_state(s0, v0, b0)
+        flush = 256 << 20
+        g.set_l2_flush(flush)
+        # ---- warm-up (captures the CUDA graphs) and device-timed region
+        g.run(1, args.warmup)
+        barrier(pg)
+        l0 = g.timing()["launches"]
+        with Clocks(local) as clk:
+            g.run(1 + args.warmup, args.steps)
+        tm = g.timing()
+        launches = tm["launches"] - l0
+        ms = reduce_max(pg, tm["run_ms"])
+        barrier(pg)
+        value = world * n * args.steps / (ms / 1000.0)
+        # ---- roofline of the nonbonded kernel (event-timed stage pass)
+        g.set_l2_flush(flush)
+        g.set_timing(True)
+        k_roof = min(args.steps, 200)
+        g.run(1 + args.warmup + args.steps, k_roof)
+        t2 = g.timing()
+        g.set_timing(False)
+        _, nn = g.neighbour_list(0)
+        pairs = float(nn.sum())
+        nb_launch_s = t2["nonbonded_ms"] / max(1, t2["nonbonded_launches"]) / 1000.0
+        bytes_launch = 16.0 * n + 4.0 * pairs
+        peak, peak_kind = measured_peak()
+        achieved = bytes_launch / nb_launch_s / 1e9
+        tr = ncu_traffic("nonbonded_melt40k.md")
+        roof = {"bound": "hbm", "kernel": "k_nonbonded", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": (tr * n if tr else None),
+                "peak_kind": peak_kind, "launch_us": nb_launch_s * 1e6,
+                "algorithmic_bytes_per_launch": bytes_launch, "mean_half_list": pairs / n}
+        stage = {k: t2[k] / k_roof for k in ("list_ms", "nonbonded_ms", "bonded_ms", "integrate_ms", "other_ms")}
+        # ---- end to end through the C ABI with host buffers
+        sp = np.ascontiguousarray(s0, np.float32)
+        vp = np.ascontiguousarray(v0, np.float32)
+        bp = np.ascontiguousarray(b0, np.float32)
+        out = {k: np.zeros((nitems, 3), np.float32) for k in ("s", "r", "f")}
+        vo = np.zeros((n, 3), np.float32)
+        obs = native.IbgObs()
+        L = native.lib()
+        k_e2e = args.steps
+        barrier(pg)
+        t0 = time.perf_counter()
+        g.set_state(sp, vp, bp)
+        for k in range(k_e2e):
+            rc = L.ibg_step(g._h, 1 + k, ctypes.byref(obs))
+            if rc:
+                raise native.IbiscoError(rc, L.ibg_last_error(g._h).decode())
+        g._check(L.ibg_get_state(g._h, native._fp(out["s"]), native._fp(out["r"]), native._fp(vo),
+                                 native._fp(out["f"])))
+        e2e_s = reduce_max(pg, time.perf_counter() - t0)
+        h2d = (sp.nbytes + vp.nbytes + bp.nbytes) / k_e2e
+        d2h = ctypes.sizeof(native.IbgObs) + (3 * out["s"].nbytes + vo.nbytes) / k_e2e
+        e2e = {"value": world * n * k_e2e / e2e_s, "unit": "atom-steps/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h}
+        # ---- plain FP64 path, same workload and timing
+        fp64 = None
+        if prec == native.IBG_PREC_FP32_FIXED and not args.no_fp64:
+            g64 = native.System(setup, native.IBG_PREC_FP64_PLAIN)
+            g64.set_state(s0, v0, b0)
+            g64.set_l2_flush(flush)
+            g64.run(1, args.warmup)
+            g64.run(1 + args.warmup, args.steps)
+            ms64 = reduce_max(pg, g64.timing()["run_ms"])
+            fp64 = {"value": world * n * args.steps / (ms64 / 1000.0), "ms_per_step": ms64 / args.steps,
+                    "ratio_fp32_fixed_over_fp64": ms64 / ms}
+            g64.close()
+        cpu = None
+        if rank == 0 and world == 1 and not args.no_cpu:
+            cpu = cpu_baseline(d, n)
+        if rank == 0:
+            steps_per_s = args.steps / (ms / 1000.0)
+            line = {
+                "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32" if prec == native.IBG_PREC_FP32_FIXED else "f64",
+                "data": "synthetic",
+                "config": {"workload": args.workload, "description": WORKLOADS[args.workload], "particles": n,
+                           "precision": "FP32 pair math, int64 fixed-point force sums, FP64 integration"
+                           if prec == native.IBG_PREC_FP32_FIXED else "FP64 throughout",
+                           "parallelism": f"{world} independent replica(s), one per GPU",
+                           "l2": "flushed before every step (256 MiB write, outside the timed interval)"},
+                "ns_per_day": steps_per_s * dt_ps * 1e-3 * 86400.0,
+                "roofline": roof, "stage_ms_per_step": stage,
+                "cpu_baseline": cpu, "e2e": e2e, "fp64_plain": fp64, "gpu_launches": launches,
+                "clocks": clk.summary(),
+            }
+            print(json.dumps(line), flush=True)
+        g.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="melt40k")
+    ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world, rank, local, pg = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank, pg)
+        else:
+            run_b200(args, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

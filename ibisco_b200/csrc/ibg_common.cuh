@@ -1,0 +1,91 @@
+// Shared definitions of the B200 step: precision policies, device scalar
+// block, error bits and warp/block reduction helpers.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ibg {
+
+// Error bits raised by kernels; the host maps the lowest set bit to a status.
+enum : unsigned {
+  EB_LIST_OVERFLOW = 1u << 0,  // a particle reached MAXNAB neighbours
+  EB_TORSION = 1u << 1,        // torsion angle outside its table
+  EB_OOP = 1u << 2,            // out-of-plane angle outside its table
+  EB_FIXED = 1u << 3,          // a force left the fixed-point range
+  EB_CELL_GRID = 1u << 4,      // fewer than 3 cells per dimension
+  EB_TABLE_RANGE = 1u << 5,    // nonbonded distance beyond its table
+  EB_MISSING_TABLE = 1u << 6,  // listed pair without a nonbonded table
+  EB_CAPACITY = 1u << 7,       // neighbour-list / cell storage exhausted
+};
+
+// 64-bit fixed-point force accumulation: value * 2^32, two's complement in
+// unsigned long long so that atomicAdd wraps like signed addition.  The
+// representable range is |F| < 2^31 reduced force units per particle at a
+// resolution of 2^-32.
+constexpr float kFixScale = 4294967296.0f;        // 2^32
+constexpr double kFixInv = 1.0 / 4294967296.0;   // 2^-32
+constexpr float kFixMax = 2147483520.0f;          // largest float below 2^31
+
+// Observables in the order of ibg_obs (ek[2] .. pt[6], box[3]).
+struct ObsD {
+  double ek[2], temp, temp_atom, temp_bead;
+  double v_nb[3], v_bond[3], v_angle[3], v_torsion[3], v_oop[3];
+  double pt[6];
+  double box[3];
+  long long bond_overext, cell_clamps;
+  int step, status;
+};
+
+// Device-resident scalars of one system.
+struct Scalars {
+  int step;          // current step number
+  int rebuild;       // list rebuild this step
+  int mts_m;         // MOD(step, 3+NMTS), -1 without MTS
+  int ring_base;     // step whose observables go to ring slot 0
+  double box[3], boxinv[3], box2[3];  // FP64 box (integration, FP64 path)
+  float boxf[3], boxinvf[3], box2f[3];  // REAL*4 box (FP32 path geometry)
+  int ncell[2][3];   // cell grid of the atom / bead list
+  double lam[2];     // Berendsen factors for atoms / beads (MOVE.F90:73-79)
+  double temp_atom, temp_bead;
+  double miu;        // SCALEBP factor of this step (1 if none)
+  // MTS history (module_MTS.f90): V_NB(label) and PT11..PT13 for m=1..3
+  double mts_vnb[3][3];
+  double mts_pt[6][3];
+  // SCALEBP running window (SCALEBP.f90:240-243)
+  int iavp, pad1;
+  double sp[10];
+  unsigned err;
+  unsigned pad2;
+  unsigned long long bond_overext, cell_clamps;
+  double mom[3];     // momentum removal (MOMENTUM.f90)
+  ObsD obs;          // observables of the last step
+};
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Deterministic block sum of K values per thread; thread 0 of the block gets
+// the result in out[].  Needs K*32 doubles of shared memory.
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K], double* smem, double* out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = warp_sum(v[k]);
+  if (lane == 0)
+    for (int k = 0; k < K; ++k) smem[warp * K + k] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < K; ++k) {
+      double s = 0.0;
+      for (int w = 0; w < nw; ++w) s += smem[w * K + k];
+      out[k] = s;
+    }
+  }
+  __syncthreads();
+}
+
+}  // namespace ibg

@@ -1,0 +1,1138 @@
+// Device context of one Hybrid IBIsCO system and the C ABI of ibisco_gpu.h.
+//
+// Layout in HBM (per system):
+//   S, V            FP64 (3,NATOMS[+NVIRTA]) unwrapped positions / velocities
+//   su              unwrapped positions in the step precision (bonded terms)
+//   fnb, fb         nonbonded / bonded forces, global order, 64-bit fixed
+//                   point (FP32 path) or double (FP64 path)
+//   per list (atom list, bead list):
+//     pos4          wrapped positions in cell order, type|label in .w
+//     fsort         nonbonded forces per slot (cell order)
+//     cells         counting-sorted cell index (LINKS.f90 grid)
+//     entries       Verlet list as slot indices, sliced-ELL: slice g of 32
+//                   slots stores entry k of slot s at off[g] + 32 k + (s & 31)
+//     tables        the nonbonded tables of the list's type pairs
+//   bonded terms    flat (i,j[,k[,l]],table,label) arrays + float4 tables
+//   Scalars         box, thermostat, MTS/barostat history, error bits
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "../../include/ibisco_gpu.h"
+#include "ibg_common.cuh"
+#include "ibg_kernels.cuh"
+
+using namespace ibg;
+
+namespace {
+
+struct CudaError {
+  cudaError_t e;
+};
+
+#define CK(x)                                 \
+  do {                                        \
+    cudaError_t e_ = (x);                     \
+    if (e_ != cudaSuccess) throw CudaError{e_}; \
+  } while (0)
+
+template <typename T>
+T* dalloc(size_t n, std::vector<void*>& owned) {
+  void* p = nullptr;
+  if (n == 0) n = 1;
+  CK(cudaMalloc(&p, n * sizeof(T)));
+  CK(cudaMemset(p, 0, n * sizeof(T)));
+  owned.push_back(p);
+  return (T*)p;
+}
+template <typename T>
+T* dupload(const std::vector<T>& h, std::vector<void*>& owned) {
+  T* p = dalloc<T>(h.size(), owned);
+  if (!h.empty()) CK(cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return p;
+}
+
+enum Variant : unsigned {
+  V_REBUILD = 1u,
+  V_MOMENTUM = 2u,
+  V_SCALE = 4u,
+  V_FORCE_ONLY = 8u,
+  V_MTS_APPROX = 16u,
+};
+
+struct DevList {
+  int n = 0, which = 0, present = 0;
+  int cell_cap = 0, nslices = 0;
+  long long cap_entries = 0;
+  int *idx = nullptr, *cell_of = nullptr, *cell_count = nullptr, *cell_start = nullptr, *cell_fill = nullptr;
+  int *sorted = nullptr, *sorted_new = nullptr, *slot_of = nullptr, *slot_of_new = nullptr;
+  int *counts = nullptr, *slice_w = nullptr, *entries = nullptr;
+  long long* slice_off = nullptr;
+  void *pos4 = nullptr, *pos4_new = nullptr, *fsort = nullptr, *mtsf = nullptr;
+  size_t pos_bytes = 0;
+  // tables of this list
+  int *ltab = nullptr, *toff = nullptr, *tndat = nullptr;
+  void *tbin = nullptr, *tfp = nullptr, *tx = nullptr;
+  int ntab = 0, nrows = 0;
+  size_t smem = 0;
+  bool use_smem = false;
+  float rlist = 0, rlistsq = 0, rcutsq = 0;
+  int grid_nb = 0;
+  double* part = nullptr;
+};
+
+}  // namespace
+
+struct ibg_ctx {
+  int prec = 0;
+  int dev = 0, nsm = 148;
+  cudaStream_t st = nullptr;
+  std::vector<void*> owned;
+  std::string err;
+  // descriptor scalars
+  int natoms = 0, nvirta = 0, nitems = 0, ntype = 0, numatoms = 0, numbeads = 0, ncoarse = 0;
+  int ensemble = 0, nupdate = 1, halt_drift = 1, nmts = 0, ibrdescr = 1, maxnab = 1000;
+  float dt = 0, fac = 0, pfac = 0, temp_in = 0, pressure = 0, mktemp = 0, mktemp_atom = 0, mktemp_bead = 0;
+  float r2d = 0;
+  // device arrays
+  double *S = nullptr, *V = nullptr, *mass = nullptr, *invmass = nullptr;
+  void *su = nullptr, *fnb = nullptr, *fb = nullptr;
+  int *tbits = nullptr, *gslot = nullptr, *excl_n = nullptr, *excl = nullptr;
+  int *vcenter = nullptr, *vnum = nullptr, *vmem = nullptr;
+  float *vmass = nullptr, *vinv = nullptr, *vcoef = nullptr;
+  // bonded
+  int nb = 0, na = 0, nt = 0, no = 0;
+  int4 *bonds = nullptr, *angles = nullptr, *tors = nullptr, *oops = nullptr;
+  int2 *tors_t = nullptr, *oops_t = nullptr;
+  float4 *tb = nullptr, *ta = nullptr, *tt = nullptr, *to = nullptr;
+  int *tb_off = nullptr, *ta_off = nullptr, *tt_off = nullptr, *to_off = nullptr;
+  int *tb_nd = nullptr, *ta_nd = nullptr, *tt_nd = nullptr, *to_nd = nullptr;
+  float *tb_bin = nullptr, *ta_bin = nullptr, *tt_bin = nullptr, *to_bin = nullptr;
+  DevList L[2];
+  Scalars* sc = nullptr;
+  ObsD* ring = nullptr;
+  int ring_cap = 0;
+  double *p_b = nullptr, *p_mv = nullptr, *p_mom = nullptr;
+  int g_b = 0, g_mv = 0, g_pos = 0;
+  bool fb_dirty = false;
+  bool state_set = false;
+  std::map<unsigned, cudaGraphExec_t> graphs;
+  std::vector<cudaGraph_t> graph_defs;
+  long long launches_per_variant[32] = {0};
+  // timing: stage events (timing mode, direct launches) and whole-run events
+  bool timing = false;
+  double stage_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  std::vector<std::pair<cudaEvent_t, int>> marks;  // event, stage that starts there
+  cudaEvent_t run_ev[2] = {nullptr, nullptr};
+  long long launches = 0;
+  // L2 flush between timed steps
+  size_t flush_bytes = 0;
+  void* flush_buf = nullptr;
+  std::vector<cudaEvent_t> step_ev;
+};
+
+namespace {
+
+int fail(ibg_ctx* c, int code, const std::string& m) {
+  if (c) c->err = m;
+  return code;
+}
+
+int status_from_bits(unsigned b) {
+  if (!b) return IBG_OK;
+  if (b & EB_LIST_OVERFLOW) return IBG_E_LIST_OVERFLOW;
+  if (b & EB_TORSION) return IBG_E_TORSION_TABLE;
+  if (b & EB_OOP) return IBG_E_OOP_RANGE;
+  if (b & EB_FIXED) return IBG_E_FIXED_OVERFLOW;
+  if (b & EB_CELL_GRID) return IBG_E_CELL_GRID;
+  if (b & EB_TABLE_RANGE) return IBG_E_TABLE_RANGE;
+  if (b & EB_MISSING_TABLE) return IBG_E_MISSING_TABLE;
+  if (b & EB_CAPACITY) return IBG_E_CAPACITY;
+  return IBG_E_INVALID;
+}
+const char* bits_message(unsigned b) {
+  if (b & EB_LIST_OVERFLOW) return "LIST TOO SMALL: a particle reached MAXNAB neighbours";
+  if (b & EB_TORSION) return "FATAL ERROR: Entry in torsion table does not exist";
+  if (b & EB_OOP) return "out of plane angle outside its table";
+  if (b & EB_FIXED) return "force outside the 64-bit fixed-point range";
+  if (b & EB_CELL_GRID) return "fewer than 3 cells per dimension for the neighbour list";
+  if (b & EB_TABLE_RANGE) return "distance or angle outside its table";
+  if (b & EB_MISSING_TABLE) return "listed pair without a nonbonded table";
+  if (b & EB_CAPACITY) return "device neighbour-list or cell storage exhausted";
+  return "unknown device error";
+}
+
+size_t rsize(const ibg_ctx* c) { return c->prec == IBG_PREC_FP32_FIXED ? sizeof(float) : sizeof(double); }
+size_t accsize(const ibg_ctx* c) { return c->prec == IBG_PREC_FP32_FIXED ? sizeof(unsigned long long) : sizeof(double); }
+size_t possize(const ibg_ctx* c) { return c->prec == IBG_PREC_FP32_FIXED ? sizeof(float4) : sizeof(double4); }
+
+// ----------------------------------------------------------- list setup
+void build_list(ibg_ctx* c, const ibg_desc* d, int which) {
+  DevList& L = c->L[which];
+  L.which = which;
+  std::vector<int> idx;
+  if (which == 0) for (int a = 0; a < d->numatoms; ++a) idx.push_back(d->atom[a] - 1);
+  else for (int a = 0; a < d->ncoarse; ++a) idx.push_back(d->bead[a] - 1);
+  L.n = (int)idx.size();
+  L.present = L.n > 0;
+  if (!L.present) return;
+  L.rlist = which == 0 ? d->rlist_atom : d->rlist_bead;
+  L.rlistsq = L.rlist * L.rlist;  // RLISTSQ = RLIST*RLIST (NEW_NEIGHBOUR_WITHLIST.f90:26)
+  L.rcutsq = which == 0 ? d->rcutsq_atom : d->rcutsq_bead;
+  L.nslices = (L.n + 31) / 32;
+  auto& o = c->owned;
+  L.idx = dupload(idx, o);
+  L.cell_of = dalloc<int>(L.n, o);
+  L.sorted = dalloc<int>(L.n, o);
+  L.sorted_new = dalloc<int>(L.n, o);
+  std::vector<int> ident(L.n);
+  for (int a = 0; a < L.n; ++a) ident[a] = a;
+  L.slot_of = dupload(ident, o);
+  CK(cudaMemcpy(L.sorted, ident.data(), sizeof(int) * L.n, cudaMemcpyHostToDevice));
+  L.slot_of_new = dalloc<int>(L.n, o);
+  L.counts = dalloc<int>(L.n, o);
+  L.slice_w = dalloc<int>(L.nslices, o);
+  L.slice_off = dalloc<long long>(L.nslices + 1, o);
+  L.pos_bytes = possize(c) * L.n;
+  L.pos4 = dalloc<unsigned char>(L.pos_bytes, o);
+  L.pos4_new = dalloc<unsigned char>(L.pos_bytes, o);
+  L.fsort = dalloc<unsigned char>(accsize(c) * 3 * L.n, o);
+  if (which == 1 && c->nmts > 0) L.mtsf = dalloc<unsigned char>(accsize(c) * 9 * L.n, o);
+  L.cell_cap = 0;  // sized in ibg_set_state once the box is known
+  // nonbonded tables of the type pairs present in this list
+  std::set<int> types;
+  for (int a = 0; a < L.n; ++a) types.insert(d->itype[idx[a]] - 1);
+  const int NT = d->ntype;
+  std::vector<int> ltab((size_t)NT * NT, -1);
+  std::map<int, int> local;
+  std::vector<int> order;
+  for (int ti : types)
+    for (int tj : types) {
+      int g = d->inbondt[(size_t)ti + (size_t)NT * tj];
+      if (g <= 0) continue;
+      if (!local.count(g)) { local[g] = (int)order.size(); order.push_back(g); }
+      ltab[(size_t)ti * NT + tj] = local[g];
+    }
+  L.ntab = (int)order.size();
+  std::vector<int> toff(L.ntab + 1, 0), tnd(L.ntab, 0);
+  std::vector<double> fp, xx, bin(L.ntab);
+  for (int t = 0; t < L.ntab; ++t) {
+    int g = order[t];  // 1-based table
+    int nd = d->ndatnb[g - 1];
+    tnd[t] = nd;
+    bin[t] = d->binnb[g - 1];
+    toff[t] = (int)xx.size();
+    int rows = std::min(nd + 2, d->ld_nb);
+    for (int k = 0; k < rows; ++k) {
+      size_t at = (size_t)k + (size_t)d->ld_nb * (g - 1);
+      fp.push_back(d->nbond_force[at]);
+      fp.push_back(d->nbond_pot[at]);
+      xx.push_back(d->rnbond[at]);
+    }
+    for (int k = rows; k < nd + 2; ++k) { fp.push_back(0); fp.push_back(0); xx.push_back(0); }
+  }
+  toff[L.ntab] = (int)xx.size();
+  L.nrows = (int)xx.size();
+  L.ltab = dupload(ltab, o);
+  L.toff = dupload(toff, o);
+  L.tndat = dupload(tnd, o);
+  if (c->prec == IBG_PREC_FP32_FIXED) {
+    std::vector<float> f1(fp.begin(), fp.end()), x1(xx.begin(), xx.end()), b1(bin.begin(), bin.end());
+    L.tfp = dupload(f1, o); L.tx = dupload(x1, o); L.tbin = dupload(b1, o);
+  } else {
+    L.tfp = dupload(fp, o); L.tx = dupload(xx, o); L.tbin = dupload(bin, o);
+  }
+  const size_t rs = rsize(c);
+  L.smem = 9 * 8 * sizeof(double) + rs * 3 * (size_t)L.nrows + rs * L.ntab + sizeof(int) * ((size_t)NT * NT + 2 * L.ntab + 1) + 64;
+  L.use_smem = L.smem <= 200 * 1024;
+}
+
+void alloc_cells(ibg_ctx* c, DevList& L, const float* box) {
+  if (!L.present) return;
+  long long ncap = 1;
+  for (int k = 0; k < 3; ++k) ncap *= std::max(3, (int)std::ceil(box[k] * 1.25f / L.rlist) + 1);
+  if (ncap <= L.cell_cap) return;
+  auto& o = c->owned;
+  L.cell_cap = (int)ncap;
+  L.cell_count = dalloc<int>(ncap, o);
+  L.cell_start = dalloc<int>(ncap + 1, o);
+  L.cell_fill = dalloc<int>(ncap, o);
+}
+
+ListArgs list_args(ibg_ctx* c, DevList& L) {
+  ListArgs a;
+  a.n = L.n; a.which = L.which; a.natoms = c->natoms; a.hybrid = c->ibrdescr == 0; a.maxnab = c->maxnab;
+  a.cell_cap = L.cell_cap;
+  a.rlist = L.rlist; a.rlistsq = L.rlistsq; a.rlistd = (double)L.rlist; a.rlistsqd = (double)L.rlist * (double)L.rlist;
+  a.idx = L.idx; a.cell_of = L.cell_of; a.cell_count = L.cell_count; a.cell_start = L.cell_start; a.cell_fill = L.cell_fill;
+  a.sorted = L.sorted; a.sorted_new = L.sorted_new; a.slot_of = L.slot_of; a.slot_of_new = L.slot_of_new;
+  a.gslot = c->gslot; a.pos4 = L.pos4; a.pos4_new = L.pos4_new;
+  a.counts = L.counts; a.slice_w = L.slice_w; a.slice_off = L.slice_off; a.entries = L.entries;
+  a.cap_entries = L.cap_entries; a.excl_n = c->excl_n; a.excl = c->excl;
+  return a;
+}
+
+int grid_for(ibg_ctx* c, long long work, int per_sm = 8) {
+  long long g = (work + 255) / 256;
+  return (int)std::max<long long>(1, std::min<long long>(g, (long long)c->nsm * per_sm));
+}
+
+// ------------------------------------------------------------ step stages
+// Stage marks (timing mode only): 0 list build, 1 nonbonded, 2 bonded,
+// 3 integrate and reductions, 4 other; 7 ends a step.
+void mark(ibg_ctx* c, int stage) {
+  if (!c->timing) return;
+  cudaEvent_t e;
+  CK(cudaEventCreate(&e));
+  CK(cudaEventRecord(e, c->st));
+  c->marks.emplace_back(e, stage);
+}
+
+void collect_marks(ibg_ctx* c) {
+  if (c->marks.empty()) return;
+  CK(cudaStreamSynchronize(c->st));
+  for (size_t k = 0; k + 1 < c->marks.size(); ++k) {
+    int stg = c->marks[k].second;
+    if (stg == 7) continue;
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->marks[k].first, c->marks[k + 1].first));
+    c->stage_ms[stg] += ms;
+    if (stg == 1) c->stage_ms[6] += 0;  // counted at launch
+  }
+  for (auto& m : c->marks) cudaEventDestroy(m.first);
+  c->marks.clear();
+}
+
+template <typename R>
+void enq_positions(ibg_ctx* c) {
+  PosArgs a;
+  a.natoms = c->natoms; a.nvirta = c->nvirta; a.S = c->S; a.su = c->su; a.Svs = c->S + 3 * (size_t)c->natoms;
+  a.tbits = c->tbits; a.gslot = c->gslot;
+  a.pos4[0] = c->L[0].pos4; a.pos4[1] = c->L[1].pos4;
+  a.vcenter = c->vcenter; a.vnum = c->vnum; a.vmem = c->vmem; a.vmass = c->vmass; a.vinv = c->vinv;
+  k_positions<R><<<c->g_pos, 256, 0, c->st>>>(a, c->sc);
+  ++c->launches;
+}
+
+template <typename R>
+void enq_rebuild(ibg_ctx* c, DevList& L) {
+  if (!L.present) return;
+  ListArgs a = list_args(c, L);
+  k_regrid<R><<<1, 32, 0, c->st>>>(a, c->sc);
+  CK(cudaMemsetAsync(L.cell_count, 0, sizeof(int) * L.cell_cap, c->st));
+  k_cell_assign<R><<<grid_for(c, L.n), 256, 0, c->st>>>(a, c->sc);
+  k_scan_int<<<1, 1024, 0, c->st>>>(L.cell_count, L.cell_start, L.cell_cap, L.cell_fill);
+  k_cell_fill<<<grid_for(c, L.n), 256, 0, c->st>>>(a);
+  k_cell_sort<<<grid_for(c, L.cell_cap), 256, 0, c->st>>>(a, c->sc);
+  k_reslot<R><<<grid_for(c, L.n), 256, 0, c->st>>>(a);
+  CK(cudaMemcpyAsync(L.pos4, L.pos4_new, L.pos_bytes, cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaMemcpyAsync(L.slot_of, L.slot_of_new, sizeof(int) * L.n, cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaMemcpyAsync(L.sorted, L.sorted_new, sizeof(int) * L.n, cudaMemcpyDeviceToDevice, c->st));
+  const int gl = grid_for(c, (long long)L.nslices * 32, 16);
+  k_list_build<R, false><<<gl, 256, 0, c->st>>>(a, c->sc);
+  k_scan_slices<<<1, 1024, 0, c->st>>>(L.slice_w, L.slice_off, L.nslices);
+  k_list_build<R, true><<<gl, 256, 0, c->st>>>(a, c->sc);
+  c->launches += 9;
+}
+
+template <typename R>
+void enq_nonbonded(ibg_ctx* c, DevList& L) {
+  NBArgs<R> A;
+  A.n = L.n; A.nslices = L.nslices; A.ntype = c->ntype;
+  A.pos4 = L.pos4; A.counts = L.counts; A.slice_w = L.slice_w; A.slice_off = L.slice_off; A.entries = L.entries;
+  A.cap_entries = L.cap_entries;
+  A.fsort = (typename Prec<R>::acc_t*)L.fsort;
+  A.ltab = L.ltab; A.toff = L.toff; A.tndat = L.tndat; A.tbin = (const R*)L.tbin; A.tfp = (const R*)L.tfp; A.tx = (const R*)L.tx;
+  A.ntab = L.ntab; A.nrows = L.nrows; A.rcutsq = (R)L.rcutsq;
+  A.part = L.part; A.part_stride = L.grid_nb;
+  if (L.use_smem) k_nonbonded<R, true><<<L.grid_nb, 256, L.smem, c->st>>>(A, c->sc);
+  else k_nonbonded<R, false><<<L.grid_nb, 256, 9 * 8 * sizeof(double), c->st>>>(A, c->sc);
+  ++c->launches;
+}
+
+template <typename R>
+void enq_collect(ibg_ctx* c, DevList& L) {
+  CollectArgs<R> C;
+  C.n = L.n; C.mts = (L.which == 1 && c->nmts > 0); C.sorted = L.sorted; C.idx = L.idx;
+  C.fsort = (typename Prec<R>::acc_t*)L.fsort; C.fnb = (typename Prec<R>::acc_t*)c->fnb;
+  C.mtsf = (typename Prec<R>::acc_t*)L.mtsf;
+  k_nb_collect<R><<<grid_for(c, L.n), 256, 0, c->st>>>(C, c->sc);
+  ++c->launches;
+}
+
+template <typename R>
+void enq_distribute(ibg_ctx* c, void* F) {
+  if (c->nvirta == 0) return;
+  k_distribute<R><<<grid_for(c, c->nvirta), 256, 0, c->st>>>((typename Prec<R>::acc_t*)F, c->natoms, c->nvirta, c->vnum,
+                                                           c->vmem, c->vcoef, c->sc);
+  ++c->launches;
+}
+
+template <typename R>
+void enq_bonded(ibg_ctx* c) {
+  BondedArgs<R> B;
+  B.su = (const R*)c->su; B.fb = (typename Prec<R>::acc_t*)c->fb;
+  B.nb = c->nb; B.na = c->na; B.nt = c->nt; B.no = c->no;
+  B.bonds = c->bonds; B.angles = c->angles; B.tors = c->tors; B.tors_t = c->tors_t; B.oops = c->oops; B.oops_t = c->oops_t;
+  B.tb = c->tb; B.tb_off = c->tb_off; B.tb_ndat = c->tb_nd; B.tb_bin = c->tb_bin;
+  B.ta = c->ta; B.ta_off = c->ta_off; B.ta_ndat = c->ta_nd; B.ta_bin = c->ta_bin;
+  B.tt = c->tt; B.tt_off = c->tt_off; B.tt_ndat = c->tt_nd; B.tt_bin = c->tt_bin;
+  B.to = c->to; B.to_off = c->to_off; B.to_ndat = c->to_nd; B.to_bin = c->to_bin;
+  B.r2d = c->r2d; B.part = c->p_b; B.part_stride = c->g_b;
+  k_bonded<R><<<c->g_b, 256, 0, c->st>>>(B, c->sc);
+  ++c->launches;
+}
+
+template <typename R>
+void enq_move(ibg_ctx* c, int update) {
+  MoveArgs<R> M;
+  M.natoms = c->natoms; M.S = c->S; M.V = c->V;
+  M.fnb = (const typename Prec<R>::acc_t*)c->fnb; M.fb = (const typename Prec<R>::acc_t*)c->fb;
+  M.tbits = c->tbits; M.mass = c->mass; M.invmass = c->invmass; M.dt = (double)c->dt; M.update = update;
+  M.part = c->p_mv; M.part_stride = c->g_mv;
+  k_move<R><<<c->g_mv, 256, 0, c->st>>>(M, c->sc);
+  ++c->launches;
+}
+
+void enq_finalize(ibg_ctx* c, int move) {
+  FinalArgs F;
+  F.p_nb[0] = c->L[0].present ? c->L[0].part : nullptr;
+  F.p_nb[1] = c->L[1].present ? c->L[1].part : nullptr;
+  F.g_nb = c->L[0].present ? c->L[0].grid_nb : c->L[1].grid_nb;
+  F.p_b = c->p_b; F.g_b = c->g_b; F.p_mv = c->p_mv; F.g_mv = c->g_mv;
+  F.mts = c->nmts > 0; F.move = move; F.ensemble = c->ensemble;
+  F.temp_in = c->temp_in; F.fac = c->fac; F.pfac = c->pfac; F.pressure = c->pressure;
+  F.mktemp = c->mktemp; F.mktemp_atom = c->mktemp_atom; F.mktemp_bead = c->mktemp_bead;
+  F.ring = c->ring; F.ring_cap = c->ring_cap;
+  k_finalize<<<1, 1024, 0, c->st>>>(F, c->sc);
+  ++c->launches;
+}
+
+template <typename R>
+void enqueue_step(ibg_ctx* c, unsigned v) {
+  mark(c, 4);
+  k_begin<<<1, 1, 0, c->st>>>(c->sc, c->nupdate, c->nmts);
+  ++c->launches;
+  enq_positions<R>(c);
+  if (v & V_REBUILD) {
+    mark(c, 0);
+    enq_rebuild<R>(c, c->L[0]);
+    enq_rebuild<R>(c, c->L[1]);
+  }
+  // nonbonded: MTS runs the bead list first (MTS_LOOP.f90:100-116); sums are
+  // order independent, so one sequence serves both loops
+  mark(c, 1);
+  if (c->L[1].present && !(v & V_MTS_APPROX)) { enq_nonbonded<R>(c, c->L[1]); c->stage_ms[6] += c->timing; }
+  if (c->L[0].present) { enq_nonbonded<R>(c, c->L[0]); c->stage_ms[6] += c->timing; }
+  mark(c, 4);
+  if (c->L[1].present) enq_collect<R>(c, c->L[1]);
+  if (c->L[0].present) enq_collect<R>(c, c->L[0]);
+  enq_distribute<R>(c, c->fnb);
+  CK(cudaMemsetAsync(c->fb, 0, accsize(c) * 3 * (size_t)c->nitems, c->st));
+  mark(c, 2);
+  enq_bonded<R>(c);
+  mark(c, 4);
+  enq_distribute<R>(c, c->fb);
+  mark(c, 3);
+  if (v & V_FORCE_ONLY) {
+    enq_move<R>(c, 0);
+    enq_finalize(c, 0);
+    mark(c, 7);
+    return;
+  }
+  enq_move<R>(c, 1);
+  if (v & V_MOMENTUM) {
+    k_mom_sum<<<c->g_mv, 256, 0, c->st>>>(c->natoms, c->V, c->mass, c->p_mom, c->g_mv);
+    k_mom_apply<<<c->g_mv, 256, 0, c->st>>>(c->natoms, c->V, c->invmass, c->p_mom, c->g_mv, c->g_mv);
+    c->launches += 2;
+  }
+  enq_finalize(c, 1);
+  if (v & V_SCALE) {
+    k_scale_positions<<<c->g_mv, 256, 0, c->st>>>(c->natoms, c->S, c->sc);
+    ++c->launches;
+  }
+  mark(c, 7);
+}
+
+unsigned variant_of(const ibg_ctx* c, int step, bool force_only) {
+  unsigned v = 0;
+  if (step % c->nupdate == 0) v |= V_REBUILD;
+  if (c->nmts > 0) {
+    int m = step % (3 + c->nmts);
+    if (!(m >= 1 && m <= 3)) v |= V_MTS_APPROX;
+  }
+  if (force_only) return v | V_FORCE_ONLY;
+  if (step % c->halt_drift == 0) v |= V_MOMENTUM;
+  if (c->ensemble == 2 && step % 10 == 0) v |= V_SCALE;
+  return v;
+}
+
+void enqueue(ibg_ctx* c, unsigned v) {
+  if (c->prec == IBG_PREC_FP32_FIXED) enqueue_step<float>(c, v);
+  else enqueue_step<double>(c, v);
+}
+
+void set_step_counter(ibg_ctx* c, int step_before) {
+  int base = step_before + 1;
+  CK(cudaMemcpyAsync(&c->sc->step, &step_before, sizeof(int), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(&c->sc->ring_base, &base, sizeof(int), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+}
+
+int check_device(ibg_ctx* c) {
+  unsigned bits = 0;
+  CK(cudaMemcpyAsync(&bits, &c->sc->err, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (bits) {
+    unsigned zero = 0;
+    CK(cudaMemcpy(&c->sc->err, &zero, sizeof(unsigned), cudaMemcpyHostToDevice));
+    return fail(c, status_from_bits(bits), bits_message(bits));
+  }
+  return IBG_OK;
+}
+
+void obs_to_c(const ObsD& o, ibg_obs* out) {
+  std::memcpy(out->ek, o.ek, sizeof(double) * 2);
+  out->temp = o.temp; out->temp_atom = o.temp_atom; out->temp_bead = o.temp_bead;
+  std::memcpy(out->v_nb, o.v_nb, sizeof(double) * 3);
+  std::memcpy(out->v_bond, o.v_bond, sizeof(double) * 3);
+  std::memcpy(out->v_angle, o.v_angle, sizeof(double) * 3);
+  std::memcpy(out->v_torsion, o.v_torsion, sizeof(double) * 3);
+  std::memcpy(out->v_oop, o.v_oop, sizeof(double) * 3);
+  std::memcpy(out->pt, o.pt, sizeof(double) * 6);
+  std::memcpy(out->box, o.box, sizeof(double) * 3);
+  out->bond_overext = o.bond_overext;
+  out->cell_clamps = o.cell_clamps;
+  out->step = o.step;
+  out->status = o.status;
+}
+
+int read_obs(ibg_ctx* c, ibg_obs* out) {
+  if (!out) return IBG_OK;
+  ObsD o;
+  CK(cudaMemcpyAsync(&o, &c->sc->obs, sizeof(ObsD), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  obs_to_c(o, out);
+  return IBG_OK;
+}
+
+// Grow the list storage to the counts of the last rebuild (between steps),
+// with 50 % headroom so that later rebuilds inside a run fit.  Returns 1 when
+// any list grew (the rebuild must then be repeated).
+int ensure_list_capacity(ibg_ctx* c) {
+  int grew = 0;
+  for (auto& L : c->L) {
+    if (!L.present) continue;
+    long long tot = 0;
+    CK(cudaMemcpyAsync(&tot, L.slice_off + L.nslices, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (tot <= L.cap_entries) continue;
+    long long cap = tot + tot / 2 + 32 * 64;
+    if (L.entries) {
+      auto it = std::find(c->owned.begin(), c->owned.end(), (void*)L.entries);
+      if (it != c->owned.end()) c->owned.erase(it);
+      CK(cudaFree(L.entries));
+    }
+    L.entries = dalloc<int>((size_t)cap, c->owned);
+    L.cap_entries = cap;
+    grew = 1;
+  }
+  if (grew) {  // the graphs bake the old pointers
+    for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+    c->graphs.clear();
+  }
+  return grew;
+}
+
+template <typename R>
+void rebuild_now(ibg_ctx* c) {
+  for (auto& L : c->L) {
+    if (!L.present) continue;
+    enq_rebuild<R>(c, L);
+  }
+}
+
+}  // namespace
+
+// ======================================================================= C ABI
+extern "C" {
+
+const char* ibg_version(void) { return "ibisco_b200 0.1 (sm_100a)"; }
+
+int ibg_set_device(int device) { return cudaSetDevice(device) == cudaSuccess ? IBG_OK : IBG_E_CUDA; }
+
+int ibg_set_l2_flush(ibg_ctx* c, long long bytes) {
+  if (!c || bytes < 0) return IBG_E_INVALID;
+  if (c->flush_buf && (size_t)bytes != c->flush_bytes) {
+    cudaFree(c->flush_buf);
+    c->flush_buf = nullptr;
+  }
+  c->flush_bytes = (size_t)bytes;
+  return IBG_OK;
+}
+
+const char* ibg_last_error(const ibg_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int ibg_create(const ibg_desc* d, int precision, ibg_ctx** out) {
+  if (!d || !out) return IBG_E_INVALID;
+  *out = nullptr;
+  if (precision != IBG_PREC_FP32_FIXED && precision != IBG_PREC_FP64_PLAIN) return IBG_E_INVALID;
+  if (d->natoms <= 0 || d->nitems != d->natoms + d->nvirta || d->ntype <= 0 || d->nupdate <= 0 || d->halt_drift <= 0)
+    return IBG_E_INVALID;
+  auto c = std::make_unique<ibg_ctx>();
+  try {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    c->dev = dev;
+    CK(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    c->prec = precision;
+    c->natoms = d->natoms; c->nvirta = d->nvirta; c->nitems = d->nitems; c->ntype = d->ntype;
+    c->numatoms = d->numatoms; c->numbeads = d->numbeads; c->ncoarse = d->ncoarse;
+    c->ensemble = d->ensemble; c->nupdate = d->nupdate; c->halt_drift = d->halt_drift; c->nmts = d->nmts;
+    c->ibrdescr = d->ibrdescr; c->maxnab = d->maxnab > 0 ? d->maxnab : 1000;
+    c->dt = d->dt; c->fac = d->fac; c->pfac = d->pfac; c->temp_in = d->temp_in; c->pressure = d->pressure;
+    c->mktemp = d->mktemp; c->mktemp_atom = d->mktemp_atom; c->mktemp_bead = d->mktemp_bead;
+    c->r2d = 180.0f / 3.14159265358f;  // UNIT.f90:22
+    const int N = d->nitems, NA = d->natoms, NT = d->ntype;
+    auto& o = c->owned;
+    // particles
+    std::vector<int> tbits(N), gslot(N, 0);
+    std::vector<double> mass(N), inv(N);
+    for (int i = 0; i < N; ++i) {
+      int t = d->itype[i];
+      if (t < 1 || t > NT) return fail(nullptr, IBG_E_INVALID, "");
+      int lab = i < NA ? d->type_label[i] : 3;
+      tbits[i] = (t - 1) | (lab << 16);
+      mass[i] = d->mass[t - 1];
+      inv[i] = d->invmass[t - 1];
+    }
+    c->tbits = dupload(tbits, o);
+    c->mass = dupload(mass, o);
+    c->invmass = dupload(inv, o);
+    c->S = dalloc<double>(3 * (size_t)N, o);
+    c->V = dalloc<double>(3 * (size_t)NA, o);
+    if (precision == IBG_PREC_FP32_FIXED) c->su = dalloc<float>(3 * (size_t)N, o);
+    else c->su = c->S;
+    c->fnb = dalloc<unsigned char>(accsize(c.get()) * 3 * N, o);
+    c->fb = dalloc<unsigned char>(accsize(c.get()) * 3 * N, o);
+    // exclusions
+    std::vector<int> en(N), ex((size_t)N * 20, -1);
+    for (int i = 0; i < N; ++i) {
+      en[i] = d->connections[i];
+      if (en[i] < 0 || en[i] > 20) return fail(nullptr, IBG_E_INVALID, "");
+      for (int k = 0; k < en[i]; ++k) ex[(size_t)i * 20 + k] = d->connected_to[(size_t)k * d->ld_conn + i] - 1;
+    }
+    c->excl_n = dupload(en, o);
+    c->excl = dupload(ex, o);
+    // virtual sites
+    {
+      const int nv = d->nvirta;
+      std::vector<int> ctr(std::max(nv, 1), -1), num(std::max(nv, 1), 0), mem((size_t)std::max(nv, 1) * 15, 0);
+      std::vector<float> vm((size_t)std::max(nv, 1) * 15, 0.f), vi(std::max(nv, 1), 0.f), vc((size_t)std::max(nv, 1) * 15, 0.f);
+      for (int v = 0; v < nv; ++v) {
+        int t = d->vitype[v];
+        ctr[v] = d->virt_center[v] > 0 ? d->virt_center[v] - 1 : -1;
+        num[v] = d->virt_numatoms[t - 1];
+        if (num[v] > 15 || num[v] > d->vs_maxatoms) return fail(nullptr, IBG_E_INVALID, "");
+        vi[v] = d->virt_invmass[t - 1];
+        for (int k = 0; k < num[v]; ++k) {
+          int a = d->virt_atm_ind[(size_t)k * d->ld_vs + v];
+          if (a < 1 || a > NA) return fail(nullptr, IBG_E_INVALID, "");
+          mem[(size_t)v * 15 + k] = a - 1;
+          int ta = d->itype[a - 1];
+          vm[(size_t)v * 15 + k] = d->mass[ta - 1];
+          vc[(size_t)v * 15 + k] = d->virt_masscoeff[(size_t)(t - 1) + (size_t)NT * (ta - 1)];
+        }
+      }
+      c->vcenter = dupload(ctr, o); c->vnum = dupload(num, o); c->vmem = dupload(mem, o);
+      c->vmass = dupload(vm, o); c->vinv = dupload(vi, o); c->vcoef = dupload(vc, o);
+    }
+    // bonded terms in the reference's loop order (BONDED_FORCE.F90:70-91)
+    {
+      std::vector<int4> bonds, angles, tors, oops;
+      std::vector<int2> tors_t, oops_t;
+      auto T2 = [&](int a, int b) { return (size_t)(a - 1) + (size_t)NT * (b - 1); };
+      auto T3 = [&](int a, int b, int cc) { return T2(a, b) + (size_t)NT * NT * (cc - 1); };
+      auto T4 = [&](int a, int b, int cc, int e) { return T3(a, b, cc) + (size_t)NT * NT * NT * (e - 1); };
+      for (int I = 1; I <= N; ++I) {
+        const int TI = d->itype[I - 1];
+        const int nbnd = d->nbonds ? d->nbonds[I - 1] : 0;
+        for (int a = 0; a < nbnd; ++a) {
+          int J = d->jbond[(size_t)a * d->ld_bond + I - 1];
+          if (J > I) {
+            int t = d->ibondt[T2(TI, d->itype[J - 1])];
+            if (t < 1) return fail(nullptr, IBG_E_INVALID, "");
+            bonds.push_back(make_int4(I - 1, J - 1, t - 1, d->bond_type_label[t - 1]));
+          }
+        }
+        const int nang = d->nijk ? d->nijk[I - 1] : 0;
+        for (int a = 0; a < nang; ++a) {
+          int J = d->jangleijk[(size_t)a * d->ld_angle + I - 1], K = d->kangleijk[(size_t)a * d->ld_angle + I - 1];
+          int t = d->iangt[T3(TI, d->itype[J - 1], d->itype[K - 1])];
+          if (t < 1) return fail(nullptr, IBG_E_INVALID, "");
+          angles.push_back(make_int4(I - 1, J - 1, K - 1, (t - 1) | (d->angle_type_label[t - 1] << 24)));
+        }
+        if (I <= NA && d->nijkl) {
+          for (int a = 0; a < d->nijkl[I - 1]; ++a) {
+            int J = d->jtorijkl[(size_t)a * d->ld_torsion + I - 1], K = d->ktorijkl[(size_t)a * d->ld_torsion + I - 1],
+                Lq = d->ltorijkl[(size_t)a * d->ld_torsion + I - 1];
+            int t = d->itort[T4(TI, d->itype[J - 1], d->itype[K - 1], d->itype[Lq - 1])];
+            if (t < 1) return fail(nullptr, IBG_E_INVALID, "");
+            tors.push_back(make_int4(I - 1, J - 1, K - 1, Lq - 1));
+            tors_t.push_back(make_int2(t - 1, d->torsion_type_label[t - 1]));
+          }
+        }
+        if (I <= NA && d->noopijkl) {
+          for (int a = 0; a < d->noopijkl[I - 1]; ++a) {
+            int J = d->joopijkl[(size_t)a * d->ld_oop + I - 1], K = d->koopijkl[(size_t)a * d->ld_oop + I - 1],
+                Lq = d->loopijkl[(size_t)a * d->ld_oop + I - 1];
+            int t = d->ioopt[T4(TI, d->itype[J - 1], d->itype[K - 1], d->itype[Lq - 1])];
+            if (t < 1) return fail(nullptr, IBG_E_INVALID, "");
+            oops.push_back(make_int4(I - 1, J - 1, K - 1, Lq - 1));
+            oops_t.push_back(make_int2(t - 1, d->oop_type_label[t - 1]));
+          }
+        }
+      }
+      c->nb = (int)bonds.size(); c->na = (int)angles.size(); c->nt = (int)tors.size(); c->no = (int)oops.size();
+      c->bonds = dupload(bonds, o); c->angles = dupload(angles, o); c->tors = dupload(tors, o); c->oops = dupload(oops, o);
+      c->tors_t = dupload(tors_t, o); c->oops_t = dupload(oops_t, o);
+      // bonded tables: rows {X, F, P, 0}, type-fastest input layout
+      auto tables = [&](int ntab, int ld, const int* nd, const float* bin, const float* X, const float* F, const float* P,
+                        float4** rows, int** off, int** ndat, float** binout) {
+        std::vector<float4> r;
+        std::vector<int> of(std::max(ntab, 1), 0), ndv(std::max(ntab, 1), 0);
+        std::vector<float> bv(std::max(ntab, 1), 1.f);
+        for (int t = 0; t < ntab; ++t) {
+          of[t] = (int)r.size();
+          ndv[t] = nd[t];
+          bv[t] = bin[t];
+          for (int k = 0; k < nd[t] + 3; ++k) {
+            if (k < ld) {
+              size_t at = (size_t)t + (size_t)ntab * k;
+              r.push_back(make_float4(X[at], F[at], P[at], 0.f));
+            } else {
+              r.push_back(make_float4(0.f, 0.f, 0.f, 0.f));
+            }
+          }
+        }
+        *rows = dupload(r, o); *off = dupload(of, o); *ndat = dupload(ndv, o); *binout = dupload(bv, o);
+      };
+      tables(d->nbtype, d->ld_b, d->ndatb, d->binb, d->rbond, d->bond_force, d->bond_pot, &c->tb, &c->tb_off, &c->tb_nd, &c->tb_bin);
+      tables(d->natype, d->ld_a, d->ndatan, d->bina, d->angle, d->bend_force, d->bend_pot, &c->ta, &c->ta_off, &c->ta_nd, &c->ta_bin);
+      tables(d->nttype, d->ld_t, d->ndatt, d->bint, d->angle_tor, d->tor_force, d->tor_pot, &c->tt, &c->tt_off, &c->tt_nd, &c->tt_bin);
+      tables(d->notype, d->ld_o, d->ndato, d->bino, d->angle_oop, d->oop_force, d->oop_pot, &c->to, &c->to_off, &c->to_nd, &c->to_bin);
+    }
+    // Verlet lists
+    build_list(c.get(), d, 0);
+    if (d->ibrdescr == 0) build_list(c.get(), d, 1);
+    {  // every particle belongs to exactly one list
+      std::vector<int> gs(N, -1);
+      for (int a = 0; a < c->L[0].n; ++a) gs[d->atom[a] - 1] = a * 2 + 0;
+      for (int a = 0; a < c->L[1].n; ++a) gs[d->bead[a] - 1] = a * 2 + 1;
+      for (int i = 0; i < N; ++i)
+        if (gs[i] < 0) return fail(nullptr, IBG_E_INVALID, "");
+      c->gslot = dupload(gs, o);
+    }
+    // grids and partial sums
+    size_t smem_max = 0;
+    for (auto& L : c->L)
+      if (L.present && L.use_smem) smem_max = std::max(smem_max, L.smem);
+    if (smem_max) {
+      if (precision == IBG_PREC_FP32_FIXED) CK(cudaFuncSetAttribute(k_nonbonded<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
+      else CK(cudaFuncSetAttribute(k_nonbonded<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
+    }
+    for (auto& L : c->L) {
+      if (!L.present) continue;
+      int per = 0;
+      if (precision == IBG_PREC_FP32_FIXED)
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, L.use_smem ? (const void*)k_nonbonded<float, true> : (const void*)k_nonbonded<float, false>, 256, L.use_smem ? L.smem : 9 * 64));
+      else
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, L.use_smem ? (const void*)k_nonbonded<double, true> : (const void*)k_nonbonded<double, false>, 256, L.use_smem ? L.smem : 9 * 64));
+      per = std::max(1, per);
+      L.grid_nb = std::max(1, std::min(c->nsm * per, (L.nslices + 7) / 8));
+    }
+    int gnb = std::max(c->L[0].present ? c->L[0].grid_nb : 0, c->L[1].present ? c->L[1].grid_nb : 0);
+    for (auto& L : c->L)
+      if (L.present) { L.grid_nb = gnb; L.part = dalloc<double>(9 * (size_t)gnb, o); }
+    c->g_b = grid_for(c.get(), (long long)c->nb + c->na + c->nt + c->no, 4);
+    c->g_mv = grid_for(c.get(), NA, 4);
+    c->g_pos = grid_for(c.get(), N, 8);
+    c->p_b = dalloc<double>(12 * (size_t)c->g_b, o);
+    c->p_mv = dalloc<double>(18 * (size_t)c->g_mv, o);
+    c->p_mom = dalloc<double>(3 * (size_t)c->g_mv, o);
+    c->sc = dalloc<Scalars>(1, o);
+    c->ring_cap = 1;
+    c->ring = nullptr;
+    CK(cudaDeviceSynchronize());
+  } catch (CudaError& e) {
+    for (void* p : c->owned) cudaFree(p);
+    c->owned.clear();
+    return IBG_E_CUDA;
+  }
+  *out = c.release();
+  return IBG_OK;
+}
+
+int ibg_set_state(ibg_ctx* c, const float* sxyz, const float* vxyz, const float* box) {
+  if (!c || !sxyz || !vxyz || !box) return IBG_E_INVALID;
+  try {
+    const int NA = c->natoms;
+    std::vector<double> s(3 * (size_t)c->nitems, 0.0), v(3 * (size_t)NA);
+    for (size_t k = 0; k < 3 * (size_t)NA; ++k) { s[k] = sxyz[k]; v[k] = vxyz[k]; }
+    CK(cudaMemcpy(c->S, s.data(), sizeof(double) * s.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->V, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice));
+    Scalars h;
+    std::memset(&h, 0, sizeof(h));
+    for (int k = 0; k < 3; ++k) {
+      h.boxf[k] = box[k];
+      h.boxinvf[k] = 1.0f / box[k];       // RDCOOR.f90:70-71
+      h.box2f[k] = box[k] / 2.0f;
+      h.box[k] = (double)box[k];
+      h.boxinv[k] = 1.0 / h.box[k];
+      h.box2[k] = h.box[k] / 2.0;
+    }
+    h.step = 0;
+    h.mts_m = -1;
+    h.miu = 1.0;
+    h.lam[0] = h.lam[1] = 1.0;
+    CK(cudaMemcpy(c->sc, &h, sizeof(h), cudaMemcpyHostToDevice));
+    for (auto& L : c->L) {
+      if (!L.present) continue;
+      alloc_cells(c, L, box);
+      std::vector<int> ident(L.n);
+      for (int a = 0; a < L.n; ++a) ident[a] = a;
+      CK(cudaMemcpy(L.slot_of, ident.data(), sizeof(int) * L.n, cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(L.sorted, ident.data(), sizeof(int) * L.n, cudaMemcpyHostToDevice));
+      CK(cudaMemset(L.fsort, 0, accsize(c) * 3 * (size_t)L.n));
+      if (L.mtsf) CK(cudaMemset(L.mtsf, 0, accsize(c) * 9 * (size_t)L.n));
+    }
+    {  // slots = list order before the first sort
+      std::vector<int> gs(c->nitems, 0);
+      std::vector<int> idx0, idx1;
+      for (int w = 0; w < 2; ++w) {
+        if (!c->L[w].present) continue;
+        std::vector<int> idx(c->L[w].n);
+        CK(cudaMemcpy(idx.data(), c->L[w].idx, sizeof(int) * idx.size(), cudaMemcpyDeviceToHost));
+        for (int a = 0; a < (int)idx.size(); ++a) gs[idx[a]] = a * 2 + w;
+      }
+      CK(cudaMemcpy(c->gslot, gs.data(), sizeof(int) * gs.size(), cudaMemcpyHostToDevice));
+    }
+    for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+    c->graphs.clear();
+    // main.F90:150-234: virtual sites, SHIFT, initial temperatures, first lists
+    if (c->prec == IBG_PREC_FP32_FIXED) enq_positions<float>(c);
+    else enq_positions<double>(c);
+    k_kinetic<<<c->g_mv, 256, 0, c->st>>>(NA, c->V, c->tbits, c->mass, c->p_mv, c->g_mv);
+    k_init_temps<<<1, 64, 0, c->st>>>(c->p_mv, c->g_mv, c->sc, c->mktemp, c->mktemp_atom, c->mktemp_bead, c->temp_in, c->fac,
+                                      c->ensemble);
+    int grew = 1;
+    for (int pass = 0; pass < 2 && grew; ++pass) {
+      if (c->prec == IBG_PREC_FP32_FIXED) rebuild_now<float>(c);
+      else rebuild_now<double>(c);
+      CK(cudaStreamSynchronize(c->st));
+      unsigned bits = 0;
+      CK(cudaMemcpy(&bits, &c->sc->err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+      if (bits & ~EB_CAPACITY) return check_device(c);
+      grew = ensure_list_capacity(c);
+      unsigned zero = 0;
+      CK(cudaMemcpy(&c->sc->err, &zero, sizeof(unsigned), cudaMemcpyHostToDevice));
+      // a repeated build sorts already sorted slots and yields the same lists
+    }
+    if (grew) return fail(c, IBG_E_CAPACITY, "neighbour-list storage could not be sized");
+    int rc = check_device(c);
+    if (rc) return rc;
+    c->state_set = true;
+    c->fb_dirty = false;
+  } catch (CudaError& e) {
+    return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
+  }
+  return IBG_OK;
+}
+
+static int run_steps(ibg_ctx* c, int first, int nsteps, ibg_obs* per_step, bool force_only, bool use_graphs) {
+  if (!c) return IBG_E_INVALID;
+  if (!c->state_set) return fail(c, IBG_E_INVALID, "ibg_set_state has not been called");
+  try {
+    if (per_step && nsteps > c->ring_cap) {
+      if (c->ring) {
+        auto it = std::find(c->owned.begin(), c->owned.end(), (void*)c->ring);
+        if (it != c->owned.end()) c->owned.erase(it);
+        CK(cudaFree(c->ring));
+      }
+      c->ring_cap = std::max(nsteps, 64);
+      c->ring = dalloc<ObsD>(c->ring_cap, c->owned);
+      for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+      c->graphs.clear();
+    }
+    set_step_counter(c, first - 1);
+    if (c->flush_bytes) {
+      if (!c->flush_buf) CK(cudaMalloc(&c->flush_buf, c->flush_bytes));
+      while ((int)c->step_ev.size() < 2 * nsteps) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        c->step_ev.push_back(e);
+      }
+    }
+    if (!c->run_ev[0]) {
+      CK(cudaEventCreate(&c->run_ev[0]));
+      CK(cudaEventCreate(&c->run_ev[1]));
+    }
+    CK(cudaEventRecord(c->run_ev[0], c->st));
+    int done = 0;
+    while (done < nsteps) {
+      const int step = first + done;
+      const unsigned v = variant_of(c, step, force_only);
+      const bool flush = c->flush_bytes && c->flush_buf;
+      if (flush) {
+        CK(cudaMemsetAsync(c->flush_buf, done & 0xff, c->flush_bytes, c->st));
+        CK(cudaEventRecord(c->step_ev[2 * done], c->st));
+      }
+      if (use_graphs && !c->timing) {
+        auto it = c->graphs.find(v);
+        if (it == c->graphs.end()) {
+          cudaGraph_t g;
+          CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+          long long l0 = c->launches;
+          enqueue(c, v);
+          CK(cudaStreamEndCapture(c->st, &g));
+          c->launches_per_variant[v & 31] = c->launches - l0;
+          cudaGraphExec_t ge;
+          CK(cudaGraphInstantiate(&ge, g, 0));
+          CK(cudaGraphDestroy(g));
+          it = c->graphs.emplace(v, ge).first;
+        }
+        CK(cudaGraphLaunch(it->second, c->st));
+        c->launches += c->launches_per_variant[v & 31];
+      } else {
+        enqueue(c, v);
+      }
+      if (flush) CK(cudaEventRecord(c->step_ev[2 * done + 1], c->st));
+      ++done;
+    }
+    CK(cudaEventRecord(c->run_ev[1], c->st));
+    collect_marks(c);
+    CK(cudaStreamSynchronize(c->st));
+    {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, c->run_ev[0], c->run_ev[1]));
+      c->stage_ms[5] = ms;
+      if (c->flush_bytes && c->flush_buf) {  // only the steps, not the flushes
+        double tot = 0.0;
+        for (int k = 0; k < nsteps; ++k) {
+          CK(cudaEventElapsedTime(&ms, c->step_ev[2 * k], c->step_ev[2 * k + 1]));
+          tot += ms;
+        }
+        c->stage_ms[5] = tot;
+      }
+    }
+    int rc = check_device(c);
+    if (rc) return rc;
+    if (per_step) {
+      std::vector<ObsD> h(nsteps);
+      CK(cudaMemcpy(h.data(), c->ring, sizeof(ObsD) * nsteps, cudaMemcpyDeviceToHost));
+      for (int k = 0; k < nsteps; ++k) obs_to_c(h[k], &per_step[k]);
+    }
+  } catch (CudaError& e) {
+    return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
+  }
+  return IBG_OK;
+}
+
+int ibg_step(ibg_ctx* c, int step, ibg_obs* out) {
+  int rc = run_steps(c, step, 1, nullptr, false, true);
+  if (rc) return rc;
+  try {
+    read_obs(c, out);
+  } catch (CudaError& e) {
+    return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
+  }
+  return IBG_OK;
+}
+
+int ibg_forces(ibg_ctx* c, int step, ibg_obs* out) {
+  int rc = run_steps(c, step, 1, nullptr, true, false);
+  if (rc) return rc;
+  try {
+    read_obs(c, out);
+  } catch (CudaError& e) {
+    return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
+  }
+  return IBG_OK;
+}
+
+int ibg_run(ibg_ctx* c, int first_step, int nsteps, ibg_obs* per_step) {
+  if (nsteps < 0) return IBG_E_INVALID;
+  return run_steps(c, first_step, nsteps, per_step, false, true);
+}
+
+int ibg_get_state(ibg_ctx* c, float* sxyz, float* rxyz, float* vxyz, float* fxyz) {
+  if (!c) return IBG_E_INVALID;
+  try {
+    CK(cudaStreamSynchronize(c->st));
+    const size_t N = c->nitems, NA = c->natoms;
+    if (sxyz) {
+      std::vector<double> s(3 * N);
+      CK(cudaMemcpy(s.data(), c->S, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost));
+      for (size_t k = 0; k < 3 * N; ++k) sxyz[k] = (float)s[k];
+    }
+    if (vxyz) {
+      std::vector<double> v(3 * NA);
+      CK(cudaMemcpy(v.data(), c->V, sizeof(double) * 3 * NA, cudaMemcpyDeviceToHost));
+      for (size_t k = 0; k < 3 * NA; ++k) vxyz[k] = (float)v[k];
+    }
+    if (rxyz) {
+      std::vector<int> gs(N);
+      CK(cudaMemcpy(gs.data(), c->gslot, sizeof(int) * N, cudaMemcpyDeviceToHost));
+      std::vector<unsigned char> p[2];
+      for (int w = 0; w < 2; ++w) {
+        if (!c->L[w].present) continue;
+        p[w].resize(c->L[w].pos_bytes);
+        CK(cudaMemcpy(p[w].data(), c->L[w].pos4, c->L[w].pos_bytes, cudaMemcpyDeviceToHost));
+      }
+      for (size_t i = 0; i < N; ++i) {
+        int w = gs[i] & 1, s = gs[i] >> 1;
+        if (c->prec == IBG_PREC_FP32_FIXED) {
+          const float4* q = (const float4*)p[w].data();
+          rxyz[3 * i] = q[s].x; rxyz[3 * i + 1] = q[s].y; rxyz[3 * i + 2] = q[s].z;
+        } else {
+          const double4* q = (const double4*)p[w].data();
+          rxyz[3 * i] = (float)q[s].x; rxyz[3 * i + 1] = (float)q[s].y; rxyz[3 * i + 2] = (float)q[s].z;
+        }
+      }
+    }
+    if (fxyz) {
+      if (c->prec == IBG_PREC_FP32_FIXED) {
+        std::vector<long long> a(3 * N), b(3 * N);
+        CK(cudaMemcpy(a.data(), c->fnb, sizeof(long long) * 3 * N, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(b.data(), c->fb, sizeof(long long) * 3 * N, cudaMemcpyDeviceToHost));
+        for (size_t k = 0; k < 3 * N; ++k) fxyz[k] = (float)((double)(a[k] + b[k]) * kFixInv);
+      } else {
+        std::vector<double> a(3 * N), b(3 * N);
+        CK(cudaMemcpy(a.data(), c->fnb, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(b.data(), c->fb, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost));
+        for (size_t k = 0; k < 3 * N; ++k) fxyz[k] = (float)(a[k] + b[k]);
+      }
+    }
+  } catch (CudaError& e) {
+    return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
+  }
+  return IBG_OK;
+}
+
+int ibg_get_state_f64(ibg_ctx* c, double* sxyz, double* vxyz, double* fxyz) {
+  if (!c) return IBG_E_INVALID;
+  try {
+    CK(cudaStreamSynchronize(c->st));
+    const size_t N = c->nitems, NA = c->natoms;
+    if (sxyz) CK(cudaMemcpy(sxyz, c->S, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost));
+    if (vxyz) CK(cudaMemcpy(vxyz, c->V, sizeof(double) * 3 * NA, cudaMemcpyDeviceToHost));
+    if (fxyz) {
+      if (c->prec == IBG_PREC_FP32_FIXED) {
+        std::vector<long long> a(3 * N), b(3 * N);
+        CK(cudaMemcpy(a.data(), c->fnb, sizeof(long long) * 3 * N, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(b.data(), c->fb, sizeof(long long) * 3 * N, cudaMemcpyDeviceToHost));
+        for (size_t k = 0; k < 3 * N; ++k) fxyz[k] = (double)(a[k] + b[k]) * kFixInv;
+      } else {
+        std::vector<double> a(3 * N), b(3 * N);
+        CK(cudaMemcpy(a.data(), c->fnb, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(b.data(), c->fb, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost));
+        for (size_t k = 0; k < 3 * N; ++k) fxyz[k] = a[k] + b[k];
+      }
+    }
+  } catch (CudaError& e) {
+    return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
+  }
+  return IBG_OK;
+}
+
+int ibg_get_neighbour_list(ibg_ctx* c, int which, int* list, int maxnab, int* nnebs) {
+  if (!c || which < 0 || which > 1) return IBG_E_INVALID;
+  DevList& L = c->L[which];
+  if (!L.present) return 0;
+  try {
+    CK(cudaStreamSynchronize(c->st));
+    std::vector<int> counts(L.n), w(L.nslices), sorted(L.n), idx(L.n);
+    std::vector<long long> off(L.nslices + 1);
+    CK(cudaMemcpy(counts.data(), L.counts, sizeof(int) * L.n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(off.data(), L.slice_off, sizeof(long long) * (L.nslices + 1), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(sorted.data(), L.sorted, sizeof(int) * L.n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(idx.data(), L.idx, sizeof(int) * L.n, cudaMemcpyDeviceToHost));
+    std::vector<int> e((size_t)off[L.nslices]);
+    if (!e.empty()) CK(cudaMemcpy(e.data(), L.entries, sizeof(int) * e.size(), cudaMemcpyDeviceToHost));
+    for (int s = 0; s < L.n; ++s) {
+      const int a = sorted[s];
+      const int g = s >> 5, lane = s & 31;
+      if (nnebs) nnebs[a] = counts[s];
+      if (!list) continue;
+      if (counts[s] >= maxnab) return fail(c, IBG_E_INVALID, "maxnab smaller than a list");
+      int* col = list + (size_t)a * maxnab;
+      for (int k = 0; k < maxnab; ++k) {
+        if (k < counts[s]) {
+          int t = e[(size_t)off[g] + (size_t)k * 32 + lane];
+          col[k] = idx[sorted[t]] + 1;
+        } else {
+          col[k] = 0;
+        }
+      }
+    }
+  } catch (CudaError& e) {
+    return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
+  }
+  return L.n;
+}
+
+int ibg_get_exclusions(ibg_ctx* c, int* connections, int* connected_to) {
+  if (!c) return IBG_E_INVALID;
+  try {
+    const int N = c->nitems;
+    std::vector<int> en(N), ex((size_t)N * 20);
+    CK(cudaMemcpy(en.data(), c->excl_n, sizeof(int) * N, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ex.data(), c->excl, sizeof(int) * ex.size(), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < N; ++i) {
+      if (connections) connections[i] = en[i];
+      if (connected_to)
+        for (int k = 0; k < 20; ++k) connected_to[(size_t)k * N + i] = k < en[i] ? ex[(size_t)i * 20 + k] + 1 : 0;
+    }
+  } catch (CudaError& e) {
+    return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
+  }
+  return IBG_OK;
+}
+
+int ibg_set_timing(ibg_ctx* c, int on) {
+  if (!c) return IBG_E_INVALID;
+  c->timing = on != 0;
+  for (double& x : c->stage_ms) x = 0.0;
+  return IBG_OK;
+}
+
+int ibg_get_timing(ibg_ctx* c, double* stage_ms, int nstage, long long* launches) {
+  if (!c) return IBG_E_INVALID;
+  for (int k = 0; k < nstage && k < 8; ++k) stage_ms[k] = c->stage_ms[k];
+  if (launches) *launches = c->launches;
+  return IBG_OK;
+}
+
+void ibg_destroy(ibg_ctx* c) {
+  if (!c) return;
+  cudaStreamSynchronize(c->st);
+  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+  for (void* p : c->owned) cudaFree(p);
+  for (auto* e : c->run_ev)
+    if (e) cudaEventDestroy(e);
+  for (auto* e : c->step_ev) cudaEventDestroy(e);
+  if (c->flush_buf) cudaFree(c->flush_buf);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+}  // extern "C"

@@ -1,0 +1,1143 @@
+// Kernels of the B200 force-and-integrate step.  Each kernel names the
+// reference routine whose arithmetic it restates.  The file is compiled with
+// --fmad=false, IEEE division and square root, so every REAL*4 expression is
+// evaluated with the same roundings as gfortran -O2 on x86-64 (no FMA).
+#pragma once
+#include "ibg_common.cuh"
+
+namespace ibg {
+
+// ------------------------------------------------------------ precision policy
+// FP32 path: REAL*4 geometry and table math, forces summed as 64-bit
+// fixed-point integers (order independent, reproducible run to run).
+// FP64 path: the same algorithm in double with double atomics.
+template <typename R>
+struct Prec;
+
+template <>
+struct Prec<float> {
+  using pos_t = float4;
+  using acc_t = unsigned long long;  // global accumulator element
+  using reg_t = long long;           // per-thread partial sum
+  static __device__ __forceinline__ reg_t q(float v, unsigned* err) {
+    if (!(fabsf(v) < kFixMax)) {  // also catches NaN
+      atomicOr(err, EB_FIXED);
+      v = (v == v) ? copysignf(kFixMax, v) : 0.0f;
+    }
+    return __float2ll_rn(v * kFixScale);
+  }
+  static __device__ __forceinline__ void add(acc_t* p, reg_t v) { atomicAdd(p, (unsigned long long)v); }
+  static __device__ __forceinline__ double get(acc_t v) { return (double)(long long)v * kFixInv; }
+  static __device__ __forceinline__ reg_t from_double(double v, unsigned* err) {
+    double s = v * 4294967296.0;
+    if (!(fabs(s) < 9.2e18)) {
+      atomicOr(err, EB_FIXED);
+      s = (s == s) ? copysign(9.2e18, s) : 0.0;
+    }
+    return __double2ll_rn(s);
+  }
+  static __device__ __forceinline__ float tbits(int b) { return __int_as_float(b); }
+  static __device__ __forceinline__ int bits(float w) { return __float_as_int(w); }
+};
+
+template <>
+struct Prec<double> {
+  using pos_t = double4;
+  using acc_t = double;
+  using reg_t = double;
+  static __device__ __forceinline__ reg_t q(double v, unsigned*) { return v; }
+  static __device__ __forceinline__ void add(acc_t* p, reg_t v) { atomicAdd(p, v); }
+  static __device__ __forceinline__ double get(acc_t v) { return v; }
+  static __device__ __forceinline__ reg_t from_double(double v, unsigned*) { return v; }
+  static __device__ __forceinline__ double tbits(int b) { return __longlong_as_double((long long)b); }
+  static __device__ __forceinline__ int bits(double w) { return (int)__double_as_longlong(w); }
+};
+
+__device__ __forceinline__ float r_round(float x) { return roundf(x); }
+__device__ __forceinline__ double r_round(double x) { return round(x); }
+__device__ __forceinline__ float r_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double r_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float r_acos(float x) { return acosf(x); }
+__device__ __forceinline__ double r_acos(double x) { return acos(x); }
+__device__ __forceinline__ float r_abs(float x) { return fabsf(x); }
+__device__ __forceinline__ double r_abs(double x) { return fabs(x); }
+
+// Fortran INT: truncation; values outside the int range saturate.
+template <typename R>
+__device__ __forceinline__ int fint(R x) {
+  if (!(x == x)) return INT_MIN;
+  if (x >= (R)2147483647.0) return INT_MAX;
+  if (x <= (R)-2147483647.0) return -INT_MAX;
+  return (int)x;
+}
+
+template <typename R>
+__device__ __forceinline__ void box_of(const Scalars* sc, R* b, R* bi, R* b2);
+template <>
+__device__ __forceinline__ void box_of<float>(const Scalars* sc, float* b, float* bi, float* b2) {
+  for (int c = 0; c < 3; ++c) { b[c] = sc->boxf[c]; bi[c] = sc->boxinvf[c]; b2[c] = sc->box2f[c]; }
+}
+template <>
+__device__ __forceinline__ void box_of<double>(const Scalars* sc, double* b, double* bi, double* b2) {
+  for (int c = 0; c < 3; ++c) { b[c] = sc->box[c]; bi[c] = sc->boxinv[c]; b2[c] = sc->box2[c]; }
+}
+
+// ------------------------------------------------------------------ per step
+__global__ void k_begin(Scalars* sc, int nupdate, int nmts) {
+  int st = ++sc->step;
+  sc->rebuild = (st % nupdate) == 0;
+  sc->mts_m = nmts > 0 ? st % (3 + nmts) : -1;
+  sc->miu = 1.0;
+}
+
+// Fold into the primary box (SHIFT.f90:37-43): applied to all three
+// components when any one lies outside [-L/2, L/2].
+template <typename R>
+__device__ __forceinline__ void fold3(R* r, const R* b2) {
+  bool out = false;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) out |= (r[c] > b2[c]) || (r[c] < -b2[c]);
+  if (!out) return;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    R x = r[c] / b2[c];
+    R sp = x - (R)2.0 * (R)fint(x / (R)2.0);
+    r[c] = (sp - (R)2.0 * (R)fint(sp)) * b2[c];
+  }
+}
+
+struct PosArgs {
+  int natoms, nvirta;
+  const double* S;     // unwrapped positions (3,NITEMS), FP64 state
+  void* su;            // unwrapped positions in R for the bonded terms (3,NITEMS)
+  double* Svs;         // VS rows of S (written for the FP64 path and output)
+  const int* tbits;    // type | label<<16 per particle
+  const int* gslot;    // slot*2 + list per particle
+  void* pos4[2];       // per-list wrapped positions, slot order
+  const int* vcenter;  // VIRT_CENTER (0-based atom id or -1 for COM)
+  const int* vnum;     // members per VS
+  const int* vmem;     // members, [v*15 + k], 0-based
+  const float* vmass;  // member masses per [v*15 + k]
+  const float* vinv;   // VIRT_INVMASS per VS
+};
+
+// SHIFT.f90:36-44 for atoms and VIRTUAL_DEF.f90:67-95 for virtual sites
+// (centre-of-mass sums with all three components reset per site).
+template <typename R>
+__global__ void k_positions(PosArgs a, Scalars* sc) {
+  using PT = typename Prec<R>::pos_t;
+  const int n = a.natoms + a.nvirta;
+  R b[3], bi[3], b2[3];
+  box_of<R>(sc, b, bi, b2);
+  R* su = (R*)a.su;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    R s[3];
+    if (i < a.natoms) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) s[c] = (R)a.S[3 * (size_t)i + c];
+    } else {
+      int v = i - a.natoms;
+      int ctr = a.vcenter[v];
+      if (ctr >= 0) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) s[c] = (R)a.S[3 * (size_t)ctr + c];
+      } else {
+        R acc[3] = {0, 0, 0};
+        int nm = a.vnum[v];
+        for (int k = 0; k < nm; ++k) {
+          int m = a.vmem[v * 15 + k];
+          R mm = (R)a.vmass[v * 15 + k];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) acc[c] = acc[c] + mm * (R)a.S[3 * (size_t)m + c];
+        }
+        R inv = (R)a.vinv[v];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) s[c] = acc[c] * inv;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) a.Svs[3 * (size_t)v + c] = (double)s[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) su[3 * (size_t)i + c] = s[c];
+    R r[3] = {s[0], s[1], s[2]};
+    fold3<R>(r, b2);
+    int g = a.gslot[i];
+    PT p;
+    p.x = r[0]; p.y = r[1]; p.z = r[2];
+    p.w = Prec<R>::tbits(a.tbits[i]);
+    ((PT*)a.pos4[g & 1])[g >> 1] = p;
+  }
+}
+
+// ------------------------------------------------------------ cell lists
+struct ListArgs {
+  int n;             // particles in the list
+  int which;         // 0 atoms, 1 beads
+  int natoms;        // NATOMS (VS-VS exclusion)
+  int hybrid;        // IBRDESCR == 0
+  int maxnab;        // reference STOP threshold
+  int cell_cap;      // capacity of the cell arrays
+  float rlist, rlistsq;
+  double rlistd, rlistsqd;
+  const int* idx;    // INDEX_LIST, 0-based global ids
+  int* cell_of;      // [n] cell of list entry A
+  int* cell_count;   // [cell_cap]
+  int* cell_start;   // [cell_cap + 1]
+  int* cell_fill;    // [cell_cap]
+  int* sorted;       // [n] slot -> A
+  int* sorted_new;   // [n]
+  int* slot_of;      // [n] A -> slot
+  int* slot_of_new;  // [n]
+  int* gslot;        // [NITEMS]
+  void* pos4;        // [n]
+  void* pos4_new;    // [n]
+  int* counts;       // [n] per slot
+  int* slice_w;      // [nslices]
+  long long* slice_off;  // [nslices + 1]
+  int* entries;      // list storage, sliced-ELL by 32 slots
+  long long cap_entries;
+  const int* excl_n; // CONNECTIONS, by global id
+  const int* excl;   // CONNECTED_TO, [i*20 + c], 0-based
+};
+
+// UPDATE_NEIGHBOURLIST.F90:14-48 / ALLOCATEVAR2.f90:156-180: cells per
+// dimension = INT(BOX/RLIST).
+template <typename R>
+__global__ void k_regrid(ListArgs L, Scalars* sc) {
+  if (threadIdx.x || blockIdx.x) return;
+  int nc[3];
+  for (int c = 0; c < 3; ++c) {
+    if (sizeof(R) == 4) nc[c] = fint(sc->boxf[c] / L.rlist);
+    else nc[c] = fint(sc->box[c] / L.rlistd);
+  }
+  bool bad = nc[0] < 3 || nc[1] < 3 || nc[2] < 3;
+  long long tot = (long long)nc[0] * nc[1] * nc[2];
+  if (bad) atomicOr(&sc->err, EB_CELL_GRID);
+  if (tot > L.cell_cap) atomicOr(&sc->err, EB_CAPACITY);
+  if (bad || tot > L.cell_cap) nc[0] = nc[1] = nc[2] = 1;
+  for (int c = 0; c < 3; ++c) sc->ncell[L.which][c] = nc[c];
+}
+
+// LINKS.f90:192-194.  A component equal to NCELL (coordinate at +L/2 after
+// rounding) would address a cell outside the grid; it is clamped and counted.
+template <typename R>
+__global__ void k_cell_assign(ListArgs L, Scalars* sc) {
+  using PT = typename Prec<R>::pos_t;
+  const int nx = sc->ncell[L.which][0], ny = sc->ncell[L.which][1], nz = sc->ncell[L.which][2];
+  R b[3], bi[3], b2[3];
+  box_of<R>(sc, b, bi, b2);
+  const PT* pos = (const PT*)L.pos4;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < L.n; a += gridDim.x * blockDim.x) {
+    PT p = pos[L.slot_of[a]];
+    R x[3] = {p.x, p.y, p.z};
+    int nc[3] = {nx, ny, nz}, k[3];
+    int clamps = 0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      k[c] = fint((x[c] * bi[c] + (R)0.5) * (R)nc[c]);
+      if (k[c] >= nc[c]) { k[c] = nc[c] - 1; ++clamps; }
+      if (k[c] < 0) { k[c] = 0; ++clamps; }
+    }
+    if (clamps) atomicAdd(&sc->cell_clamps, (unsigned long long)clamps);
+    int cell = k[0] * nz * ny + k[1] * nz + k[2];
+    L.cell_of[a] = cell;
+    atomicAdd(&L.cell_count[cell], 1);
+  }
+}
+
+// Single-block exclusive scan of m ints (out has m+1 entries); zeroes zero[]
+// (m entries) when given.
+__global__ void k_scan_int(const int* in, int* out, int m, int* zero) {
+  __shared__ int part[1024];
+  const int t = threadIdx.x, T = blockDim.x;
+  const int chunk = (m + T - 1) / T;
+  const int b = t * chunk, e = min(m, b + chunk);
+  int s = 0;
+  for (int i = b; i < e; ++i) s += in[i];
+  part[t] = s;
+  __syncthreads();
+  if (t == 0) {
+    int run = 0;
+    for (int i = 0; i < T; ++i) { int v = part[i]; part[i] = run; run += v; }
+    out[m] = run;
+  }
+  __syncthreads();
+  int run = part[t];
+  for (int i = b; i < e; ++i) { int v = in[i]; out[i] = run; run += v; if (zero) zero[i] = 0; }
+}
+
+__global__ void k_cell_fill(ListArgs L) {
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < L.n; a += gridDim.x * blockDim.x) {
+    int c = L.cell_of[a];
+    int s = L.cell_start[c] + atomicAdd(&L.cell_fill[c], 1);
+    L.sorted_new[s] = a;
+  }
+}
+
+// Within a cell the reference's linked list visits entries by decreasing A
+// (LINKS.f90:195-196); slots are kept in increasing A so the list build can
+// walk them backwards.
+__global__ void k_cell_sort(ListArgs L, const Scalars* sc) {
+  const int ncell = sc->ncell[L.which][0] * sc->ncell[L.which][1] * sc->ncell[L.which][2];
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+    int b = L.cell_start[c], e = L.cell_start[c + 1];
+    for (int i = b + 1; i < e; ++i) {
+      int v = L.sorted_new[i], j = i - 1;
+      while (j >= b && L.sorted_new[j] > v) { L.sorted_new[j + 1] = L.sorted_new[j]; --j; }
+      L.sorted_new[j + 1] = v;
+    }
+  }
+}
+
+template <typename R>
+__global__ void k_reslot(ListArgs L) {
+  using PT = typename Prec<R>::pos_t;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < L.n; s += gridDim.x * blockDim.x) {
+    int a = L.sorted_new[s];
+    ((PT*)L.pos4_new)[s] = ((const PT*)L.pos4)[L.slot_of[a]];
+    L.slot_of_new[a] = s;
+    L.gslot[L.idx[a]] = s * 2 + L.which;
+  }
+}
+
+// NEW_NEIGHBOUR_WITHLIST.f90:34-123.  One thread per slot; a warp covers one
+// slice of 32 consecutive slots.  Candidates are visited in the reference's
+// order: the particle's own cell below it (decreasing A), then the 13 cells
+// of the MAPS.f90:137-149 stencil, each by decreasing A.  FILL=false counts
+// and records the slice width; FILL=true writes slot indices.
+template <typename R, bool FILL>
+__global__ void k_list_build(ListArgs L, Scalars* sc) {
+  using PT = typename Prec<R>::pos_t;
+  const int nx = sc->ncell[L.which][0], ny = sc->ncell[L.which][1], nz = sc->ncell[L.which][2];
+  R b[3], bi[3], b2[3];
+  box_of<R>(sc, b, bi, b2);
+  const R rlsq = sizeof(R) == 4 ? (R)L.rlistsq : (R)L.rlistsqd;
+  const PT* pos = (const PT*)L.pos4;
+  const int lane = threadIdx.x & 31;
+  const int nslices = (L.n + 31) >> 5;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < nslices; g += warps) {
+    const int s = g * 32 + lane;
+    const bool valid = s < L.n;
+    int cnt = 0;
+    long long base = 0;
+    bool room = true;
+    if (FILL) {
+      base = L.slice_off[g];
+      room = base + 32LL * L.slice_w[g] <= L.cap_entries;
+    }
+    if (valid && room) {
+      const int a = L.sorted[s];
+      const int i = L.idx[a];
+      const PT pi = pos[s];
+      const int ne = L.excl_n[i];
+      const int* ex = L.excl + (size_t)i * 20;
+      const bool i_vs = L.hybrid && i >= L.natoms;
+      const int c0 = L.cell_of[a];
+      const int ix = c0 / (nz * ny), iy = (c0 / nz) % ny, iz = c0 % nz;
+      auto consider = [&](int t) {
+        const int j = L.idx[L.sorted[t]];
+        for (int e = 0; e < ne; ++e)
+          if (ex[e] == j) return;
+        if (i_vs && j >= L.natoms) return;
+        const PT pj = pos[t];
+        R d0 = pi.x - pj.x, d1 = pi.y - pj.y, d2 = pi.z - pj.z;
+        d0 = d0 - r_round(d0 * bi[0]) * b[0];
+        d1 = d1 - r_round(d1 * bi[1]) * b[1];
+        d2 = d2 - r_round(d2 * bi[2]) * b[2];
+        R r2 = d0 * d0;
+        r2 = r2 + d1 * d1;
+        r2 = r2 + d2 * d2;
+        if (r2 < rlsq) {
+          if (FILL) L.entries[base + (long long)cnt * 32 + lane] = t;
+          ++cnt;
+        }
+      };
+      for (int t = s - 1; t >= L.cell_start[c0]; --t) consider(t);
+      const int off[13][3] = {{1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {-1, 1, 0}, {1, 0, -1}, {1, 1, -1}, {0, 1, -1},
+                              {-1, 1, -1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}, {-1, 1, 1}, {0, 0, 1}};
+#pragma unroll 1
+      for (int q = 0; q < 13; ++q) {
+        int jx = (ix + off[q][0] + nx) % nx, jy = (iy + off[q][1] + ny) % ny, jz = (iz + off[q][2] + nz) % nz;
+        int c = jx * nz * ny + jy * nz + jz;
+        for (int t = L.cell_start[c + 1] - 1; t >= L.cell_start[c]; --t) consider(t);
+      }
+      if (!FILL) {
+        L.counts[s] = cnt;
+        if (cnt >= L.maxnab) atomicOr(&sc->err, EB_LIST_OVERFLOW);
+      }
+    }
+    if (FILL && !room && lane == 0) atomicOr(&sc->err, EB_CAPACITY);
+    if (!FILL) {
+      int w = __reduce_max_sync(0xffffffffu, valid ? cnt : 0);
+      if (lane == 0) L.slice_w[g] = w;
+    }
+  }
+}
+
+// Exclusive scan of 32*slice_w into slice_off (single block).
+__global__ void k_scan_slices(const int* w, long long* off, int m) {
+  __shared__ long long part[1024];
+  const int t = threadIdx.x, T = blockDim.x;
+  const int chunk = (m + T - 1) / T;
+  const int b = t * chunk, e = min(m, b + chunk);
+  long long s = 0;
+  for (int i = b; i < e; ++i) s += 32LL * w[i];
+  part[t] = s;
+  __syncthreads();
+  if (t == 0) {
+    long long run = 0;
+    for (int i = 0; i < T; ++i) { long long v = part[i]; part[i] = run; run += v; }
+    off[m] = run;
+  }
+  __syncthreads();
+  long long run = part[t];
+  for (int i = b; i < e; ++i) { off[i] = run; run += 32LL * w[i]; }
+}
+
+// ------------------------------------------------------------- nonbonded
+template <typename R>
+struct NBArgs {
+  int n, nslices, ntype;
+  const void* pos4;
+  const int* counts;
+  const int* slice_w;
+  const long long* slice_off;
+  const int* entries;
+  long long cap_entries;           // slices reaching past it are skipped (capacity error)
+  typename Prec<R>::acc_t* fsort;  // [3n] per slot
+  // tables of this list: ltab[ti*ntype+tj] = local table or -1; rows of table
+  // t are [toff[t], toff[t+1]); fp = {F,P} per row, x = RNBOND per row
+  const int* ltab;
+  const int* toff;
+  const int* tndat;
+  const R* tbin;
+  const R* tfp;  // 2 per row
+  const R* tx;
+  int ntab, nrows;
+  R rcutsq;
+  double* part;  // 9 per block: V_NB(1..3), PT11,PT22,PT33,PT12,PT13,PT23
+  int part_stride;
+};
+
+// NONBONDED_FORCE.F90:173-232.  Persistent grid; each warp owns one slice of
+// 32 consecutive slots at a time and walks the 32 lists in lock step; list
+// reads are coalesced (sliced-ELL), neighbour positions are float4 gathers
+// from the cell-ordered array.  i-forces stay in registers, j-forces are
+// 64-bit integer atomics.  Tables are staged in shared memory when SMEM.
+template <typename R, bool SMEM>
+__global__ void __launch_bounds__(256) k_nonbonded(NBArgs<R> A, Scalars* sc) {
+  using P = Prec<R>;
+  using PT = typename P::pos_t;
+  using reg_t = typename P::reg_t;
+  extern __shared__ unsigned char smem_raw[];
+  const int* ltab = A.ltab;
+  const int* toff = A.toff;
+  const int* tndat = A.tndat;
+  const R* tbin = A.tbin;
+  const R* tfp = A.tfp;
+  const R* tx = A.tx;
+  double* red = (double*)smem_raw;  // 9 * 8 doubles, reused at the end
+  if (SMEM) {
+    unsigned char* p = smem_raw + 9 * 8 * sizeof(double);
+    R* s_fp = (R*)p;               p += sizeof(R) * 2 * A.nrows;
+    R* s_x = (R*)p;                p += sizeof(R) * A.nrows;
+    R* s_bin = (R*)p;              p += sizeof(R) * A.ntab;
+    int* s_ltab = (int*)p;         p += sizeof(int) * A.ntype * A.ntype;
+    int* s_toff = (int*)p;         p += sizeof(int) * (A.ntab + 1);
+    int* s_ndat = (int*)p;
+    for (int k = threadIdx.x; k < 2 * A.nrows; k += blockDim.x) s_fp[k] = A.tfp[k];
+    for (int k = threadIdx.x; k < A.nrows; k += blockDim.x) s_x[k] = A.tx[k];
+    for (int k = threadIdx.x; k < A.ntab; k += blockDim.x) { s_bin[k] = A.tbin[k]; s_ndat[k] = A.tndat[k]; }
+    for (int k = threadIdx.x; k < A.ntype * A.ntype; k += blockDim.x) s_ltab[k] = A.ltab[k];
+    for (int k = threadIdx.x; k <= A.ntab; k += blockDim.x) s_toff[k] = A.toff[k];
+    __syncthreads();
+    ltab = s_ltab; toff = s_toff; tndat = s_ndat; tbin = s_bin; tfp = s_fp; tx = s_x;
+  }
+  R b[3], bi[3], b2[3];
+  box_of<R>(sc, b, bi, b2);
+  const PT* pos = (const PT*)A.pos4;
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  double acc[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+  unsigned err = 0;
+  for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < A.nslices; g += warps) {
+    const int s = g * 32 + lane;
+    const bool valid = s < A.n;
+    const int cnt = valid ? A.counts[s] : 0;
+    int w = A.slice_w[g];
+    const long long base = A.slice_off[g];
+    if (base + 32LL * w > A.cap_entries) {
+      err |= EB_CAPACITY;
+      w = 0;
+    }
+    PT pi;
+    if (valid) pi = pos[s];
+    else { pi.x = pi.y = pi.z = 0; pi.w = P::tbits(0); }
+    const int wi = P::bits(pi.w);
+    const int ti = wi & 0xffff, li = wi >> 16;
+    reg_t fi0 = 0, fi1 = 0, fi2 = 0;
+    for (int k = 0; k < w; ++k) {
+      if (k >= cnt) continue;
+      const int t = A.entries[base + (long long)k * 32 + lane];
+      const PT pj = pos[t];
+      R d0 = pi.x - pj.x, d1 = pi.y - pj.y, d2 = pi.z - pj.z;
+      d0 = d0 - r_round(d0 * bi[0]) * b[0];
+      d1 = d1 - r_round(d1 * bi[1]) * b[1];
+      d2 = d2 - r_round(d2 * bi[2]) * b[2];
+      R r2 = d0 * d0;
+      r2 = r2 + d1 * d1;
+      r2 = r2 + d2 * d2;
+      if (!(r2 < A.rcutsq)) continue;
+      const int wj = P::bits(pj.w);
+      const int tj = wj & 0xffff, lj = wj >> 16;
+      const int tab = ltab[ti * A.ntype + tj];
+      if (tab < 0) { err |= EB_MISSING_TABLE; continue; }
+      const R r = r_sqrt(r2);
+      const R bin = tbin[tab];
+      const int ni = fint(r / bin);
+      if (ni < 0 || ni > tndat[tab]) { err |= EB_TABLE_RANGE; continue; }
+      const int row = toff[tab] + ni;
+      const R alpha = (r - tx[row]) / bin;
+      const R f0 = tfp[2 * row], p0 = tfp[2 * row + 1], f1 = tfp[2 * row + 2], p1 = tfp[2 * row + 3];
+      const R one_a = (R)1.0 - alpha;
+      const R fij = f0 * one_a + f1 * alpha;
+      const R vij = p0 * one_a + p1 * alpha;
+      if (li == 1) acc[0] += (double)vij;
+      else if (li == 2) {
+        if (lj == 2) acc[1] += (double)vij;
+        else if (lj == 3) acc[2] += (double)vij;
+      } else if (li == 3) acc[2] += (double)vij;
+      const R fx = fij * d0, fy = fij * d1, fz = fij * d2;
+      const reg_t qx = P::q(fx, &sc->err), qy = P::q(fy, &sc->err), qz = P::q(fz, &sc->err);
+      fi0 += qx; fi1 += qy; fi2 += qz;
+      P::add(&A.fsort[3 * (size_t)t + 0], -qx);
+      P::add(&A.fsort[3 * (size_t)t + 1], -qy);
+      P::add(&A.fsort[3 * (size_t)t + 2], -qz);
+      acc[3] += (double)(fx * d0);
+      acc[4] += (double)(fy * d1);
+      acc[5] += (double)(fz * d2);
+      acc[6] += (double)(fy * d0);
+      acc[7] += (double)(fz * d0);
+      acc[8] += (double)(fz * d1);
+    }
+    if (valid && cnt > 0) {
+      P::add(&A.fsort[3 * (size_t)s + 0], fi0);
+      P::add(&A.fsort[3 * (size_t)s + 1], fi1);
+      P::add(&A.fsort[3 * (size_t)s + 2], fi2);
+    }
+  }
+  if (err) atomicOr(&sc->err, err);
+  __syncthreads();
+  double out[9];
+  block_sum<9>(acc, red, out);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 9; ++k) A.part[k * A.part_stride + blockIdx.x] = out[k];
+}
+
+// Per-slot forces of both lists into the global-order nonbonded force
+// array; the bead list's MTS history is saved (MTS_SAVEFORCE, explicit steps)
+// or used for the extrapolation F = F3 + (m-3)/2 (F3 - F1) (MTS_APPROX,
+// MTS_LOOP.f90:176).  The slot buffer is cleared for the next step.
+template <typename R>
+struct CollectArgs {
+  int n;                         // slots in this list
+  int mts;                       // 1 for the bead list of an MTS run
+  const int* sorted;             // slot -> A
+  const int* idx;                // A -> global id
+  typename Prec<R>::acc_t* fsort;
+  typename Prec<R>::acc_t* fnb;  // (3,NITEMS) global order
+  typename Prec<R>::acc_t* mtsf; // [3][n][3] by A
+};
+
+template <typename R>
+__global__ void k_nb_collect(CollectArgs<R> C, Scalars* sc) {
+  using P = Prec<R>;
+  const int m = sc->mts_m;
+  const bool explicit_step = !C.mts || (m >= 1 && m <= 3);
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < C.n; s += gridDim.x * blockDim.x) {
+    const int a = C.sorted[s];
+    const int gi = C.idx[a];
+    if (explicit_step) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        typename P::acc_t v = C.fsort[3 * (size_t)s + c];
+        C.fnb[3 * (size_t)gi + c] = v;
+        if (C.mts) C.mtsf[((size_t)(m - 1) * C.n + a) * 3 + c] = v;
+        C.fsort[3 * (size_t)s + c] = 0;
+      }
+    } else {
+      const double coef = (double)(m - 3) * 0.5;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double f3 = P::get(C.mtsf[((size_t)2 * C.n + a) * 3 + c]);
+        double f1 = P::get(C.mtsf[((size_t)0 * C.n + a) * 3 + c]);
+        C.fnb[3 * (size_t)gi + c] = (typename P::acc_t)P::from_double(f3 + coef * (f3 - f1), &sc->err);
+      }
+    }
+  }
+}
+
+// DISTRIBUTE_VSFORCE.f90:27-37: F(atom) += F(vs) * VIRT_MASSCOEFF; F(vs) = 0.
+template <typename R>
+__global__ void k_distribute(typename Prec<R>::acc_t* F, int natoms, int nvirta, const int* vnum, const int* vmem,
+                             const float* vcoef, Scalars* sc) {
+  using P = Prec<R>;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nvirta; v += gridDim.x * blockDim.x) {
+    const size_t vs = (size_t)(natoms + v);
+    double f[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) f[c] = P::get(F[3 * vs + c]);
+    const int nm = vnum[v];
+    for (int k = 0; k < nm; ++k) {
+      const int j = vmem[v * 15 + k];
+      const double cf = (double)vcoef[v * 15 + k];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) P::add(&F[3 * (size_t)j + c], P::from_double(f[c] * cf, &sc->err));
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) F[3 * vs + c] = 0;
+  }
+}
+
+// --------------------------------------------------------------- bonded
+template <typename R>
+struct BondedArgs {
+  const R* su;                     // unwrapped positions (3,NITEMS)
+  typename Prec<R>::acc_t* fb;     // bonded forces (3,NITEMS)
+  int nb, na, nt, no;
+  const int4* bonds;               // i, j, table, label
+  const int4* angles;              // i, j, k, table | label<<24
+  const int4* tors;                // i, j, k, l
+  const int2* tors_t;              // table, label
+  const int4* oops;
+  const int2* oops_t;
+  // tables: rows {X, F, P, 0}; table t starts at off[t]
+  const float4* tb; const int* tb_off; const int* tb_ndat; const float* tb_bin;
+  const float4* ta; const int* ta_off; const int* ta_ndat; const float* ta_bin;
+  const float4* tt; const int* tt_off; const int* tt_ndat; const float* tt_bin;
+  const float4* to; const int* to_off; const int* to_ndat; const float* to_bin;
+  float r2d;
+  double* part;   // 12 per block: V_BOND(3), V_ANGLE(3), V_TORSION(3), V_OOP(3)
+  int part_stride;
+};
+
+template <typename R>
+__device__ __forceinline__ R lerp_mixed(R y0, R y1, R alpha) {
+  // y0*(1.0D0-alpha) + alpha*y1 with the FP64 promotion of BONDS.inc:141-145
+  return (R)((double)y0 * (1.0 - (double)alpha) + (double)(alpha * y1));
+}
+
+template <typename R>
+__device__ __forceinline__ void addf(typename Prec<R>::acc_t* F, int i, const R* f, unsigned* err) {
+  using P = Prec<R>;
+  P::add(&F[3 * (size_t)i + 0], P::q(f[0], err));
+  P::add(&F[3 * (size_t)i + 1], P::q(f[1], err));
+  P::add(&F[3 * (size_t)i + 2], P::q(f[2], err));
+}
+
+// BONDS.inc:3-57, ANGLES.inc:2-75, TORSIONS.inc:1-152, OUTOFPLANES.inc:1-141
+// with one thread per term; the four term kinds share the grid.
+template <typename R>
+__global__ void __launch_bounds__(256) k_bonded(BondedArgs<R> B, Scalars* sc) {
+  using P = Prec<R>;
+  __shared__ double red[12 * 8];
+  double acc[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) acc[k] = 0.0;
+  unsigned long long overext = 0;
+  unsigned* err = &sc->err;
+  const R* S = B.su;
+  auto pos = [&](int i, R* o) { o[0] = S[3 * (size_t)i]; o[1] = S[3 * (size_t)i + 1]; o[2] = S[3 * (size_t)i + 2]; };
+  const int total = B.nb + B.na + B.nt + B.no;
+  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < total; u += gridDim.x * blockDim.x) {
+    if (u < B.nb) {  // -------------------------------- bond
+      const int4 e = B.bonds[u];
+      R ri[3], rj[3], d[3];
+      pos(e.x, ri); pos(e.y, rj);
+      for (int c = 0; c < 3; ++c) d[c] = ri[c] - rj[c];
+      R rsq = d[0] * d[0] + d[1] * d[1];
+      rsq = rsq + d[2] * d[2];
+      const R rij = r_sqrt(rsq);
+      const int t = e.z;
+      const float4* T = B.tb + B.tb_off[t];
+      const R bin = (R)B.tb_bin[t];
+      int k = fint((rij - (R)T[0].x) / bin);
+      if (k > B.tb_ndat[t]) { ++overext; k = B.tb_ndat[t]; }
+      else if (k < 0) k = 0;
+      const float4 r0 = T[k], r1 = T[k + 1];
+      const R alpha = (rij - (R)r0.x) / bin;
+      const R fij = lerp_mixed<R>((R)r0.y, (R)r1.y, alpha);
+      const R vij = lerp_mixed<R>((R)r0.z, (R)r1.z, alpha);
+      acc[e.w - 1] += (double)vij;
+      R f[3], mf[3];
+      for (int c = 0; c < 3; ++c) { f[c] = fij * d[c]; mf[c] = -f[c]; }
+      addf<R>(B.fb, e.x, f, err);
+      addf<R>(B.fb, e.y, mf, err);
+    } else if (u < B.nb + B.na) {  // ---------------- angle
+      const int4 e = B.angles[u - B.nb];
+      const int t = e.w & 0xffffff, lab = e.w >> 24;
+      R ri[3], rj[3], rk[3], ij[3], kj[3];
+      pos(e.x, ri); pos(e.y, rj); pos(e.z, rk);
+      for (int c = 0; c < 3; ++c) { ij[c] = ri[c] - rj[c]; kj[c] = rk[c] - rj[c]; }
+      const R rij = r_sqrt((ij[0] * ij[0] + ij[1] * ij[1]) + ij[2] * ij[2]);
+      const R rkj = r_sqrt((kj[0] * kj[0] + kj[1] * kj[1]) + kj[2] * kj[2]);
+      const R ct = ((ij[0] * kj[0] + ij[1] * kj[1]) + ij[2] * kj[2]) / rij / rkj;
+      const R theta = r_acos(ct) * (R)B.r2d;
+      R m[3];
+      m[0] = -(ij[1] * kj[2] - ij[2] * kj[1]);
+      m[1] = -(-ij[0] * kj[2] + ij[2] * kj[0]);
+      m[2] = -(ij[0] * kj[1] - ij[1] * kj[0]);
+      const R rm = r_sqrt((m[0] * m[0] + m[1] * m[1]) + m[2] * m[2]);
+      for (int c = 0; c < 3; ++c) m[c] = m[c] / rm;
+      R nn[3], ss[3];
+      nn[0] = (m[1] * ij[2] - m[2] * ij[1]) / rij;
+      nn[1] = (-m[0] * ij[2] + m[2] * ij[0]) / rij;
+      nn[2] = (m[0] * ij[1] - m[1] * ij[0]) / rij;
+      ss[0] = -(m[1] * kj[2] - m[2] * kj[1]) / rkj;
+      ss[1] = -(-m[0] * kj[2] + m[2] * kj[0]) / rkj;
+      ss[2] = -(m[0] * kj[1] - m[1] * kj[0]) / rkj;
+      const float4* T = B.ta + B.ta_off[t];
+      const R bin = (R)B.ta_bin[t];
+      int k = fint(theta / bin);
+      if (k < 0 || k > B.ta_ndat[t] + 1) { atomicOr(err, EB_TABLE_RANGE); continue; }
+      R fijk, vijk;
+      const float4 r0 = T[k];
+      if (theta == (R)180.0) {
+        fijk = (R)r0.y; vijk = (R)r0.z;
+      } else {
+        const float4 r1 = T[k + 1];
+        const R alpha = (theta - (R)r0.x) / bin;
+        fijk = lerp_mixed<R>((R)r0.y, (R)r1.y, alpha);
+        vijk = lerp_mixed<R>((R)r0.z, (R)r1.z, alpha);
+      }
+      acc[3 + lab - 1] += (double)vijk;
+      R fI[3], fK[3], mI[3], mK[3];
+      for (int c = 0; c < 3; ++c) {
+        fI[c] = fijk * nn[c] / rij;
+        fK[c] = fijk * ss[c] / rkj;
+        mI[c] = -fI[c]; mK[c] = -fK[c];
+      }
+      addf<R>(B.fb, e.x, fI, err);
+      addf<R>(B.fb, e.z, fK, err);
+      addf<R>(B.fb, e.y, mK, err);
+      addf<R>(B.fb, e.y, mI, err);
+    } else if (u < B.nb + B.na + B.nt) {  // -------- torsion
+      const int q = u - B.nb - B.na;
+      const int4 e = B.tors[q];
+      const int2 tl = B.tors_t[q];
+      R ri[3], rj[3], rk[3], rl[3], ij[3], jk[3], kl[3];
+      pos(e.x, ri); pos(e.y, rj); pos(e.z, rk); pos(e.w, rl);
+      for (int c = 0; c < 3; ++c) { ij[c] = ri[c] - rj[c]; jk[c] = rj[c] - rk[c]; kl[c] = rk[c] - rl[c]; }
+      R rij = r_sqrt((ij[0] * ij[0] + ij[1] * ij[1]) + ij[2] * ij[2]);
+      const R rjk = r_sqrt((jk[0] * jk[0] + jk[1] * jk[1]) + jk[2] * jk[2]);
+      R rkl = r_sqrt((kl[0] * kl[0] + kl[1] * kl[1]) + kl[2] * kl[2]);
+      R m[3], nn[3], cosm = 0, sinm = 0, cotanm = 0, cosn = 0, sinn = 0, cotann = 0;
+      auto crossm = [&]() {
+        m[0] = ij[1] * jk[2] - ij[2] * jk[1];
+        m[1] = -ij[0] * jk[2] + ij[2] * jk[0];
+        m[2] = ij[0] * jk[1] - ij[1] * jk[0];
+      };
+      auto crossn = [&]() {
+        nn[0] = jk[1] * kl[2] - jk[2] * kl[1];
+        nn[1] = -jk[0] * kl[2] + jk[2] * kl[0];
+        nn[2] = jk[0] * kl[1] - jk[1] * kl[0];
+      };
+      crossm();
+      R rm = r_sqrt((m[0] * m[0] + m[1] * m[1]) + m[2] * m[2]);
+      if (rm == (R)0) {  // TORSIONS.inc:47-60: perturb collinear i-j-k
+        ij[0] = ri[0] * (R)0.99f - rj[0];
+        rij = r_sqrt((ij[0] * ij[0] + ij[1] * ij[1]) + ij[2] * ij[2]);
+        crossm();
+        rm = r_sqrt((m[0] * m[0] + m[1] * m[1]) + m[2] * m[2]);
+      }
+      if (rm > (R)0 || rm == (R)0) {
+        for (int c = 0; c < 3; ++c) m[c] = m[c] / rm;
+        cosm = ((ij[0] * jk[0] + ij[1] * jk[1]) + ij[2] * jk[2]) / rij / rjk;
+        sinm = r_sqrt((R)1 - cosm * cosm);
+        cotanm = cosm / sinm;
+      }
+      crossn();
+      R rn = r_sqrt((nn[0] * nn[0] + nn[1] * nn[1]) + nn[2] * nn[2]);
+      if (rn == (R)0) {  // TORSIONS.inc:75-88
+        kl[0] = rk[0] - rl[0] * (R)0.99f;
+        rkl = r_sqrt((kl[0] * kl[0] + kl[1] * kl[1]) + kl[2] * kl[2]);
+        crossn();
+        rn = r_sqrt((nn[0] * nn[0] + nn[1] * nn[1]) + nn[2] * nn[2]);
+      }
+      if (rn > (R)0 || rn == (R)0) {
+        for (int c = 0; c < 3; ++c) nn[c] = nn[c] / rn;
+        cosn = ((jk[0] * kl[0] + jk[1] * kl[1]) + jk[2] * kl[2]) / rjk / rkl;
+        sinn = r_sqrt((R)1 - cosn * cosn);
+        cotann = cosn / sinn;
+      }
+      R cost = (m[0] * nn[0] + m[1] * nn[1]) + m[2] * nn[2];
+      const R signt = -((m[0] * kl[0] + m[1] * kl[1]) + m[2] * kl[2]);
+      if (cost > (R)1.0) cost = (R)1.0;
+      else if (cost < (R)-1.0) cost = (R)-1.0;
+      R phi = r_acos(cost) * (R)B.r2d;
+      if (signt < (R)0) phi = (R)360.0 - phi;
+      const int t = tl.x;
+      const float4* T = B.tt + B.tt_off[t];
+      const R bin = (R)B.tt_bin[t];
+      const int k = fint(phi / bin);
+      if (k < 0 || k > B.tt_ndat[t]) { atomicOr(err, EB_TORSION); continue; }
+      R fijkl, vijkl;
+      const float4 r0 = T[k];
+      if (phi == (R)360.0) {
+        fijkl = (R)r0.y; vijkl = (R)r0.z;
+      } else {
+        const float4 r1 = T[k + 1];
+        const R alpha = (phi - (R)r0.x) / bin;
+        fijkl = (R)r0.y * ((R)1.0 - alpha) + alpha * (R)r1.y;
+        vijkl = (R)r0.z * ((R)1.0 - alpha) + alpha * (R)r1.z;
+      }
+      acc[6 + tl.y - 1] += (double)vijkl;
+      R f1[3], f4[3], f12[3], a[3];
+      for (int c = 0; c < 3; ++c) {
+        f1[c] = -(fijkl * m[c] / sinm / rij);
+        f4[c] = fijkl * nn[c] / sinn / rkl;
+        f12[c] = fijkl * (cotanm * m[c] + cotann * nn[c]) / rjk;
+      }
+      addf<R>(B.fb, e.x, f1, err);
+      addf<R>(B.fb, e.w, f4, err);
+      for (int c = 0; c < 3; ++c) a[c] = -f1[c];
+      addf<R>(B.fb, e.y, a, err);
+      addf<R>(B.fb, e.y, f12, err);
+      for (int c = 0; c < 3; ++c) a[c] = -f4[c];
+      addf<R>(B.fb, e.z, a, err);
+      for (int c = 0; c < 3; ++c) a[c] = -f12[c];
+      addf<R>(B.fb, e.z, a, err);
+    } else {  // ------------------------------------------ out of plane
+      const int q = u - B.nb - B.na - B.nt;
+      const int4 e = B.oops[q];
+      const int2 tl = B.oops_t[q];
+      R ri[3], rj[3], rk[3], rl[3], ij[3], jk[3], kl[3];
+      pos(e.x, ri); pos(e.y, rj); pos(e.z, rk); pos(e.w, rl);
+      for (int c = 0; c < 3; ++c) { ij[c] = ri[c] - rj[c]; jk[c] = rk[c] - rj[c]; kl[c] = rk[c] - rl[c]; }
+      const R rij = r_sqrt((ij[0] * ij[0] + ij[1] * ij[1]) + ij[2] * ij[2]);
+      const R rjk = r_sqrt((jk[0] * jk[0] + jk[1] * jk[1]) + jk[2] * jk[2]);
+      const R rkl = r_sqrt((kl[0] * kl[0] + kl[1] * kl[1]) + kl[2] * kl[2]);
+      R m[3], nn[3], mn[3];
+      m[0] = ij[1] * jk[2] - ij[2] * jk[1];
+      m[1] = -ij[0] * jk[2] + ij[2] * jk[0];
+      m[2] = ij[0] * jk[1] - ij[1] * jk[0];
+      const R rm = r_sqrt((m[0] * m[0] + m[1] * m[1]) + m[2] * m[2]);
+      for (int c = 0; c < 3; ++c) m[c] = m[c] / rm;
+      const R cm = ((ij[0] * jk[0] + ij[1] * jk[1]) + ij[2] * jk[2]) / rij / rjk;
+      const R sm = r_sqrt((R)1 - cm * cm);
+      const R ctm = cm / sm;
+      nn[0] = jk[1] * kl[2] - jk[2] * kl[1];
+      nn[1] = -jk[0] * kl[2] + jk[2] * kl[0];
+      nn[2] = jk[0] * kl[1] - jk[1] * kl[0];
+      const R rn = r_sqrt((nn[0] * nn[0] + nn[1] * nn[1]) + nn[2] * nn[2]);
+      for (int c = 0; c < 3; ++c) nn[c] = nn[c] / rn;
+      const R cn = ((jk[0] * kl[0] + jk[1] * kl[1]) + jk[2] * kl[2]) / rjk / rkl;
+      const R sn = r_sqrt((R)1 - cn * cn);
+      const R ctn = cn / sn;
+      R cost = (m[0] * nn[0] + m[1] * nn[1]) + m[2] * nn[2];
+      mn[0] = m[1] * nn[2] - m[2] * nn[1];
+      mn[1] = -m[0] * nn[2] + m[2] * nn[0];
+      mn[2] = m[0] * nn[1] - m[1] * nn[0];
+      const R sgn = copysign((R)1.0, (mn[0] * jk[0] + mn[1] * jk[1]) + mn[2] * jk[2]);
+      const R eps = (R)1.0e-7f;
+      if (cost > (R)1.0 + eps || cost < -((R)1.0 + eps)) { atomicOr(err, EB_OOP); continue; }
+      if (cost > (R)1.0) cost = (R)1.0;
+      else if (cost < (R)-1.0) cost = (R)-1.0;
+      R phi = r_acos(cost);
+      phi = sgn * phi;
+      phi = phi * (R)B.r2d;
+      const R phit = (R)180.0 + phi;
+      const int t = tl.x;
+      const float4* T = B.to + B.to_off[t];
+      const R bin = (R)B.to_bin[t];
+      int k = fint(r_round(phit / bin));
+      if (k < 0 || k > B.to_ndat[t]) { atomicOr(err, EB_OOP); continue; }
+      R alpha = r_abs(r_abs(phi) - r_abs((R)T[k].x)) / bin;
+      if (alpha > (R)1.0) {
+        k = k + 1;
+        alpha = r_abs(r_abs(phi) - r_abs((R)T[k].x)) / bin;
+      }
+      const float4 r0 = T[k], r1 = T[k + 1];
+      const R fijkl = (R)r0.y * ((R)1.0 - alpha) + alpha * (R)r1.y;
+      const R vijkl = (R)r0.z * ((R)1.0 - alpha) + alpha * (R)r1.z;
+      acc[9 + tl.y - 1] += (double)vijkl;
+      R f1[3], f4[3], f12[3], a[3];
+      for (int c = 0; c < 3; ++c) {
+        f1[c] = fijkl * m[c] / sm / rij;
+        f4[c] = -(fijkl * nn[c] / sn / rkl);
+        f12[c] = fijkl * (ctm * m[c] + ctn * nn[c]) / rjk;
+      }
+      addf<R>(B.fb, e.x, f1, err);
+      addf<R>(B.fb, e.w, f4, err);
+      for (int c = 0; c < 3; ++c) a[c] = -f1[c];
+      addf<R>(B.fb, e.y, a, err);
+      addf<R>(B.fb, e.y, f12, err);
+      for (int c = 0; c < 3; ++c) a[c] = -f4[c];
+      addf<R>(B.fb, e.z, a, err);
+      for (int c = 0; c < 3; ++c) a[c] = -f12[c];
+      addf<R>(B.fb, e.z, a, err);
+    }
+  }
+  if (overext) atomicAdd(&sc->bond_overext, overext);
+  double out[12];
+  block_sum<12>(acc, red, out);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 12; ++k) B.part[k * B.part_stride + blockIdx.x] = out[k];
+}
+
+// ------------------------------------------------------------ integration
+template <typename R>
+struct MoveArgs {
+  int natoms;
+  double* S;  // (3,NATOMS) unwrapped, FP64 state
+  double* V;  // (3,NATOMS)
+  const typename Prec<R>::acc_t* fnb;
+  const typename Prec<R>::acc_t* fb;
+  const int* tbits;         // label in bits 16.. (1 atom, 2 bead)
+  const double* mass;       // per particle
+  const double* invmass;    // per particle
+  double dt;
+  int update;               // 0: bonded virial only (force stage without MOVE)
+  double* part;             // 18 per block
+  int part_stride;
+};
+
+// MOVE.F90:81-129 (leap-frog with Berendsen factors per class) and the
+// bonded virial sum of NEW_FORCE.F90:73-80, which uses the positions before
+// the update.  Partials: PTK(6) atoms, PTK(6) beads, bonded virial(6).
+template <typename R>
+__global__ void __launch_bounds__(256) k_move(MoveArgs<R> M, Scalars* sc) {
+  using P = Prec<R>;
+  __shared__ double red[18 * 8];
+  double acc[18];
+#pragma unroll
+  for (int k = 0; k < 18; ++k) acc[k] = 0.0;
+  const double lam0 = sc->lam[0], lam1 = sc->lam[1];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M.natoms; i += gridDim.x * blockDim.x) {
+    double s[3], v[3], fb[3], f[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      s[c] = M.S[3 * (size_t)i + c];
+      v[c] = M.V[3 * (size_t)i + c];
+      fb[c] = P::get(M.fb[3 * (size_t)i + c]);
+      f[c] = P::get(M.fnb[3 * (size_t)i + c]) + fb[c];
+    }
+    acc[12] += fb[0] * s[0];
+    acc[13] += fb[1] * s[1];
+    acc[14] += fb[2] * s[2];
+    acc[15] += fb[1] * s[0];
+    acc[16] += fb[2] * s[0];
+    acc[17] += fb[2] * s[1];
+    if (!M.update) continue;
+    const int cls = (M.tbits[i] >> 16) == 2 ? 1 : 0;
+    const double lam = cls ? lam1 : lam0;
+    const double m = M.mass[i], im = M.invmass[i];
+    double vt[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double vn = (v[c] + M.dt * f[c] * im) * lam;
+      M.V[3 * (size_t)i + c] = vn;
+      M.S[3 * (size_t)i + c] = s[c] + M.dt * vn;
+      vt[c] = 0.5 * (vn + v[c]);
+    }
+    const int o = 6 * cls;
+    acc[o + 0] += m * vt[0] * vt[0];
+    acc[o + 1] += m * vt[1] * vt[1];
+    acc[o + 2] += m * vt[2] * vt[2];
+    acc[o + 3] += m * vt[0] * vt[1];
+    acc[o + 4] += m * vt[0] * vt[2];
+    acc[o + 5] += m * vt[1] * vt[2];
+  }
+  double out[18];
+  block_sum<18>(acc, red, out);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 18; ++k) M.part[k * M.part_stride + blockIdx.x] = out[k];
+}
+
+// Initial kinetic energies (main.F90:179-195).  Partials: EK atoms, EK beads.
+__global__ void k_kinetic(int natoms, const double* V, const int* tbits, const double* mass, double* part, int stride) {
+  __shared__ double red[2 * 8];
+  double acc[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < natoms; i += gridDim.x * blockDim.x) {
+    const double* v = V + 3 * (size_t)i;
+    acc[(tbits[i] >> 16) == 2 ? 1 : 0] += mass[i] * ((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]);
+  }
+  double out[2];
+  block_sum<2>(acc, red, out);
+  if (threadIdx.x == 0) { part[blockIdx.x] = out[0]; part[stride + blockIdx.x] = out[1]; }
+}
+
+// MOMENTUM.f90:14-29 in FP64: partial sums of m v, then the removal.
+__global__ void k_mom_sum(int natoms, const double* V, const double* mass, double* part, int stride) {
+  __shared__ double red[3 * 8];
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < natoms; i += gridDim.x * blockDim.x)
+    for (int c = 0; c < 3; ++c) acc[c] += V[3 * (size_t)i + c] * mass[i];
+  double out[3];
+  block_sum<3>(acc, red, out);
+  if (threadIdx.x == 0)
+    for (int c = 0; c < 3; ++c) part[c * stride + blockIdx.x] = out[c];
+}
+
+__global__ void k_mom_apply(int natoms, double* V, const double* invmass, const double* part, int stride, int nblocks) {
+  __shared__ double tot[3];
+  if (threadIdx.x < 32) {
+    for (int c = 0; c < 3; ++c) {
+      double s = 0.0;
+      for (int b = threadIdx.x; b < nblocks; b += 32) s += part[c * stride + b];
+      s = warp_sum(s);
+      if (threadIdx.x == 0) tot[c] = s / (double)natoms;
+    }
+  }
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < natoms; i += gridDim.x * blockDim.x)
+    for (int c = 0; c < 3; ++c) V[3 * (size_t)i + c] -= tot[c] * invmass[i];
+}
+
+// SCALEBP.f90:259-261: positions scaled with the box.
+__global__ void k_scale_positions(int natoms, double* S, const Scalars* sc) {
+  const double miu = sc->miu;
+  if (miu == 1.0) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < natoms; i += gridDim.x * blockDim.x)
+    for (int c = 0; c < 3; ++c) S[3 * (size_t)i + c] *= miu;
+}
+
+// ------------------------------------------------------------- reductions
+struct FinalArgs {
+  const double* p_nb[2]; int g_nb;   // nonbonded partials of the atom / bead list (9 x g_nb)
+  const double* p_b; int g_b;        // bonded partials (12 x g_b)
+  const double* p_mv; int g_mv;      // move partials (18 x g_mv)
+  int mts;                           // MTS run
+  int move;                          // 1: full step (kinetic part, thermostat, barostat)
+  int ensemble;
+  double temp_in, fac, pfac, pressure, mktemp, mktemp_atom, mktemp_bead;
+  ObsD* ring; int ring_cap;
+};
+
+__device__ double wsum(const double* p, int g) {
+  double s = 0.0;
+  for (int b = threadIdx.x & 31; b < g; b += 32) s += p[b];
+  return warp_sum(s);
+}
+
+// Deterministic reduction of all partials into the observables, the MTS
+// auxiliary history (MTS_SAVEAUXS / MTS_LOADAUXS), the thermostat factors of
+// the next step and the barostat window (SCALEBP.f90:240-263).
+__global__ void k_finalize(FinalArgs F, Scalars* sc) {
+  __shared__ double q[64];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  // q[0..8] atom NB, q[9..17] bead NB, q[18..29] bonded, q[30..47] move
+  for (int k = warp; k < 48; k += nw) {
+    double v;
+    if (k < 9) v = F.p_nb[0] ? wsum(F.p_nb[0] + (size_t)k * F.g_nb, F.g_nb) : 0.0;
+    else if (k < 18) v = F.p_nb[1] ? wsum(F.p_nb[1] + (size_t)(k - 9) * F.g_nb, F.g_nb) : 0.0;
+    else if (k < 30) v = wsum(F.p_b + (size_t)(k - 18) * F.g_b, F.g_b);
+    else v = wsum(F.p_mv + (size_t)(k - 30) * F.g_mv, F.g_mv);
+    if (lane == 0) q[k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x) return;
+  ObsD& o = sc->obs;
+  double bead_v[3], bead_pt[6];
+  for (int c = 0; c < 3; ++c) bead_v[c] = q[9 + c];
+  for (int c = 0; c < 6; ++c) bead_pt[c] = q[12 + c];
+  const int m = sc->mts_m;
+  if (F.mts) {
+    if (m >= 1 && m <= 3) {
+      for (int c = 0; c < 3; ++c) sc->mts_vnb[m - 1][c] = bead_v[c];
+      for (int c = 0; c < 5; ++c) sc->mts_pt[c][m - 1] = bead_pt[c];  // PT23 is not saved (MTS_LOOP.f90:193-199)
+    } else {
+      const double coef = (double)(m - 3) * 0.5;
+      for (int c = 0; c < 3; ++c) bead_v[c] = sc->mts_vnb[2][c] + coef * (sc->mts_vnb[2][c] - sc->mts_vnb[0][c]);
+      for (int c = 0; c < 6; ++c) bead_pt[c] = sc->mts_pt[c][2] + coef * (sc->mts_pt[c][2] - sc->mts_pt[c][0]);
+    }
+  }
+  for (int c = 0; c < 3; ++c) {
+    o.v_nb[c] = q[c] + bead_v[c];
+    o.v_bond[c] = q[18 + c];
+    o.v_angle[c] = q[21 + c];
+    o.v_torsion[c] = q[24 + c];
+    o.v_oop[c] = q[27 + c];
+  }
+  double pt[6];
+  for (int c = 0; c < 6; ++c) pt[c] = q[3 + c] + bead_pt[c] + q[42 + c];
+  if (F.move) {
+    // MOVE.F90:131-156
+    for (int c = 0; c < 6; ++c) pt[c] += q[30 + c] + q[36 + c];
+    o.ek[0] = 0.5 * (q[30] + q[31] + q[32]);
+    o.ek[1] = 0.5 * (q[36] + q[37] + q[38]);
+    o.temp = (o.ek[0] + o.ek[1]) * F.mktemp;
+    o.temp_atom = o.ek[0] * F.mktemp_atom;
+    o.temp_bead = o.ek[1] * F.mktemp_bead;
+    sc->temp_atom = o.temp_atom;
+    sc->temp_bead = o.temp_bead;
+    const double vol = sc->box[0] * sc->box[1] * sc->box[2];
+    for (int c = 0; c < 6; ++c) pt[c] /= vol;
+    if (F.ensemble == 1 || F.ensemble == 2) {  // MOVE.F90:73-79, for the next step
+      sc->lam[0] = sqrt(1.0 + F.fac * ((F.temp_in / o.temp_atom) - 1.0));
+      sc->lam[1] = sqrt(1.0 + F.fac * ((F.temp_in / o.temp_bead) - 1.0));
+    }
+    if (F.ensemble == 2) {  // SCALEBP.f90:240-263
+      sc->iavp = sc->iavp + 1;
+      if (sc->iavp > 10) sc->iavp -= 10;
+      sc->sp[sc->iavp - 1] = (pt[0] + pt[1] + pt[2]) / 3.0;
+      if (sc->step % 10 == 0) {
+        double avp = 0.0;
+        for (int i = 0; i < 10; ++i) avp += sc->sp[i];
+        const double p = avp / 10.0;
+        const double miu = pow(1.0 + (p - F.pressure) * F.pfac, 1.0 / 3.0);
+        sc->miu = miu;
+        for (int c = 0; c < 3; ++c) {
+          sc->box[c] *= miu;
+          sc->boxinv[c] = 1.0 / sc->box[c];
+          sc->box2[c] = sc->box[c] / 2.0;
+          sc->boxf[c] = (float)sc->box[c];
+          sc->boxinvf[c] = 1.0f / sc->boxf[c];
+          sc->box2f[c] = sc->boxf[c] / 2.0f;
+        }
+      }
+    }
+  }
+  for (int c = 0; c < 6; ++c) o.pt[c] = pt[c];
+  for (int c = 0; c < 3; ++c) o.box[c] = sc->box[c];
+  o.bond_overext = (long long)sc->bond_overext;
+  o.cell_clamps = (long long)sc->cell_clamps;
+  o.step = sc->step;
+  o.status = (int)sc->err;
+  if (F.ring) {
+    int slot = sc->step - sc->ring_base;
+    if (slot >= 0 && slot < F.ring_cap) F.ring[slot] = o;
+  }
+}
+
+// Initial temperatures and Berendsen factors (main.F90:174-195).
+__global__ void k_init_temps(const double* part, int g, Scalars* sc, double mktemp, double mktemp_atom,
+                             double mktemp_bead, double temp_in, double fac, int ensemble) {
+  __shared__ double q[2];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp < 2) {
+    double v = wsum(part + (size_t)warp * g, g);
+    if (lane == 0) q[warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x) return;
+  ObsD& o = sc->obs;
+  o.ek[0] = 0.5 * q[0];
+  o.ek[1] = 0.5 * q[1];
+  o.temp = (o.ek[0] + o.ek[1]) * mktemp;
+  o.temp_atom = o.ek[0] * mktemp_atom;
+  o.temp_bead = o.ek[1] * mktemp_bead;
+  sc->temp_atom = o.temp_atom;
+  sc->temp_bead = o.temp_bead;
+  if (ensemble == 1 || ensemble == 2) {
+    sc->lam[0] = sqrt(1.0 + fac * ((temp_in / o.temp_atom) - 1.0));
+    sc->lam[1] = sqrt(1.0 + fac * ((temp_in / o.temp_bead) - 1.0));
+  } else {
+    sc->lam[0] = sc->lam[1] = 1.0;
+  }
+}
+
+}  // namespace ibg

@@ -1,0 +1,320 @@
+"""ctypes bindings of ``include/ibisco_gpu.h`` and a small host-side driver.
+
+The driver mirrors the reference's program flow: the setup phase of
+``main.F90:107-237`` (``ibg_setup_read`` + ``ibg_create`` + ``ibg_set_state``)
+followed by the loop body of ``NEW_LOOP.F90`` / ``MTS_LOOP.f90`` (``ibg_step``
+or the graph-replayed ``ibg_run``).  Status codes are those of the header; a
+non-zero status raises :class:`IbiscoError`, the analogue of the reference's
+``ISTOP``/``STOP`` paths.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+IBG_PREC_FP32_FIXED = 0
+IBG_PREC_FP64_PLAIN = 1
+
+STATUS = {
+    0: "IBG_OK", -1: "IBG_E_INVALID", -2: "IBG_E_LIST_OVERFLOW", -3: "IBG_E_TORSION_TABLE",
+    -4: "IBG_E_OOP_RANGE", -5: "IBG_E_FIXED_OVERFLOW", -6: "IBG_E_CELL_GRID", -7: "IBG_E_CUDA",
+    -8: "IBG_E_TIMEOUT", -9: "IBG_E_TABLE_RANGE", -10: "IBG_E_MISSING_TABLE", -11: "IBG_E_CAPACITY",
+    -12: "IBG_E_IO", -13: "IBG_E_MEMORY",
+}
+
+# Every entry point the header declares (checked by the CPU tests).
+EXPORTS = [
+    "ibg_setup_read", "ibg_setup_desc", "ibg_setup_initial_state", "ibg_setup_control",
+    "ibg_setup_array_i", "ibg_setup_array_f", "ibg_setup_free",
+    "ibg_create", "ibg_set_state", "ibg_step", "ibg_forces", "ibg_run", "ibg_get_state",
+    "ibg_get_state_f64", "ibg_get_neighbour_list", "ibg_get_exclusions", "ibg_set_timing",
+    "ibg_get_timing", "ibg_last_error", "ibg_destroy", "ibg_version", "ibg_set_l2_flush", "ibg_set_device",
+]
+
+
+_I, _F, _PI, _PF = ctypes.c_int, ctypes.c_float, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)
+
+
+class IbgDesc(ctypes.Structure):
+    """Mirror of ``ibg_desc`` (field order of include/ibisco_gpu.h)."""
+    _fields_ = (
+        [(n, _I) for n in ("natoms", "nvirta", "nitems", "ntype", "numatoms", "numbeads", "ncoarse", "ensemble",
+                           "nupdate", "halt_drift", "nmts", "ibrdescr", "maxnab")]
+        + [(n, _F) for n in ("dt", "fac", "pfac", "temp_in", "pressure", "mktemp", "mktemp_atom", "mktemp_bead",
+                             "rcut_atom", "rcutsq_atom", "rlist_atom", "rcut_bead", "rcutsq_bead", "rlist_bead")]
+        + [("mass", _PF), ("invmass", _PF), ("itype", _PI), ("type_label", _PI), ("atom", _PI), ("bead", _PI),
+           ("nbonds", _PI), ("jbond", _PI), ("ld_bond", _I),
+           ("nijk", _PI), ("jangleijk", _PI), ("kangleijk", _PI), ("ld_angle", _I),
+           ("nijkl", _PI), ("jtorijkl", _PI), ("ktorijkl", _PI), ("ltorijkl", _PI), ("ld_torsion", _I),
+           ("noopijkl", _PI), ("joopijkl", _PI), ("koopijkl", _PI), ("loopijkl", _PI), ("ld_oop", _I),
+           ("connections", _PI), ("connected_to", _PI), ("ld_conn", _I),
+           ("ibondt", _PI), ("inbondt", _PI), ("iangt", _PI), ("itort", _PI), ("ioopt", _PI),
+           ("bond_type_label", _PI), ("angle_type_label", _PI), ("torsion_type_label", _PI),
+           ("oop_type_label", _PI),
+           ("nbtype", _I), ("natype", _I), ("nttype", _I), ("nnbtype", _I), ("notype", _I),
+           ("ld_b", _I), ("ld_a", _I), ("ld_t", _I), ("ld_nb", _I), ("ld_o", _I)]
+        + [(f"{p}{q}", t) for p in ("b", "a", "t", "nb", "o")
+           for q, t in (("_ndat", _PI), ("_bin", _PF), ("_x", _PF), ("_pot", _PF), ("_force", _PF))]
+        + [("ld_vs", _I), ("vs_maxatoms", _I), ("vitype", _PI), ("virt_center", _PI), ("virt_numatoms", _PI),
+           ("virt_atm_ind", _PI), ("virt_invmass", _PF), ("virt_masscoeff", _PF)]
+    )
+
+
+class IbgObs(ctypes.Structure):
+    _fields_ = [
+        ("ek", ctypes.c_double * 2), ("temp", ctypes.c_double), ("temp_atom", ctypes.c_double),
+        ("temp_bead", ctypes.c_double), ("v_nb", ctypes.c_double * 3), ("v_bond", ctypes.c_double * 3),
+        ("v_angle", ctypes.c_double * 3), ("v_torsion", ctypes.c_double * 3), ("v_oop", ctypes.c_double * 3),
+        ("pt", ctypes.c_double * 6), ("box", ctypes.c_double * 3), ("bond_overext", ctypes.c_longlong),
+        ("cell_clamps", ctypes.c_longlong), ("step", ctypes.c_int), ("status", ctypes.c_int),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {"EK1": self.ek[0], "EK2": self.ek[1], "TEMP": self.temp, "TEMP_ATOM": self.temp_atom,
+             "TEMP_BEAD": self.temp_bead}
+        for name in ("v_nb", "v_bond", "v_angle", "v_torsion", "v_oop"):
+            for k in range(3):
+                d[f"{name.upper()}{k + 1}"] = getattr(self, name)[k]
+        for k, n in enumerate(("PT11", "PT22", "PT33", "PT12", "PT13", "PT23")):
+            d[n] = self.pt[k]
+        for k in range(3):
+            d[f"BOX{k + 1}"] = self.box[k]
+        d["BOND_OVEREXT"] = self.bond_overext
+        d["CELL_CLAMPS"] = self.cell_clamps
+        d["STEP"] = self.step
+        return d
+
+
+_lib = None
+
+
+def library_path() -> str:
+    return _build.LIB
+
+
+def lib(build_if_missing: bool = True):
+    """Load ``libibisco_b200.so`` (building it in-tree when it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.LIB
+    if not os.path.exists(path):
+        if not build_if_missing:
+            raise OSError(f"{path} is not built")
+        _build.build()
+    L = ctypes.CDLL(path)
+    vp, cp, ip, fp, dp = (ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int),
+                          ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double))
+    pvp = ctypes.POINTER(ctypes.c_void_p)
+    sig = {
+        "ibg_setup_read": (ctypes.c_int, [cp, pvp, cp, ctypes.c_int]),
+        "ibg_setup_desc": (vp, [vp]),
+        "ibg_setup_initial_state": (ctypes.c_int, [vp, fp, fp, fp]),
+        "ibg_setup_control": (ctypes.c_int, [vp, ip, ctypes.c_int]),
+        "ibg_setup_array_i": (ctypes.c_long, [vp, cp, ip, ctypes.c_long]),
+        "ibg_setup_array_f": (ctypes.c_long, [vp, cp, fp, ctypes.c_long]),
+        "ibg_setup_free": (None, [vp]),
+        "ibg_create": (ctypes.c_int, [vp, ctypes.c_int, pvp]),
+        "ibg_set_state": (ctypes.c_int, [vp, fp, fp, fp]),
+        "ibg_step": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(IbgObs)]),
+        "ibg_forces": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(IbgObs)]),
+        "ibg_run": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(IbgObs)]),
+        "ibg_get_state": (ctypes.c_int, [vp, fp, fp, fp, fp]),
+        "ibg_get_state_f64": (ctypes.c_int, [vp, dp, dp, dp]),
+        "ibg_get_neighbour_list": (ctypes.c_int, [vp, ctypes.c_int, ip, ctypes.c_int, ip]),
+        "ibg_get_exclusions": (ctypes.c_int, [vp, ip, ip]),
+        "ibg_set_timing": (ctypes.c_int, [vp, ctypes.c_int]),
+        "ibg_get_timing": (ctypes.c_int, [vp, dp, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]),
+        "ibg_last_error": (cp, [vp]),
+        "ibg_destroy": (None, [vp]),
+        "ibg_version": (cp, []),
+        "ibg_set_l2_flush": (ctypes.c_int, [vp, ctypes.c_longlong]),
+        "ibg_set_device": (ctypes.c_int, [ctypes.c_int]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return _lib
+
+
+class IbiscoError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def _fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Setup:
+    """The reference's setup phase run on the host from an input directory."""
+
+    def __init__(self, directory: str):
+        L = lib()
+        h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        rc = L.ibg_setup_read(directory.encode(), ctypes.byref(h), err, 512)
+        if rc != 0:
+            raise IbiscoError(rc, err.value.decode())
+        self._h = h
+        iv = np.zeros(8, np.int32)
+        L.ibg_setup_control(h, _ip(iv), 8)
+        self.nstep, self.ntrj, self.restart = int(iv[0]), int(iv[1]), int(iv[2])
+
+    @property
+    def handle(self):
+        return self._h
+
+    def desc(self):
+        return lib().ibg_setup_desc(self._h)
+
+    def array(self, name: str) -> np.ndarray:
+        L = lib()
+        n = L.ibg_setup_array_i(self._h, name.encode(), None, 0)
+        if n >= 0:
+            a = np.zeros(max(n, 1), np.int32)
+            L.ibg_setup_array_i(self._h, name.encode(), _ip(a), n)
+            return a[:n]
+        n = L.ibg_setup_array_f(self._h, name.encode(), None, 0)
+        if n < 0:
+            raise KeyError(name)
+        a = np.zeros(max(n, 1), np.float32)
+        L.ibg_setup_array_f(self._h, name.encode(), _fp(a), n)
+        return a[:n]
+
+    def initial_state(self):
+        itype = self.array("ITYPE")
+        n = len(self.array("SXYZ")) // 3
+        s = np.zeros((n, 3), np.float32)
+        v = np.zeros((n, 3), np.float32)
+        b = np.zeros(3, np.float32)
+        lib().ibg_setup_initial_state(self._h, _fp(s), _fp(v), _fp(b))
+        del itype
+        return s, v, b
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ibg_setup_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+class System:
+    """One system on the current CUDA device (``ibg_ctx``)."""
+
+    def __init__(self, setup: Setup, precision: int = IBG_PREC_FP32_FIXED, **desc_overrides):
+        L = lib()
+        h = ctypes.c_void_p()
+        desc = setup.desc()
+        if desc_overrides:  # e.g. maxnab=...: a modified copy of the descriptor
+            copy = IbgDesc.from_address(desc)
+            copy = IbgDesc.from_buffer_copy(copy)
+            for k, v in desc_overrides.items():
+                setattr(copy, k, v)
+            self._desc_copy = copy
+            desc = ctypes.addressof(copy)
+        rc = L.ibg_create(desc, int(precision), ctypes.byref(h))
+        if rc != 0:
+            raise IbiscoError(rc, "ibg_create failed")
+        self._h = h
+        self.setup = setup
+        self.precision = precision
+        s, _, _ = setup.initial_state()
+        self.natoms = s.shape[0]
+        self.nitems = len(setup.array("ITYPE"))
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise IbiscoError(rc, lib().ibg_last_error(self._h).decode())
+
+    def set_state(self, sxyz=None, vxyz=None, box=None):
+        s0, v0, b0 = self.setup.initial_state()
+        s = np.ascontiguousarray(s0 if sxyz is None else sxyz, np.float32)
+        v = np.ascontiguousarray(v0 if vxyz is None else vxyz, np.float32)
+        b = np.ascontiguousarray(b0 if box is None else box, np.float32)
+        self._check(lib().ibg_set_state(self._h, _fp(s), _fp(v), _fp(b)))
+
+    def step(self, step: int) -> dict:
+        o = IbgObs()
+        self._check(lib().ibg_step(self._h, int(step), ctypes.byref(o)))
+        return o.as_dict()
+
+    def forces(self, step: int) -> dict:
+        o = IbgObs()
+        self._check(lib().ibg_forces(self._h, int(step), ctypes.byref(o)))
+        return o.as_dict()
+
+    def run(self, first: int, nsteps: int, observe: bool = False):
+        if observe:
+            arr = (IbgObs * max(nsteps, 1))()
+            self._check(lib().ibg_run(self._h, int(first), int(nsteps), arr))
+            return [arr[k].as_dict() for k in range(nsteps)]
+        self._check(lib().ibg_run(self._h, int(first), int(nsteps), None))
+        return None
+
+    def state(self) -> dict:
+        n, na = self.nitems, self.natoms
+        s = np.zeros((n, 3), np.float32); r = np.zeros((n, 3), np.float32)
+        f = np.zeros((n, 3), np.float32); v = np.zeros((na, 3), np.float32)
+        self._check(lib().ibg_get_state(self._h, _fp(s), _fp(r), _fp(v), _fp(f)))
+        return {"sxyz": s, "rxyz": r, "vxyz": v, "fxyz": f}
+
+    def state64(self) -> dict:
+        n, na = self.nitems, self.natoms
+        s = np.zeros((n, 3)); f = np.zeros((n, 3)); v = np.zeros((na, 3))
+        self._check(lib().ibg_get_state_f64(self._h, _dp(s), _dp(v), _dp(f)))
+        return {"sxyz": s, "vxyz": v, "fxyz": f}
+
+    def neighbour_list(self, which: int, maxnab: int = 1000):
+        n = len(self.setup.array("ATOM")) if which == 0 else len(self.setup.array("BEAD"))
+        lst = np.zeros((max(n, 1), maxnab), np.int32)
+        nn = np.zeros(max(n, 1), np.int32)
+        rc = lib().ibg_get_neighbour_list(self._h, which, _ip(lst), maxnab, _ip(nn))
+        if rc < 0:
+            self._check(rc)
+        return lst[:n], nn[:n]
+
+    def exclusions(self):
+        n = self.nitems
+        c = np.zeros(n, np.int32)
+        t = np.zeros(n * 20, np.int32)
+        self._check(lib().ibg_get_exclusions(self._h, _ip(c), _ip(t)))
+        return c, t
+
+    def timing(self) -> dict:
+        ms = (ctypes.c_double * 8)()
+        n = ctypes.c_longlong()
+        lib().ibg_get_timing(self._h, ms, 8, ctypes.byref(n))
+        return {"list_ms": ms[0], "nonbonded_ms": ms[1], "bonded_ms": ms[2], "integrate_ms": ms[3],
+                "other_ms": ms[4], "run_ms": ms[5], "nonbonded_launches": int(ms[6]), "launches": n.value}
+
+    def set_timing(self, on: bool):
+        self._check(lib().ibg_set_timing(self._h, 1 if on else 0))
+
+    def set_l2_flush(self, nbytes: int):
+        self._check(lib().ibg_set_l2_flush(self._h, int(nbytes)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ibg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()

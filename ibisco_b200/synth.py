@@ -1,0 +1,497 @@
+"""Seeded synthetic systems written in the reference's input formats.
+
+A system is a directory with the files the reference reads: ``control``
+(RDCONTROL.f90), ``interaction`` plus one two-column table file per entry
+(RDINTERACT.f90), ``coordinate`` (RDCOOR.f90) and, for hybrid systems,
+``virtual`` (RDVIRTUAL.f90), ``virtbonds`` (RDVIRTBONDS.f90) and
+``virtangles`` (RDVIRTANGLES.f90).  Units are the files' units: nm, ps,
+kJ/mol, degrees, kg/mol.
+
+``config1`` .. ``config4`` build the benchmark workloads (single-type LJ
+fluid, bead-spring melt, hybrid atom/CG melt, large CG melt); ``feature_mix``
+builds a small system that exercises every term the step supports
+(bonds, angles, torsions, out-of-planes, exclusions with non_bonded 4 and 5,
+explicit beads, centre and centre-of-mass virtual sites, virtbonds,
+virtangles, MTS, NPT).
+"""
+from __future__ import annotations
+
+import math
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+KB_KJ = 0.0083144626  # kJ/mol/K
+
+
+@dataclass
+class Tab:
+    fname: str
+    x: np.ndarray
+    v: np.ndarray
+
+
+@dataclass
+class SystemSpec:
+    control: dict
+    types: list                      # [(name, mass kg/mol, 'A'|'B')]
+    pos: np.ndarray                  # (N,3) nm, unwrapped
+    vel: np.ndarray                  # (N,3) nm/ps
+    itype: np.ndarray                # (N,) 1-based
+    bonds: list                      # adjacency lists, 1-based partners, <=4 each
+    molecules: list                  # [(name, count)] in particle order
+    box: tuple
+    bond_tabs: list = field(default_factory=list)     # [((a,b), Tab)]
+    angle_tabs: list = field(default_factory=list)    # [((a,b,c), Tab)]
+    torsion_tabs: list = field(default_factory=list)  # [((a,b,c,d), Tab)]
+    nb_tabs: list = field(default_factory=list)       # [((a,b), Tab)]
+    oop_tabs: list = field(default_factory=list)      # [((a,b,c,d), Tab)]
+    virtual: list = field(default_factory=list)       # [(vtype, [members 1-based], centre or 0)]
+    virtbonds: list = field(default_factory=list)     # [(i, j)] global 1-based
+    virtangles: list = field(default_factory=list)    # [(i, j, k, t)]
+
+
+CONTROL_ORDER = [
+    "ensemble", "temperature", "pressure", "atoms", "num_of_time_steps", "time_step",
+    "temperature_coupling_time", "pressure_coupling_time", "isothermal_compressibility",
+    "virtual_sites", "mts", "bead_cutoff", "bead_neighbour_list_cutoff", "non_bonded_bead",
+    "cutoff", "neighbour_list_cutoff", "update_neighbour_list", "trajectory", "halt_drift",
+    "non_bonded", "initialize_velocities",
+]
+
+
+def _fmt(x) -> str:
+    return repr(float(np.float32(x)))
+
+
+def write_system(spec: SystemSpec, directory: str) -> str:
+    os.makedirs(directory, exist_ok=True)
+    c = dict(spec.control)
+    with open(os.path.join(directory, "control"), "w") as f:
+        for k in CONTROL_ORDER:
+            if k in c:
+                f.write(f"{k:<27}{c[k]}\n")
+        f.write("end\n")
+    written = set()
+
+    def table(t: Tab):
+        if t.fname in written:
+            return
+        written.add(t.fname)
+        with open(os.path.join(directory, t.fname), "w") as f:
+            for a, b in zip(t.x, t.v):
+                f.write(f"{a:.9e}  {b:.9e}\n")
+
+    with open(os.path.join(directory, "interaction"), "w") as f:
+        f.write(f"atom_types {len(spec.types)}\n# type label mass A/B\n")
+        for i, (name, mass, lab) in enumerate(spec.types, 1):
+            f.write(f"  {i}  {name}  {mass:.8g}  {lab}\n")
+        for key, tabs in (("bond_types", spec.bond_tabs), ("angle_types", spec.angle_tabs),
+                          ("torsion_types", spec.torsion_tabs),
+                          ("non_bonded_interaction_types", spec.nb_tabs), ("Out_of_Planes", spec.oop_tabs)):
+            f.write(f"{key} {len(tabs)}\n# types file\n")
+            for types, t in tabs:
+                table(t)
+                f.write("  " + "  ".join(str(x) for x in types) + f"  {t.fname}\n")
+    n = spec.pos.shape[0]
+    lines = [" " + "*" * 70,
+             " ********** Time    0.0000000000000000       (ps)",
+             " ********** Box Length(X, Y, Z in nanometres)                **********",
+             "   " + "   ".join(_fmt(b) for b in spec.box),
+             " " + "*" * 70,
+             " ********** Record for each atom is in the form:-            **********",
+             " ********** Index Atom_Type No._of_bonds X Y Z (coords.in nm) *******",
+             " ********** Vx Vy Vz (in nm/ps) Indices_of_bonded_atoms         *******",
+             " " + "*" * 70,
+             f" num_of_molecules: {len(spec.molecules)}"]
+    i = 0
+    out = []
+    for m, (name, cnt) in enumerate(spec.molecules, 1):
+        out.append(f" {cnt} atoms_in_molecule_no. {m} {name}")
+        for _ in range(cnt):
+            b = spec.bonds[i]
+            lab = spec.types[spec.itype[i] - 1][2]
+            out.append(f" {i + 1} {spec.itype[i]} {len(b)} {_fmt(spec.pos[i, 0])} {_fmt(spec.pos[i, 1])} "
+                       f"{_fmt(spec.pos[i, 2])} {lab}")
+            out.append("   " + " ".join(_fmt(x) for x in spec.vel[i]) + "  " + " ".join(str(x) for x in b))
+            i += 1
+    assert i == n
+    with open(os.path.join(directory, "coordinate"), "w") as f:
+        f.write("\n".join(lines + out) + "\n")
+    if spec.virtual:
+        with open(os.path.join(directory, "virtual"), "w") as f:
+            f.write(" **********synthetic\n # Number of virtual sites:\n")
+            f.write(f" {len(spec.virtual)}\n Type of VS, Natoms in VS, Centre or 0 for COM\n Members\n")
+            for k, (vt, mem, ctr) in enumerate(spec.virtual, 1):
+                f.write(f" {k} {vt} {len(mem)} {ctr}\n " + " ".join(str(x) for x in mem) + "\n")
+    if spec.virtbonds:
+        with open(os.path.join(directory, "virtbonds"), "w") as f:
+            for a, b in spec.virtbonds:
+                f.write(f"{a} {b}\n")
+    if spec.virtangles:
+        with open(os.path.join(directory, "virtangles"), "w") as f:
+            for a, b, cc, t in spec.virtangles:
+                f.write(f"{a} {b} {cc} {t}\n")
+    return directory
+
+
+# ------------------------------------------------------------------ tables
+def lj_table(fname, sigma, eps, rmax, dr, vcap=1.0e20):
+    n = int(round(rmax / dr)) + 1
+    r = np.arange(n) * dr
+    with np.errstate(divide="ignore", over="ignore"):
+        sr6 = (sigma / np.where(r > 0, r, 1.0)) ** 6
+        v = 4.0 * eps * (sr6 * sr6 - sr6)
+    v[0] = v[1]
+    v = np.minimum(v, vcap)
+    return Tab(fname, r, v)
+
+
+def perturbed_lj_table(fname, sigma, eps, rmax, dr, amps):
+    t = lj_table(fname, sigma, eps, rmax, dr)
+    r = t.x
+    add = sum(a * np.sin((k + 1) * np.pi * r / rmax) for k, a in enumerate(amps))
+    return Tab(fname, r, t.v + add)
+
+
+def harmonic_bond_table(fname, r0, k, rmax, dr):
+    n = int(round(rmax / dr)) + 1
+    r = np.arange(n) * dr
+    return Tab(fname, r, 0.5 * k * (r - r0) ** 2)
+
+
+def harmonic_angle_table(fname, theta0_deg, k, dtheta=0.18):
+    n = int(round(180.0 / dtheta)) + 1
+    th = np.arange(n) * dtheta
+    return Tab(fname, th, 0.5 * k * np.radians(th - theta0_deg) ** 2)
+
+
+def cosine_torsion_table(fname, k, mult=3, dphi=1.8):
+    n = int(round(360.0 / dphi)) + 1
+    ph = np.arange(n) * dphi
+    return Tab(fname, ph, k * (1.0 + np.cos(np.radians(mult * ph))))
+
+
+def oop_table(fname, k, dphi=1.8):
+    # signed out-of-plane angle, tabulated from -180 (first row, index 0 after the
+    # row-0 rule keeps it) to 180 degrees
+    n = int(round(360.0 / dphi)) + 1
+    ph = -180.0 + np.arange(n) * dphi
+    return Tab(fname, ph, 0.5 * k * np.radians(ph) ** 2)
+
+
+def maxwell_boltzmann(rng, masses_kg_mol, temp):
+    sd = np.sqrt(KB_KJ * temp / (np.asarray(masses_kg_mol) * 1000.0))  # nm/ps
+    v = rng.normal(size=(len(masses_kg_mol), 3)) * sd[:, None]
+    m = np.asarray(masses_kg_mol)[:, None]
+    v -= (m * v).sum(0) / m.sum()
+    return v
+
+
+# ----------------------------------------------------------- placements
+def random_fluid(rng, n, box, dmin):
+    """Uniform positions in [-L/2, L/2)^3 with rejection below dmin (cell grid)."""
+    L = float(box)
+    nc = max(1, int(L / dmin))
+    cs = L / nc
+    grid: dict = {}
+    pts = np.zeros((n, 3))
+    k = 0
+    tries = 0
+    while k < n:
+        p = (rng.random(3) - 0.5) * L
+        c = tuple(((p + L / 2) / cs).astype(int) % nc)
+        ok = True
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    for q in grid.get(((c[0] + dx) % nc, (c[1] + dy) % nc, (c[2] + dz) % nc), ()):
+                        d = p - pts[q]
+                        d -= L * np.round(d / L)
+                        if d @ d < dmin * dmin:
+                            ok = False
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+        tries += 1
+        if ok or tries > 200 * n:
+            grid.setdefault(c, []).append(k)
+            pts[k] = p
+            k += 1
+    return pts
+
+
+def random_walk_chains(rng, nchains, nper, box, bond, theta_deg, dmin, max_tries=100, max_restarts=50):
+    """Chains grown bead by bead with fixed bond length and bond angle and a
+    random dihedral.  A bead may not come closer than dmin to any earlier bead
+    except its two bonded predecessors; a chain that cannot continue is
+    restarted from a new random point."""
+    L = float(box)
+    nc = max(1, int(L / max(dmin, 1e-3)))
+    cs = L / nc
+    grid: dict = {}
+    n = nchains * nper
+    pts = np.zeros((n, 3))
+    th = math.radians(theta_deg)
+
+    def cell(p):
+        return tuple((((p + L / 2) % L) / cs).astype(int) % nc)
+
+    def clear(p, k, first):
+        c = cell(p)
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    for q in grid.get(((c[0] + dx) % nc, (c[1] + dy) % nc, (c[2] + dz) % nc), ()):
+                        if q >= k - 2 and q >= first:
+                            continue
+                        d = p - pts[q]
+                        d -= L * np.round(d / L)
+                        if d @ d < dmin * dmin:
+                            return False
+        return True
+
+    k = 0
+    for ch in range(nchains):
+        start = k
+        for restart in range(max_restarts + 1):
+            k = start
+            placed = []
+            ok_chain = True
+            for b in range(nper):
+                ok = False
+                for t in range(max_tries):
+                    if b == 0:
+                        p = (rng.random(3) - 0.5) * L
+                    elif b == 1:
+                        u = rng.normal(size=3)
+                        p = pts[k - 1] + bond * u / np.linalg.norm(u)
+                    else:
+                        a, bb = pts[k - 2], pts[k - 1]
+                        u = bb - a
+                        u /= np.linalg.norm(u)
+                        w = rng.normal(size=3)
+                        w -= (w @ u) * u
+                        w /= np.linalg.norm(w)
+                        p = bb + bond * (math.cos(math.pi - th) * u + math.sin(math.pi - th) * w)
+                    if clear(p, k, start):
+                        ok = True
+                        break
+                if not ok and restart < max_restarts:
+                    ok_chain = False
+                    break
+                pts[k] = p
+                c = cell(p)
+                grid.setdefault(c, []).append(k)
+                placed.append((c, k))
+                k += 1
+            if ok_chain:
+                break
+            for c, q in placed:  # undo the partial chain
+                grid[c].remove(q)
+    return pts
+
+
+def chain_bonds(nchains, nper, offset=0):
+    bonds = []
+    for ch in range(nchains):
+        base = offset + ch * nper
+        for b in range(nper):
+            nb = []
+            if b > 0:
+                nb.append(base + b)  # previous (1-based id of base+b-1 is base+b)
+            if b < nper - 1:
+                nb.append(base + b + 2)
+            bonds.append(nb)
+    return bonds
+
+
+def _all_angle_keys(types):
+    keys = []
+    for b in types:
+        for a in types:
+            for c in types:
+                if a <= c:
+                    keys.append((a, b, c))
+    return keys
+
+
+def _all_torsion_keys(types):
+    keys, seen = [], set()
+    for a in types:
+        for b in types:
+            for c in types:
+                for d in types:
+                    k, r = (a, b, c, d), (d, c, b, a)
+                    if r in seen or k in seen:
+                        continue
+                    seen.add(k)
+                    keys.append(k)
+    return keys
+
+
+# ------------------------------------------------------------------ configs
+def config1(n=4000, rho=8.0, seed=1, nsteps=1000):
+    """Single-type LJ bead fluid."""
+    rng = np.random.default_rng(seed)
+    box = (n / rho) ** (1.0 / 3.0)
+    pos = random_fluid(rng, n, box, 0.3)
+    mass = 0.072
+    vel = maxwell_boltzmann(rng, [mass] * n, 300.0)
+    control = dict(ensemble="NVE", temperature=300, pressure=101.3, atoms=n, num_of_time_steps=nsteps,
+                   time_step=0.010, temperature_coupling_time="0.1D0", pressure_coupling_time="5.0D0",
+                   isothermal_compressibility="1.0D-6", virtual_sites=0, mts=0, bead_cutoff=1.2,
+                   bead_neighbour_list_cutoff=1.4, non_bonded_bead=4, cutoff=1.2, neighbour_list_cutoff=1.4,
+                   update_neighbour_list=10, trajectory=nsteps, halt_drift=nsteps + 1, non_bonded=4,
+                   initialize_velocities="N")
+    return SystemSpec(control=control, types=[("CG", mass, "A")], pos=pos, vel=vel, itype=np.ones(n, int),
+                      bonds=[[] for _ in range(n)], molecules=[("bead", 1)] * n, box=(box, box, box),
+                      nb_tabs=[((1, 1), lj_table("nb11", 0.47, 3.5, 1.2, 0.002))])
+
+
+def polymer_melt(nchains=400, nper=100, rho=20.0, ntypes=3, seed=2, nsteps=5000, temp=500.0, dt=0.001,
+                 rcut=1.0, rlist=1.2, nupdate=10, ensemble="NVT", mass=0.014, bond=0.153, theta0=112.0):
+    """Bead-spring melt with tabulated bond/angle/torsion."""
+    rng = np.random.default_rng(seed)
+    n = nchains * nper
+    box = (n / rho) ** (1.0 / 3.0)
+    pos = random_walk_chains(rng, nchains, nper, box, bond, theta0, 0.8 * 0.30)
+    itype = np.array([1 + (k % ntypes) for ch in range(nchains) for k in range(nper)])
+    vel = maxwell_boltzmann(rng, [mass] * n, temp)
+    types = list(range(1, ntypes + 1))
+    sig = {t: 0.30 + 0.10 * (t - 1) / max(1, ntypes - 1) for t in types}
+    bond_t = harmonic_bond_table("bond.tab", bond, 2.5e5, 0.3, 0.0003)
+    ang_t = harmonic_angle_table("ang.tab", theta0, 500.0)
+    tor_t = cosine_torsion_table("tors.tab", 5.0)
+    control = dict(ensemble=ensemble, temperature=temp, pressure=101.3, atoms=n, num_of_time_steps=nsteps,
+                   time_step=dt, temperature_coupling_time="0.1D0", pressure_coupling_time="5.0D0",
+                   isothermal_compressibility="1.0D-6", virtual_sites=0, mts=0, bead_cutoff=rcut,
+                   bead_neighbour_list_cutoff=rlist, non_bonded_bead=4, cutoff=rcut, neighbour_list_cutoff=rlist,
+                   update_neighbour_list=nupdate, trajectory=nsteps, halt_drift=nsteps + 1, non_bonded=4,
+                   initialize_velocities="N")
+    return SystemSpec(
+        control=control, types=[(f"C{t}", mass, "A") for t in types], pos=pos, vel=vel, itype=itype,
+        bonds=chain_bonds(nchains, nper), molecules=[("chain", nper)] * nchains, box=(box, box, box),
+        bond_tabs=[((a, b), bond_t) for a in types for b in types if a <= b],
+        angle_tabs=[(k, ang_t) for k in _all_angle_keys(types)],
+        torsion_tabs=[(k, tor_t) for k in _all_torsion_keys(types)],
+        nb_tabs=[((a, b), lj_table(f"nb{a}{b}", 0.5 * (sig[a] + sig[b]), 0.5, rcut, 0.002))
+                 for a in types for b in types if a <= b])
+
+
+def config2(**kw):
+    return polymer_melt(**kw)
+
+
+def config4(nchains=10000, nper=200, rho=8.0, seed=4, nsteps=2000):
+    """Large CG melt for the roofline study."""
+    spec = polymer_melt(nchains=nchains, nper=nper, rho=rho, ntypes=4, seed=seed, nsteps=nsteps, temp=300.0,
+                        dt=0.010, rcut=1.4, rlist=1.6, mass=0.072, bond=0.47, theta0=120.0)
+    types = [1, 2, 3, 4]
+    spec.bond_tabs = [((a, b), harmonic_bond_table("bond.tab", 0.47, 5.0e3, 0.9, 0.0009)) for a in types for b in types
+                      if a <= b]
+    spec.torsion_tabs = []
+    spec.nb_tabs = [((a, b), lj_table(f"nb{a}{b}", 0.45 + 0.01 * (a + b), 2.0, 1.4, 0.001)) for a in types for b in types
+                    if a <= b]
+    spec.control["non_bonded"] = 4
+    return spec
+
+
+def feature_mix(seed=7, nmol=6, ensemble="NVT", nmts=0, non_bonded=4, rho=60.0, temp=400.0):
+    """A small hybrid system exercising every supported term.
+
+    Each molecule is a backbone of atoms (label A) with a three-bonded branch
+    point per monomer (out-of-plane terms), two coarse-grained beads (label B)
+    bonded to the backbone, one virtual site per monomer placed on a centre
+    atom and one at a centre of mass; virtbonds exclude site-bead pairs and a
+    virtangle couples a site to two beads.
+    """
+    rng = np.random.default_rng(seed)
+    types = [("C", 0.012, "A"), ("H", 0.001008, "A"), ("N", 0.014, "A"), ("B1", 0.043, "B"),
+             ("B2", 0.040, "B"), ("V1", 0.05, "B"), ("V2", 0.05, "B")]
+    # monomer: C(1)-N(3)(-H)(-C) backbone: atoms C N H C ; beads B1 B2 per molecule end
+    mono = [1, 3, 2, 1]
+    nmono = 4
+    pos, itype, bonds, mols, virt, vb, va = [], [], [], [], [], [], []
+    box = 3.2
+    for m in range(nmol):
+        start = len(itype)
+        origin = (rng.random(3) - 0.5) * box
+        ids = []
+        for k in range(nmono):
+            for a, t in enumerate(mono):
+                ids.append(len(itype) + 1)
+                itype.append(t)
+                bonds.append([])
+        # backbone bonds C-N-C-...; H on N; second C bonded to N
+        for k in range(nmono):
+            c1, n1, h1, c2 = [start + 4 * k + j + 1 for j in range(4)]
+            for a, b in ((c1, n1), (n1, h1), (n1, c2)):
+                bonds[a - 1].append(b)
+                bonds[b - 1].append(a)
+            if k + 1 < nmono:
+                nxt = start + 4 * (k + 1) + 1
+                bonds[c2 - 1].append(nxt)
+                bonds[nxt - 1].append(c2)
+        # two CG beads bonded to the first and last backbone atom
+        b1 = len(itype) + 1
+        itype.append(4); bonds.append([])
+        b2 = len(itype) + 1
+        itype.append(5); bonds.append([])
+        for a, b in ((start + 1, b1), (start + 4 * nmono, b2)):
+            bonds[a - 1].append(b)
+            bonds[b - 1].append(a)
+        # geometry: a zig-zag backbone with small noise
+        nat = len(itype) - start
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        for j in range(nat):
+            pos.append(origin + d * 0.11 * j + rng.normal(scale=0.035, size=3))
+        mols.append((f"mol{m + 1}", nat))
+        for k in range(nmono):
+            members = [start + 4 * k + j + 1 for j in range(4)]
+            virt.append((6, members, members[1]) if k % 2 == 0 else (7, members, 0))
+    natoms = len(itype)
+    # virtual sites are appended after all atoms; exclusions between a site and
+    # the beads of its molecule, and one virtangle per molecule
+    for m in range(nmol):
+        v0 = natoms + m * nmono + 1
+        bead_a = sum(c for _, c in mols[:m]) + 4 * nmono + 1
+        vb.append((v0, bead_a))
+        va.append((bead_a, v0, v0 + 1, 1))
+    pos = np.array(pos)
+    masses = [types[t - 1][1] for t in itype]
+    vel = maxwell_boltzmann(rng, masses, temp)
+    at, bt = [1, 2, 3], [4, 5, 6, 7]
+    all_t = at + bt
+    bond_t = harmonic_bond_table("bond.tab", 0.11, 1.5e5, 0.6, 0.0003)
+    ang_t = harmonic_angle_table("ang.tab", 115.0, 300.0)
+    tor_t = cosine_torsion_table("tors.tab", 4.0)
+    oop_t = oop_table("oop.tab", 40.0)
+    bond_keys = sorted({tuple(sorted((itype[i], itype[j - 1]))) for i in range(natoms) for j in bonds[i]})
+    control = dict(ensemble=ensemble, temperature=temp, pressure=101.3, atoms=natoms, num_of_time_steps=100,
+                   time_step=0.0005, temperature_coupling_time="0.1D0", pressure_coupling_time="1.0D0",
+                   isothermal_compressibility="4.5D-5", virtual_sites=len(virt), mts=nmts, bead_cutoff=0.9,
+                   bead_neighbour_list_cutoff=1.0, non_bonded_bead=non_bonded, cutoff=0.7,
+                   neighbour_list_cutoff=0.8, update_neighbour_list=5, trajectory=100, halt_drift=7,
+                   non_bonded=non_bonded, initialize_velocities="N")
+    nb_tabs = []
+    for a in all_t:
+        for b in all_t:
+            if a <= b:
+                both_cg = a in bt and b in bt
+                rc = 0.9 if both_cg else 0.7
+                sig = 0.45 if both_cg else 0.25
+                nb_tabs.append(((a, b), perturbed_lj_table(f"nb{a}_{b}", sig, 0.8, rc + 0.1, 0.002,
+                                                           [0.1, -0.05, 0.02])))
+    return SystemSpec(
+        control=control, types=types, pos=pos, vel=vel, itype=np.array(itype), bonds=bonds, molecules=mols,
+        box=(box, box, box), bond_tabs=[(k, bond_t) for k in bond_keys],
+        angle_tabs=[(k, ang_t) for k in _all_angle_keys(all_t)],
+        torsion_tabs=[(k, tor_t) for k in _all_torsion_keys(at)],
+        nb_tabs=nb_tabs,
+        oop_tabs=[((3, 1, 2, 1), oop_t), ((3, 1, 1, 2), oop_t)],
+        virtual=virt, virtbonds=vb, virtangles=va)

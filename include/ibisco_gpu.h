@@ -1,0 +1,208 @@
+/*
+ * ibisco_gpu.h — C ABI of the B200 force-and-integrate step for Hybrid IBIsCO.
+ *
+ * The Fortran host keeps its input/setup phase (main.F90:107-237) and its
+ * observables/output (AVERAGE.f90, OUTPUT.F90, WRITETRJ.F90) and replaces the
+ * body of its MD loop (NEW_LOOP.F90:327-390, MTS_LOOP.f90:26-44) by calls into
+ * this library.  Every entry point is plain C: pointers, sizes and status
+ * codes; arrays are passed in the Fortran layout of the reference's MODULE VAR
+ * (module_var.F90), column-major with 1-based particle ids.
+ *
+ * Status codes: 0 on success, a negative IBG_E_* otherwise; the message of the
+ * last failure of a context is returned by ibg_last_error().
+ */
+#ifndef IBISCO_GPU_H
+#define IBISCO_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The first group mirrors the reference's fatal STOPs. */
+#define IBG_OK 0
+#define IBG_E_INVALID (-1)        /* bad argument or descriptor                          */
+#define IBG_E_LIST_OVERFLOW (-2)  /* NEW_NEIGHBOUR_WITHLIST.f90:72,113 'LIST TOO SMALL'  */
+#define IBG_E_TORSION_TABLE (-3)  /* TORSIONS.inc:105-109 entry not in torsion table     */
+#define IBG_E_OOP_RANGE (-4)      /* OUTOFPLANES.inc:214-252 angle outside its table     */
+#define IBG_E_FIXED_OVERFLOW (-5) /* a force left the 64-bit fixed-point range           */
+#define IBG_E_CELL_GRID (-6)      /* fewer than 3 cells per dimension (MAPS.f90 stencil) */
+#define IBG_E_CUDA (-7)           /* CUDA runtime failure                                */
+#define IBG_E_TIMEOUT (-8)        /* a bounded device wait ran out                       */
+#define IBG_E_TABLE_RANGE (-9)    /* nonbonded distance beyond its table                 */
+#define IBG_E_MISSING_TABLE (-10) /* a listed pair has no nonbonded table (INBONDT = 0)   */
+#define IBG_E_CAPACITY (-11)      /* device neighbour-list or cell storage exhausted     */
+#define IBG_E_IO (-12)            /* input file missing or malformed                     */
+#define IBG_E_MEMORY (-13)        /* device memory budget exceeded                       */
+
+/* Precision of the step. */
+#define IBG_PREC_FP32_FIXED 0 /* FP32 pair math, 64-bit fixed-point force sums, FP64 integration */
+#define IBG_PREC_FP64_PLAIN 1 /* everything in FP64, FP64 atomics (comparison path)             */
+
+/*
+ * Descriptor of one system after the reference's setup phase: UNIT, RDCONTROL,
+ * ALLOCATEVAR, RDINTERACT, RDCOOR, RDVIRTUAL, MAKE_LISTS, FTABLE, SETLIS,
+ * RDVIRTANGLES, BUILD_CONNECTIVITY and RDVIRTBONDS have run.  Field names are
+ * the reference's (module_var.F90).  ibg_create deep-copies everything; no
+ * pointer is retained after it returns.
+ */
+typedef struct ibg_desc {
+  /* counts */
+  int natoms, nvirta, nitems, ntype;
+  int numatoms, numbeads, ncoarse;
+  /* control (RDCONTROL.f90, ALLOCATEVAR.f90:42-46, main.F90:177-178) */
+  int ensemble;   /* 0 NVE, 1 NVT, 2 NPT                                 */
+  int nupdate;    /* update_neighbour_list                               */
+  int halt_drift; /* halt_drift                                          */
+  int nmts;       /* mts; 0 runs the NEW_LOOP body                       */
+  int ibrdescr;   /* 0 hybrid (virtual sites present), 1 otherwise       */
+  int maxnab;     /* list length at which the reference stops (1000)     */
+  float dt, fac, pfac, temp_in, pressure;
+  float mktemp, mktemp_atom, mktemp_bead;
+  float rcut_atom, rcutsq_atom, rlist_atom;
+  float rcut_bead, rcutsq_bead, rlist_bead;
+  /* particles */
+  const float* mass;       /* MASS(NTYPE)                 */
+  const float* invmass;    /* INVMASS(NTYPE)              */
+  const int* itype;        /* ITYPE(NITEMS)               */
+  const int* type_label;   /* TYPE_LABEL(NITEMS) 1 atom, 2 bead (3 is set for VS on the device) */
+  const int* atom;         /* ATOM(NUMATOMS)              */
+  const int* bead;         /* BEAD(NCOARSE)               */
+  /* topology (SETLIS.f90 output; ld = leading dimension of the 2-D arrays) */
+  const int* nbonds;       /* NBONDS(NITEMS)              */
+  const int* jbond;        /* JBOND(ld_bond, 4)           */
+  int ld_bond;
+  const int* nijk;         /* NIJK(NITEMS)                */
+  const int* jangleijk;    /* JANGLEIJK(ld_angle, 10)     */
+  const int* kangleijk;
+  int ld_angle;
+  const int* nijkl;        /* NIJKL(NITEMS)               */
+  const int* jtorijkl;     /* JTORIJKL(ld_torsion, 10)    */
+  const int* ktorijkl;
+  const int* ltorijkl;
+  int ld_torsion;
+  const int* noopijkl;     /* NOOPIJKL(NITEMS)            */
+  const int* joopijkl;     /* JOOPIJKL(ld_oop, 20)        */
+  const int* koopijkl;
+  const int* loopijkl;
+  int ld_oop;
+  /* exclusions (BUILD_CONNECTIVITY.f90, RDVIRTBONDS.f90) */
+  const int* connections;  /* CONNECTIONS(NITEMS)         */
+  const int* connected_to; /* CONNECTED_TO(ld_conn, 20)   */
+  int ld_conn;
+  /* type maps, dense, first index fastest */
+  const int* ibondt;  /* IBONDT(NTYPE,NTYPE)             */
+  const int* inbondt; /* INBONDT(NTYPE,NTYPE)            */
+  const int* iangt;   /* IANGT(NTYPE,NTYPE,NTYPE)        */
+  const int* itort;   /* ITORT(NTYPE,NTYPE,NTYPE,NTYPE)  */
+  const int* ioopt;   /* IOOPT(NTYPE,NTYPE,NTYPE,NTYPE)  */
+  const int* bond_type_label;    /* (NBTYPE) 1 atomistic, 2 CG, 3 mixed */
+  const int* angle_type_label;   /* (NATYPE)  */
+  const int* torsion_type_label; /* (NTTYPE)  */
+  const int* oop_type_label;     /* (NOTYPE)  */
+  /* tables after FTABLE.f90.  Bonded tables are X(NTYPES, 0:ld-1), type fastest;
+     the nonbonded tables are X(0:ld_nb-1, NNBTYPE), index fastest, as in the
+     reference (ld = MAXINPUT+1 there). */
+  int nbtype, natype, nttype, nnbtype, notype;
+  int ld_b, ld_a, ld_t, ld_nb, ld_o;
+  const int* ndatb;  const float* binb;  const float* rbond;     const float* bond_pot; const float* bond_force;
+  const int* ndatan; const float* bina;  const float* angle;     const float* bend_pot; const float* bend_force;
+  const int* ndatt;  const float* bint;  const float* angle_tor; const float* tor_pot;  const float* tor_force;
+  const int* ndatnb; const float* binnb; const float* rnbond;    const float* nbond_pot; const float* nbond_force;
+  const int* ndato;  const float* bino;  const float* angle_oop; const float* oop_pot;  const float* oop_force;
+  /* virtual sites (RDVIRTUAL.f90) */
+  int ld_vs, vs_maxatoms;
+  const int* vitype;          /* VITYPE(NVIRTA)                        */
+  const int* virt_center;     /* VIRT_CENTER(NVIRTA), 0 = centre of mass */
+  const int* virt_numatoms;   /* VIRT_NUMATOMS(NTYPE)                  */
+  const int* virt_atm_ind;    /* VIRT_ATM_IND(ld_vs, vs_maxatoms)      */
+  const float* virt_invmass;  /* VIRT_INVMASS(NTYPE)                   */
+  const float* virt_masscoeff;/* VIRT_MASSCOEFF(NTYPE,NTYPE)           */
+} ibg_desc;
+
+/* Per-step observables: what AVERAGE.f90, OUTPUT.F90 and WRITETRJ.F90 read. */
+typedef struct ibg_obs {
+  double ek[2];          /* EK(1) atoms, EK(2) beads                         */
+  double temp, temp_atom, temp_bead;
+  double v_nb[3], v_bond[3], v_angle[3], v_torsion[3], v_oop[3];
+  double pt[6];          /* PT11, PT22, PT33, PT12, PT13, PT23 (after /V)    */
+  double box[3];
+  long long bond_overext;/* BONDS.inc:21-28 warnings this step               */
+  long long cell_clamps; /* coordinates at +L/2 folded into the last cell    */
+  int step, status;
+} ibg_obs;
+
+typedef struct ibg_ctx ibg_ctx;
+typedef struct ibg_setup ibg_setup;
+
+/* ---------------------------------------------------------------- setup --
+ * Host-side setup from a directory of reference input files (control,
+ * interaction and its tables, coordinate, virtual, virtbonds, virtangles).
+ * Replaces main.F90:107-218 for hosts that are not the Fortran program; the
+ * descriptor it yields is what a Fortran host fills from MODULE VAR.
+ * initial_state receives SXYZ(3,NATOMS), VXYZ(3,NATOMS) (reduced units) and BOX.
+ */
+int ibg_setup_read(const char* dir, ibg_setup** out, char* err, int errlen);
+const ibg_desc* ibg_setup_desc(const ibg_setup* s);
+int ibg_setup_initial_state(const ibg_setup* s, float* sxyz, float* vxyz, float* box);
+/* Integer/float scalars of the control file not carried by the descriptor:
+   [0] num_of_time_steps [1] trajectory [2] initialize_velocities (1 = Y). */
+int ibg_setup_control(const ibg_setup* s, int* ivals, int n);
+/* Named array of the setup (e.g. "CONNECTED_TO", "BOND_FORCE"); returns its
+   length, or -1 when the name is unknown.  out may be NULL to query. */
+long ibg_setup_array_i(const ibg_setup* s, const char* name, int* out, long n);
+long ibg_setup_array_f(const ibg_setup* s, const char* name, float* out, long n);
+void ibg_setup_free(ibg_setup* s);
+
+/* --------------------------------------------------------------- device --
+ * ibg_create: copies the descriptor to the current CUDA device.
+ * ibg_set_state: positions SXYZ(3,NATOMS) (unwrapped), velocities
+ *   VXYZ(3,NATOMS), box(3); then runs the reference's pre-loop
+ *   initialisation (main.F90:150-234: virtual sites, SHIFT, initial
+ *   temperatures, cell maps, first Verlet lists).
+ * ibg_step: one loop body (NEW_LOOP.F90:327-384 or MTS_LOOP.f90:26-44) for
+ *   step number `step`; `out` (may be NULL) receives the observables.
+ * ibg_forces: the same body up to and including the force stage, without
+ *   MOVE/MOMENTUM/SCALEBP (for force parity checks).
+ * ibg_run: steps first..first+nsteps-1 with CUDA-graph replay; per_step (may
+ *   be NULL) receives nsteps observables.
+ * ibg_get_state: SXYZ/RXYZ/FXYZ (3,NITEMS) and VXYZ (3,NATOMS) as REAL*4;
+ *   any pointer may be NULL.  ibg_get_state_f64: the FP64 state.
+ * ibg_get_neighbour_list: LIST(maxnab,N) of list `which` (0 atoms, 1 beads)
+ *   in the reference's order, 1-based global ids, 0-terminated, and
+ *   NNEBS(INDEX_LIST(A)) for A=1..N; list or nnebs may be NULL.
+ * ibg_get_exclusions: CONNECTIONS(NITEMS) and CONNECTED_TO(NITEMS,20) as held
+ *   on the device.
+ */
+int ibg_create(const ibg_desc* d, int precision, ibg_ctx** out);
+int ibg_set_state(ibg_ctx* c, const float* sxyz, const float* vxyz, const float* box);
+int ibg_step(ibg_ctx* c, int step, ibg_obs* out);
+int ibg_forces(ibg_ctx* c, int step, ibg_obs* out);
+int ibg_run(ibg_ctx* c, int first_step, int nsteps, ibg_obs* per_step);
+int ibg_get_state(ibg_ctx* c, float* sxyz, float* rxyz, float* vxyz, float* fxyz);
+int ibg_get_state_f64(ibg_ctx* c, double* sxyz, double* vxyz, double* fxyz);
+int ibg_get_neighbour_list(ibg_ctx* c, int which, int* list, int maxnab, int* nnebs);
+int ibg_get_exclusions(ibg_ctx* c, int* connections, int* connected_to);
+/* Device-side timing with CUDA events on the context's stream.
+   stage_ms[5] = milliseconds of the last ibg_run/ibg_step call (always).
+   With timing on (ibg_set_timing(c,1): direct launches, no graph replay),
+   stage_ms[0..4] accumulate the time of the list build, nonbonded, bonded,
+   integration/reduction and remaining kernels since ibg_set_timing, and
+   stage_ms[6] counts the nonbonded launches.  launches = kernels enqueued by
+   this context so far. */
+int ibg_set_timing(ibg_ctx* c, int on);
+int ibg_get_timing(ibg_ctx* c, double* stage_ms, int nstage, long long* launches);
+/* Benchmark support: before every step of ibg_run write `bytes` of scratch
+   memory (evicting the L2 cache) and time only the steps (stage_ms[5]). */
+int ibg_set_l2_flush(ibg_ctx* c, long long bytes);
+/* Select the CUDA device of the calling thread for subsequent ibg_create. */
+int ibg_set_device(int device);
+const char* ibg_last_error(const ibg_ctx* c);
+void ibg_destroy(ibg_ctx* c);
+
+/* Library version string. */
+const char* ibg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IBISCO_GPU_H */

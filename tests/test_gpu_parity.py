@@ -1,0 +1,191 @@
+"""CUDA path against the oracle, through the C ABI.
+
+* neighbour lists: identical to the reference's, including order, for the
+  same REAL*4 state (NEW_NEIGHBOUR_WITHLIST.f90); exclusions identical;
+* forces and energies of the FP32/fixed-point path within 1e-5 relative
+  (max-norm over particles) of the oracle's FP64 engine on the same positions;
+* the FP64 path agrees with the oracle's FP64 engine to 1e-9;
+* short trajectories (NVT, NVE, NPT, MTS) track the FP64 oracle;
+* FP32/fixed-point results are bitwise reproducible run to run.
+"""
+import numpy as np
+import pytest
+
+from ibisco_b200 import native
+from oracle.oracle import Oracle
+
+from conftest import rel_maxnorm
+
+pytestmark = pytest.mark.gpu
+
+FORCE_TOL = 1e-5     # FP32/fixed vs FP64, max-norm relative
+ENERGY_TOL = 1e-5
+FP64_TOL = 1e-9      # FP64 path vs FP64 oracle
+
+SYSTEMS = ["fluid", "melt", "mix4", "mix5_mts", "mix_npt", "mix_nve"]
+
+
+def make(d, prec):
+    s = native.Setup(d)
+    g = native.System(s, prec)
+    g.set_state()
+    return s, g
+
+
+def oracle_init(d, prec):
+    o = Oracle(d)
+    o.init(prec)
+    return o
+
+
+@pytest.mark.parametrize("name", SYSTEMS)
+def test_neighbour_lists_match_reference_order(sysdir, name):
+    d = sysdir(name)
+    _, g = make(d, native.IBG_PREC_FP32_FIXED)
+    o = oracle_init(d, 0)
+    for which in (0, 1):
+        if which == 1 and o.info["NCOARSE"] == 0:
+            continue
+        lg, ng = g.neighbour_list(which)
+        lo, no = o.neighbour_list(which, 0)
+        np.testing.assert_array_equal(ng, no)
+        np.testing.assert_array_equal(lg, lo)
+
+
+@pytest.mark.parametrize("name", ["mix4", "mix5_mts"])
+def test_exclusions_on_device(sysdir, name):
+    d = sysdir(name)
+    s, g = make(d, native.IBG_PREC_FP32_FIXED)
+    c, t = g.exclusions()
+    np.testing.assert_array_equal(c, s.array("CONNECTIONS"))
+    np.testing.assert_array_equal(t, s.array("CONNECTED_TO"))
+
+
+def energies(obs):
+    keys = [k for k in obs if k.startswith(("V_NB", "V_BOND", "V_ANGLE", "V_TORSION", "V_OOP"))]
+    return np.array([obs[k] for k in sorted(keys)])
+
+
+@pytest.mark.parametrize("name", SYSTEMS)
+def test_forces_fp32_fixed_against_fp64_oracle(sysdir, name):
+    d = sysdir(name)
+    _, g = make(d, native.IBG_PREC_FP32_FIXED)
+    o = oracle_init(d, 1)
+    og = g.forces(1)
+    o.forces(1, 1)
+    fo = o.state(1)["fxyz"]
+    fg = g.state64()["fxyz"]
+    assert rel_maxnorm(fg, fo) < FORCE_TOL
+    eo = o.obs(1)
+    e_gpu, e_orc = energies(og), energies(eo)
+    scale = max(np.abs(e_orc).max(), 1.0)
+    assert np.abs(e_gpu - e_orc).max() / scale < ENERGY_TOL
+    pt_g = np.array([og[k] for k in ("PT11", "PT22", "PT33", "PT12", "PT13", "PT23")])
+    pt_o = np.array([eo[k] for k in ("PT11", "PT22", "PT33", "PT12", "PT13", "PT23")])
+    assert np.abs(pt_g - pt_o).max() / max(np.abs(pt_o).max(), 1.0) < ENERGY_TOL
+
+
+@pytest.mark.parametrize("name", SYSTEMS)
+def test_forces_fp64_path_against_fp64_oracle(sysdir, name):
+    d = sysdir(name)
+    _, g = make(d, native.IBG_PREC_FP64_PLAIN)
+    o = oracle_init(d, 1)
+    og = g.forces(1)
+    o.forces(1, 1)
+    assert rel_maxnorm(g.state64()["fxyz"], o.state(1)["fxyz"]) < FP64_TOL
+    e_gpu, e_orc = energies(og), energies(o.obs(1))
+    assert np.abs(e_gpu - e_orc).max() / max(np.abs(e_orc).max(), 1.0) < FP64_TOL
+
+
+@pytest.mark.parametrize("name", SYSTEMS)
+def test_trajectory_against_fp64_oracle(sysdir, name):
+    """12 steps (two list rebuilds, MTS explicit and extrapolated steps, a
+    momentum removal and a barostat update where the system has them)."""
+    d = sysdir(name)
+    _, g = make(d, native.IBG_PREC_FP32_FIXED)
+    _, g64 = make(d, native.IBG_PREC_FP64_PLAIN)
+    o = oracle_init(d, 1)
+    nsteps = 12
+    obs = g.run(1, nsteps, observe=True)
+    obs64 = g64.run(1, nsteps, observe=True)
+    for st in range(1, nsteps + 1):
+        o.step(st, 1)
+    so = o.state(1)
+    s32, s64 = g.state64(), g64.state64()
+    na = so["vxyz"].shape[0]
+    span = np.abs(so["sxyz"][:na]).max()
+    assert np.abs(s64["sxyz"][:na] - so["sxyz"][:na]).max() / span < 1e-9
+    assert rel_maxnorm(s64["vxyz"], so["vxyz"]) < 1e-8
+    assert np.abs(s32["sxyz"][:na] - so["sxyz"][:na]).max() / span < 1e-6
+    assert rel_maxnorm(s32["vxyz"], so["vxyz"]) < 1e-4
+    eo = o.obs(1)
+    for k in ("TEMP", "BOX1"):
+        assert abs(obs64[-1][k] - eo[k]) <= 1e-9 * max(abs(eo[k]), 1.0)
+        assert abs(obs[-1][k] - eo[k]) <= 1e-5 * max(abs(eo[k]), 1.0)
+    assert [o_["STEP"] for o_ in obs] == list(range(1, nsteps + 1))
+
+
+def test_run_is_bitwise_reproducible(sysdir):
+    d = sysdir("melt")
+    _, a = make(d, native.IBG_PREC_FP32_FIXED)
+    _, b = make(d, native.IBG_PREC_FP32_FIXED)
+    a.run(1, 25)
+    b.run(1, 25)
+    sa, sb = a.state64(), b.state64()
+    assert np.array_equal(sa["sxyz"], sb["sxyz"])
+    assert np.array_equal(sa["vxyz"], sb["vxyz"])
+    assert np.array_equal(sa["fxyz"], sb["fxyz"])
+
+
+def test_step_and_run_agree(sysdir):
+    """Direct kernel launches (timing mode) and CUDA-graph replay give the same state."""
+    d = sysdir("mix5_mts")
+    _, a = make(d, native.IBG_PREC_FP32_FIXED)
+    _, b = make(d, native.IBG_PREC_FP32_FIXED)
+    native.lib().ibg_set_timing(a._h, 1)
+    for st in range(1, 11):
+        a.step(st)
+    b.run(1, 10)
+    assert np.array_equal(a.state64()["sxyz"], b.state64()["sxyz"])
+
+
+def test_lists_after_steps_match_reference(sysdir):
+    """After the system has moved, the lists built from the current REAL*4
+    state are again identical to the reference's."""
+    d = sysdir("fluid")
+    _, g = make(d, native.IBG_PREC_FP32_FIXED)
+    g.run(1, 15)
+    st = g.state()
+    _, v, b = native.Setup(d).initial_state()
+    box = np.array([g.step(16)["BOX1"]] * 3, np.float32)
+    st = g.state()
+    g.set_state(st["sxyz"][: g.natoms], st["vxyz"], box)
+    o = Oracle(d)
+    o.set_state(st["sxyz"][: g.natoms], st["vxyz"], box, 0)
+    lg, ng = g.neighbour_list(0)
+    lo, no = o.neighbour_list(0, 0)
+    np.testing.assert_array_equal(ng, no)
+    np.testing.assert_array_equal(lg, lo)
+
+
+def test_list_overflow_is_reported(sysdir):
+    """A neighbour count reaching MAXNAB is the reference's 'LIST TOO SMALL'
+    STOP (NEW_NEIGHBOUR_WITHLIST.f90:72); here it is a status code."""
+    s = native.Setup(sysdir("fluid"))
+    g = native.System(s, native.IBG_PREC_FP32_FIXED, maxnab=20)
+    with pytest.raises(native.IbiscoError) as e:
+        g.set_state()
+    assert e.value.code == -2
+
+
+def test_too_few_cells_is_reported(sysdir, tmp_path):
+    """MAPS.f90's 13-cell stencil needs 3 cells per dimension."""
+    import shutil
+    d = str(tmp_path / "coarse")
+    shutil.copytree(sysdir("fluid"), d)
+    ctl = open(d + "/control").read().replace("neighbour_list_cutoff      1.4", "neighbour_list_cutoff      2.9")
+    open(d + "/control", "w").write(ctl)
+    g = native.System(native.Setup(d), native.IBG_PREC_FP32_FIXED)
+    with pytest.raises(native.IbiscoError) as e:
+        g.set_state()
+    assert e.value.code == -6

@@ -1,0 +1,103 @@
+"""The product's host setup (ibg_setup_read) reproduces the reference's setup
+phase bit for bit: type maps, SETLIS angle/torsion/out-of-plane lists,
+exclusions (BUILD_CONNECTIVITY + RDVIRTBONDS), virtual-site maps (RDVIRTUAL)
+and the FTABLE force tables, checked against the oracle's restatement."""
+import numpy as np
+import pytest
+
+from ibisco_b200 import native
+from oracle.oracle import Oracle
+
+ONE_BASED = {"ITYPE", "NBONDS", "NIJK", "NOANGLEIJK", "NIJKL", "FNIJKL", "NOOPIJKL", "CONNECTIONS", "ATOM", "BEAD",
+             "VITYPE", "VIRT_CENTER", "VIRT_NUMATOMS", "NDATB", "NDATAN", "NDATT", "NDATNB", "NDATO", "MASS",
+             "INVMASS", "VIRT_INVMASS", "VIRT_MASS", "BINB", "BINA", "BINNB", "BINO", "BINT", "BOND_TYPE_LABEL",
+             "ANGLE_TYPE_LABEL", "TORSION_TYPE_LABEL", "OOP_TYPE_LABEL"}
+INT_ARRAYS = ["ITYPE", "NBONDS", "JBOND", "NIJK", "JANGLEIJK", "KANGLEIJK", "NOANGLEIJK", "NOJANGLEIJK",
+              "NOKANGLEIJK", "NIJKL", "JTORIJKL", "KTORIJKL", "LTORIJKL", "FNIJKL", "FJTORIJKL", "FKTORIJKL",
+              "FLTORIJKL", "NOOPIJKL", "JOOPIJKL", "KOOPIJKL", "LOOPIJKL", "CONNECTIONS", "CONNECTED_TO", "IBONDT",
+              "INBONDT", "IANGT", "ITORT", "IOOPT", "VITYPE", "VIRT_CENTER", "VIRT_NUMATOMS", "VIRT_ATM_IND",
+              "NDATB", "NDATAN", "NDATT", "NDATNB", "NDATO", "ATOM", "BEAD", "BOND_TYPE_LABEL",
+              "ANGLE_TYPE_LABEL", "TORSION_TYPE_LABEL", "OOP_TYPE_LABEL"]
+FLOAT_ARRAYS = ["MASS", "INVMASS", "VXYZ", "VIRT_INVMASS", "VIRT_MASSCOEFF", "BINB", "BINA", "BINNB", "BINO",
+                "BINT"]
+TABLES = [("NBTYPE", "NDATB", ["RBOND", "BOND_POT", "BOND_FORCE"], False),
+          ("NATYPE", "NDATAN", ["ANGLE", "BEND_POT", "BEND_FORCE"], False),
+          ("NTTYPE", "NDATT", ["ANGLE_TOR", "TOR_POT", "TOR_FORCE"], False),
+          ("NNBTYPE", "NDATNB", ["RNBOND", "NBOND_POT", "NBOND_FORCE"], False),
+          ("NOTYPE", "NDATO", ["ANGLE_OOP", "OOP_POT", "OOP_FORCE"], False)]
+
+
+def compare_setup(d):
+    o = Oracle(d)
+    s = native.Setup(d)
+    for name in INT_ARRAYS + FLOAT_ARRAYS:
+        a = o.array(name)
+        b = s.array(name)
+        if name in ONE_BASED:
+            a = a[1:]
+        n = min(len(a), len(b)) if name in ("VIRT_ATM_IND",) else None
+        if len(a) == 0 and len(b) <= 1:
+            continue
+        np.testing.assert_array_equal(a if n is None else a[:n], b if n is None else b[:n], err_msg=name)
+    sx = o.array("SXYZ")[: 3 * o.info["NATOMS"]]
+    np.testing.assert_array_equal(sx, s.array("SXYZ"))
+    # tables: the oracle keeps X(NT, 0:W-1), the product X(NT, 0:ld-1); rows
+    # 0..NDAT+1 (everything the step can read) must agree bit for bit
+    for count, ndat_name, names, _ in TABLES:
+        nt = o.info[count]
+        if nt == 0:
+            continue
+        nd = o.array(ndat_name)[1:]
+        for name in names:
+            a = o.array(name)
+            b = s.array(name)
+            wa = len(a) // nt
+            wb = len(b) // nt
+            for t in range(nt):
+                rows = nd[t] + 2
+                if name.startswith(("RNBOND", "NBOND")):
+                    # product keeps the reference's index-fastest nonbonded layout
+                    ra = a[t + nt * np.arange(rows)]
+                    rb = b[wb * t + np.arange(rows)]
+                else:
+                    ra = a[t + nt * np.arange(rows)]
+                    rb = b[t + nt * np.arange(rows)]
+                np.testing.assert_array_equal(ra, rb, err_msg=f"{name} table {t + 1}")
+
+
+@pytest.mark.parametrize("name", ["fluid", "melt", "mix4", "mix5_mts", "mix_npt"])
+def test_host_setup_matches_oracle(sysdir, name):
+    compare_setup(sysdir(name))
+
+
+@pytest.mark.parametrize("fixture", ["atomisticPA", "hybridPA"])
+def test_host_setup_matches_oracle_on_reference_fixtures(reftree, fixture):
+    compare_setup(reftree(fixture))
+
+
+def test_setup_reports_missing_keyword(tmp_path, sysdir):
+    import shutil
+    d = str(tmp_path / "bad")
+    shutil.copytree(sysdir("fluid"), d)
+    lines = [l for l in open(d + "/control").read().splitlines() if not l.startswith("mts")]
+    open(d + "/control", "w").write("\n".join(lines) + "\n")
+    with pytest.raises(native.IbiscoError) as e:
+        native.Setup(d)
+    assert e.value.code == -12 and "mts" in str(e.value)
+
+
+def test_setup_reports_missing_file(tmp_path):
+    with pytest.raises(native.IbiscoError) as e:
+        native.Setup(str(tmp_path / "nothing"))
+    assert e.value.code == -12
+
+
+def test_exclusions_rows_are_sorted_and_bounded(sysdir):
+    s = native.Setup(sysdir("mix5_mts"))
+    n = len(s.array("ITYPE"))
+    conn = s.array("CONNECTIONS")
+    to = s.array("CONNECTED_TO").reshape(20, n)
+    natoms = len(s.array("SXYZ")) // 3
+    for i in range(natoms):
+        row = to[: conn[i], i]
+        assert (conn[i] <= 20) and np.all(row[:-1] < row[1:]) if len(row) > 1 else True
