@@ -245,7 +245,7 @@ def run_b200(args, world, rank, local, pg):
         s0, v0, b0 = setup.initial_state()
         n = s0.shape[0]
         nitems = len(setup.array("ITYPE"))
-        dt_ps = float(open(os.path.join(d, "control")).read().split("time_step")[1].split()[0])
+        dt_ps = next(float(l.split()[1]) for l in open(os.path.join(d, "control")) if l.split()[0] == "time_step")
         prec = native.IBG_PREC_FP64_PLAIN if args.precision == "fp64" else native.IBG_PREC_FP32_FIXED
         g = native.System(setup, prec)
         g.set_state(s0, v0, b0)

@@ -400,33 +400,33 @@ def config4(nchains=10000, nper=200, rho=8.0, seed=4, nsteps=2000):
     return spec
 
 
-def feature_mix(seed=7, nmol=6, ensemble="NVT", nmts=0, non_bonded=4, rho=60.0, temp=400.0):
+def feature_mix(seed=7, nmol=6, ensemble="NVT", nmts=0, non_bonded=4, temp=400.0):
     """A small hybrid system exercising every supported term.
 
     Each molecule is a backbone of atoms (label A) with a three-bonded branch
-    point per monomer (out-of-plane terms), two coarse-grained beads (label B)
-    bonded to the backbone, one virtual site per monomer placed on a centre
-    atom and one at a centre of mass; virtbonds exclude site-bead pairs and a
-    virtangle couples a site to two beads.
+    point per monomer (out-of-plane terms) and two coarse-grained beads
+    (label B) bonded to its ends; every monomer carries one virtual site, on a
+    centre atom or at its centre of mass.  virtbonds exclude each bead from
+    its own molecule's sites and one virtangle couples a bead to two sites.
+    Molecules lie on separate lattice rows, so no two particles overlap.
     """
     rng = np.random.default_rng(seed)
     types = [("C", 0.012, "A"), ("H", 0.001008, "A"), ("N", 0.014, "A"), ("B1", 0.043, "B"),
              ("B2", 0.040, "B"), ("V1", 0.05, "B"), ("V2", 0.05, "B")]
-    # monomer: C(1)-N(3)(-H)(-C) backbone: atoms C N H C ; beads B1 B2 per molecule end
-    mono = [1, 3, 2, 1]
+    mono = [1, 3, 2, 1]  # C N H C; N carries H and the second C
     nmono = 4
-    pos, itype, bonds, mols, virt, vb, va = [], [], [], [], [], [], []
     box = 3.2
+    pos, itype, bonds, mols, virt, vb, va = [], [], [], [], [], [], []
+    slots = rng.permutation(25)[:nmol]
     for m in range(nmol):
         start = len(itype)
-        origin = (rng.random(3) - 0.5) * box
-        ids = []
+        iy, iz = divmod(int(slots[m]), 5)
+        y0, z0 = -1.4 + 0.6 * iy, -1.4 + 0.6 * iz
+        x0 = -1.0 + 0.4 * rng.random()
         for k in range(nmono):
-            for a, t in enumerate(mono):
-                ids.append(len(itype) + 1)
+            for t in mono:
                 itype.append(t)
                 bonds.append([])
-        # backbone bonds C-N-C-...; H on N; second C bonded to N
         for k in range(nmono):
             c1, n1, h1, c2 = [start + 4 * k + j + 1 for j in range(4)]
             for a, b in ((c1, n1), (n1, h1), (n1, c2)):
@@ -436,32 +436,43 @@ def feature_mix(seed=7, nmol=6, ensemble="NVT", nmts=0, non_bonded=4, rho=60.0, 
                 nxt = start + 4 * (k + 1) + 1
                 bonds[c2 - 1].append(nxt)
                 bonds[nxt - 1].append(c2)
-        # two CG beads bonded to the first and last backbone atom
-        b1 = len(itype) + 1
-        itype.append(4); bonds.append([])
-        b2 = len(itype) + 1
-        itype.append(5); bonds.append([])
-        for a, b in ((start + 1, b1), (start + 4 * nmono, b2)):
+        # planar zig-zag backbone c1-n1-c2-c1'... (bond 0.11 nm, angle 115 deg);
+        # H on N along the bisector, beads continuing the zig-zag at both ends
+        nat = 4 * nmono
+        dx, dy = 0.11 * math.sin(math.radians(57.5)), 0.5 * 0.11 * math.cos(math.radians(57.5))
+        xyz = [None] * (nat + 2)
+        for k in range(nmono):
+            for q, slot in enumerate((0, 1, 3)):  # c1, n1, c2 are backbone sites 3k, 3k+1, 3k+2
+                bidx = 3 * k + q
+                sgn = 1.0 if bidx % 2 == 0 else -1.0
+                xyz[4 * k + slot] = np.array([x0 + dx * bidx, y0 + sgn * dy, z0])
+            n_ = xyz[4 * k + 1]
+            sgn = 1.0 if (3 * k + 1) % 2 == 0 else -1.0
+            xyz[4 * k + 2] = n_ + np.array([0.0, sgn * 0.11, 0.0])
+        xyz[nat] = np.array([x0 - dx, y0 - dy, z0])
+        last = 3 * nmono - 1
+        xyz[nat + 1] = np.array([x0 + dx * (last + 1), y0 + (dy if (last + 1) % 2 == 0 else -dy), z0])
+        for p_ in xyz:
+            pos.append(p_ + rng.normal(scale=0.008, size=3))
+        b1, b2 = len(itype) + 1, len(itype) + 2
+        itype += [4, 5]
+        bonds += [[], []]
+        for a, b in ((start + 1, b1), (start + 4 * (nmono - 1) + 4, b2)):
             bonds[a - 1].append(b)
             bonds[b - 1].append(a)
-        # geometry: a zig-zag backbone with small noise
-        nat = len(itype) - start
-        d = rng.normal(size=3)
-        d /= np.linalg.norm(d)
-        for j in range(nat):
-            pos.append(origin + d * 0.11 * j + rng.normal(scale=0.035, size=3))
-        mols.append((f"mol{m + 1}", nat))
+        mols.append((f"mol{m + 1}", nat + 2))
         for k in range(nmono):
             members = [start + 4 * k + j + 1 for j in range(4)]
             virt.append((6, members, members[1]) if k % 2 == 0 else (7, members, 0))
     natoms = len(itype)
-    # virtual sites are appended after all atoms; exclusions between a site and
-    # the beads of its molecule, and one virtangle per molecule
     for m in range(nmol):
-        v0 = natoms + m * nmono + 1
-        bead_a = sum(c for _, c in mols[:m]) + 4 * nmono + 1
-        vb.append((v0, bead_a))
-        va.append((bead_a, v0, v0 + 1, 1))
+        first = sum(c for _, c in mols[:m])
+        beads = (first + 4 * nmono + 1, first + 4 * nmono + 2)
+        sites = [natoms + m * nmono + k + 1 for k in range(nmono)]
+        for bd in beads:
+            for v in sites:
+                vb.append((bd, v))
+        va.append((beads[0], sites[0], sites[1], 1))
     pos = np.array(pos)
     masses = [types[t - 1][1] for t in itype]
     vel = maxwell_boltzmann(rng, masses, temp)
@@ -484,7 +495,7 @@ def feature_mix(seed=7, nmol=6, ensemble="NVT", nmts=0, non_bonded=4, rho=60.0, 
             if a <= b:
                 both_cg = a in bt and b in bt
                 rc = 0.9 if both_cg else 0.7
-                sig = 0.45 if both_cg else 0.25
+                sig = 0.35 if both_cg else 0.25
                 nb_tabs.append(((a, b), perturbed_lj_table(f"nb{a}_{b}", sig, 0.8, rc + 0.1, 0.002,
                                                            [0.1, -0.05, 0.02])))
     return SystemSpec(
