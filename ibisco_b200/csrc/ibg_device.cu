@@ -70,6 +70,7 @@ enum Variant : unsigned {
 
 struct DevList {
   int n = 0, which = 0, present = 0;
+  int T = 1;  // lanes per particle in the list build and the nonbonded kernel (1, 2, 4 or 8)
   int cell_cap = 0, nslices = 0;
   long long cap_entries = 0;
   int *idx = nullptr, *cell_of = nullptr, *cell_count = nullptr, *cell_start = nullptr, *cell_fill = nullptr;
@@ -148,6 +149,7 @@ int fail(ibg_ctx* c, int code, const std::string& m) {
 
 int status_from_bits(unsigned b) {
   if (!b) return IBG_OK;
+  if (b & EB_CELL_GRID) return IBG_E_CELL_GRID;  // a bad grid also overflows the lists
   if (b & EB_LIST_OVERFLOW) return IBG_E_LIST_OVERFLOW;
   if (b & EB_TORSION) return IBG_E_TORSION_TABLE;
   if (b & EB_OOP) return IBG_E_OOP_RANGE;
@@ -159,6 +161,7 @@ int status_from_bits(unsigned b) {
   return IBG_E_INVALID;
 }
 const char* bits_message(unsigned b) {
+  if (b & EB_CELL_GRID) return "fewer than 3 cells per dimension for the neighbour list";
   if (b & EB_LIST_OVERFLOW) return "LIST TOO SMALL: a particle reached MAXNAB neighbours";
   if (b & EB_TORSION) return "FATAL ERROR: Entry in torsion table does not exist";
   if (b & EB_OOP) return "out of plane angle outside its table";
@@ -187,7 +190,10 @@ void build_list(ibg_ctx* c, const ibg_desc* d, int which) {
   L.rlist = which == 0 ? d->rlist_atom : d->rlist_bead;
   L.rlistsq = L.rlist * L.rlist;  // RLISTSQ = RLIST*RLIST (NEW_NEIGHBOUR_WITHLIST.f90:26)
   L.rcutsq = which == 0 ? d->rcutsq_atom : d->rcutsq_bead;
-  L.nslices = (L.n + 31) / 32;
+  // lanes per particle: enough warps to fill the GPU (about 32 per SM)
+  L.T = 1;
+  while (L.T < 8 && (long long)L.n * L.T < 32LL * 32 * c->nsm) L.T *= 2;
+  L.nslices = (L.n + 32 / L.T - 1) / (32 / L.T);
   auto& o = c->owned;
   L.idx = dupload(idx, o);
   L.cell_of = dalloc<int>(L.n, o);
@@ -314,7 +320,7 @@ void collect_marks(ibg_ctx* c) {
 template <typename R>
 void enq_positions(ibg_ctx* c) {
   PosArgs a;
-  a.natoms = c->natoms; a.nvirta = c->nvirta; a.S = c->S; a.su = c->su; a.Svs = c->S + 3 * (size_t)c->natoms;
+  a.natoms = c->natoms; a.nvirta = c->nvirta; a.S = c->S; a.Svs = c->S + 3 * (size_t)c->natoms;
   a.tbits = c->tbits; a.gslot = c->gslot;
   a.pos4[0] = c->L[0].pos4; a.pos4[1] = c->L[1].pos4;
   a.vcenter = c->vcenter; a.vnum = c->vnum; a.vmem = c->vmem; a.vmass = c->vmass; a.vinv = c->vinv;
@@ -337,10 +343,51 @@ void enq_rebuild(ibg_ctx* c, DevList& L) {
   CK(cudaMemcpyAsync(L.slot_of, L.slot_of_new, sizeof(int) * L.n, cudaMemcpyDeviceToDevice, c->st));
   CK(cudaMemcpyAsync(L.sorted, L.sorted_new, sizeof(int) * L.n, cudaMemcpyDeviceToDevice, c->st));
   const int gl = grid_for(c, (long long)L.nslices * 32, 16);
-  k_list_build<R, false><<<gl, 256, 0, c->st>>>(a, c->sc);
+  switch (L.T) {
+    case 1: k_list_build<R, false, 1><<<gl, 256, 0, c->st>>>(a, c->sc); break;
+    case 2: k_list_build<R, false, 2><<<gl, 256, 0, c->st>>>(a, c->sc); break;
+    case 4: k_list_build<R, false, 4><<<gl, 256, 0, c->st>>>(a, c->sc); break;
+    default: k_list_build<R, false, 8><<<gl, 256, 0, c->st>>>(a, c->sc); break;
+  }
   k_scan_slices<<<1, 1024, 0, c->st>>>(L.slice_w, L.slice_off, L.nslices);
-  k_list_build<R, true><<<gl, 256, 0, c->st>>>(a, c->sc);
+  switch (L.T) {
+    case 1: k_list_build<R, true, 1><<<gl, 256, 0, c->st>>>(a, c->sc); break;
+    case 2: k_list_build<R, true, 2><<<gl, 256, 0, c->st>>>(a, c->sc); break;
+    case 4: k_list_build<R, true, 4><<<gl, 256, 0, c->st>>>(a, c->sc); break;
+    default: k_list_build<R, true, 8><<<gl, 256, 0, c->st>>>(a, c->sc); break;
+  }
   c->launches += 9;
+}
+
+template <typename R>
+using NBKernel = void (*)(NBArgs<R>, Scalars*);
+
+template <typename R>
+NBKernel<R> nb_kernel(bool smem, int T) {
+  if (smem) {
+    switch (T) {
+      case 1: return k_nonbonded<R, true, 1>;
+      case 2: return k_nonbonded<R, true, 2>;
+      case 4: return k_nonbonded<R, true, 4>;
+      default: return k_nonbonded<R, true, 8>;
+    }
+  }
+  switch (T) {
+    case 1: return k_nonbonded<R, false, 1>;
+    case 2: return k_nonbonded<R, false, 2>;
+    case 4: return k_nonbonded<R, false, 4>;
+    default: return k_nonbonded<R, false, 8>;
+  }
+}
+
+template <typename R>
+void nb_configure(ibg_ctx* c, DevList& L) {
+  NBKernel<R> k = nb_kernel<R>(L.use_smem, L.T);
+  if (L.use_smem) CK(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
+  int per = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k, 256, L.use_smem ? L.smem : 9 * 64));
+  per = std::max(1, per);
+  L.grid_nb = std::max(1, std::min(c->nsm * per, (L.nslices + 7) / 8));
 }
 
 template <typename R>
@@ -353,8 +400,8 @@ void enq_nonbonded(ibg_ctx* c, DevList& L) {
   A.ltab = L.ltab; A.toff = L.toff; A.tndat = L.tndat; A.tbin = (const R*)L.tbin; A.tfp = (const R*)L.tfp; A.tx = (const R*)L.tx;
   A.ntab = L.ntab; A.nrows = L.nrows; A.rcutsq = (R)L.rcutsq;
   A.part = L.part; A.part_stride = L.grid_nb;
-  if (L.use_smem) k_nonbonded<R, true><<<L.grid_nb, 256, L.smem, c->st>>>(A, c->sc);
-  else k_nonbonded<R, false><<<L.grid_nb, 256, 9 * 8 * sizeof(double), c->st>>>(A, c->sc);
+  const size_t sm = L.use_smem ? L.smem : 9 * 8 * sizeof(double);
+  nb_kernel<R>(L.use_smem, L.T)<<<L.grid_nb, 256, sm, c->st>>>(A, c->sc);
   ++c->launches;
 }
 
@@ -379,7 +426,7 @@ void enq_distribute(ibg_ctx* c, void* F) {
 template <typename R>
 void enq_bonded(ibg_ctx* c) {
   BondedArgs<R> B;
-  B.su = (const R*)c->su; B.fb = (typename Prec<R>::acc_t*)c->fb;
+  B.su = c->S; B.fb = (typename Prec<R>::acc_t*)c->fb;
   B.nb = c->nb; B.na = c->na; B.nt = c->nt; B.no = c->no;
   B.bonds = c->bonds; B.angles = c->angles; B.tors = c->tors; B.tors_t = c->tors_t; B.oops = c->oops; B.oops_t = c->oops_t;
   B.tb = c->tb; B.tb_off = c->tb_off; B.tb_ndat = c->tb_nd; B.tb_bin = c->tb_bin;
@@ -620,8 +667,7 @@ int ibg_create(const ibg_desc* d, int precision, ibg_ctx** out) {
     c->invmass = dupload(inv, o);
     c->S = dalloc<double>(3 * (size_t)N, o);
     c->V = dalloc<double>(3 * (size_t)NA, o);
-    if (precision == IBG_PREC_FP32_FIXED) c->su = dalloc<float>(3 * (size_t)N, o);
-    else c->su = c->S;
+    c->su = c->S;
     c->fnb = dalloc<unsigned char>(accsize(c.get()) * 3 * N, o);
     c->fb = dalloc<unsigned char>(accsize(c.get()) * 3 * N, o);
     // exclusions
@@ -743,22 +789,10 @@ int ibg_create(const ibg_desc* d, int precision, ibg_ctx** out) {
       c->gslot = dupload(gs, o);
     }
     // grids and partial sums
-    size_t smem_max = 0;
-    for (auto& L : c->L)
-      if (L.present && L.use_smem) smem_max = std::max(smem_max, L.smem);
-    if (smem_max) {
-      if (precision == IBG_PREC_FP32_FIXED) CK(cudaFuncSetAttribute(k_nonbonded<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
-      else CK(cudaFuncSetAttribute(k_nonbonded<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
-    }
     for (auto& L : c->L) {
       if (!L.present) continue;
-      int per = 0;
-      if (precision == IBG_PREC_FP32_FIXED)
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, L.use_smem ? (const void*)k_nonbonded<float, true> : (const void*)k_nonbonded<float, false>, 256, L.use_smem ? L.smem : 9 * 64));
-      else
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, L.use_smem ? (const void*)k_nonbonded<double, true> : (const void*)k_nonbonded<double, false>, 256, L.use_smem ? L.smem : 9 * 64));
-      per = std::max(1, per);
-      L.grid_nb = std::max(1, std::min(c->nsm * per, (L.nslices + 7) / 8));
+      if (precision == IBG_PREC_FP32_FIXED) nb_configure<float>(c.get(), L);
+      else nb_configure<double>(c.get(), L);
     }
     int gnb = std::max(c->L[0].present ? c->L[0].grid_nb : 0, c->L[1].present ? c->L[1].grid_nb : 0);
     for (auto& L : c->L)
@@ -1068,16 +1102,17 @@ int ibg_get_neighbour_list(ibg_ctx* c, int which, int* list, int maxnab, int* nn
     CK(cudaMemcpy(idx.data(), L.idx, sizeof(int) * L.n, cudaMemcpyDeviceToHost));
     std::vector<int> e((size_t)off[L.nslices]);
     if (!e.empty()) CK(cudaMemcpy(e.data(), L.entries, sizeof(int) * e.size(), cudaMemcpyDeviceToHost));
+    const int T = L.T, P = 32 / L.T;
     for (int s = 0; s < L.n; ++s) {
       const int a = sorted[s];
-      const int g = s >> 5, lane = s & 31;
+      const int g = s / P, lane0 = (s % P) * T;
       if (nnebs) nnebs[a] = counts[s];
       if (!list) continue;
       if (counts[s] >= maxnab) return fail(c, IBG_E_INVALID, "maxnab smaller than a list");
       int* col = list + (size_t)a * maxnab;
       for (int k = 0; k < maxnab; ++k) {
         if (k < counts[s]) {
-          int t = e[(size_t)off[g] + (size_t)k * 32 + lane];
+          int t = e[(size_t)off[g] + (size_t)(k / T) * 32 + lane0 + (k % T)];
           col[k] = idx[sorted[t]] + 1;
         } else {
           col[k] = 0;

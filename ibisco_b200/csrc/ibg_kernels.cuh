@@ -109,7 +109,6 @@ __device__ __forceinline__ void fold3(R* r, const R* b2) {
 struct PosArgs {
   int natoms, nvirta;
   const double* S;     // unwrapped positions (3,NITEMS), FP64 state
-  void* su;            // unwrapped positions in R for the bonded terms (3,NITEMS)
   double* Svs;         // VS rows of S (written for the FP64 path and output)
   const int* tbits;    // type | label<<16 per particle
   const int* gslot;    // slot*2 + list per particle
@@ -129,7 +128,6 @@ __global__ void k_positions(PosArgs a, Scalars* sc) {
   const int n = a.natoms + a.nvirta;
   R b[3], bi[3], b2[3];
   box_of<R>(sc, b, bi, b2);
-  R* su = (R*)a.su;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     R s[3];
     if (i < a.natoms) {
@@ -157,8 +155,6 @@ __global__ void k_positions(PosArgs a, Scalars* sc) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) a.Svs[3 * (size_t)v + c] = (double)s[c];
     }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) su[3 * (size_t)i + c] = s[c];
     R r[3] = {s[0], s[1], s[2]};
     fold3<R>(r, b2);
     int g = a.gslot[i];
@@ -300,24 +296,33 @@ __global__ void k_reslot(ListArgs L) {
   }
 }
 
-// NEW_NEIGHBOUR_WITHLIST.f90:34-123.  One thread per slot; a warp covers one
-// slice of 32 consecutive slots.  Candidates are visited in the reference's
-// order: the particle's own cell below it (decreasing A), then the 13 cells
-// of the MAPS.f90:137-149 stencil, each by decreasing A.  FILL=false counts
-// and records the slice width; FILL=true writes slot indices.
-template <typename R, bool FILL>
-__global__ void k_list_build(ListArgs L, Scalars* sc) {
+// NEW_NEIGHBOUR_WITHLIST.f90:34-123.  T lanes share one slot (particle); a
+// warp covers one slice of P = 32/T consecutive slots.  Candidates are
+// visited in the reference's order -- the particle's own cell below it
+// (decreasing A), then the 13 cells of the MAPS.f90:137-149 stencil, each by
+// decreasing A -- T at a time; a ballot over the slot's lanes keeps accepted
+// candidates in that order.  The distance test runs first and the exclusion
+// scan only for candidates inside RLIST (the accepted set is the same).
+// Entry k of slot s (slice g) is stored at off[g] + (k/T)*32 + (s%P)*T + k%T.
+// FILL=false counts and records the slice width in rows of 32; FILL=true
+// writes slot indices.
+template <typename R, bool FILL, int T>
+__global__ void __launch_bounds__(256) k_list_build(ListArgs L, Scalars* sc) {
   using PT = typename Prec<R>::pos_t;
+  constexpr int P = 32 / T;
   const int nx = sc->ncell[L.which][0], ny = sc->ncell[L.which][1], nz = sc->ncell[L.which][2];
   R b[3], bi[3], b2[3];
   box_of<R>(sc, b, bi, b2);
   const R rlsq = sizeof(R) == 4 ? (R)L.rlistsq : (R)L.rlistsqd;
   const PT* pos = (const PT*)L.pos4;
-  const int lane = threadIdx.x & 31;
-  const int nslices = (L.n + 31) >> 5;
+  const int lane = threadIdx.x & 31, grp = lane / T, q = lane % T;
+  const unsigned gmask = (T == 32 ? 0xffffffffu : (((1u << T) - 1u) << (grp * T)));
+  const int nslices = (L.n + P - 1) / P;
   const int warps = (gridDim.x * blockDim.x) >> 5;
+  const int off[13][3] = {{1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {-1, 1, 0}, {1, 0, -1}, {1, 1, -1}, {0, 1, -1},
+                          {-1, 1, -1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}, {-1, 1, 1}, {0, 0, 1}};
   for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < nslices; g += warps) {
-    const int s = g * 32 + lane;
+    const int s = g * P + grp;
     const bool valid = s < L.n;
     int cnt = 0;
     long long base = 0;
@@ -335,42 +340,51 @@ __global__ void k_list_build(ListArgs L, Scalars* sc) {
       const bool i_vs = L.hybrid && i >= L.natoms;
       const int c0 = L.cell_of[a];
       const int ix = c0 / (nz * ny), iy = (c0 / nz) % ny, iz = c0 % nz;
-      auto consider = [&](int t) {
-        const int j = L.idx[L.sorted[t]];
-        for (int e = 0; e < ne; ++e)
-          if (ex[e] == j) return;
-        if (i_vs && j >= L.natoms) return;
-        const PT pj = pos[t];
-        R d0 = pi.x - pj.x, d1 = pi.y - pj.y, d2 = pi.z - pj.z;
-        d0 = d0 - r_round(d0 * bi[0]) * b[0];
-        d1 = d1 - r_round(d1 * bi[1]) * b[1];
-        d2 = d2 - r_round(d2 * bi[2]) * b[2];
-        R r2 = d0 * d0;
-        r2 = r2 + d1 * d1;
-        r2 = r2 + d2 * d2;
-        if (r2 < rlsq) {
-          if (FILL) L.entries[base + (long long)cnt * 32 + lane] = t;
-          ++cnt;
+      // candidates t = hi, hi-1, ..., lo
+      auto segment = [&](int hi, int lo) {
+        for (int t0 = hi; t0 >= lo; t0 -= T) {
+          const int t = t0 - q;
+          bool ok = false;
+          if (t >= lo) {
+            const PT pj = pos[t];
+            R d0 = pi.x - pj.x, d1 = pi.y - pj.y, d2 = pi.z - pj.z;
+            d0 = d0 - r_round(d0 * bi[0]) * b[0];
+            d1 = d1 - r_round(d1 * bi[1]) * b[1];
+            d2 = d2 - r_round(d2 * bi[2]) * b[2];
+            R r2 = d0 * d0;
+            r2 = r2 + d1 * d1;
+            r2 = r2 + d2 * d2;
+            if (r2 < rlsq) {
+              const int j = L.idx[L.sorted[t]];
+              ok = !(i_vs && j >= L.natoms);
+              for (int e = 0; e < ne && ok; ++e)
+                if (ex[e] == j) ok = false;
+            }
+          }
+          const unsigned bits = (__ballot_sync(gmask, ok) >> (grp * T)) & (T == 32 ? 0xffffffffu : ((1u << T) - 1u));
+          if (FILL && ok) {
+            const int k = cnt + __popc(bits & ((1u << q) - 1u));
+            L.entries[base + (long long)(k / T) * 32 + grp * T + (k % T)] = t;
+          }
+          cnt += __popc(bits);
         }
       };
-      for (int t = s - 1; t >= L.cell_start[c0]; --t) consider(t);
-      const int off[13][3] = {{1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {-1, 1, 0}, {1, 0, -1}, {1, 1, -1}, {0, 1, -1},
-                              {-1, 1, -1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}, {-1, 1, 1}, {0, 0, 1}};
+      segment(s - 1, L.cell_start[c0]);
 #pragma unroll 1
-      for (int q = 0; q < 13; ++q) {
-        int jx = (ix + off[q][0] + nx) % nx, jy = (iy + off[q][1] + ny) % ny, jz = (iz + off[q][2] + nz) % nz;
-        int c = jx * nz * ny + jy * nz + jz;
-        for (int t = L.cell_start[c + 1] - 1; t >= L.cell_start[c]; --t) consider(t);
+      for (int u = 0; u < 13; ++u) {
+        const int jx = (ix + off[u][0] + nx) % nx, jy = (iy + off[u][1] + ny) % ny, jz = (iz + off[u][2] + nz) % nz;
+        const int c = jx * nz * ny + jy * nz + jz;
+        segment(L.cell_start[c + 1] - 1, L.cell_start[c]);
       }
-      if (!FILL) {
+      if (!FILL && q == 0) {
         L.counts[s] = cnt;
         if (cnt >= L.maxnab) atomicOr(&sc->err, EB_LIST_OVERFLOW);
       }
     }
     if (FILL && !room && lane == 0) atomicOr(&sc->err, EB_CAPACITY);
     if (!FILL) {
-      int w = __reduce_max_sync(0xffffffffu, valid ? cnt : 0);
-      if (lane == 0) L.slice_w[g] = w;
+      const int w = __reduce_max_sync(0xffffffffu, valid ? cnt : 0);
+      if (lane == 0) L.slice_w[g] = (w + T - 1) / T;
     }
   }
 }
@@ -420,16 +434,18 @@ struct NBArgs {
   int part_stride;
 };
 
-// NONBONDED_FORCE.F90:173-232.  Persistent grid; each warp owns one slice of
-// 32 consecutive slots at a time and walks the 32 lists in lock step; list
-// reads are coalesced (sliced-ELL), neighbour positions are float4 gathers
-// from the cell-ordered array.  i-forces stay in registers, j-forces are
-// 64-bit integer atomics.  Tables are staged in shared memory when SMEM.
-template <typename R, bool SMEM>
+// NONBONDED_FORCE.F90:173-232.  Persistent grid; a warp owns one slice of
+// P = 32/T slots at a time and T lanes walk each slot's list; list reads are
+// coalesced 128-byte rows, neighbour positions are float4 gathers from the
+// cell-ordered array.  i-forces are summed in registers and reduced exactly
+// over the slot's lanes (integer shuffles); j-forces are 64-bit integer
+// atomics.  Tables are staged in shared memory when SMEM.
+template <typename R, bool SMEM, int T>
 __global__ void __launch_bounds__(256) k_nonbonded(NBArgs<R> A, Scalars* sc) {
   using P = Prec<R>;
   using PT = typename P::pos_t;
   using reg_t = typename P::reg_t;
+  constexpr int PS = 32 / T;
   extern __shared__ unsigned char smem_raw[];
   const int* ltab = A.ltab;
   const int* toff = A.toff;
@@ -457,14 +473,14 @@ __global__ void __launch_bounds__(256) k_nonbonded(NBArgs<R> A, Scalars* sc) {
   R b[3], bi[3], b2[3];
   box_of<R>(sc, b, bi, b2);
   const PT* pos = (const PT*)A.pos4;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, grp = lane / T, q = lane % T;
   const int warps = (gridDim.x * blockDim.x) >> 5;
   double acc[9];
 #pragma unroll
   for (int k = 0; k < 9; ++k) acc[k] = 0.0;
   unsigned err = 0;
   for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < A.nslices; g += warps) {
-    const int s = g * 32 + lane;
+    const int s = g * PS + grp;
     const bool valid = s < A.n;
     const int cnt = valid ? A.counts[s] : 0;
     int w = A.slice_w[g];
@@ -479,9 +495,9 @@ __global__ void __launch_bounds__(256) k_nonbonded(NBArgs<R> A, Scalars* sc) {
     const int wi = P::bits(pi.w);
     const int ti = wi & 0xffff, li = wi >> 16;
     reg_t fi0 = 0, fi1 = 0, fi2 = 0;
-    for (int k = 0; k < w; ++k) {
-      if (k >= cnt) continue;
-      const int t = A.entries[base + (long long)k * 32 + lane];
+    for (int it = 0; it < w; ++it) {
+      if (it * T + q >= cnt) continue;
+      const int t = A.entries[base + (long long)it * 32 + lane];
       const PT pj = pos[t];
       R d0 = pi.x - pj.x, d1 = pi.y - pj.y, d2 = pi.z - pj.z;
       d0 = d0 - r_round(d0 * bi[0]) * b[0];
@@ -523,7 +539,13 @@ __global__ void __launch_bounds__(256) k_nonbonded(NBArgs<R> A, Scalars* sc) {
       acc[7] += (double)(fz * d0);
       acc[8] += (double)(fz * d1);
     }
-    if (valid && cnt > 0) {
+#pragma unroll
+    for (int o = T / 2; o > 0; o >>= 1) {
+      fi0 += __shfl_down_sync(0xffffffffu, fi0, o, T);
+      fi1 += __shfl_down_sync(0xffffffffu, fi1, o, T);
+      fi2 += __shfl_down_sync(0xffffffffu, fi2, o, T);
+    }
+    if (q == 0 && valid && cnt > 0) {
       P::add(&A.fsort[3 * (size_t)s + 0], fi0);
       P::add(&A.fsort[3 * (size_t)s + 1], fi1);
       P::add(&A.fsort[3 * (size_t)s + 2], fi2);
@@ -603,10 +625,10 @@ __global__ void k_distribute(typename Prec<R>::acc_t* F, int natoms, int nvirta,
 }
 
 // --------------------------------------------------------------- bonded
-template <typename R>
+template <typename A>
 struct BondedArgs {
-  const R* su;                     // unwrapped positions (3,NITEMS)
-  typename Prec<R>::acc_t* fb;     // bonded forces (3,NITEMS)
+  const double* su;                // unwrapped positions (3,NITEMS), FP64
+  typename Prec<A>::acc_t* fb;     // bonded forces (3,NITEMS)
   int nb, na, nt, no;
   const int4* bonds;               // i, j, table, label
   const int4* angles;              // i, j, k, table | label<<24
@@ -630,19 +652,23 @@ __device__ __forceinline__ R lerp_mixed(R y0, R y1, R alpha) {
   return (R)((double)y0 * (1.0 - (double)alpha) + (double)(alpha * y1));
 }
 
-template <typename R>
-__device__ __forceinline__ void addf(typename Prec<R>::acc_t* F, int i, const R* f, unsigned* err) {
-  using P = Prec<R>;
-  P::add(&F[3 * (size_t)i + 0], P::q(f[0], err));
-  P::add(&F[3 * (size_t)i + 1], P::q(f[1], err));
-  P::add(&F[3 * (size_t)i + 2], P::q(f[2], err));
+template <typename A>
+__device__ __forceinline__ void addf(typename Prec<A>::acc_t* F, int i, const double* f, unsigned* err) {
+  using P = Prec<A>;
+  P::add(&F[3 * (size_t)i + 0], P::from_double(f[0], err));
+  P::add(&F[3 * (size_t)i + 1], P::from_double(f[1], err));
+  P::add(&F[3 * (size_t)i + 2], P::from_double(f[2], err));
 }
 
 // BONDS.inc:3-57, ANGLES.inc:2-75, TORSIONS.inc:1-152, OUTOFPLANES.inc:1-141
-// with one thread per term; the four term kinds share the grid.
-template <typename R>
-__global__ void __launch_bounds__(256) k_bonded(BondedArgs<R> B, Scalars* sc) {
-  using P = Prec<R>;
+// with one thread per term; the four term kinds share the grid.  The bonded
+// geometry is evaluated in FP64 on both paths: acos near straight angles and
+// trans dihedrals amplifies REAL*4 rounding (about 1e-5 of the largest force
+// in a strained chain), while the terms are few; the forces are summed in the
+// path's accumulator (64-bit fixed point on the FP32 path).
+template <typename A>
+__global__ void __launch_bounds__(256) k_bonded(BondedArgs<A> B, Scalars* sc) {
+  using R = double;
   __shared__ double red[12 * 8];
   double acc[12];
 #pragma unroll
@@ -674,8 +700,8 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs<R> B, Scalars* sc) {
       acc[e.w - 1] += (double)vij;
       R f[3], mf[3];
       for (int c = 0; c < 3; ++c) { f[c] = fij * d[c]; mf[c] = -f[c]; }
-      addf<R>(B.fb, e.x, f, err);
-      addf<R>(B.fb, e.y, mf, err);
+      addf<A>(B.fb, e.x, f, err);
+      addf<A>(B.fb, e.y, mf, err);
     } else if (u < B.nb + B.na) {  // ---------------- angle
       const int4 e = B.angles[u - B.nb];
       const int t = e.w & 0xffffff, lab = e.w >> 24;
@@ -720,10 +746,10 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs<R> B, Scalars* sc) {
         fK[c] = fijk * ss[c] / rkj;
         mI[c] = -fI[c]; mK[c] = -fK[c];
       }
-      addf<R>(B.fb, e.x, fI, err);
-      addf<R>(B.fb, e.z, fK, err);
-      addf<R>(B.fb, e.y, mK, err);
-      addf<R>(B.fb, e.y, mI, err);
+      addf<A>(B.fb, e.x, fI, err);
+      addf<A>(B.fb, e.z, fK, err);
+      addf<A>(B.fb, e.y, mK, err);
+      addf<A>(B.fb, e.y, mI, err);
     } else if (u < B.nb + B.na + B.nt) {  // -------- torsion
       const int q = u - B.nb - B.na;
       const int4 e = B.tors[q];
@@ -801,15 +827,15 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs<R> B, Scalars* sc) {
         f4[c] = fijkl * nn[c] / sinn / rkl;
         f12[c] = fijkl * (cotanm * m[c] + cotann * nn[c]) / rjk;
       }
-      addf<R>(B.fb, e.x, f1, err);
-      addf<R>(B.fb, e.w, f4, err);
+      addf<A>(B.fb, e.x, f1, err);
+      addf<A>(B.fb, e.w, f4, err);
       for (int c = 0; c < 3; ++c) a[c] = -f1[c];
-      addf<R>(B.fb, e.y, a, err);
-      addf<R>(B.fb, e.y, f12, err);
+      addf<A>(B.fb, e.y, a, err);
+      addf<A>(B.fb, e.y, f12, err);
       for (int c = 0; c < 3; ++c) a[c] = -f4[c];
-      addf<R>(B.fb, e.z, a, err);
+      addf<A>(B.fb, e.z, a, err);
       for (int c = 0; c < 3; ++c) a[c] = -f12[c];
-      addf<R>(B.fb, e.z, a, err);
+      addf<A>(B.fb, e.z, a, err);
     } else {  // ------------------------------------------ out of plane
       const int q = u - B.nb - B.na - B.nt;
       const int4 e = B.oops[q];
@@ -870,15 +896,15 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs<R> B, Scalars* sc) {
         f4[c] = -(fijkl * nn[c] / sn / rkl);
         f12[c] = fijkl * (ctm * m[c] + ctn * nn[c]) / rjk;
       }
-      addf<R>(B.fb, e.x, f1, err);
-      addf<R>(B.fb, e.w, f4, err);
+      addf<A>(B.fb, e.x, f1, err);
+      addf<A>(B.fb, e.w, f4, err);
       for (int c = 0; c < 3; ++c) a[c] = -f1[c];
-      addf<R>(B.fb, e.y, a, err);
-      addf<R>(B.fb, e.y, f12, err);
+      addf<A>(B.fb, e.y, a, err);
+      addf<A>(B.fb, e.y, f12, err);
       for (int c = 0; c < 3; ++c) a[c] = -f4[c];
-      addf<R>(B.fb, e.z, a, err);
+      addf<A>(B.fb, e.z, a, err);
       for (int c = 0; c < 3; ++c) a[c] = -f12[c];
-      addf<R>(B.fb, e.z, a, err);
+      addf<A>(B.fb, e.z, a, err);
     }
   }
   if (overext) atomicAdd(&sc->bond_overext, overext);

@@ -334,11 +334,13 @@ def _all_torsion_keys(types):
 
 
 # ------------------------------------------------------------------ configs
-def config1(n=4000, rho=8.0, seed=1, nsteps=1000):
-    """Single-type LJ bead fluid."""
+def config1(n=4000, rho=8.0, seed=1, nsteps=1000, dmin=0.3):
+    """Single-type LJ bead fluid: uniform positions rejected below dmin, LJ
+    sigma 0.47 nm.  (With dmin 0.3 nm the first steps at dt 10 fs meet pair
+    forces beyond the fixed-point range; a larger dmin avoids that.)"""
     rng = np.random.default_rng(seed)
     box = (n / rho) ** (1.0 / 3.0)
-    pos = random_fluid(rng, n, box, 0.3)
+    pos = random_fluid(rng, n, box, dmin)
     mass = 0.072
     vel = maxwell_boltzmann(rng, [mass] * n, 300.0)
     control = dict(ensemble="NVE", temperature=300, pressure=101.3, atoms=n, num_of_time_steps=nsteps,
