@@ -55,7 +55,9 @@ struct Scalars {
   int iavp, pad1;
   double sp[10];
   unsigned err;
-  unsigned pad2;
+  int abort;          // a list outgrew its storage: the rest of the run is a no-op
+  int need_rows[2];   // rows of 32 entries a slice of each list needed
+  unsigned work[4];   // dynamic work counters: nonbonded atom/bead, list build atom/bead
   unsigned long long bond_overext, cell_clamps;
   double mom[3];     // momentum removal (MOMENTUM.f90)
   ObsD obs;          // observables of the last step

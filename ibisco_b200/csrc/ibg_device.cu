@@ -72,11 +72,10 @@ struct DevList {
   int n = 0, which = 0, present = 0;
   int T = 1;  // lanes per particle in the list build and the nonbonded kernel (1, 2, 4 or 8)
   int cell_cap = 0, nslices = 0;
-  long long cap_entries = 0;
+  int w_cap = 0;  // rows of 32 list entries per slice
   int *idx = nullptr, *cell_of = nullptr, *cell_count = nullptr, *cell_start = nullptr, *cell_fill = nullptr;
   int *sorted = nullptr, *sorted_new = nullptr, *slot_of = nullptr, *slot_of_new = nullptr;
   int *counts = nullptr, *slice_w = nullptr, *entries = nullptr;
-  long long* slice_off = nullptr;
   void *pos4 = nullptr, *pos4_new = nullptr, *fsort = nullptr, *mtsf = nullptr;
   size_t pos_bytes = 0;
   // tables of this list
@@ -206,7 +205,6 @@ void build_list(ibg_ctx* c, const ibg_desc* d, int which) {
   L.slot_of_new = dalloc<int>(L.n, o);
   L.counts = dalloc<int>(L.n, o);
   L.slice_w = dalloc<int>(L.nslices, o);
-  L.slice_off = dalloc<long long>(L.nslices + 1, o);
   L.pos_bytes = possize(c) * L.n;
   L.pos4 = dalloc<unsigned char>(L.pos_bytes, o);
   L.pos4_new = dalloc<unsigned char>(L.pos_bytes, o);
@@ -281,8 +279,8 @@ ListArgs list_args(ibg_ctx* c, DevList& L) {
   a.idx = L.idx; a.cell_of = L.cell_of; a.cell_count = L.cell_count; a.cell_start = L.cell_start; a.cell_fill = L.cell_fill;
   a.sorted = L.sorted; a.sorted_new = L.sorted_new; a.slot_of = L.slot_of; a.slot_of_new = L.slot_of_new;
   a.gslot = c->gslot; a.pos4 = L.pos4; a.pos4_new = L.pos4_new;
-  a.counts = L.counts; a.slice_w = L.slice_w; a.slice_off = L.slice_off; a.entries = L.entries;
-  a.cap_entries = L.cap_entries; a.excl_n = c->excl_n; a.excl = c->excl;
+  a.counts = L.counts; a.slice_w = L.slice_w; a.entries = L.entries; a.w_cap = L.w_cap;
+  a.excl_n = c->excl_n; a.excl = c->excl;
   return a;
 }
 
@@ -332,31 +330,24 @@ template <typename R>
 void enq_rebuild(ibg_ctx* c, DevList& L) {
   if (!L.present) return;
   ListArgs a = list_args(c, L);
+  const int gn = grid_for(c, L.n);
   k_regrid<R><<<1, 32, 0, c->st>>>(a, c->sc);
   CK(cudaMemsetAsync(L.cell_count, 0, sizeof(int) * L.cell_cap, c->st));
-  k_cell_assign<R><<<grid_for(c, L.n), 256, 0, c->st>>>(a, c->sc);
+  k_cell_assign<R><<<gn, 256, 0, c->st>>>(a, c->sc);
   k_scan_int<<<1, 1024, 0, c->st>>>(L.cell_count, L.cell_start, L.cell_cap, L.cell_fill);
-  k_cell_fill<<<grid_for(c, L.n), 256, 0, c->st>>>(a);
-  k_cell_sort<<<grid_for(c, L.cell_cap), 256, 0, c->st>>>(a, c->sc);
-  k_reslot<R><<<grid_for(c, L.n), 256, 0, c->st>>>(a);
+  k_cell_fill<<<gn, 256, 0, c->st>>>(a);
+  k_cell_rank<<<gn, 256, 0, c->st>>>(a, c->sc);
+  k_reslot<R><<<gn, 256, 0, c->st>>>(a);
   CK(cudaMemcpyAsync(L.pos4, L.pos4_new, L.pos_bytes, cudaMemcpyDeviceToDevice, c->st));
-  CK(cudaMemcpyAsync(L.slot_of, L.slot_of_new, sizeof(int) * L.n, cudaMemcpyDeviceToDevice, c->st));
-  CK(cudaMemcpyAsync(L.sorted, L.sorted_new, sizeof(int) * L.n, cudaMemcpyDeviceToDevice, c->st));
-  const int gl = grid_for(c, (long long)L.nslices * 32, 16);
+  k_slot_of<<<gn, 256, 0, c->st>>>(a);
+  const int gl = std::max(1, std::min(L.nslices / 8 + 1, c->nsm * 8));
   switch (L.T) {
-    case 1: k_list_build<R, false, 1><<<gl, 256, 0, c->st>>>(a, c->sc); break;
-    case 2: k_list_build<R, false, 2><<<gl, 256, 0, c->st>>>(a, c->sc); break;
-    case 4: k_list_build<R, false, 4><<<gl, 256, 0, c->st>>>(a, c->sc); break;
-    default: k_list_build<R, false, 8><<<gl, 256, 0, c->st>>>(a, c->sc); break;
+    case 1: k_list_build<R, 1><<<gl, 256, 0, c->st>>>(a, c->sc); break;
+    case 2: k_list_build<R, 2><<<gl, 256, 0, c->st>>>(a, c->sc); break;
+    case 4: k_list_build<R, 4><<<gl, 256, 0, c->st>>>(a, c->sc); break;
+    default: k_list_build<R, 8><<<gl, 256, 0, c->st>>>(a, c->sc); break;
   }
-  k_scan_slices<<<1, 1024, 0, c->st>>>(L.slice_w, L.slice_off, L.nslices);
-  switch (L.T) {
-    case 1: k_list_build<R, true, 1><<<gl, 256, 0, c->st>>>(a, c->sc); break;
-    case 2: k_list_build<R, true, 2><<<gl, 256, 0, c->st>>>(a, c->sc); break;
-    case 4: k_list_build<R, true, 4><<<gl, 256, 0, c->st>>>(a, c->sc); break;
-    default: k_list_build<R, true, 8><<<gl, 256, 0, c->st>>>(a, c->sc); break;
-  }
-  c->launches += 9;
+  c->launches += 8;
 }
 
 template <typename R>
@@ -394,8 +385,8 @@ template <typename R>
 void enq_nonbonded(ibg_ctx* c, DevList& L) {
   NBArgs<R> A;
   A.n = L.n; A.nslices = L.nslices; A.ntype = c->ntype;
-  A.pos4 = L.pos4; A.counts = L.counts; A.slice_w = L.slice_w; A.slice_off = L.slice_off; A.entries = L.entries;
-  A.cap_entries = L.cap_entries;
+  A.pos4 = L.pos4; A.counts = L.counts; A.slice_w = L.slice_w; A.entries = L.entries;
+  A.w_cap = L.w_cap; A.work = L.which;
   A.fsort = (typename Prec<R>::acc_t*)L.fsort;
   A.ltab = L.ltab; A.toff = L.toff; A.tndat = L.tndat; A.tbin = (const R*)L.tbin; A.tfp = (const R*)L.tfp; A.tx = (const R*)L.tx;
   A.ntab = L.ntab; A.nrows = L.nrows; A.rcutsq = (R)L.rcutsq;
@@ -498,7 +489,7 @@ void enqueue_step(ibg_ctx* c, unsigned v) {
   enq_move<R>(c, 1);
   if (v & V_MOMENTUM) {
     k_mom_sum<<<c->g_mv, 256, 0, c->st>>>(c->natoms, c->V, c->mass, c->p_mom, c->g_mv);
-    k_mom_apply<<<c->g_mv, 256, 0, c->st>>>(c->natoms, c->V, c->invmass, c->p_mom, c->g_mv, c->g_mv);
+    k_mom_apply<<<c->g_mv, 256, 0, c->st>>>(c->natoms, c->V, c->invmass, c->p_mom, c->g_mv, c->g_mv, c->sc);
     c->launches += 2;
   }
   enq_finalize(c, 1);
@@ -527,8 +518,8 @@ void enqueue(ibg_ctx* c, unsigned v) {
   else enqueue_step<double>(c, v);
 }
 
-void set_step_counter(ibg_ctx* c, int step_before) {
-  int base = step_before + 1;
+// Next step = step_before + 1; observables of step k go to ring slot k - base.
+void set_step_counter(ibg_ctx* c, int step_before, int base) {
   CK(cudaMemcpyAsync(&c->sc->step, &step_before, sizeof(int), cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(&c->sc->ring_base, &base, sizeof(int), cudaMemcpyHostToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -571,36 +562,40 @@ int read_obs(ibg_ctx* c, ibg_obs* out) {
   return IBG_OK;
 }
 
-// Grow the list storage to the counts of the last rebuild (between steps),
-// with 50 % headroom so that later rebuilds inside a run fit.  Returns 1 when
-// any list grew (the rebuild must then be repeated).
-int ensure_list_capacity(ibg_ctx* c) {
-  int grew = 0;
-  for (auto& L : c->L) {
-    if (!L.present) continue;
-    long long tot = 0;
-    CK(cudaMemcpyAsync(&tot, L.slice_off + L.nslices, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    if (tot <= L.cap_entries) continue;
-    long long cap = tot + tot / 2 + 32 * 64;
+// A list build that outgrew its slices raised the abort flag (the remaining
+// kernels of the run did nothing).  Enlarge the slices to the recorded need
+// plus 25 %, clear the flag and return 1 so the caller repeats from the step
+// that aborted.
+int grow_lists(ibg_ctx* c) {
+  int abort_flag = 0;
+  int need[2] = {0, 0};
+  CK(cudaStreamSynchronize(c->st));
+  CK(cudaMemcpy(&abort_flag, &c->sc->abort, sizeof(int), cudaMemcpyDeviceToHost));
+  if (!abort_flag) return 0;
+  CK(cudaMemcpy(need, c->sc->need_rows, sizeof(need), cudaMemcpyDeviceToHost));
+  for (int w = 0; w < 2; ++w) {
+    DevList& L = c->L[w];
+    if (!L.present || need[w] <= L.w_cap) continue;
+    const int cap = need[w] + need[w] / 4 + 2;
     if (L.entries) {
       auto it = std::find(c->owned.begin(), c->owned.end(), (void*)L.entries);
       if (it != c->owned.end()) c->owned.erase(it);
       CK(cudaFree(L.entries));
     }
-    L.entries = dalloc<int>((size_t)cap, c->owned);
-    L.cap_entries = cap;
-    grew = 1;
+    L.entries = dalloc<int>((size_t)L.nslices * 32 * cap, c->owned);
+    L.w_cap = cap;
   }
-  if (grew) {  // the graphs bake the old pointers
-    for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
-    c->graphs.clear();
-  }
-  return grew;
+  const int zero[3] = {0, 0, 0};
+  CK(cudaMemcpy(&c->sc->abort, zero, sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->sc->need_rows, zero, 2 * sizeof(int), cudaMemcpyHostToDevice));
+  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);  // they bake the old pointers
+  c->graphs.clear();
+  return 1;
 }
 
 template <typename R>
 void rebuild_now(ibg_ctx* c) {
+  CK(cudaMemsetAsync(c->sc->work, 0, sizeof(c->sc->work), c->st));
   for (auto& L : c->L) {
     if (!L.present) continue;
     enq_rebuild<R>(c, L);
@@ -869,16 +864,14 @@ int ibg_set_state(ibg_ctx* c, const float* sxyz, const float* vxyz, const float*
     k_init_temps<<<1, 64, 0, c->st>>>(c->p_mv, c->g_mv, c->sc, c->mktemp, c->mktemp_atom, c->mktemp_bead, c->temp_in, c->fac,
                                       c->ensemble);
     int grew = 1;
-    for (int pass = 0; pass < 2 && grew; ++pass) {
+    for (int pass = 0; pass < 4 && grew; ++pass) {
       if (c->prec == IBG_PREC_FP32_FIXED) rebuild_now<float>(c);
       else rebuild_now<double>(c);
       CK(cudaStreamSynchronize(c->st));
       unsigned bits = 0;
       CK(cudaMemcpy(&bits, &c->sc->err, sizeof(unsigned), cudaMemcpyDeviceToHost));
-      if (bits & ~EB_CAPACITY) return check_device(c);
-      grew = ensure_list_capacity(c);
-      unsigned zero = 0;
-      CK(cudaMemcpy(&c->sc->err, &zero, sizeof(unsigned), cudaMemcpyHostToDevice));
+      if (bits) return check_device(c);
+      grew = grow_lists(c);
       // a repeated build sorts already sorted slots and yields the same lists
     }
     if (grew) return fail(c, IBG_E_CAPACITY, "neighbour-list storage could not be sized");
@@ -907,67 +900,77 @@ static int run_steps(ibg_ctx* c, int first, int nsteps, ibg_obs* per_step, bool 
       for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
       c->graphs.clear();
     }
-    set_step_counter(c, first - 1);
-    if (c->flush_bytes) {
-      if (!c->flush_buf) CK(cudaMalloc(&c->flush_buf, c->flush_bytes));
-      while ((int)c->step_ev.size() < 2 * nsteps) {
-        cudaEvent_t e;
-        CK(cudaEventCreate(&e));
-        c->step_ev.push_back(e);
-      }
-    }
-    if (!c->run_ev[0]) {
-      CK(cudaEventCreate(&c->run_ev[0]));
-      CK(cudaEventCreate(&c->run_ev[1]));
-    }
-    CK(cudaEventRecord(c->run_ev[0], c->st));
     int done = 0;
-    while (done < nsteps) {
-      const int step = first + done;
-      const unsigned v = variant_of(c, step, force_only);
-      const bool flush = c->flush_bytes && c->flush_buf;
-      if (flush) {
-        CK(cudaMemsetAsync(c->flush_buf, done & 0xff, c->flush_bytes, c->st));
-        CK(cudaEventRecord(c->step_ev[2 * done], c->st));
-      }
-      if (use_graphs && !c->timing) {
-        auto it = c->graphs.find(v);
-        if (it == c->graphs.end()) {
-          cudaGraph_t g;
-          CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
-          long long l0 = c->launches;
-          enqueue(c, v);
-          CK(cudaStreamEndCapture(c->st, &g));
-          c->launches_per_variant[v & 31] = c->launches - l0;
-          cudaGraphExec_t ge;
-          CK(cudaGraphInstantiate(&ge, g, 0));
-          CK(cudaGraphDestroy(g));
-          it = c->graphs.emplace(v, ge).first;
+    float run_ms_total = 0.f;
+    for (int attempt = 0; attempt < 8 && done < nsteps; ++attempt) {
+      set_step_counter(c, first + done - 1, first);
+      if (c->flush_bytes) {
+        if (!c->flush_buf) CK(cudaMalloc(&c->flush_buf, c->flush_bytes));
+        while ((int)c->step_ev.size() < 2 * nsteps) {
+          cudaEvent_t e;
+          CK(cudaEventCreate(&e));
+          c->step_ev.push_back(e);
         }
-        CK(cudaGraphLaunch(it->second, c->st));
-        c->launches += c->launches_per_variant[v & 31];
-      } else {
-        enqueue(c, v);
       }
-      if (flush) CK(cudaEventRecord(c->step_ev[2 * done + 1], c->st));
-      ++done;
-    }
-    CK(cudaEventRecord(c->run_ev[1], c->st));
-    collect_marks(c);
-    CK(cudaStreamSynchronize(c->st));
-    {
+      if (!c->run_ev[0]) {
+        CK(cudaEventCreate(&c->run_ev[0]));
+        CK(cudaEventCreate(&c->run_ev[1]));
+      }
+      CK(cudaEventRecord(c->run_ev[0], c->st));
+      const int begin = done;
+      for (int k = begin; k < nsteps; ++k) {
+        const int step = first + k;
+        const unsigned v = variant_of(c, step, force_only);
+        const bool flush = c->flush_bytes && c->flush_buf;
+        if (flush) {
+          CK(cudaMemsetAsync(c->flush_buf, k & 0xff, c->flush_bytes, c->st));
+          CK(cudaEventRecord(c->step_ev[2 * k], c->st));
+        }
+        if (use_graphs && !c->timing) {
+          auto it = c->graphs.find(v);
+          if (it == c->graphs.end()) {
+            cudaGraph_t g;
+            CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+            long long l0 = c->launches;
+            enqueue(c, v);
+            CK(cudaStreamEndCapture(c->st, &g));
+            c->launches_per_variant[v & 31] = c->launches - l0;
+            cudaGraphExec_t ge;
+            CK(cudaGraphInstantiate(&ge, g, 0));
+            CK(cudaGraphDestroy(g));
+            it = c->graphs.emplace(v, ge).first;
+          }
+          CK(cudaGraphLaunch(it->second, c->st));
+          c->launches += c->launches_per_variant[v & 31];
+        } else {
+          enqueue(c, v);
+        }
+        if (flush) CK(cudaEventRecord(c->step_ev[2 * k + 1], c->st));
+      }
+      CK(cudaEventRecord(c->run_ev[1], c->st));
+      collect_marks(c);
+      CK(cudaStreamSynchronize(c->st));
       float ms = 0.f;
       CK(cudaEventElapsedTime(&ms, c->run_ev[0], c->run_ev[1]));
-      c->stage_ms[5] = ms;
       if (c->flush_bytes && c->flush_buf) {  // only the steps, not the flushes
-        double tot = 0.0;
-        for (int k = 0; k < nsteps; ++k) {
-          CK(cudaEventElapsedTime(&ms, c->step_ev[2 * k], c->step_ev[2 * k + 1]));
-          tot += ms;
+        ms = 0.f;
+        for (int k = begin; k < nsteps; ++k) {
+          float m = 0.f;
+          CK(cudaEventElapsedTime(&m, c->step_ev[2 * k], c->step_ev[2 * k + 1]));
+          ms += m;
         }
-        c->stage_ms[5] = tot;
       }
+      run_ms_total += ms;
+      if (grow_lists(c)) {
+        int st = 0;  // the step that aborted did not complete
+        CK(cudaMemcpy(&st, &c->sc->step, sizeof(int), cudaMemcpyDeviceToHost));
+        done = st - first;
+        continue;
+      }
+      done = nsteps;
     }
+    c->stage_ms[5] = run_ms_total;
+    if (done < nsteps) return fail(c, IBG_E_CAPACITY, "neighbour-list storage could not be sized");
     int rc = check_device(c);
     if (rc) return rc;
     if (per_step) {
@@ -1094,13 +1097,11 @@ int ibg_get_neighbour_list(ibg_ctx* c, int which, int* list, int maxnab, int* nn
   if (!L.present) return 0;
   try {
     CK(cudaStreamSynchronize(c->st));
-    std::vector<int> counts(L.n), w(L.nslices), sorted(L.n), idx(L.n);
-    std::vector<long long> off(L.nslices + 1);
+    std::vector<int> counts(L.n), sorted(L.n), idx(L.n);
     CK(cudaMemcpy(counts.data(), L.counts, sizeof(int) * L.n, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(off.data(), L.slice_off, sizeof(long long) * (L.nslices + 1), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(sorted.data(), L.sorted, sizeof(int) * L.n, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(idx.data(), L.idx, sizeof(int) * L.n, cudaMemcpyDeviceToHost));
-    std::vector<int> e((size_t)off[L.nslices]);
+    std::vector<int> e((size_t)L.nslices * 32 * L.w_cap);
     if (!e.empty()) CK(cudaMemcpy(e.data(), L.entries, sizeof(int) * e.size(), cudaMemcpyDeviceToHost));
     const int T = L.T, P = 32 / L.T;
     for (int s = 0; s < L.n; ++s) {
@@ -1112,7 +1113,7 @@ int ibg_get_neighbour_list(ibg_ctx* c, int which, int* list, int maxnab, int* nn
       int* col = list + (size_t)a * maxnab;
       for (int k = 0; k < maxnab; ++k) {
         if (k < counts[s]) {
-          int t = e[(size_t)off[g] + (size_t)(k / T) * 32 + lane0 + (k % T)];
+          int t = e[((size_t)g * L.w_cap + (size_t)(k / T)) * 32 + lane0 + (k % T)];
           col[k] = idx[sorted[t]] + 1;
         } else {
           col[k] = 0;

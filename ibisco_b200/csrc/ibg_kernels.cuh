@@ -84,6 +84,8 @@ __device__ __forceinline__ void box_of<double>(const Scalars* sc, double* b, dou
 
 // ------------------------------------------------------------------ per step
 __global__ void k_begin(Scalars* sc, int nupdate, int nmts) {
+  if (sc->abort) return;
+  for (int k = 0; k < 4; ++k) sc->work[k] = 0u;
   int st = ++sc->step;
   sc->rebuild = (st % nupdate) == 0;
   sc->mts_m = nmts > 0 ? st % (3 + nmts) : -1;
@@ -188,10 +190,9 @@ struct ListArgs {
   void* pos4;        // [n]
   void* pos4_new;    // [n]
   int* counts;       // [n] per slot
-  int* slice_w;      // [nslices]
-  long long* slice_off;  // [nslices + 1]
-  int* entries;      // list storage, sliced-ELL by 32 slots
-  long long cap_entries;
+  int* slice_w;      // [nslices] rows of 32 entries used by each slice
+  int* entries;      // list storage: slice g owns rows [g*w_cap, (g+1)*w_cap) of 32 entries
+  int w_cap;         // rows of 32 entries per slice
   const int* excl_n; // CONNECTIONS, by global id
   const int* excl;   // CONNECTED_TO, [i*20 + c], 0-based
 };
@@ -272,41 +273,50 @@ __global__ void k_cell_fill(ListArgs L) {
 
 // Within a cell the reference's linked list visits entries by decreasing A
 // (LINKS.f90:195-196); slots are kept in increasing A so the list build can
-// walk them backwards.
-__global__ void k_cell_sort(ListArgs L, const Scalars* sc) {
-  const int ncell = sc->ncell[L.which][0] * sc->ncell[L.which][1] * sc->ncell[L.which][2];
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
-    int b = L.cell_start[c], e = L.cell_start[c + 1];
-    for (int i = b + 1; i < e; ++i) {
-      int v = L.sorted_new[i], j = i - 1;
-      while (j >= b && L.sorted_new[j] > v) { L.sorted_new[j + 1] = L.sorted_new[j]; --j; }
-      L.sorted_new[j + 1] = v;
-    }
+// walk them backwards.  k_cell_fill placed a cell's entries in arbitrary order
+// (atomics); here each entry finds its rank among its cell's entries.
+__global__ void k_cell_rank(ListArgs L, const Scalars* sc) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < L.n; s += gridDim.x * blockDim.x) {
+    const int a = L.sorted_new[s];
+    const int c = L.cell_of[a];
+    const int b = L.cell_start[c], e = L.cell_start[c + 1];
+    int rank = 0;
+    for (int k = b; k < e; ++k) rank += L.sorted_new[k] < a;
+    L.slot_of_new[b + rank] = a;  // scratch: the ordered cell segment
   }
 }
 
+// New slot order: positions move to their new slots, and the slot of every
+// entry (and of its global particle) is updated.  Reads the ordered cells from
+// the scratch k_cell_rank wrote; writes the new order to sorted.
 template <typename R>
 __global__ void k_reslot(ListArgs L) {
   using PT = typename Prec<R>::pos_t;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < L.n; s += gridDim.x * blockDim.x) {
-    int a = L.sorted_new[s];
+    int a = L.slot_of_new[s];
     ((PT*)L.pos4_new)[s] = ((const PT*)L.pos4)[L.slot_of[a]];
-    L.slot_of_new[a] = s;
+    L.sorted[s] = a;
     L.gslot[L.idx[a]] = s * 2 + L.which;
   }
 }
 
+// slot_of from the new order (after k_reslot and the position copy).
+__global__ void k_slot_of(ListArgs L) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < L.n; s += gridDim.x * blockDim.x) L.slot_of[L.sorted[s]] = s;
+}
+
 // NEW_NEIGHBOUR_WITHLIST.f90:34-123.  T lanes share one slot (particle); a
-// warp covers one slice of P = 32/T consecutive slots.  Candidates are
-// visited in the reference's order -- the particle's own cell below it
-// (decreasing A), then the 13 cells of the MAPS.f90:137-149 stencil, each by
-// decreasing A -- T at a time; a ballot over the slot's lanes keeps accepted
-// candidates in that order.  The distance test runs first and the exclusion
-// scan only for candidates inside RLIST (the accepted set is the same).
-// Entry k of slot s (slice g) is stored at off[g] + (k/T)*32 + (s%P)*T + k%T.
-// FILL=false counts and records the slice width in rows of 32; FILL=true
-// writes slot indices.
-template <typename R, bool FILL, int T>
+// warp takes one slice of P = 32/T consecutive slots at a time (dynamic
+// scheduling).  Candidates are visited in the reference's order -- the
+// particle's own cell below it (decreasing A), then the 13 cells of the
+// MAPS.f90:137-149 stencil, each by decreasing A -- T at a time; a ballot over
+// the slot's lanes keeps accepted candidates in that order.  The distance test
+// runs first and the exclusion scan only for candidates inside RLIST (the
+// accepted set is the same).  Entry k of slot s (slice g) is stored at
+// (g*w_cap + k/T)*32 + (s%P)*T + k%T.  A slice that needs more than w_cap rows
+// records its need and raises the abort flag (the host enlarges the storage
+// and repeats the step).
+template <typename R, int T>
 __global__ void __launch_bounds__(256) k_list_build(ListArgs L, Scalars* sc) {
   using PT = typename Prec<R>::pos_t;
   constexpr int P = 32 / T;
@@ -316,22 +326,21 @@ __global__ void __launch_bounds__(256) k_list_build(ListArgs L, Scalars* sc) {
   const R rlsq = sizeof(R) == 4 ? (R)L.rlistsq : (R)L.rlistsqd;
   const PT* pos = (const PT*)L.pos4;
   const int lane = threadIdx.x & 31, grp = lane / T, q = lane % T;
-  const unsigned gmask = (T == 32 ? 0xffffffffu : (((1u << T) - 1u) << (grp * T)));
+  const unsigned gmask = ((1u << T) - 1u) << (grp * T);
   const int nslices = (L.n + P - 1) / P;
-  const int warps = (gridDim.x * blockDim.x) >> 5;
+  const int cap = L.w_cap * T;  // entries a slot may hold
   const int off[13][3] = {{1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {-1, 1, 0}, {1, 0, -1}, {1, 1, -1}, {0, 1, -1},
                           {-1, 1, -1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}, {-1, 1, 1}, {0, 0, 1}};
-  for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < nslices; g += warps) {
+  for (;;) {
+    int g = 0;
+    if (lane == 0) g = (int)atomicAdd(&sc->work[2 + L.which], 1u);
+    g = __shfl_sync(0xffffffffu, g, 0);
+    if (g >= nslices) break;
     const int s = g * P + grp;
     const bool valid = s < L.n;
+    const long long base = (long long)g * L.w_cap * 32;
     int cnt = 0;
-    long long base = 0;
-    bool room = true;
-    if (FILL) {
-      base = L.slice_off[g];
-      room = base + 32LL * L.slice_w[g] <= L.cap_entries;
-    }
-    if (valid && room) {
+    if (valid) {
       const int a = L.sorted[s];
       const int i = L.idx[a];
       const PT pi = pos[s];
@@ -361,10 +370,10 @@ __global__ void __launch_bounds__(256) k_list_build(ListArgs L, Scalars* sc) {
                 if (ex[e] == j) ok = false;
             }
           }
-          const unsigned bits = (__ballot_sync(gmask, ok) >> (grp * T)) & (T == 32 ? 0xffffffffu : ((1u << T) - 1u));
-          if (FILL && ok) {
+          const unsigned bits = (__ballot_sync(gmask, ok) >> (grp * T)) & ((1u << T) - 1u);
+          if (ok) {
             const int k = cnt + __popc(bits & ((1u << q) - 1u));
-            L.entries[base + (long long)(k / T) * 32 + grp * T + (k % T)] = t;
+            if (k < cap) L.entries[base + (long long)(k / T) * 32 + grp * T + (k % T)] = t;
           }
           cnt += __popc(bits);
         }
@@ -376,37 +385,21 @@ __global__ void __launch_bounds__(256) k_list_build(ListArgs L, Scalars* sc) {
         const int c = jx * nz * ny + jy * nz + jz;
         segment(L.cell_start[c + 1] - 1, L.cell_start[c]);
       }
-      if (!FILL && q == 0) {
+      if (q == 0) {
         L.counts[s] = cnt;
         if (cnt >= L.maxnab) atomicOr(&sc->err, EB_LIST_OVERFLOW);
       }
     }
-    if (FILL && !room && lane == 0) atomicOr(&sc->err, EB_CAPACITY);
-    if (!FILL) {
-      const int w = __reduce_max_sync(0xffffffffu, valid ? cnt : 0);
-      if (lane == 0) L.slice_w[g] = (w + T - 1) / T;
+    const int w = __reduce_max_sync(0xffffffffu, valid ? cnt : 0);
+    if (lane == 0) {
+      const int rows = (w + T - 1) / T;
+      L.slice_w[g] = rows;
+      if (rows > L.w_cap) {
+        atomicMax(&sc->need_rows[L.which], rows);
+        sc->abort = 1;
+      }
     }
   }
-}
-
-// Exclusive scan of 32*slice_w into slice_off (single block).
-__global__ void k_scan_slices(const int* w, long long* off, int m) {
-  __shared__ long long part[1024];
-  const int t = threadIdx.x, T = blockDim.x;
-  const int chunk = (m + T - 1) / T;
-  const int b = t * chunk, e = min(m, b + chunk);
-  long long s = 0;
-  for (int i = b; i < e; ++i) s += 32LL * w[i];
-  part[t] = s;
-  __syncthreads();
-  if (t == 0) {
-    long long run = 0;
-    for (int i = 0; i < T; ++i) { long long v = part[i]; part[i] = run; run += v; }
-    off[m] = run;
-  }
-  __syncthreads();
-  long long run = part[t];
-  for (int i = b; i < e; ++i) { off[i] = run; run += 32LL * w[i]; }
 }
 
 // ------------------------------------------------------------- nonbonded
@@ -416,9 +409,9 @@ struct NBArgs {
   const void* pos4;
   const int* counts;
   const int* slice_w;
-  const long long* slice_off;
   const int* entries;
-  long long cap_entries;           // slices reaching past it are skipped (capacity error)
+  int w_cap;                       // rows of 32 entries per slice
+  int work;                        // index of this launch's work counter
   typename Prec<R>::acc_t* fsort;  // [3n] per slot
   // tables of this list: ltab[ti*ntype+tj] = local table or -1; rows of table
   // t are [toff[t], toff[t+1]); fp = {F,P} per row, x = RNBOND per row
@@ -441,7 +434,7 @@ struct NBArgs {
 // over the slot's lanes (integer shuffles); j-forces are 64-bit integer
 // atomics.  Tables are staged in shared memory when SMEM.
 template <typename R, bool SMEM, int T>
-__global__ void __launch_bounds__(256) k_nonbonded(NBArgs<R> A, Scalars* sc) {
+__global__ void __launch_bounds__(256, 4) k_nonbonded(NBArgs<R> A, Scalars* sc) {
   using P = Prec<R>;
   using PT = typename P::pos_t;
   using reg_t = typename P::reg_t;
@@ -474,31 +467,28 @@ __global__ void __launch_bounds__(256) k_nonbonded(NBArgs<R> A, Scalars* sc) {
   box_of<R>(sc, b, bi, b2);
   const PT* pos = (const PT*)A.pos4;
   const int lane = threadIdx.x & 31, grp = lane / T, q = lane % T;
-  const int warps = (gridDim.x * blockDim.x) >> 5;
   double acc[9];
 #pragma unroll
   for (int k = 0; k < 9; ++k) acc[k] = 0.0;
   unsigned err = 0;
-  for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < A.nslices; g += warps) {
+  const bool run = !sc->abort;
+  for (;;) {
+    int g = 0;
+    if (lane == 0) g = run ? (int)atomicAdd(&sc->work[A.work], 1u) : A.nslices;
+    g = __shfl_sync(0xffffffffu, g, 0);
+    if (g >= A.nslices) break;
     const int s = g * PS + grp;
     const bool valid = s < A.n;
     const int cnt = valid ? A.counts[s] : 0;
-    int w = A.slice_w[g];
-    const long long base = A.slice_off[g];
-    if (base + 32LL * w > A.cap_entries) {
-      err |= EB_CAPACITY;
-      w = 0;
-    }
+    const int w = A.slice_w[g];
+    const int* ent = A.entries + (long long)g * A.w_cap * 32 + lane;
     PT pi;
     if (valid) pi = pos[s];
     else { pi.x = pi.y = pi.z = 0; pi.w = P::tbits(0); }
     const int wi = P::bits(pi.w);
     const int ti = wi & 0xffff, li = wi >> 16;
     reg_t fi0 = 0, fi1 = 0, fi2 = 0;
-    for (int it = 0; it < w; ++it) {
-      if (it * T + q >= cnt) continue;
-      const int t = A.entries[base + (long long)it * 32 + lane];
-      const PT pj = pos[t];
+    auto pair = [&](int t, const PT& pj) {
       R d0 = pi.x - pj.x, d1 = pi.y - pj.y, d2 = pi.z - pj.z;
       d0 = d0 - r_round(d0 * bi[0]) * b[0];
       d1 = d1 - r_round(d1 * bi[1]) * b[1];
@@ -506,15 +496,15 @@ __global__ void __launch_bounds__(256) k_nonbonded(NBArgs<R> A, Scalars* sc) {
       R r2 = d0 * d0;
       r2 = r2 + d1 * d1;
       r2 = r2 + d2 * d2;
-      if (!(r2 < A.rcutsq)) continue;
+      if (!(r2 < A.rcutsq)) return;
       const int wj = P::bits(pj.w);
       const int tj = wj & 0xffff, lj = wj >> 16;
       const int tab = ltab[ti * A.ntype + tj];
-      if (tab < 0) { err |= EB_MISSING_TABLE; continue; }
+      if (tab < 0) { err |= EB_MISSING_TABLE; return; }
       const R r = r_sqrt(r2);
       const R bin = tbin[tab];
       const int ni = fint(r / bin);
-      if (ni < 0 || ni > tndat[tab]) { err |= EB_TABLE_RANGE; continue; }
+      if (ni < 0 || ni > tndat[tab]) { err |= EB_TABLE_RANGE; return; }
       const int row = toff[tab] + ni;
       const R alpha = (r - tx[row]) / bin;
       const R f0 = tfp[2 * row], p0 = tfp[2 * row + 1], f1 = tfp[2 * row + 2], p1 = tfp[2 * row + 3];
@@ -538,6 +528,18 @@ __global__ void __launch_bounds__(256) k_nonbonded(NBArgs<R> A, Scalars* sc) {
       acc[6] += (double)(fy * d0);
       acc[7] += (double)(fz * d0);
       acc[8] += (double)(fz * d1);
+    };
+    // two rows per iteration: both entry loads and both position gathers are
+    // in flight before either pair is evaluated
+    for (int it = 0; it < w; it += 2) {
+      const bool v0 = it * T + q < cnt;
+      const bool v1 = (it + 1) * T + q < cnt;
+      const int t0 = v0 ? ent[it * 32] : 0;
+      const int t1 = v1 ? ent[(it + 1) * 32] : 0;
+      const PT p0 = pos[t0];
+      const PT p1 = pos[t1];
+      if (v0) pair(t0, p0);
+      if (v1) pair(t1, p1);
     }
 #pragma unroll
     for (int o = T / 2; o > 0; o >>= 1) {
@@ -577,6 +579,7 @@ struct CollectArgs {
 template <typename R>
 __global__ void k_nb_collect(CollectArgs<R> C, Scalars* sc) {
   using P = Prec<R>;
+  if (sc->abort) return;
   const int m = sc->mts_m;
   const bool explicit_step = !C.mts || (m >= 1 && m <= 3);
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < C.n; s += gridDim.x * blockDim.x) {
@@ -607,6 +610,7 @@ template <typename R>
 __global__ void k_distribute(typename Prec<R>::acc_t* F, int natoms, int nvirta, const int* vnum, const int* vmem,
                              const float* vcoef, Scalars* sc) {
   using P = Prec<R>;
+  if (sc->abort) return;
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nvirta; v += gridDim.x * blockDim.x) {
     const size_t vs = (size_t)(natoms + v);
     double f[3];
@@ -676,8 +680,8 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs<A> B, Scalars* sc) {
   unsigned long long overext = 0;
   unsigned* err = &sc->err;
   const R* S = B.su;
+  const int total = sc->abort ? 0 : B.nb + B.na + B.nt + B.no;
   auto pos = [&](int i, R* o) { o[0] = S[3 * (size_t)i]; o[1] = S[3 * (size_t)i + 1]; o[2] = S[3 * (size_t)i + 2]; };
-  const int total = B.nb + B.na + B.nt + B.no;
   for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < total; u += gridDim.x * blockDim.x) {
     if (u < B.nb) {  // -------------------------------- bond
       const int4 e = B.bonds[u];
@@ -942,7 +946,8 @@ __global__ void __launch_bounds__(256) k_move(MoveArgs<R> M, Scalars* sc) {
 #pragma unroll
   for (int k = 0; k < 18; ++k) acc[k] = 0.0;
   const double lam0 = sc->lam[0], lam1 = sc->lam[1];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M.natoms; i += gridDim.x * blockDim.x) {
+  const int nrun = sc->abort ? 0 : M.natoms;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrun; i += gridDim.x * blockDim.x) {
     double s[3], v[3], fb[3], f[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -1008,8 +1013,10 @@ __global__ void k_mom_sum(int natoms, const double* V, const double* mass, doubl
     for (int c = 0; c < 3; ++c) part[c * stride + blockIdx.x] = out[c];
 }
 
-__global__ void k_mom_apply(int natoms, double* V, const double* invmass, const double* part, int stride, int nblocks) {
+__global__ void k_mom_apply(int natoms, double* V, const double* invmass, const double* part, int stride, int nblocks,
+                            const Scalars* sc) {
   __shared__ double tot[3];
+  if (sc->abort) return;
   if (threadIdx.x < 32) {
     for (int c = 0; c < 3; ++c) {
       double s = 0.0;
@@ -1025,6 +1032,7 @@ __global__ void k_mom_apply(int natoms, double* V, const double* invmass, const 
 
 // SCALEBP.f90:259-261: positions scaled with the box.
 __global__ void k_scale_positions(int natoms, double* S, const Scalars* sc) {
+  if (sc->abort) return;
   const double miu = sc->miu;
   if (miu == 1.0) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < natoms; i += gridDim.x * blockDim.x)
@@ -1054,6 +1062,7 @@ __device__ double wsum(const double* p, int g) {
 // the next step and the barostat window (SCALEBP.f90:240-263).
 __global__ void k_finalize(FinalArgs F, Scalars* sc) {
   __shared__ double q[64];
+  if (sc->abort) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   // q[0..8] atom NB, q[9..17] bead NB, q[18..29] bonded, q[30..47] move
   for (int k = warp; k < 48; k += nw) {
