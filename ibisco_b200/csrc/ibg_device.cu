@@ -94,7 +94,8 @@ struct DevList {
 struct ibg_ctx {
   int prec = 0;
   int dev = 0, nsm = 148;
-  cudaStream_t st = nullptr;
+  cudaStream_t st = nullptr, st2 = nullptr;  // st2: bonded branch of a step
+  cudaEvent_t fork_ev[2] = {nullptr, nullptr};
   std::vector<void*> owned;
   std::string err;
   // descriptor scalars
@@ -133,6 +134,7 @@ struct ibg_ctx {
   std::vector<std::pair<cudaEvent_t, int>> marks;  // event, stage that starts there
   cudaEvent_t run_ev[2] = {nullptr, nullptr};
   long long launches = 0;
+  long long list_growths = 0;
   // L2 flush between timed steps
   size_t flush_bytes = 0;
   void* flush_buf = nullptr;
@@ -316,8 +318,9 @@ void collect_marks(ibg_ctx* c) {
 }
 
 template <typename R>
-void enq_positions(ibg_ctx* c) {
+void enq_positions(ibg_ctx* c, int begin = 0) {
   PosArgs a;
+  a.begin = begin; a.nupdate = c->nupdate; a.nmts = c->nmts;
   a.natoms = c->natoms; a.nvirta = c->nvirta; a.S = c->S; a.Svs = c->S + 3 * (size_t)c->natoms;
   a.tbits = c->tbits; a.gslot = c->gslot;
   a.pos4[0] = c->L[0].pos4; a.pos4[1] = c->L[1].pos4;
@@ -454,12 +457,31 @@ void enq_finalize(ibg_ctx* c, int move) {
   ++c->launches;
 }
 
+// One loop body.  In graph mode the bonded branch (zero fb, bonded terms,
+// their VS distribution) runs concurrently with the list build and the
+// nonbonded branch; both join before MOVE.  Timing mode keeps one stream so
+// that the stage times add up.
 template <typename R>
 void enqueue_step(ibg_ctx* c, unsigned v) {
+  const bool fork = !c->timing;
   mark(c, 4);
-  k_begin<<<1, 1, 0, c->st>>>(c->sc, c->nupdate, c->nmts);
-  ++c->launches;
-  enq_positions<R>(c);
+  enq_positions<R>(c, 1);
+  auto bonded_branch = [&]() {
+    CK(cudaMemsetAsync(c->fb, 0, accsize(c) * 3 * (size_t)c->nitems, c->st));
+    mark(c, 2);
+    enq_bonded<R>(c);
+    mark(c, 4);
+    enq_distribute<R>(c, c->fb);
+  };
+  cudaStream_t main_st = c->st;
+  if (fork) {
+    CK(cudaEventRecord(c->fork_ev[0], main_st));
+    CK(cudaStreamWaitEvent(c->st2, c->fork_ev[0], 0));
+    c->st = c->st2;
+    bonded_branch();
+    CK(cudaEventRecord(c->fork_ev[1], c->st2));
+    c->st = main_st;
+  }
   if (v & V_REBUILD) {
     mark(c, 0);
     enq_rebuild<R>(c, c->L[0]);
@@ -474,11 +496,8 @@ void enqueue_step(ibg_ctx* c, unsigned v) {
   if (c->L[1].present) enq_collect<R>(c, c->L[1]);
   if (c->L[0].present) enq_collect<R>(c, c->L[0]);
   enq_distribute<R>(c, c->fnb);
-  CK(cudaMemsetAsync(c->fb, 0, accsize(c) * 3 * (size_t)c->nitems, c->st));
-  mark(c, 2);
-  enq_bonded<R>(c);
-  mark(c, 4);
-  enq_distribute<R>(c, c->fb);
+  if (fork) CK(cudaStreamWaitEvent(main_st, c->fork_ev[1], 0));
+  else bonded_branch();
   mark(c, 3);
   if (v & V_FORCE_ONLY) {
     enq_move<R>(c, 0);
@@ -584,6 +603,7 @@ int grow_lists(ibg_ctx* c) {
     }
     L.entries = dalloc<int>((size_t)L.nslices * 32 * cap, c->owned);
     L.w_cap = cap;
+    ++c->list_growths;
   }
   const int zero[3] = {0, 0, 0};
   CK(cudaMemcpy(&c->sc->abort, zero, sizeof(int), cudaMemcpyHostToDevice));
@@ -611,6 +631,28 @@ const char* ibg_version(void) { return "ibisco_b200 0.1 (sm_100a)"; }
 
 int ibg_set_device(int device) { return cudaSetDevice(device) == cudaSuccess ? IBG_OK : IBG_E_CUDA; }
 
+int ibg_set_list_rows(ibg_ctx* c, int rows) {
+  if (!c || rows < 1) return IBG_E_INVALID;
+  try {
+    CK(cudaStreamSynchronize(c->st));
+    for (auto& L : c->L) {
+      if (!L.present) continue;
+      if (L.entries) {
+        auto it = std::find(c->owned.begin(), c->owned.end(), (void*)L.entries);
+        if (it != c->owned.end()) c->owned.erase(it);
+        CK(cudaFree(L.entries));
+      }
+      L.entries = dalloc<int>((size_t)L.nslices * 32 * rows, c->owned);
+      L.w_cap = rows;
+    }
+    for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+    c->graphs.clear();
+  } catch (CudaError& e) {
+    return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
+  }
+  return IBG_OK;
+}
+
 int ibg_set_l2_flush(ibg_ctx* c, long long bytes) {
   if (!c || bytes < 0) return IBG_E_INVALID;
   if (c->flush_buf && (size_t)bytes != c->flush_bytes) {
@@ -636,6 +678,9 @@ int ibg_create(const ibg_desc* d, int precision, ibg_ctx** out) {
     c->dev = dev;
     CK(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev));
     CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->fork_ev[0], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->fork_ev[1], cudaEventDisableTiming));
     c->prec = precision;
     c->natoms = d->natoms; c->nvirta = d->nvirta; c->nitems = d->nitems; c->ntype = d->ntype;
     c->numatoms = d->numatoms; c->numbeads = d->numbeads; c->ncoarse = d->ncoarse;
@@ -1153,6 +1198,7 @@ int ibg_set_timing(ibg_ctx* c, int on) {
 
 int ibg_get_timing(ibg_ctx* c, double* stage_ms, int nstage, long long* launches) {
   if (!c) return IBG_E_INVALID;
+  c->stage_ms[7] = (double)c->list_growths;
   for (int k = 0; k < nstage && k < 8; ++k) stage_ms[k] = c->stage_ms[k];
   if (launches) *launches = c->launches;
   return IBG_OK;
@@ -1167,6 +1213,9 @@ void ibg_destroy(ibg_ctx* c) {
     if (e) cudaEventDestroy(e);
   for (auto* e : c->step_ev) cudaEventDestroy(e);
   if (c->flush_buf) cudaFree(c->flush_buf);
+  for (auto* e : c->fork_ev)
+    if (e) cudaEventDestroy(e);
+  if (c->st2) cudaStreamDestroy(c->st2);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
 }

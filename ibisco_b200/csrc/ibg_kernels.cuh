@@ -110,6 +110,7 @@ __device__ __forceinline__ void fold3(R* r, const R* b2) {
 
 struct PosArgs {
   int natoms, nvirta;
+  int begin, nupdate, nmts;  // begin != 0: also start the step (k_begin)
   const double* S;     // unwrapped positions (3,NITEMS), FP64 state
   double* Svs;         // VS rows of S (written for the FP64 path and output)
   const int* tbits;    // type | label<<16 per particle
@@ -124,9 +125,18 @@ struct PosArgs {
 
 // SHIFT.f90:36-44 for atoms and VIRTUAL_DEF.f90:67-95 for virtual sites
 // (centre-of-mass sums with all three components reset per site).
+// begin: when set, block 0 first advances the step counter (k_begin's work);
+// the positions do not depend on it.
 template <typename R>
 __global__ void k_positions(PosArgs a, Scalars* sc) {
   using PT = typename Prec<R>::pos_t;
+  if (a.begin && blockIdx.x == 0 && threadIdx.x == 0 && !sc->abort) {
+    for (int k = 0; k < 4; ++k) sc->work[k] = 0u;
+    const int st = ++sc->step;
+    sc->rebuild = (st % a.nupdate) == 0;
+    sc->mts_m = a.nmts > 0 ? st % (3 + a.nmts) : -1;
+    sc->miu = 1.0;
+  }
   const int n = a.natoms + a.nvirta;
   R b[3], bi[3], b2[3];
   box_of<R>(sc, b, bi, b2);
@@ -472,15 +482,24 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded(NBArgs<R> A, Scalars* sc) 
   for (int k = 0; k < 9; ++k) acc[k] = 0.0;
   unsigned err = 0;
   const bool run = !sc->abort;
+  // work unit = up to ROWS rows of 32 entries of one slice; units are taken
+  // dynamically so that warps finish within one unit of each other
+  constexpr int ROWS = 8;
+  const int U = (A.w_cap + ROWS - 1) / ROWS;
+  const int nunits = A.nslices * U;
   for (;;) {
-    int g = 0;
-    if (lane == 0) g = run ? (int)atomicAdd(&sc->work[A.work], 1u) : A.nslices;
-    g = __shfl_sync(0xffffffffu, g, 0);
-    if (g >= A.nslices) break;
+    int u = 0;
+    if (lane == 0) u = run ? (int)atomicAdd(&sc->work[A.work], 1u) : nunits;
+    u = __shfl_sync(0xffffffffu, u, 0);
+    if (u >= nunits) break;
+    const int g = u / U;
+    const int r0 = (u - g * U) * ROWS;
+    const int w = min(A.slice_w[g], A.w_cap);
+    if (r0 >= w) continue;
+    const int r1 = min(w, r0 + ROWS);
     const int s = g * PS + grp;
     const bool valid = s < A.n;
     const int cnt = valid ? A.counts[s] : 0;
-    const int w = A.slice_w[g];
     const int* ent = A.entries + (long long)g * A.w_cap * 32 + lane;
     PT pi;
     if (valid) pi = pos[s];
@@ -531,9 +550,9 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded(NBArgs<R> A, Scalars* sc) 
     };
     // two rows per iteration: both entry loads and both position gathers are
     // in flight before either pair is evaluated
-    for (int it = 0; it < w; it += 2) {
+    for (int it = r0; it < r1; it += 2) {
       const bool v0 = it * T + q < cnt;
-      const bool v1 = (it + 1) * T + q < cnt;
+      const bool v1 = it + 1 < r1 && (it + 1) * T + q < cnt;
       const int t0 = v0 ? ent[it * 32] : 0;
       const int t1 = v1 ? ent[(it + 1) * 32] : 0;
       const PT p0 = pos[t0];
@@ -547,7 +566,7 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded(NBArgs<R> A, Scalars* sc) 
       fi1 += __shfl_down_sync(0xffffffffu, fi1, o, T);
       fi2 += __shfl_down_sync(0xffffffffu, fi2, o, T);
     }
-    if (q == 0 && valid && cnt > 0) {
+    if (q == 0 && valid && r0 * T < cnt) {
       P::add(&A.fsort[3 * (size_t)s + 0], fi0);
       P::add(&A.fsort[3 * (size_t)s + 1], fi1);
       P::add(&A.fsort[3 * (size_t)s + 2], fi2);

@@ -32,7 +32,7 @@ EXPORTS = [
     "ibg_setup_array_i", "ibg_setup_array_f", "ibg_setup_free",
     "ibg_create", "ibg_set_state", "ibg_step", "ibg_forces", "ibg_run", "ibg_get_state",
     "ibg_get_state_f64", "ibg_get_neighbour_list", "ibg_get_exclusions", "ibg_set_timing",
-    "ibg_get_timing", "ibg_last_error", "ibg_destroy", "ibg_version", "ibg_set_l2_flush", "ibg_set_device",
+    "ibg_get_timing", "ibg_last_error", "ibg_destroy", "ibg_version", "ibg_set_l2_flush", "ibg_set_device", "ibg_set_list_rows",
 ]
 
 
@@ -134,6 +134,7 @@ def lib(build_if_missing: bool = True):
         "ibg_version": (cp, []),
         "ibg_set_l2_flush": (ctypes.c_int, [vp, ctypes.c_longlong]),
         "ibg_set_device": (ctypes.c_int, [ctypes.c_int]),
+        "ibg_set_list_rows": (ctypes.c_int, [vp, ctypes.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -303,7 +304,8 @@ class System:
         n = ctypes.c_longlong()
         lib().ibg_get_timing(self._h, ms, 8, ctypes.byref(n))
         return {"list_ms": ms[0], "nonbonded_ms": ms[1], "bonded_ms": ms[2], "integrate_ms": ms[3],
-                "other_ms": ms[4], "run_ms": ms[5], "nonbonded_launches": int(ms[6]), "launches": n.value}
+                "other_ms": ms[4], "run_ms": ms[5], "nonbonded_launches": int(ms[6]), "list_growths": int(ms[7]),
+                "launches": n.value}
 
     def set_timing(self, on: bool):
         self._check(lib().ibg_set_timing(self._h, 1 if on else 0))

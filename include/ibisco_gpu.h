@@ -187,13 +187,21 @@ int ibg_get_exclusions(ibg_ctx* c, int* connections, int* connected_to);
    With timing on (ibg_set_timing(c,1): direct launches, no graph replay),
    stage_ms[0..4] accumulate the time of the list build, nonbonded, bonded,
    integration/reduction and remaining kernels since ibg_set_timing, and
-   stage_ms[6] counts the nonbonded launches.  launches = kernels enqueued by
-   this context so far. */
+   stage_ms[6] counts the nonbonded launches; stage_ms[7] counts the growths of
+   the Verlet-list storage.  launches = kernels enqueued by this context so
+   far. */
 int ibg_set_timing(ibg_ctx* c, int on);
 int ibg_get_timing(ibg_ctx* c, double* stage_ms, int nstage, long long* launches);
 /* Benchmark support: before every step of ibg_run write `bytes` of scratch
    memory (evicting the L2 cache) and time only the steps (stage_ms[5]). */
 int ibg_set_l2_flush(ibg_ctx* c, long long bytes);
+/* Diagnostic: replace the Verlet-list storage by `rows` rows of 32 entries per
+   slice.  The stored lists are discarded, so call it only right before a step
+   that rebuilds them (step % update_neighbour_list == 0); a build that does not
+   fit stops the run at that step, the storage grows and the step is repeated
+   (the same path a growing system takes).  stage_ms[7] of ibg_get_timing
+   counts the growths. */
+int ibg_set_list_rows(ibg_ctx* c, int rows);
 /* Select the CUDA device of the calling thread for subsequent ibg_create. */
 int ibg_set_device(int device);
 const char* ibg_last_error(const ibg_ctx* c);

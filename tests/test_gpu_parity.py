@@ -149,6 +149,25 @@ def test_step_and_run_agree(sysdir):
     assert np.array_equal(a.state64()["sxyz"], b.state64()["sxyz"])
 
 
+def test_list_storage_growth_mid_run_is_exact(sysdir):
+    """A rebuild that outgrows the list storage stops the run at that step; the
+    storage grows and the step is repeated.  The result is bitwise the run that
+    never ran out of storage."""
+    d = sysdir("melt")
+    _, a = make(d, native.IBG_PREC_FP32_FIXED)
+    _, b = make(d, native.IBG_PREC_FP32_FIXED)
+    a.run(1, 29)
+    b.run(1, 9)
+    g0 = b.timing()["list_growths"]
+    native.lib().ibg_set_list_rows(b._h, 1)  # step 10 rebuilds the lists
+    obs = b.run(10, 20, observe=True)
+    assert b.timing()["list_growths"] > g0
+    assert [o["STEP"] for o in obs] == list(range(10, 30))
+    sa, sb = a.state64(), b.state64()
+    assert np.array_equal(sa["sxyz"], sb["sxyz"])
+    assert np.array_equal(sa["vxyz"], sb["vxyz"])
+
+
 def test_lists_after_steps_match_reference(sysdir):
     """After the system has moved, the lists built from the current REAL*4
     state are again identical to the reference's."""
