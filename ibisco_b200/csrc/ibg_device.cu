@@ -80,7 +80,7 @@ struct DevList {
   size_t pos_bytes = 0;
   // tables of this list
   int *ltab = nullptr, *toff = nullptr, *tndat = nullptr;
-  void *tbin = nullptr, *tfp = nullptr, *tx = nullptr;
+  void *tbin = nullptr, *tinv = nullptr, *tfp = nullptr, *tx = nullptr;
   int ntab = 0, nrows = 0;
   size_t smem = 0;
   bool use_smem = false;
@@ -251,13 +251,15 @@ void build_list(ibg_ctx* c, const ibg_desc* d, int which) {
   L.toff = dupload(toff, o);
   L.tndat = dupload(tnd, o);
   if (c->prec == IBG_PREC_FP32_FIXED) {
-    std::vector<float> f1(fp.begin(), fp.end()), x1(xx.begin(), xx.end()), b1(bin.begin(), bin.end());
-    L.tfp = dupload(f1, o); L.tx = dupload(x1, o); L.tbin = dupload(b1, o);
+    std::vector<float> f1(fp.begin(), fp.end()), x1(xx.begin(), xx.end()), b1(bin.begin(), bin.end()), i1(bin.size());
+    for (size_t k = 0; k < bin.size(); ++k) i1[k] = (float)(1.0 / (double)(float)bin[k]);
+    L.tfp = dupload(f1, o); L.tx = dupload(x1, o); L.tbin = dupload(b1, o); L.tinv = dupload(i1, o);
   } else {
     L.tfp = dupload(fp, o); L.tx = dupload(xx, o); L.tbin = dupload(bin, o);
   }
   const size_t rs = rsize(c);
-  L.smem = 9 * 8 * sizeof(double) + rs * 3 * (size_t)L.nrows + rs * L.ntab + sizeof(int) * ((size_t)NT * NT + 2 * L.ntab + 1) + 64;
+  L.smem = 9 * 256 * sizeof(double) + rs * 3 * (size_t)L.nrows + 2 * rs * L.ntab +
+           sizeof(int) * ((size_t)NT * NT + 2 * L.ntab + 1) + 64;
   L.use_smem = L.smem <= 200 * 1024;
 }
 
@@ -357,31 +359,55 @@ template <typename R>
 using NBKernel = void (*)(NBArgs<R>, Scalars*);
 
 template <typename R>
-NBKernel<R> nb_kernel(bool smem, int T) {
+NBKernel<R> nb_kernel(bool smem, int T);
+
+template <>
+NBKernel<float> nb_kernel<float>(bool smem, int T) {
   if (smem) {
     switch (T) {
-      case 1: return k_nonbonded<R, true, 1>;
-      case 2: return k_nonbonded<R, true, 2>;
-      case 4: return k_nonbonded<R, true, 4>;
-      default: return k_nonbonded<R, true, 8>;
+      case 1: return k_nonbonded_f32<true, 1>;
+      case 2: return k_nonbonded_f32<true, 2>;
+      case 4: return k_nonbonded_f32<true, 4>;
+      default: return k_nonbonded_f32<true, 8>;
     }
   }
   switch (T) {
-    case 1: return k_nonbonded<R, false, 1>;
-    case 2: return k_nonbonded<R, false, 2>;
-    case 4: return k_nonbonded<R, false, 4>;
-    default: return k_nonbonded<R, false, 8>;
+    case 1: return k_nonbonded_f32<false, 1>;
+    case 2: return k_nonbonded_f32<false, 2>;
+    case 4: return k_nonbonded_f32<false, 4>;
+    default: return k_nonbonded_f32<false, 8>;
+  }
+}
+
+template <>
+NBKernel<double> nb_kernel<double>(bool smem, int T) {
+  if (smem) {
+    switch (T) {
+      case 1: return k_nonbonded<double, true, 1>;
+      case 2: return k_nonbonded<double, true, 2>;
+      case 4: return k_nonbonded<double, true, 4>;
+      default: return k_nonbonded<double, true, 8>;
+    }
+  }
+  switch (T) {
+    case 1: return k_nonbonded<double, false, 1>;
+    case 2: return k_nonbonded<double, false, 2>;
+    case 4: return k_nonbonded<double, false, 4>;
+    default: return k_nonbonded<double, false, 8>;
   }
 }
 
 template <typename R>
 void nb_configure(ibg_ctx* c, DevList& L) {
   NBKernel<R> k = nb_kernel<R>(L.use_smem, L.T);
-  if (L.use_smem) CK(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
   int per = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k, 256, L.use_smem ? L.smem : 9 * 64));
+  const size_t base = c->prec == IBG_PREC_FP32_FIXED ? 9 * 256 * sizeof(double) : 9 * 8 * sizeof(double);
+  const size_t sm = L.use_smem ? L.smem : base;
+  if (sm > 48 * 1024) CK(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k, 256, sm));
   per = std::max(1, per);
-  L.grid_nb = std::max(1, std::min(c->nsm * per, (L.nslices + 7) / 8));
+  const long long units = (long long)L.nslices * 4;
+  L.grid_nb = (int)std::max<long long>(1, std::min<long long>((long long)c->nsm * per, (units + 7) / 8));
 }
 
 template <typename R>
@@ -391,10 +417,12 @@ void enq_nonbonded(ibg_ctx* c, DevList& L) {
   A.pos4 = L.pos4; A.counts = L.counts; A.slice_w = L.slice_w; A.entries = L.entries;
   A.w_cap = L.w_cap; A.work = L.which;
   A.fsort = (typename Prec<R>::acc_t*)L.fsort;
-  A.ltab = L.ltab; A.toff = L.toff; A.tndat = L.tndat; A.tbin = (const R*)L.tbin; A.tfp = (const R*)L.tfp; A.tx = (const R*)L.tx;
+  A.ltab = L.ltab; A.toff = L.toff; A.tndat = L.tndat; A.tbin = (const R*)L.tbin; A.tinv = (const R*)L.tinv;
+  A.tfp = (const R*)L.tfp; A.tx = (const R*)L.tx;
   A.ntab = L.ntab; A.nrows = L.nrows; A.rcutsq = (R)L.rcutsq;
   A.part = L.part; A.part_stride = L.grid_nb;
-  const size_t sm = L.use_smem ? L.smem : 9 * 8 * sizeof(double);
+  const size_t base = c->prec == IBG_PREC_FP32_FIXED ? 9 * 256 * sizeof(double) : 9 * 8 * sizeof(double);
+  const size_t sm = L.use_smem ? L.smem : base;
   nb_kernel<R>(L.use_smem, L.T)<<<L.grid_nb, 256, sm, c->st>>>(A, c->sc);
   ++c->launches;
 }

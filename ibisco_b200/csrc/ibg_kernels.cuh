@@ -429,6 +429,7 @@ struct NBArgs {
   const int* toff;
   const int* tndat;
   const R* tbin;
+  const R* tinv; // 1/bin per table (FP32 force kernel)
   const R* tfp;  // 2 per row
   const R* tx;
   int ntab, nrows;
@@ -576,6 +577,162 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded(NBArgs<R> A, Scalars* sc) 
   __syncthreads();
   double out[9];
   block_sum<9>(acc, red, out);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 9; ++k) A.part[k * A.part_stride + blockIdx.x] = out[k];
+}
+
+// round(v * 2^32) for |v| < 2^31 with integer operations only (the
+// conversion unit is the busiest pipe of the pair loop).  Rounds half away
+// from zero in magnitude; exact antisymmetry between i and j is kept because
+// one conversion serves both.
+__device__ __forceinline__ long long f2fix(float v) {
+  const unsigned u = __float_as_uint(v);
+  const int e = (int)((u >> 23) & 0xffu);
+  const long long m = (long long)((u & 0x7fffffu) | 0x800000u);
+  const int sh = e - 118;  // v * 2^32 = m * 2^(e - 150 + 32)
+  long long mag;
+  if (sh >= 0) mag = m << min(sh, 39);
+  else if (sh > -25) mag = (m + (1LL << (-sh - 1))) >> (-sh);
+  else mag = 0;
+  return (u >> 31) ? -mag : mag;
+}
+
+// NONBONDED_FORCE.F90:173-232, FP32 force path.  Same structure as
+// k_nonbonded (slices of P = 32/T slots, T lanes per slot, dynamic units of
+// ROWS list rows).  The arithmetic is REAL*4 as in the reference, with
+// cheaper equivalents where only the force value (not a bit pattern) is
+// compared: minimum image by compare-and-select, r from rsqrt, the table row
+// and interpolation weight from a precomputed 1/bin, float-to-fixed on the
+// integer units.  Energies and virials are summed in FP32 over one unit and
+// then in FP64 in a per-lane shared-memory slot (a fixed order, so the sums are
+// reproducible).
+template <bool SMEM, int T>
+__global__ void __launch_bounds__(256, 4) k_nonbonded_f32(NBArgs<float> A, Scalars* sc) {
+  constexpr int PS = 32 / T;
+  constexpr int ROWS = 8;
+  extern __shared__ unsigned char smem_raw[];
+  double* lacc = (double*)smem_raw;  // [9][blockDim.x] per-lane sums
+  const int* ltab = A.ltab;
+  const int* toff = A.toff;
+  const int* tndat = A.tndat;
+  const float* tinv = A.tinv;
+  const float2* tfp = (const float2*)A.tfp;
+  const float* tx = A.tx;
+  {
+    unsigned char* p = smem_raw + 9 * 256 * sizeof(double);
+    if (SMEM) {
+      float2* s_fp = (float2*)p;     p += sizeof(float2) * A.nrows;
+      float* s_x = (float*)p;        p += sizeof(float) * A.nrows;
+      float* s_inv = (float*)p;      p += sizeof(float) * A.ntab;
+      int* s_ltab = (int*)p;         p += sizeof(int) * A.ntype * A.ntype;
+      int* s_toff = (int*)p;         p += sizeof(int) * (A.ntab + 1);
+      int* s_ndat = (int*)p;
+      for (int k = threadIdx.x; k < A.nrows; k += blockDim.x) { s_fp[k] = ((const float2*)A.tfp)[k]; s_x[k] = A.tx[k]; }
+      for (int k = threadIdx.x; k < A.ntab; k += blockDim.x) { s_inv[k] = A.tinv[k]; s_ndat[k] = A.tndat[k]; }
+      for (int k = threadIdx.x; k < A.ntype * A.ntype; k += blockDim.x) s_ltab[k] = A.ltab[k];
+      for (int k = threadIdx.x; k <= A.ntab; k += blockDim.x) s_toff[k] = A.toff[k];
+      ltab = s_ltab; toff = s_toff; tndat = s_ndat; tinv = s_inv; tfp = s_fp; tx = s_x;
+    }
+  }
+  for (int k = 0; k < 9; ++k) lacc[k * blockDim.x + threadIdx.x] = 0.0;
+  __syncthreads();
+  const float bx = sc->boxf[0], by = sc->boxf[1], bz = sc->boxf[2];
+  const float hx = sc->box2f[0], hy = sc->box2f[1], hz = sc->box2f[2];
+  const float4* pos = (const float4*)A.pos4;
+  const int lane = threadIdx.x & 31, grp = lane / T, q = lane % T;
+  unsigned err = 0;
+  const bool run = !sc->abort;
+  const int U = (A.w_cap + ROWS - 1) / ROWS;
+  const int nunits = A.nslices * U;
+  for (;;) {
+    int u = 0;
+    if (lane == 0) u = run ? (int)atomicAdd(&sc->work[A.work], 1u) : nunits;
+    u = __shfl_sync(0xffffffffu, u, 0);
+    if (u >= nunits) break;
+    const int g = u / U;
+    const int r0 = (u - g * U) * ROWS;
+    const int w = min(A.slice_w[g], A.w_cap);
+    if (r0 >= w) continue;
+    const int r1 = min(w, r0 + ROWS);
+    const int s = g * PS + grp;
+    const bool valid = s < A.n;
+    const int cnt = valid ? A.counts[s] : 0;
+    const int* ent = A.entries + (long long)g * A.w_cap * 32 + lane;
+    const float4 pi = valid ? pos[s] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const int wi = __float_as_int(pi.w);
+    const int ti = wi & 0xffff, li = wi >> 16;
+    long long fi0 = 0, fi1 = 0, fi2 = 0;
+    float e[3] = {0.f, 0.f, 0.f}, vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    auto pair = [&](int t, const float4& pj) {
+      float d0 = pi.x - pj.x, d1 = pi.y - pj.y, d2 = pi.z - pj.z;
+      d0 = d0 > hx ? d0 - bx : (d0 < -hx ? d0 + bx : d0);
+      d1 = d1 > hy ? d1 - by : (d1 < -hy ? d1 + by : d1);
+      d2 = d2 > hz ? d2 - bz : (d2 < -hz ? d2 + bz : d2);
+      const float r2 = __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, d0 * d0));
+      if (!(r2 < A.rcutsq)) return;
+      const int wj = __float_as_int(pj.w);
+      const int tj = wj & 0xffff, lj = wj >> 16;
+      const int tab = ltab[ti * A.ntype + tj];
+      if (tab < 0) { err |= EB_MISSING_TABLE; return; }
+      const float r = r2 * rsqrtf(r2);
+      const float ib = tinv[tab];
+      const int ni = (int)(r * ib);
+      if (ni > tndat[tab]) { err |= EB_TABLE_RANGE; return; }
+      const int row = toff[tab] + ni;
+      const float alpha = (r - tx[row]) * ib;
+      const float2 a0 = tfp[row], a1 = tfp[row + 1];
+      const float fij = __fmaf_rn(a1.x - a0.x, alpha, a0.x);
+      const float vij = __fmaf_rn(a1.y - a0.y, alpha, a0.y);
+      const int slot = li == 1 ? 0 : (li == 2 ? (lj == 2 ? 1 : (lj == 3 ? 2 : 3)) : (li == 3 ? 2 : 3));
+      if (slot < 3) e[slot] += vij;
+      const float fx = fij * d0, fy = fij * d1, fz = fij * d2;
+      if (!(fabsf(fx) < kFixMax && fabsf(fy) < kFixMax && fabsf(fz) < kFixMax)) { err |= EB_FIXED; return; }
+      const long long qx = f2fix(fx), qy = f2fix(fy), qz = f2fix(fz);
+      fi0 += qx; fi1 += qy; fi2 += qz;
+      atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 0], (unsigned long long)(-qx));
+      atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 1], (unsigned long long)(-qy));
+      atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 2], (unsigned long long)(-qz));
+      vir[0] = __fmaf_rn(fx, d0, vir[0]);
+      vir[1] = __fmaf_rn(fy, d1, vir[1]);
+      vir[2] = __fmaf_rn(fz, d2, vir[2]);
+      vir[3] = __fmaf_rn(fy, d0, vir[3]);
+      vir[4] = __fmaf_rn(fz, d0, vir[4]);
+      vir[5] = __fmaf_rn(fz, d1, vir[5]);
+    };
+    for (int it = r0; it < r1; it += 2) {
+      const bool v0 = it * T + q < cnt;
+      const bool v1 = it + 1 < r1 && (it + 1) * T + q < cnt;
+      const int t0 = v0 ? ent[it * 32] : 0;
+      const int t1 = v1 ? ent[(it + 1) * 32] : 0;
+      const float4 p0 = pos[t0];
+      const float4 p1 = pos[t1];
+      if (v0) pair(t0, p0);
+      if (v1) pair(t1, p1);
+    }
+#pragma unroll
+    for (int o = T / 2; o > 0; o >>= 1) {
+      fi0 += __shfl_down_sync(0xffffffffu, fi0, o, T);
+      fi1 += __shfl_down_sync(0xffffffffu, fi1, o, T);
+      fi2 += __shfl_down_sync(0xffffffffu, fi2, o, T);
+    }
+    if (q == 0 && valid && r0 * T < cnt) {
+      atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)s + 0], (unsigned long long)fi0);
+      atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)s + 1], (unsigned long long)fi1);
+      atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)s + 2], (unsigned long long)fi2);
+    }
+    double* la = lacc + threadIdx.x;
+    la[0] += (double)e[0];
+    la[blockDim.x] += (double)e[1];
+    la[2 * blockDim.x] += (double)e[2];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) la[(3 + k) * blockDim.x] += (double)vir[k];
+  }
+  if (err) atomicOr(&sc->err, err);
+  double acc[9];
+  for (int k = 0; k < 9; ++k) acc[k] = lacc[k * blockDim.x + threadIdx.x];
+  __syncthreads();
+  double out[9];
+  block_sum<9>(acc, lacc, out);
   if (threadIdx.x == 0)
     for (int k = 0; k < 9; ++k) A.part[k * A.part_stride + blockIdx.x] = out[k];
 }
