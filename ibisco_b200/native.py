@@ -32,7 +32,7 @@ EXPORTS = [
     "ibg_setup_array_i", "ibg_setup_array_f", "ibg_setup_free",
     "ibg_create", "ibg_set_state", "ibg_step", "ibg_forces", "ibg_run", "ibg_get_state",
     "ibg_get_state_f64", "ibg_get_neighbour_list", "ibg_get_exclusions", "ibg_set_timing",
-    "ibg_get_timing", "ibg_last_error", "ibg_destroy", "ibg_version", "ibg_set_l2_flush", "ibg_set_device", "ibg_set_list_rows",
+    "ibg_get_timing", "ibg_last_error", "ibg_destroy", "ibg_version", "ibg_set_l2_flush", "ibg_set_device", "ibg_set_list_rows", "ibg_nonbonded_static",
 ]
 
 
@@ -135,6 +135,9 @@ def lib(build_if_missing: bool = True):
         "ibg_set_l2_flush": (ctypes.c_int, [vp, ctypes.c_longlong]),
         "ibg_set_device": (ctypes.c_int, [ctypes.c_int]),
         "ibg_set_list_rows": (ctypes.c_int, [vp, ctypes.c_int]),
+        "ibg_nonbonded_static": (ctypes.c_int, [ctypes.c_int, ctypes.c_int] + [vp] * 5 + [ctypes.c_int, vp, ctypes.c_int, vp,
+                                                ctypes.c_int, ctypes.c_int] + [vp] * 5 + [vp, ctypes.c_float, vp, vp, vp,
+                                                                                        cp, ctypes.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -210,6 +210,36 @@ void ibg_destroy(ibg_ctx* c);
 /* Library version string. */
 const char* ibg_version(void);
 
+/* ---------------------------------------------------- no-allocation path --
+ * ibg_nonbonded_static: the nonbonded forces, energies and virial of one
+ * particle list, for callers that cannot allocate device memory at the time
+ * they need them (a host whose device memory all belongs to its own
+ * allocator, a call recorded into a CUDA graph, a loop that must not let
+ * cudaMalloc/cudaFree synchronise the device).  It has no counterpart in the
+ * reference: it is NONBONDED_FORCE on the reference's own arrays, offered
+ * without a context.  Every pointer except box, err and stream is device
+ * memory owned by the caller, in the reference's layout and 1-based ids:
+ * rxyz(3,nitems) wrapped positions, itype/type_label(nitems) (3 for virtual
+ * sites), index_list(n), list(maxnab,n), nnebs(nitems), inbondt(ntype,ntype),
+ * rnbond/nbond_force/nbond_pot(ld_nb,nnbtype), binnb/ndatnb(nnbtype).
+ * Outputs: fxyz(3,nitems) in FP64 (the forces of this list alone) and sums[9]
+ * = V_NB(1..3), PT11, PT22, PT33, PT12, PT13, PT23 (not divided by the volume).
+ * Scratch is a fixed __device__ array in the library, sized for
+ * IBG_STATIC_MAX_PARTICLES particles; larger inputs return IBG_E_CAPACITY.
+ * The first call on a device looks up that array's address with the device
+ * current, so make it before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (other streams, other host threads) race.
+ * The call is synchronous on `stream` (a cudaStream_t, may be NULL) and allocates
+ * nothing.  err (may be NULL) receives a message. */
+#define IBG_STATIC_MAX_PARTICLES 262144
+#define IBG_STATIC_MAX_BLOCKS 1024
+int ibg_nonbonded_static(int nitems, int n, const float* rxyz, const int* itype, const int* type_label,
+                         const int* index_list, const int* list, int maxnab, const int* nnebs, int ntype,
+                         const int* inbondt, int nnbtype, int ld_nb, const float* rnbond,
+                         const float* nbond_force, const float* nbond_pot, const float* binnb,
+                         const int* ndatnb, const float* box, float rcutsq, double* fxyz, double* sums,
+                         void* stream, char* err, int errlen);
+
 #ifdef __cplusplus
 }
 #endif
