@@ -7,8 +7,8 @@ A system is a directory with the files the reference reads: ``control``
 ``virtangles`` (RDVIRTANGLES.f90).  Units are the files' units: nm, ps,
 kJ/mol, degrees, kg/mol.
 
-``config1`` .. ``config4`` build the benchmark workloads (single-type LJ
-fluid, bead-spring melt, hybrid atom/CG melt, large CG melt); ``feature_mix``
+``lj_fluid``, ``polymer_melt`` and ``cg_melt`` build the benchmark
+workloads (single-type LJ fluid, bead-spring melt, large CG melt); ``feature_mix``
 builds a small system that exercises every term the step supports
 (bonds, angles, torsions, out-of-planes, exclusions with non_bonded 4 and 5,
 explicit beads, centre and centre-of-mass virtual sites, virtbonds,
@@ -334,7 +334,7 @@ def _all_torsion_keys(types):
 
 
 # ------------------------------------------------------------------ configs
-def config1(n=4000, rho=8.0, seed=1, nsteps=1000, dmin=0.3):
+def lj_fluid(n=4000, rho=8.0, seed=1, nsteps=1000, dmin=0.3):
     """Single-type LJ bead fluid: uniform positions rejected below dmin, LJ
     sigma 0.47 nm.  (With dmin 0.3 nm the first steps at dt 10 fs meet pair
     forces beyond the fixed-point range; a larger dmin avoids that.)"""
@@ -356,7 +356,7 @@ def config1(n=4000, rho=8.0, seed=1, nsteps=1000, dmin=0.3):
 
 def polymer_melt(nchains=400, nper=100, rho=20.0, ntypes=3, seed=2, nsteps=5000, temp=500.0, dt=0.001,
                  rcut=1.0, rlist=1.2, nupdate=10, ensemble="NVT", mass=0.014, bond=0.153, theta0=112.0):
-    """Bead-spring melt with tabulated bond/angle/torsion."""
+    """Bead-spring melt with tabulated bond/angle/torsion: 400 chains x 100 beads by default."""
     rng = np.random.default_rng(seed)
     n = nchains * nper
     box = (n / rho) ** (1.0 / 3.0)
@@ -384,12 +384,8 @@ def polymer_melt(nchains=400, nper=100, rho=20.0, ntypes=3, seed=2, nsteps=5000,
                  for a in types for b in types if a <= b])
 
 
-def config2(**kw):
-    return polymer_melt(**kw)
-
-
-def config4(nchains=10000, nper=200, rho=8.0, seed=4, nsteps=2000):
-    """Large CG melt for the roofline study."""
+def cg_melt(nchains=10000, nper=200, rho=8.0, seed=4, nsteps=2000):
+    """Large CG melt for the roofline study: 10,000 chains x 200 beads (2,000,000) by default."""
     spec = polymer_melt(nchains=nchains, nper=nper, rho=rho, ntypes=4, seed=seed, nsteps=nsteps, temp=300.0,
                         dt=0.010, rcut=1.4, rlist=1.6, mass=0.072, bond=0.47, theta0=120.0)
     types = [1, 2, 3, 4]

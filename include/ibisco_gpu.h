@@ -3,7 +3,7 @@
  *
  * The Fortran host keeps its input/setup phase (main.F90:107-237) and its
  * observables/output (AVERAGE.f90, OUTPUT.F90, WRITETRJ.F90) and replaces the
- * body of its MD loop (NEW_LOOP.F90:327-390, MTS_LOOP.f90:26-44) by calls into
+ * body of its MD loop (NEW_LOOP.F90:66-124, MTS_LOOP.f90:26-44) by calls into
  * this library.  Every entry point is plain C: pointers, sizes and status
  * codes; arrays are passed in the Fortran layout of the reference's MODULE VAR
  * (module_var.F90), column-major with 1-based particle ids.
@@ -159,7 +159,7 @@ void ibg_setup_free(ibg_setup* s);
  *   VXYZ(3,NATOMS), box(3); then runs the reference's pre-loop
  *   initialisation (main.F90:150-234: virtual sites, SHIFT, initial
  *   temperatures, cell maps, first Verlet lists).
- * ibg_step: one loop body (NEW_LOOP.F90:327-384 or MTS_LOOP.f90:26-44) for
+ * ibg_step: one loop body (NEW_LOOP.F90:66-124 or MTS_LOOP.f90:26-44) for
  *   step number `step`; `out` (may be NULL) receives the observables.
  * ibg_forces: the same body up to and including the force stage, without
  *   MOVE/MOMENTUM/SCALEBP (for force parity checks).

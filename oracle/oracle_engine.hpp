@@ -807,7 +807,7 @@ struct Engine {
     update_neighbourlist();
   }
 
-  // one body of NEW_LOOP.F90:288-415 / MTS_LOOP.f90:24-53 without I/O
+  // one body of NEW_LOOP.F90:66-124 / MTS_LOOP.f90:24-44 without I/O
   void force_stage(int step) {
     shift();
     if (s->IBRDESCR == 0 || s->NMTS > 0) virtual_def();

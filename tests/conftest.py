@@ -46,7 +46,7 @@ def sysdir(tmp_path_factory):
     base = tmp_path_factory.mktemp("systems")
     made = {}
     builders = {
-        "fluid": lambda: synth.config1(n=1500, seed=11, nsteps=50, dmin=0.42),
+        "fluid": lambda: synth.lj_fluid(n=1500, seed=11, nsteps=50, dmin=0.42),
         "melt": lambda: synth.polymer_melt(nchains=24, nper=40, seed=12, nsteps=50),
         "mix4": lambda: synth.feature_mix(seed=7, non_bonded=4),
         "mix5_mts": lambda: synth.feature_mix(seed=8, non_bonded=5, nmts=3),
