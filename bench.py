@@ -17,6 +17,13 @@ Legs:
              from pinned host arrays, K x ibg_step with its observables read
              back each step, ibg_get_state at the end;
   fp64_plain the same K steps on the plain FP64 path (comparison path);
+  batched    B independent copies of the workload stepped as one batch
+             (ibg_batch: one launch per stage over all systems, one CUDA graph
+             per batch step), against the single-system FP64 path;
+  serving    a seeded stream of jobs of mixed sizes with Poisson arrivals,
+             replayed against the continuous-batching server (ibg_server),
+             p50/p99 latency and jobs/s, against the same jobs run one after
+             another on the plain FP64 path;
   roofline   nonbonded kernel, the dominant launch: algorithmic bytes per
              launch (16 B position + 4 B per listed pair, per particle) over its
              event-timed average duration, against the measured HBM copy peak;
@@ -232,6 +239,63 @@ def run_reference(args, world, rank, pg):
         print(json.dumps(line), flush=True)
 
 
+def run_serving(args, world, rank, local, pg, workdir):
+    """Served job stream: the first J jobs of a seeded stream (sizes log-uniform
+    in 500..50,000 beads, 1-3 types, chains of 10-100, per-job perturbed LJ
+    tables, Poisson arrivals at 20 jobs/s), replayed in wall-clock time against
+    the continuous-batching server; then the same jobs one after another on the
+    plain FP64 path, served in arrival order (computed from the measured
+    per-job times).  Jobs are split over ranks (no collective on the data
+    path); latencies and throughput are over all ranks."""
+    from ibisco_b200 import native, serving, synth
+
+    stream = synth.job_stream(args.serve_jobs, seed=5)
+    base = os.path.join(workdir, "serve")
+    jobs = serving.stream_dirs(base, stream, args.serve_steps)
+    mine = serving.partition(jobs, rank, world)
+    barrier(pg)
+    srv = native.Server(device=local, tick_steps=args.serve_tick, max_jobs=256)
+    records, ids = serving.replay(srv, mine)
+    st = srv.stats()
+    srv.close()
+    atom_steps = float(sum(j.particles * j.nsteps for j in mine))
+    # plain FP64 path, one job at a time
+    service = []
+    for j in sorted(mine, key=lambda j: j.arrival_s):
+        t0 = time.perf_counter()
+        g = native.System(native.Setup(j.directory), native.IBG_PREC_FP64_PLAIN)
+        g.set_state()
+        g.run(1, j.nsteps)
+        g.state()
+        g.close()
+        service.append(time.perf_counter() - t0)
+    arr = [j.arrival_s for j in sorted(mine, key=lambda j: j.arrival_s)]
+    serial = list(zip(arr, serving.serial_schedule(arr, service)))
+    all_served = serving.merge(pg, records)
+    all_serial = serving.merge(pg, serial)
+    total_as = reduce_sum(pg, atom_steps)
+    out = {"jobs": len(all_served), "stream": f"first {args.serve_jobs} jobs of the seeded 20 jobs/s stream",
+           "steps_per_job": args.serve_steps, "tick_steps": args.serve_tick,
+           "served": serving.summarize(all_served, total_as),
+           "serial_fp64_plain": serving.summarize(all_serial, total_as),
+           "server": {k: st[k] for k in ("peak_jobs", "peak_bytes", "budget_bytes", "ticks", "batch_builds", "gpu_s")}}
+    s_, p_ = out["served"], out["serial_fp64_plain"]
+    if s_.get("jobs_per_s") and p_.get("jobs_per_s"):
+        out["jobs_per_s_ratio"] = s_["jobs_per_s"] / p_["jobs_per_s"]
+        out["p99_ratio"] = p_["p99_s"] / s_["p99_s"]
+    return out
+
+
+def reduce_sum(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t)
+    return float(t.item())
+
+
 def run_b200(args, world, rank, local, pg):
     import ctypes
 
@@ -316,6 +380,34 @@ def run_b200(args, world, rank, local, pg):
             fp64 = {"value": world * n * args.steps / (ms64 / 1000.0), "ms_per_step": ms64 / args.steps,
                     "ratio_fp32_fixed_over_fp64": ms64 / ms}
             g64.close()
+        # ---- batched form: B independent copies of the workload, one launch per
+        # stage over all of them (ibg_batch); device time, state resident
+        batched = None
+        if prec == native.IBG_PREC_FP32_FIXED and args.batch > 1:
+            systems = []
+            for _ in range(args.batch):
+                gb = native.System(setup, native.IBG_PREC_FP32_FIXED)
+                gb.set_state(s0, v0, b0)
+                systems.append(gb)
+            bat = native.Batch(systems)
+            bat.run(args.warmup)
+            barrier(pg)
+            with Clocks(local) as clk_b:
+                bat.run(args.steps)
+            bms = reduce_max(pg, bat.timing()["run_ms"])
+            bval = world * args.batch * n * args.steps / (bms / 1000.0)
+            batched = {"systems": args.batch, "value": bval, "unit": "atom-steps/s",
+                       "ms_per_step": bms / args.steps, "particles_per_step": args.batch * n,
+                       "l2": "not flushed; the batch's working set exceeds the 126 MB L2",
+                       "clocks": clk_b.summary()}
+            if fp64:
+                batched["ratio_over_fp64_plain_single"] = bval / fp64["value"]
+            bat.close()
+            for gb in systems:
+                gb.close()
+        serving = None
+        if args.serve_jobs > 0 and prec == native.IBG_PREC_FP32_FIXED:
+            serving = run_serving(args, world, rank, local, pg, d)
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu:
             cpu = cpu_baseline(d, n)
@@ -334,7 +426,8 @@ def run_b200(args, world, rank, local, pg):
                            "l2": "flushed before every step (256 MiB write, outside the timed interval)"},
                 "ns_per_day": steps_per_s * dt_ps * 1e-3 * 86400.0,
                 "roofline": roof, "stage_ms_per_step": stage,
-                "cpu_baseline": cpu, "e2e": e2e, "fp64_plain": fp64, "gpu_launches": launches,
+                "cpu_baseline": cpu, "e2e": e2e, "fp64_plain": fp64, "batched": batched, "serving": serving,
+                "gpu_launches": launches,
                 "clocks": clk.summary(),
             }
             print(json.dumps(line), flush=True)
@@ -351,6 +444,10 @@ def main():
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--batch", type=int, default=8, help="systems in the batched leg (0 or 1: no batched leg)")
+    ap.add_argument("--serve-jobs", type=int, default=48, help="jobs of the served stream (0: no serving leg)")
+    ap.add_argument("--serve-steps", type=int, default=2000)
+    ap.add_argument("--serve-tick", type=int, default=100)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local, pg = dist_setup()

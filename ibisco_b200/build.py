@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 LIB = os.path.join(HERE, "libibisco_b200.so")
 
-SOURCES = ["ibg_device.cu", "host_setup.cpp", "ibg_static.cu"]
+SOURCES = ["ibg_device.cu", "host_setup.cpp", "ibg_static.cu", "ibg_server.cpp"]
 HEADERS = ["ibg_common.cuh", "ibg_kernels.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",

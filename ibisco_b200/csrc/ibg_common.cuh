@@ -56,12 +56,49 @@ struct Scalars {
   double sp[10];
   unsigned err;
   int abort;          // a list outgrew its storage: the rest of the run is a no-op
+  int skip;           // this step does nothing (aborted run, or the step limit reached)
+  int stop_at;        // last step this system runs (batched runs stop each system here)
+  int done;           // stop_at reached: set by the last step's k_finalize
   int need_rows[2];   // rows of 32 entries a slice of each list needed
   unsigned work[4];   // dynamic work counters: nonbonded atom/bead, list build atom/bead
+  // nonbonded V_NB(1..3) and PT11..PT23 of the atom / bead list: 64-bit fixed
+  // point at 2^-24 (FP32 path; order independent) or double (FP64 path)
+  unsigned long long nbacc[2][9];
   unsigned long long bond_overext, cell_clamps;
   double mom[3];     // momentum removal (MOMENTUM.f90)
   ObsD obs;          // observables of the last step
 };
+
+constexpr double kEnInv = 1.0 / 16777216.0;  // 2^-24, energy/virial fixed point
+
+// Blocks of a batched launch.  Block b of the grid serves system sys_of[b] as
+// its local block b - start[s] of start[s+1] - start[s].  A single-system
+// launch (B = false) uses the whole grid.
+struct BlockMap {
+  const int* sys_of;
+  const int* start;
+};
+struct Blk {
+  int sys, b, g;
+};
+template <bool B>
+__device__ __forceinline__ Blk blk(const BlockMap& m) {
+  if (!B) return Blk{0, (int)blockIdx.x, (int)gridDim.x};
+  const int s = __ldg(m.sys_of + blockIdx.x);
+  const int b0 = __ldg(m.start + s);
+  return Blk{s, (int)blockIdx.x - b0, __ldg(m.start + s + 1) - b0};
+}
+
+// Copy one system's argument block into shared memory (every thread of the
+// block takes part; returns after a barrier).  Batched kernels whose bodies
+// keep many argument fields live read them from there instead of holding them
+// in registers.
+template <typename T>
+__device__ __forceinline__ void stage_args(T* dst, const T* src) {
+  static_assert(sizeof(T) % 4 == 0, "argument blocks are whole words");
+  for (int i = threadIdx.x; i < (int)(sizeof(T) / 4); i += blockDim.x) ((int*)dst)[i] = ((const int*)src)[i];
+  __syncthreads();
+}
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -86,6 +123,26 @@ __device__ __forceinline__ void block_sum(double (&v)[K], double* smem, double* 
       for (int w = 0; w < nw; ++w) s += smem[w * K + k];
       out[k] = s;
     }
+  }
+  __syncthreads();
+}
+
+// Exact block sum of K 64-bit integers per thread; the results are left in
+// smem[0..K-1] (needs 32 + 32*K entries of shared memory) for every thread.
+template <int K>
+__device__ __forceinline__ void block_sum_i64(long long (&v)[K], long long* smem) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  if (lane == 0)
+    for (int k = 0; k < K; ++k) smem[32 + warp * K + k] = v[k];
+  __syncthreads();
+  if (threadIdx.x < K) {
+    long long s = 0;
+    for (int w = 0; w < nw; ++w) s += smem[32 + w * K + threadIdx.x];
+    smem[threadIdx.x] = s;
   }
   __syncthreads();
 }

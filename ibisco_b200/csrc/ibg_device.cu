@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -44,17 +45,39 @@ struct CudaError {
     if (e_ != cudaSuccess) throw CudaError{e_}; \
   } while (0)
 
+// Device allocations of a context or batch, with their sizes (the device
+// footprint that admission control accounts for).
+struct Owned {
+  std::vector<std::pair<void*, size_t>> a;
+  size_t bytes = 0;
+  void add(void* p, size_t n) { a.emplace_back(p, n); bytes += n; }
+  void release(void* p) {
+    for (size_t k = 0; k < a.size(); ++k)
+      if (a[k].first == p) {
+        bytes -= a[k].second;
+        a.erase(a.begin() + (long)k);
+        cudaFree(p);
+        return;
+      }
+  }
+  void free_all() {
+    for (auto& x : a) cudaFree(x.first);
+    a.clear();
+    bytes = 0;
+  }
+};
+
 template <typename T>
-T* dalloc(size_t n, std::vector<void*>& owned) {
+T* dalloc(size_t n, Owned& owned) {
   void* p = nullptr;
   if (n == 0) n = 1;
   CK(cudaMalloc(&p, n * sizeof(T)));
   CK(cudaMemset(p, 0, n * sizeof(T)));
-  owned.push_back(p);
+  owned.add(p, n * sizeof(T));
   return (T*)p;
 }
 template <typename T>
-T* dupload(const std::vector<T>& h, std::vector<void*>& owned) {
+T* dupload(const std::vector<T>& h, Owned& owned) {
   T* p = dalloc<T>(h.size(), owned);
   if (!h.empty()) CK(cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
   return p;
@@ -86,7 +109,22 @@ struct DevList {
   bool use_smem = false;
   float rlist = 0, rlistsq = 0, rcutsq = 0;
   int grid_nb = 0;
-  double* part = nullptr;
+};
+
+// Argument blocks of every kernel of one system.  The host copy is passed by
+// value to single-system launches; a device copy serves batched launches,
+// which read it through a table of per-system pointers.
+template <typename R>
+struct SysArgs {
+  PosArgs pos;
+  ListArgs list[2];
+  NBArgs<R> nb[2];
+  CollectArgs<R> col[2];
+  DistArgs<R> dist;
+  BondedArgs<R> bond;
+  MoveArgs<R> move;
+  MomArgs mom;
+  FinalArgs fin;
 };
 
 }  // namespace
@@ -96,7 +134,7 @@ struct ibg_ctx {
   int dev = 0, nsm = 148;
   cudaStream_t st = nullptr, st2 = nullptr;  // st2: bonded branch of a step
   cudaEvent_t fork_ev[2] = {nullptr, nullptr};
-  std::vector<void*> owned;
+  Owned owned;
   std::string err;
   // descriptor scalars
   int natoms = 0, nvirta = 0, nitems = 0, ntype = 0, numatoms = 0, numbeads = 0, ncoarse = 0;
@@ -119,12 +157,18 @@ struct ibg_ctx {
   float *tb_bin = nullptr, *ta_bin = nullptr, *tt_bin = nullptr, *to_bin = nullptr;
   DevList L[2];
   Scalars* sc = nullptr;
+  SysArgs<float> af;
+  SysArgs<double> ad;
+  void* dargs = nullptr;  // device copy of af or ad
+  int g_list[2] = {1, 1}, g_regrid[2] = {1, 1}, g_build[2] = {1, 1}, g_dist = 1;
   ObsD* ring = nullptr;
   int ring_cap = 0;
   double *p_b = nullptr, *p_mv = nullptr, *p_mom = nullptr;
   int g_b = 0, g_mv = 0, g_pos = 0;
   bool fb_dirty = false;
   bool state_set = false;
+  int step_now = 0;  // last completed step (host mirror of the device counter)
+  bool in_batch = false;
   std::map<unsigned, cudaGraphExec_t> graphs;
   std::vector<cudaGraph_t> graph_defs;
   long long launches_per_variant[32] = {0};
@@ -275,19 +319,6 @@ void alloc_cells(ibg_ctx* c, DevList& L, const float* box) {
   L.cell_fill = dalloc<int>(ncap, o);
 }
 
-ListArgs list_args(ibg_ctx* c, DevList& L) {
-  ListArgs a;
-  a.n = L.n; a.which = L.which; a.natoms = c->natoms; a.hybrid = c->ibrdescr == 0; a.maxnab = c->maxnab;
-  a.cell_cap = L.cell_cap;
-  a.rlist = L.rlist; a.rlistsq = L.rlistsq; a.rlistd = (double)L.rlist; a.rlistsqd = (double)L.rlist * (double)L.rlist;
-  a.idx = L.idx; a.cell_of = L.cell_of; a.cell_count = L.cell_count; a.cell_start = L.cell_start; a.cell_fill = L.cell_fill;
-  a.sorted = L.sorted; a.sorted_new = L.sorted_new; a.slot_of = L.slot_of; a.slot_of_new = L.slot_of_new;
-  a.gslot = c->gslot; a.pos4 = L.pos4; a.pos4_new = L.pos4_new;
-  a.counts = L.counts; a.slice_w = L.slice_w; a.entries = L.entries; a.w_cap = L.w_cap;
-  a.excl_n = c->excl_n; a.excl = c->excl;
-  return a;
-}
-
 int grid_for(ibg_ctx* c, long long work, int per_sm = 8) {
   long long g = (work + 255) / 256;
   return (int)std::max<long long>(1, std::min<long long>(g, (long long)c->nsm * per_sm));
@@ -320,135 +351,55 @@ void collect_marks(ibg_ctx* c) {
 }
 
 template <typename R>
-void enq_positions(ibg_ctx* c, int begin = 0) {
-  PosArgs a;
-  a.begin = begin; a.nupdate = c->nupdate; a.nmts = c->nmts;
-  a.natoms = c->natoms; a.nvirta = c->nvirta; a.S = c->S; a.Svs = c->S + 3 * (size_t)c->natoms;
-  a.tbits = c->tbits; a.gslot = c->gslot;
-  a.pos4[0] = c->L[0].pos4; a.pos4[1] = c->L[1].pos4;
-  a.vcenter = c->vcenter; a.vnum = c->vnum; a.vmem = c->vmem; a.vmass = c->vmass; a.vinv = c->vinv;
-  k_positions<R><<<c->g_pos, 256, 0, c->st>>>(a, c->sc);
-  ++c->launches;
-}
-
-template <typename R>
-void enq_rebuild(ibg_ctx* c, DevList& L) {
-  if (!L.present) return;
-  ListArgs a = list_args(c, L);
-  const int gn = grid_for(c, L.n);
-  k_regrid<R><<<1, 32, 0, c->st>>>(a, c->sc);
-  CK(cudaMemsetAsync(L.cell_count, 0, sizeof(int) * L.cell_cap, c->st));
-  k_cell_assign<R><<<gn, 256, 0, c->st>>>(a, c->sc);
-  k_scan_int<<<1, 1024, 0, c->st>>>(L.cell_count, L.cell_start, L.cell_cap, L.cell_fill);
-  k_cell_fill<<<gn, 256, 0, c->st>>>(a);
-  k_cell_rank<<<gn, 256, 0, c->st>>>(a, c->sc);
-  k_reslot<R><<<gn, 256, 0, c->st>>>(a);
-  CK(cudaMemcpyAsync(L.pos4, L.pos4_new, L.pos_bytes, cudaMemcpyDeviceToDevice, c->st));
-  k_slot_of<<<gn, 256, 0, c->st>>>(a);
-  const int gl = std::max(1, std::min(L.nslices / 8 + 1, c->nsm * 8));
-  switch (L.T) {
-    case 1: k_list_build<R, 1><<<gl, 256, 0, c->st>>>(a, c->sc); break;
-    case 2: k_list_build<R, 2><<<gl, 256, 0, c->st>>>(a, c->sc); break;
-    case 4: k_list_build<R, 4><<<gl, 256, 0, c->st>>>(a, c->sc); break;
-    default: k_list_build<R, 8><<<gl, 256, 0, c->st>>>(a, c->sc); break;
-  }
-  c->launches += 8;
-}
-
-template <typename R>
-using NBKernel = void (*)(NBArgs<R>, Scalars*);
-
-template <typename R>
-NBKernel<R> nb_kernel(bool smem, int T);
-
+SysArgs<R>& args(ibg_ctx* c);
 template <>
-NBKernel<float> nb_kernel<float>(bool smem, int T) {
-  if (smem) {
-    switch (T) {
-      case 1: return k_nonbonded_f32<true, 1>;
-      case 2: return k_nonbonded_f32<true, 2>;
-      case 4: return k_nonbonded_f32<true, 4>;
-      default: return k_nonbonded_f32<true, 8>;
-    }
-  }
-  switch (T) {
-    case 1: return k_nonbonded_f32<false, 1>;
-    case 2: return k_nonbonded_f32<false, 2>;
-    case 4: return k_nonbonded_f32<false, 4>;
-    default: return k_nonbonded_f32<false, 8>;
-  }
-}
-
+SysArgs<float>& args<float>(ibg_ctx* c) { return c->af; }
 template <>
-NBKernel<double> nb_kernel<double>(bool smem, int T) {
-  if (smem) {
-    switch (T) {
-      case 1: return k_nonbonded<double, true, 1>;
-      case 2: return k_nonbonded<double, true, 2>;
-      case 4: return k_nonbonded<double, true, 4>;
-      default: return k_nonbonded<double, true, 8>;
-    }
+SysArgs<double>& args<double>(ibg_ctx* c) { return c->ad; }
+
+// Fill the argument blocks from the context's current arrays and sizes.
+template <typename R>
+void make_args(ibg_ctx* c) {
+  using acc_t = typename Prec<R>::acc_t;
+  SysArgs<R>& A = args<R>(c);
+  std::memset(&A, 0, sizeof(A));
+  Scalars* sc = c->sc;
+  PosArgs& p = A.pos;
+  p.sc = sc; p.natoms = c->natoms; p.nvirta = c->nvirta; p.nupdate = c->nupdate; p.nmts = c->nmts;
+  p.S = c->S; p.Svs = c->S + 3 * (size_t)c->natoms; p.tbits = c->tbits; p.gslot = c->gslot;
+  p.pos4[0] = c->L[0].pos4; p.pos4[1] = c->L[1].pos4;
+  p.vcenter = c->vcenter; p.vnum = c->vnum; p.vmem = c->vmem; p.vmass = c->vmass; p.vinv = c->vinv;
+  for (int w = 0; w < 2; ++w) {
+    DevList& L = c->L[w];
+    ListArgs& a = A.list[w];
+    a.sc = sc;
+    a.n = L.n; a.which = w; a.natoms = c->natoms; a.hybrid = c->ibrdescr == 0; a.maxnab = c->maxnab;
+    a.cell_cap = L.cell_cap;
+    a.rlist = L.rlist; a.rlistsq = L.rlistsq; a.rlistd = (double)L.rlist; a.rlistsqd = (double)L.rlist * (double)L.rlist;
+    a.idx = L.idx; a.cell_of = L.cell_of; a.cell_count = L.cell_count; a.cell_start = L.cell_start;
+    a.cell_fill = L.cell_fill;
+    a.sorted = L.sorted; a.sorted_new = L.sorted_new; a.slot_of = L.slot_of; a.slot_of_new = L.slot_of_new;
+    a.gslot = c->gslot; a.pos4 = L.pos4; a.pos4_new = L.pos4_new;
+    a.counts = L.counts; a.slice_w = L.slice_w; a.entries = L.entries; a.w_cap = L.w_cap;
+    a.excl_n = c->excl_n; a.excl = c->excl;
+    NBArgs<R>& n = A.nb[w];
+    n.sc = sc; n.mts = (w == 1 && c->nmts > 0);
+    n.n = L.n; n.nslices = L.nslices; n.ntype = c->ntype;
+    n.pos4 = L.pos4; n.counts = L.counts; n.slice_w = L.slice_w; n.entries = L.entries;
+    n.w_cap = L.w_cap; n.work = w;
+    n.fsort = (acc_t*)L.fsort;
+    n.ltab = L.ltab; n.toff = L.toff; n.tndat = L.tndat; n.tbin = (const R*)L.tbin; n.tinv = (const R*)L.tinv;
+    n.tfp = (const R*)L.tfp; n.tx = (const R*)L.tx;
+    n.ntab = L.ntab; n.nrows = L.nrows; n.rcutsq = (R)L.rcutsq;
+    CollectArgs<R>& k = A.col[w];
+    k.sc = sc; k.n = L.n; k.mts = (w == 1 && c->nmts > 0); k.sorted = L.sorted; k.idx = L.idx;
+    k.fsort = (acc_t*)L.fsort; k.fnb = (acc_t*)c->fnb; k.mtsf = (acc_t*)L.mtsf;
   }
-  switch (T) {
-    case 1: return k_nonbonded<double, false, 1>;
-    case 2: return k_nonbonded<double, false, 2>;
-    case 4: return k_nonbonded<double, false, 4>;
-    default: return k_nonbonded<double, false, 8>;
-  }
-}
-
-template <typename R>
-void nb_configure(ibg_ctx* c, DevList& L) {
-  NBKernel<R> k = nb_kernel<R>(L.use_smem, L.T);
-  int per = 0;
-  const size_t base = c->prec == IBG_PREC_FP32_FIXED ? 9 * 256 * sizeof(double) : 9 * 8 * sizeof(double);
-  const size_t sm = L.use_smem ? L.smem : base;
-  if (sm > 48 * 1024) CK(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k, 256, sm));
-  per = std::max(1, per);
-  const long long units = (long long)L.nslices * 4;
-  L.grid_nb = (int)std::max<long long>(1, std::min<long long>((long long)c->nsm * per, (units + 7) / 8));
-}
-
-template <typename R>
-void enq_nonbonded(ibg_ctx* c, DevList& L) {
-  NBArgs<R> A;
-  A.n = L.n; A.nslices = L.nslices; A.ntype = c->ntype;
-  A.pos4 = L.pos4; A.counts = L.counts; A.slice_w = L.slice_w; A.entries = L.entries;
-  A.w_cap = L.w_cap; A.work = L.which;
-  A.fsort = (typename Prec<R>::acc_t*)L.fsort;
-  A.ltab = L.ltab; A.toff = L.toff; A.tndat = L.tndat; A.tbin = (const R*)L.tbin; A.tinv = (const R*)L.tinv;
-  A.tfp = (const R*)L.tfp; A.tx = (const R*)L.tx;
-  A.ntab = L.ntab; A.nrows = L.nrows; A.rcutsq = (R)L.rcutsq;
-  A.part = L.part; A.part_stride = L.grid_nb;
-  const size_t base = c->prec == IBG_PREC_FP32_FIXED ? 9 * 256 * sizeof(double) : 9 * 8 * sizeof(double);
-  const size_t sm = L.use_smem ? L.smem : base;
-  nb_kernel<R>(L.use_smem, L.T)<<<L.grid_nb, 256, sm, c->st>>>(A, c->sc);
-  ++c->launches;
-}
-
-template <typename R>
-void enq_collect(ibg_ctx* c, DevList& L) {
-  CollectArgs<R> C;
-  C.n = L.n; C.mts = (L.which == 1 && c->nmts > 0); C.sorted = L.sorted; C.idx = L.idx;
-  C.fsort = (typename Prec<R>::acc_t*)L.fsort; C.fnb = (typename Prec<R>::acc_t*)c->fnb;
-  C.mtsf = (typename Prec<R>::acc_t*)L.mtsf;
-  k_nb_collect<R><<<grid_for(c, L.n), 256, 0, c->st>>>(C, c->sc);
-  ++c->launches;
-}
-
-template <typename R>
-void enq_distribute(ibg_ctx* c, void* F) {
-  if (c->nvirta == 0) return;
-  k_distribute<R><<<grid_for(c, c->nvirta), 256, 0, c->st>>>((typename Prec<R>::acc_t*)F, c->natoms, c->nvirta, c->vnum,
-                                                           c->vmem, c->vcoef, c->sc);
-  ++c->launches;
-}
-
-template <typename R>
-void enq_bonded(ibg_ctx* c) {
-  BondedArgs<R> B;
-  B.su = c->S; B.fb = (typename Prec<R>::acc_t*)c->fb;
+  DistArgs<R>& d = A.dist;
+  d.sc = sc; d.F[0] = (acc_t*)c->fnb; d.F[1] = (acc_t*)c->fb; d.natoms = c->natoms; d.nvirta = c->nvirta;
+  d.vnum = c->vnum; d.vmem = c->vmem; d.vcoef = c->vcoef;
+  BondedArgs<R>& B = A.bond;
+  B.sc = sc; B.su = c->S; B.fb = (acc_t*)c->fb;
   B.nb = c->nb; B.na = c->na; B.nt = c->nt; B.no = c->no;
   B.bonds = c->bonds; B.angles = c->angles; B.tors = c->tors; B.tors_t = c->tors_t; B.oops = c->oops; B.oops_t = c->oops_t;
   B.tb = c->tb; B.tb_off = c->tb_off; B.tb_ndat = c->tb_nd; B.tb_bin = c->tb_bin;
@@ -456,50 +407,195 @@ void enq_bonded(ibg_ctx* c) {
   B.tt = c->tt; B.tt_off = c->tt_off; B.tt_ndat = c->tt_nd; B.tt_bin = c->tt_bin;
   B.to = c->to; B.to_off = c->to_off; B.to_ndat = c->to_nd; B.to_bin = c->to_bin;
   B.r2d = c->r2d; B.part = c->p_b; B.part_stride = c->g_b;
-  k_bonded<R><<<c->g_b, 256, 0, c->st>>>(B, c->sc);
+  MoveArgs<R>& M = A.move;
+  M.sc = sc; M.natoms = c->natoms; M.S = c->S; M.V = c->V;
+  M.fnb = (acc_t*)c->fnb; M.fb = (acc_t*)c->fb;
+  M.tbits = c->tbits; M.mass = c->mass; M.invmass = c->invmass; M.dt = (double)c->dt; M.update = 1;
+  M.part = c->p_mv; M.part_stride = c->g_mv;
+  MomArgs& m = A.mom;
+  m.sc = sc; m.natoms = c->natoms; m.halt_drift = c->halt_drift; m.V = c->V; m.mass = c->mass; m.invmass = c->invmass;
+  m.part = c->p_mom; m.nblocks = c->g_mv;
+  FinalArgs& F = A.fin;
+  F.sc = sc; F.fixed = c->prec == IBG_PREC_FP32_FIXED;
+  F.p_b = c->p_b; F.g_b = c->g_b; F.p_mv = c->p_mv; F.g_mv = c->g_mv;
+  F.mts = c->nmts > 0; F.move = 1; F.ensemble = c->ensemble;
+  F.temp_in = c->temp_in; F.fac = c->fac; F.pfac = c->pfac; F.pressure = c->pressure;
+  F.mktemp = c->mktemp; F.mktemp_atom = c->mktemp_atom; F.mktemp_bead = c->mktemp_bead;
+  F.ring = c->ring; F.ring_cap = c->ring_cap;
+}
+
+// Rebuild the argument blocks and their device copy (after any change of the
+// context's arrays: creation, cell storage, list storage, observable ring).
+void refresh_args(ibg_ctx* c) {
+  size_t bytes;
+  const void* src;
+  if (c->prec == IBG_PREC_FP32_FIXED) { make_args<float>(c); bytes = sizeof(c->af); src = &c->af; }
+  else { make_args<double>(c); bytes = sizeof(c->ad); src = &c->ad; }
+  if (!c->dargs) c->dargs = dalloc<unsigned char>(bytes, c->owned);
+  CK(cudaMemcpy(c->dargs, src, bytes, cudaMemcpyHostToDevice));
+}
+
+const BlockMap kOne{nullptr, nullptr};
+
+template <typename R>
+void enq_positions(ibg_ctx* c, int begin = 0) {
+  k_positions<R, false><<<c->g_pos, 256, 0, c->st>>>(args<R>(c).pos, nullptr, kOne, begin);
+  ++c->launches;
+}
+
+// always: rebuild whatever the step's flag says (ibg_set_state, growth).
+template <typename R>
+void enq_rebuild(ibg_ctx* c, DevList& L, int always) {
+  if (!L.present) return;
+  const ListArgs& a = args<R>(c).list[L.which];
+  const int w = L.which, gn = c->g_list[w];
+  k_regrid<R, false><<<c->g_regrid[w], 256, 0, c->st>>>(a, nullptr, kOne, always);
+  k_cell_assign<R, false><<<gn, 256, 0, c->st>>>(a, nullptr, kOne, always);
+  k_scan_cells<false><<<1, 1024, 0, c->st>>>(a, nullptr, kOne, always);
+  k_cell_fill<false><<<gn, 256, 0, c->st>>>(a, nullptr, kOne, always);
+  k_cell_rank<false><<<gn, 256, 0, c->st>>>(a, nullptr, kOne, always);
+  k_reslot<R, false><<<gn, 256, 0, c->st>>>(a, nullptr, kOne, always);
+  k_slot_of<R, false><<<gn, 256, 0, c->st>>>(a, nullptr, kOne, always);
+  const int gl = c->g_build[w];
+  switch (L.T) {
+    case 1: k_list_build<R, 1, false><<<gl, 256, 0, c->st>>>(a, nullptr, kOne, always); break;
+    case 2: k_list_build<R, 2, false><<<gl, 256, 0, c->st>>>(a, nullptr, kOne, always); break;
+    case 4: k_list_build<R, 4, false><<<gl, 256, 0, c->st>>>(a, nullptr, kOne, always); break;
+    default: k_list_build<R, 8, false><<<gl, 256, 0, c->st>>>(a, nullptr, kOne, always); break;
+  }
+  c->launches += 8;
+}
+
+template <typename R, bool B>
+using NBKernel = void (*)(const NBArgs<R>, const NBArgs<R>* const*, const BlockMap);
+
+template <typename R, bool B>
+NBKernel<R, B> nb_kernel(bool smem, int T);
+
+template <bool B>
+NBKernel<float, B> nb_kernel_f(bool smem, int T) {
+  if (smem) {
+    switch (T) {
+      case 1: return k_nonbonded_f32<true, 1, B>;
+      case 2: return k_nonbonded_f32<true, 2, B>;
+      case 4: return k_nonbonded_f32<true, 4, B>;
+      default: return k_nonbonded_f32<true, 8, B>;
+    }
+  }
+  switch (T) {
+    case 1: return k_nonbonded_f32<false, 1, B>;
+    case 2: return k_nonbonded_f32<false, 2, B>;
+    case 4: return k_nonbonded_f32<false, 4, B>;
+    default: return k_nonbonded_f32<false, 8, B>;
+  }
+}
+template <bool B>
+NBKernel<double, B> nb_kernel_d(bool smem, int T) {
+  if (smem) {
+    switch (T) {
+      case 1: return k_nonbonded<double, true, 1, B>;
+      case 2: return k_nonbonded<double, true, 2, B>;
+      case 4: return k_nonbonded<double, true, 4, B>;
+      default: return k_nonbonded<double, true, 8, B>;
+    }
+  }
+  switch (T) {
+    case 1: return k_nonbonded<double, false, 1, B>;
+    case 2: return k_nonbonded<double, false, 2, B>;
+    case 4: return k_nonbonded<double, false, 4, B>;
+    default: return k_nonbonded<double, false, 8, B>;
+  }
+}
+template <>
+NBKernel<float, false> nb_kernel<float, false>(bool smem, int T) { return nb_kernel_f<false>(smem, T); }
+template <>
+NBKernel<float, true> nb_kernel<float, true>(bool smem, int T) { return nb_kernel_f<true>(smem, T); }
+template <>
+NBKernel<double, false> nb_kernel<double, false>(bool smem, int T) { return nb_kernel_d<false>(smem, T); }
+template <>
+NBKernel<double, true> nb_kernel<double, true>(bool smem, int T) { return nb_kernel_d<true>(smem, T); }
+
+// Dynamic shared memory of a nonbonded launch over list L.
+size_t nb_smem(const ibg_ctx* c, const DevList& L) {
+  const size_t base = c->prec == IBG_PREC_FP32_FIXED ? 9 * 256 * sizeof(long long) : 9 * 8 * sizeof(double);
+  return L.use_smem ? L.smem : base;
+}
+
+// Blocks per SM the nonbonded kernel of list L reaches (after raising its
+// dynamic shared-memory limit when needed).
+template <typename R, bool B>
+int nb_occupancy(const ibg_ctx* c, const DevList& L, size_t sm) {
+  NBKernel<R, B> k = nb_kernel<R, B>(L.use_smem, L.T);
+  if (sm > 48 * 1024) CK(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  int per = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k, 256, sm));
+  return std::max(1, per);
+}
+
+template <typename R>
+void nb_configure(ibg_ctx* c, DevList& L) {
+  const int per = nb_occupancy<R, false>(c, L, nb_smem(c, L));
+  nb_occupancy<R, true>(c, L, nb_smem(c, L));
+  const long long units = (long long)L.nslices * 4;
+  L.grid_nb = (int)std::max<long long>(1, std::min<long long>((long long)c->nsm * per, (units + 7) / 8));
+}
+
+template <typename R>
+void enq_nonbonded(ibg_ctx* c, DevList& L) {
+  nb_kernel<R, false>(L.use_smem, L.T)<<<L.grid_nb, 256, nb_smem(c, L), c->st>>>(args<R>(c).nb[L.which], nullptr, kOne);
+  ++c->launches;
+}
+
+template <typename R>
+void enq_collect(ibg_ctx* c, DevList& L) {
+  k_nb_collect<R, false><<<c->g_list[L.which], 256, 0, c->st>>>(args<R>(c).col[L.which], nullptr, kOne);
+  ++c->launches;
+}
+
+template <typename R>
+void enq_distribute(ibg_ctx* c, int which) {
+  if (c->nvirta == 0) return;
+  k_distribute<R, false><<<c->g_dist, 256, 0, c->st>>>(args<R>(c).dist, nullptr, kOne, which);
+  ++c->launches;
+}
+
+template <typename R>
+void enq_bonded(ibg_ctx* c) {
+  k_bonded<R, false><<<c->g_b, 256, 0, c->st>>>(args<R>(c).bond, nullptr, kOne);
   ++c->launches;
 }
 
 template <typename R>
 void enq_move(ibg_ctx* c, int update) {
-  MoveArgs<R> M;
-  M.natoms = c->natoms; M.S = c->S; M.V = c->V;
-  M.fnb = (const typename Prec<R>::acc_t*)c->fnb; M.fb = (const typename Prec<R>::acc_t*)c->fb;
-  M.tbits = c->tbits; M.mass = c->mass; M.invmass = c->invmass; M.dt = (double)c->dt; M.update = update;
-  M.part = c->p_mv; M.part_stride = c->g_mv;
-  k_move<R><<<c->g_mv, 256, 0, c->st>>>(M, c->sc);
+  MoveArgs<R> M = args<R>(c).move;
+  M.update = update;
+  k_move<R, false><<<c->g_mv, 256, 0, c->st>>>(M, nullptr, kOne);
   ++c->launches;
 }
 
+template <typename R>
 void enq_finalize(ibg_ctx* c, int move) {
-  FinalArgs F;
-  F.p_nb[0] = c->L[0].present ? c->L[0].part : nullptr;
-  F.p_nb[1] = c->L[1].present ? c->L[1].part : nullptr;
-  F.g_nb = c->L[0].present ? c->L[0].grid_nb : c->L[1].grid_nb;
-  F.p_b = c->p_b; F.g_b = c->g_b; F.p_mv = c->p_mv; F.g_mv = c->g_mv;
-  F.mts = c->nmts > 0; F.move = move; F.ensemble = c->ensemble;
-  F.temp_in = c->temp_in; F.fac = c->fac; F.pfac = c->pfac; F.pressure = c->pressure;
-  F.mktemp = c->mktemp; F.mktemp_atom = c->mktemp_atom; F.mktemp_bead = c->mktemp_bead;
-  F.ring = c->ring; F.ring_cap = c->ring_cap;
-  k_finalize<<<1, 1024, 0, c->st>>>(F, c->sc);
+  FinalArgs F = args<R>(c).fin;
+  F.move = move;
+  k_finalize<false><<<1, 1024, 0, c->st>>>(F, nullptr, kOne);
   ++c->launches;
 }
 
-// One loop body.  In graph mode the bonded branch (zero fb, bonded terms,
-// their VS distribution) runs concurrently with the list build and the
-// nonbonded branch; both join before MOVE.  Timing mode keeps one stream so
-// that the stage times add up.
+// One loop body.  In graph mode the bonded branch (bonded terms and their VS
+// distribution) runs concurrently with the list build and the nonbonded
+// branch; both join before MOVE.  Timing mode keeps one stream so that the
+// stage times add up.
 template <typename R>
 void enqueue_step(ibg_ctx* c, unsigned v) {
   const bool fork = !c->timing;
+  const int always = 0;  // rebuild kernels follow the step's own flag
   mark(c, 4);
   enq_positions<R>(c, 1);
   auto bonded_branch = [&]() {
-    CK(cudaMemsetAsync(c->fb, 0, accsize(c) * 3 * (size_t)c->nitems, c->st));
     mark(c, 2);
     enq_bonded<R>(c);
     mark(c, 4);
-    enq_distribute<R>(c, c->fb);
+    enq_distribute<R>(c, 1);
   };
   cudaStream_t main_st = c->st;
   if (fork) {
@@ -512,8 +608,8 @@ void enqueue_step(ibg_ctx* c, unsigned v) {
   }
   if (v & V_REBUILD) {
     mark(c, 0);
-    enq_rebuild<R>(c, c->L[0]);
-    enq_rebuild<R>(c, c->L[1]);
+    enq_rebuild<R>(c, c->L[0], always);
+    enq_rebuild<R>(c, c->L[1], always);
   }
   // nonbonded: MTS runs the bead list first (MTS_LOOP.f90:100-116); sums are
   // order independent, so one sequence serves both loops
@@ -523,25 +619,25 @@ void enqueue_step(ibg_ctx* c, unsigned v) {
   mark(c, 4);
   if (c->L[1].present) enq_collect<R>(c, c->L[1]);
   if (c->L[0].present) enq_collect<R>(c, c->L[0]);
-  enq_distribute<R>(c, c->fnb);
+  enq_distribute<R>(c, 0);
   if (fork) CK(cudaStreamWaitEvent(main_st, c->fork_ev[1], 0));
   else bonded_branch();
   mark(c, 3);
   if (v & V_FORCE_ONLY) {
     enq_move<R>(c, 0);
-    enq_finalize(c, 0);
+    enq_finalize<R>(c, 0);
     mark(c, 7);
     return;
   }
   enq_move<R>(c, 1);
   if (v & V_MOMENTUM) {
-    k_mom_sum<<<c->g_mv, 256, 0, c->st>>>(c->natoms, c->V, c->mass, c->p_mom, c->g_mv);
-    k_mom_apply<<<c->g_mv, 256, 0, c->st>>>(c->natoms, c->V, c->invmass, c->p_mom, c->g_mv, c->g_mv, c->sc);
+    k_mom_sum<false><<<c->g_mv, 256, 0, c->st>>>(args<R>(c).mom, nullptr, kOne);
+    k_mom_apply<false><<<c->g_mv, 256, 0, c->st>>>(args<R>(c).mom, nullptr, kOne);
     c->launches += 2;
   }
-  enq_finalize(c, 1);
+  enq_finalize<R>(c, 1);
   if (v & V_SCALE) {
-    k_scale_positions<<<c->g_mv, 256, 0, c->st>>>(c->natoms, c->S, c->sc);
+    k_scale_positions<R, false><<<c->g_mv, 256, 0, c->st>>>(args<R>(c).move, nullptr, kOne);
     ++c->launches;
   }
   mark(c, 7);
@@ -565,10 +661,13 @@ void enqueue(ibg_ctx* c, unsigned v) {
   else enqueue_step<double>(c, v);
 }
 
-// Next step = step_before + 1; observables of step k go to ring slot k - base.
-void set_step_counter(ibg_ctx* c, int step_before, int base) {
+// The system runs steps step_before+1 .. last; observables of step k go to
+// ring slot k - base.
+void set_step_counter(ibg_ctx* c, int step_before, int base, int last) {
+  const int skip_stop[3] = {0, last, step_before >= last ? 1 : 0};  // skip, stop_at, done
   CK(cudaMemcpyAsync(&c->sc->step, &step_before, sizeof(int), cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(&c->sc->ring_base, &base, sizeof(int), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(&c->sc->skip, skip_stop, sizeof(skip_stop), cudaMemcpyHostToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
 }
 
@@ -624,18 +723,19 @@ int grow_lists(ibg_ctx* c) {
     DevList& L = c->L[w];
     if (!L.present || need[w] <= L.w_cap) continue;
     const int cap = need[w] + need[w] / 4 + 2;
-    if (L.entries) {
-      auto it = std::find(c->owned.begin(), c->owned.end(), (void*)L.entries);
-      if (it != c->owned.end()) c->owned.erase(it);
-      CK(cudaFree(L.entries));
-    }
+    if (L.entries) c->owned.release(L.entries);
     L.entries = dalloc<int>((size_t)L.nslices * 32 * cap, c->owned);
     L.w_cap = cap;
     ++c->list_growths;
   }
   const int zero[3] = {0, 0, 0};
   CK(cudaMemcpy(&c->sc->abort, zero, sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(&c->sc->skip, zero, sizeof(int), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->sc->need_rows, zero, 2 * sizeof(int), cudaMemcpyHostToDevice));
+  // the bonded branch of the aborted step may have run (it overlaps the list
+  // build); its forces are recomputed when the step is repeated
+  CK(cudaMemset(c->fb, 0, accsize(c) * 3 * (size_t)c->nitems));
+  refresh_args(c);
   for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);  // they bake the old pointers
   c->graphs.clear();
   return 1;
@@ -646,7 +746,7 @@ void rebuild_now(ibg_ctx* c) {
   CK(cudaMemsetAsync(c->sc->work, 0, sizeof(c->sc->work), c->st));
   for (auto& L : c->L) {
     if (!L.present) continue;
-    enq_rebuild<R>(c, L);
+    enq_rebuild<R>(c, L, 1);
   }
 }
 
@@ -665,14 +765,11 @@ int ibg_set_list_rows(ibg_ctx* c, int rows) {
     CK(cudaStreamSynchronize(c->st));
     for (auto& L : c->L) {
       if (!L.present) continue;
-      if (L.entries) {
-        auto it = std::find(c->owned.begin(), c->owned.end(), (void*)L.entries);
-        if (it != c->owned.end()) c->owned.erase(it);
-        CK(cudaFree(L.entries));
-      }
+      if (L.entries) c->owned.release(L.entries);
       L.entries = dalloc<int>((size_t)L.nslices * 32 * rows, c->owned);
       L.w_cap = rows;
     }
+    refresh_args(c);
     for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
     c->graphs.clear();
   } catch (CudaError& e) {
@@ -692,6 +789,42 @@ int ibg_set_l2_flush(ibg_ctx* c, long long bytes) {
 }
 
 const char* ibg_last_error(const ibg_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+long long ibg_device_bytes(const ibg_ctx* c) {
+  if (!c) return IBG_E_INVALID;
+  return (long long)(c->owned.bytes + (c->flush_buf ? c->flush_bytes : 0));
+}
+
+long long ibg_estimate_bytes(const ibg_desc* d, int precision, const float* box) {
+  if (!d || !box || d->nitems <= 0) return IBG_E_INVALID;
+  const bool f32 = precision == IBG_PREC_FP32_FIXED;
+  const double pos = f32 ? 16.0 : 32.0, acc = 8.0, rs = f32 ? 4.0 : 8.0;
+  const double vol = (double)box[0] * box[1] * box[2];
+  double b = (double)d->nitems * (4 + 8 + 8 + 24 + 2 * 3 * acc + 4 + 80 + 4) + (double)d->natoms * 24;
+  long long terms = 0;
+  for (int i = 0; i < d->nitems; ++i) {
+    terms += d->nbonds ? d->nbonds[i] : 0;
+    terms += d->nijk ? d->nijk[i] : 0;
+    if (i < d->natoms) terms += (d->nijkl ? d->nijkl[i] : 0) + (d->noopijkl ? d->noopijkl[i] : 0);
+  }
+  b += (double)terms * 24;
+  const int ntab = d->nbtype + d->natype + d->nttype + d->notype;
+  b += (double)ntab * 16.0 * 4096;  // bonded table rows, generous
+  for (int w = 0; w < 2; ++w) {
+    const int n = w == 0 ? d->numatoms : d->ncoarse;
+    if (n <= 0) continue;
+    const double rl = w == 0 ? d->rlist_atom : d->rlist_bead;
+    const double half = (double)n / vol * (2.0 / 3.0) * 3.14159265358979 * rl * rl * rl;
+    const double rows = (half * 1.25 + 8.0) * 1.25 + 2.0;  // growth margin and slice padding
+    b += (double)n * (7 * 4 + 2 * pos + 3 * acc + rows * 4);
+    if (w == 1 && d->nmts > 0) b += (double)n * 9 * acc;
+    const double cells = (box[0] * 1.25 / rl + 2) * (box[1] * 1.25 / rl + 2) * (box[2] * 1.25 / rl + 2);
+    b += cells * 12;
+    b += (double)d->nnbtype * d->ld_nb * 3 * rs;
+  }
+  b += 2.0 * 1024 * 1024;  // scalars, partial sums, argument blocks, rounding of allocations
+  return (long long)b;
+}
 
 int ibg_create(const ibg_desc* d, int precision, ibg_ctx** out) {
   if (!d || !out) return IBG_E_INVALID;
@@ -862,9 +995,13 @@ int ibg_create(const ibg_desc* d, int precision, ibg_ctx** out) {
       if (precision == IBG_PREC_FP32_FIXED) nb_configure<float>(c.get(), L);
       else nb_configure<double>(c.get(), L);
     }
-    int gnb = std::max(c->L[0].present ? c->L[0].grid_nb : 0, c->L[1].present ? c->L[1].grid_nb : 0);
-    for (auto& L : c->L)
-      if (L.present) { L.grid_nb = gnb; L.part = dalloc<double>(9 * (size_t)gnb, o); }
+    for (int w = 0; w < 2; ++w) {
+      DevList& L = c->L[w];
+      if (!L.present) continue;
+      c->g_list[w] = grid_for(c.get(), L.n);
+      c->g_build[w] = std::max(1, std::min(L.nslices / 8 + 1, c->nsm * 8));
+    }
+    c->g_dist = grid_for(c.get(), std::max(1, c->nvirta));
     c->g_b = grid_for(c.get(), (long long)c->nb + c->na + c->nt + c->no, 4);
     c->g_mv = grid_for(c.get(), NA, 4);
     c->g_pos = grid_for(c.get(), N, 8);
@@ -874,10 +1011,10 @@ int ibg_create(const ibg_desc* d, int precision, ibg_ctx** out) {
     c->sc = dalloc<Scalars>(1, o);
     c->ring_cap = 1;
     c->ring = nullptr;
+    refresh_args(c.get());
     CK(cudaDeviceSynchronize());
   } catch (CudaError& e) {
-    for (void* p : c->owned) cudaFree(p);
-    c->owned.clear();
+    c->owned.free_all();
     return IBG_E_CUDA;
   }
   *out = c.release();
@@ -905,6 +1042,7 @@ int ibg_set_state(ibg_ctx* c, const float* sxyz, const float* vxyz, const float*
     h.step = 0;
     h.mts_m = -1;
     h.miu = 1.0;
+    h.stop_at = INT_MAX;
     h.lam[0] = h.lam[1] = 1.0;
     CK(cudaMemcpy(c->sc, &h, sizeof(h), cudaMemcpyHostToDevice));
     for (auto& L : c->L) {
@@ -916,7 +1054,11 @@ int ibg_set_state(ibg_ctx* c, const float* sxyz, const float* vxyz, const float*
       CK(cudaMemcpy(L.sorted, ident.data(), sizeof(int) * L.n, cudaMemcpyHostToDevice));
       CK(cudaMemset(L.fsort, 0, accsize(c) * 3 * (size_t)L.n));
       if (L.mtsf) CK(cudaMemset(L.mtsf, 0, accsize(c) * 9 * (size_t)L.n));
+      c->g_regrid[L.which] = grid_for(c, L.cell_cap, 2);
     }
+    CK(cudaMemset(c->fnb, 0, accsize(c) * 3 * (size_t)c->nitems));
+    CK(cudaMemset(c->fb, 0, accsize(c) * 3 * (size_t)c->nitems));
+    refresh_args(c);
     {  // slots = list order before the first sort
       std::vector<int> gs(c->nitems, 0);
       std::vector<int> idx0, idx1;
@@ -951,6 +1093,7 @@ int ibg_set_state(ibg_ctx* c, const float* sxyz, const float* vxyz, const float*
     int rc = check_device(c);
     if (rc) return rc;
     c->state_set = true;
+    c->step_now = 0;
     c->fb_dirty = false;
   } catch (CudaError& e) {
     return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
@@ -963,20 +1106,17 @@ static int run_steps(ibg_ctx* c, int first, int nsteps, ibg_obs* per_step, bool 
   if (!c->state_set) return fail(c, IBG_E_INVALID, "ibg_set_state has not been called");
   try {
     if (per_step && nsteps > c->ring_cap) {
-      if (c->ring) {
-        auto it = std::find(c->owned.begin(), c->owned.end(), (void*)c->ring);
-        if (it != c->owned.end()) c->owned.erase(it);
-        CK(cudaFree(c->ring));
-      }
+      if (c->ring) c->owned.release(c->ring);
       c->ring_cap = std::max(nsteps, 64);
       c->ring = dalloc<ObsD>(c->ring_cap, c->owned);
+      refresh_args(c);
       for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
       c->graphs.clear();
     }
     int done = 0;
     float run_ms_total = 0.f;
     for (int attempt = 0; attempt < 8 && done < nsteps; ++attempt) {
-      set_step_counter(c, first + done - 1, first);
+      set_step_counter(c, first + done - 1, first, first + nsteps - 1);
       if (c->flush_bytes) {
         if (!c->flush_buf) CK(cudaMalloc(&c->flush_buf, c->flush_bytes));
         while ((int)c->step_ev.size() < 2 * nsteps) {
@@ -1043,6 +1183,7 @@ static int run_steps(ibg_ctx* c, int first, int nsteps, ibg_obs* per_step, bool 
       done = nsteps;
     }
     c->stage_ms[5] = run_ms_total;
+    c->step_now = first + done - 1;
     if (done < nsteps) return fail(c, IBG_E_CAPACITY, "neighbour-list storage could not be sized");
     int rc = check_device(c);
     if (rc) return rc;
@@ -1236,7 +1377,7 @@ void ibg_destroy(ibg_ctx* c) {
   if (!c) return;
   cudaStreamSynchronize(c->st);
   for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
-  for (void* p : c->owned) cudaFree(p);
+  c->owned.free_all();
   for (auto* e : c->run_ev)
     if (e) cudaEventDestroy(e);
   for (auto* e : c->step_ev) cudaEventDestroy(e);
@@ -1246,6 +1387,419 @@ void ibg_destroy(ibg_ctx* c) {
   if (c->st2) cudaStreamDestroy(c->st2);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
+}
+
+}  // extern "C"
+
+// ===================================================================== batch
+// Many independent systems stepped together: one launch per stage covers
+// every system (blocks map to systems through a block map, arguments come
+// from each system's device argument block), and the whole batch step is one
+// CUDA graph.  Each system keeps its own step counter, list schedule, MTS
+// phase, thermostat and barostat; device-side flags make a stage a no-op for
+// the systems it does not concern this step.  Integer force and energy sums
+// and per-system launch shapes for the statically scheduled kernels make every
+// system's result bitwise the same alone and in any batch.
+
+struct BMap {
+  int* sys_of = nullptr;
+  int* start = nullptr;
+  int grid = 0;
+  BlockMap m() const { return BlockMap{sys_of, start}; }
+};
+
+struct NBGroup {
+  int T = 1;
+  bool smem = false;
+  size_t sm = 0;
+  BMap map;
+};
+
+struct ibg_batch {
+  int prec = 0, dev = 0, nsm = 148;
+  std::vector<ibg_ctx*> sys;
+  Owned owned;
+  cudaStream_t st = nullptr, st2 = nullptr;
+  cudaEvent_t fork_ev[2] = {nullptr, nullptr}, run_ev[2] = {nullptr, nullptr};
+  // per-system pointers to the argument blocks, by kind
+  void** t_pos = nullptr;
+  void** t_list[2] = {nullptr, nullptr};
+  void** t_nb[2] = {nullptr, nullptr};
+  void** t_col[2] = {nullptr, nullptr};
+  void** t_dist = nullptr;
+  void** t_bond = nullptr;
+  void** t_move = nullptr;
+  void** t_mom = nullptr;
+  void** t_fin = nullptr;
+  BMap m_pos, m_regrid[2], m_list[2], m_scan[2], m_dist, m_bond, m_move, m_fin;
+  std::vector<NBGroup> lb[2];  // list build, by T (smem unused)
+  std::vector<NBGroup> nb[2];  // nonbonded, by (T, smem)
+  bool any_vs = false, any_list[2] = {false, false};
+  std::map<unsigned, cudaGraphExec_t> graphs;
+  long long launches = 0, launches_per_variant[8] = {0};
+  double run_ms = 0.0;
+  std::string err;
+};
+
+namespace {
+
+int bfail(ibg_batch* b, int code, const std::string& m) {
+  if (b) b->err = m;
+  return code;
+}
+
+// Block map from per-system block counts (0: the system takes no part).
+BMap make_map(ibg_batch* b, const std::vector<int>& g) {
+  BMap m;
+  std::vector<int> start(g.size() + 1, 0), sys_of;
+  for (size_t s = 0; s < g.size(); ++s) {
+    start[s + 1] = start[s] + g[s];
+    for (int k = 0; k < g[s]; ++k) sys_of.push_back((int)s);
+  }
+  m.grid = start.back();
+  m.start = dupload(start, b->owned);
+  m.sys_of = dupload(sys_of.empty() ? std::vector<int>{0} : sys_of, b->owned);
+  return m;
+}
+
+template <typename R>
+void** make_table(ibg_batch* b, size_t offset) {
+  std::vector<void*> p(b->sys.size());
+  for (size_t s = 0; s < b->sys.size(); ++s) p[s] = (char*)b->sys[s]->dargs + offset;
+  return dupload(p, b->owned);
+}
+
+template <typename R>
+void batch_layout(ibg_batch* b) {
+  using SA = SysArgs<R>;
+  const size_t n = b->sys.size();
+  b->t_pos = make_table<R>(b, offsetof(SA, pos));
+  for (int w = 0; w < 2; ++w) {
+    b->t_list[w] = make_table<R>(b, offsetof(SA, list) + w * sizeof(ListArgs));
+    b->t_nb[w] = make_table<R>(b, offsetof(SA, nb) + w * sizeof(NBArgs<R>));
+    b->t_col[w] = make_table<R>(b, offsetof(SA, col) + w * sizeof(CollectArgs<R>));
+  }
+  b->t_dist = make_table<R>(b, offsetof(SA, dist));
+  b->t_bond = make_table<R>(b, offsetof(SA, bond));
+  b->t_move = make_table<R>(b, offsetof(SA, move));
+  b->t_mom = make_table<R>(b, offsetof(SA, mom));
+  b->t_fin = make_table<R>(b, offsetof(SA, fin));
+  std::vector<int> g(n);
+  for (size_t s = 0; s < n; ++s) g[s] = b->sys[s]->g_pos;
+  b->m_pos = make_map(b, g);
+  for (size_t s = 0; s < n; ++s) g[s] = b->sys[s]->nvirta ? b->sys[s]->g_dist : 0;
+  b->m_dist = make_map(b, g);
+  for (size_t s = 0; s < n; ++s) b->any_vs |= b->sys[s]->nvirta > 0;
+  for (size_t s = 0; s < n; ++s) g[s] = b->sys[s]->g_b;
+  b->m_bond = make_map(b, g);
+  for (size_t s = 0; s < n; ++s) g[s] = b->sys[s]->g_mv;
+  b->m_move = make_map(b, g);
+  for (size_t s = 0; s < n; ++s) g[s] = 1;
+  b->m_fin = make_map(b, g);
+  for (int w = 0; w < 2; ++w) {
+    for (size_t s = 0; s < n; ++s) b->any_list[w] |= b->sys[s]->L[w].present;
+    for (size_t s = 0; s < n; ++s) g[s] = b->sys[s]->L[w].present ? b->sys[s]->g_regrid[w] : 0;
+    b->m_regrid[w] = make_map(b, g);
+    for (size_t s = 0; s < n; ++s) g[s] = b->sys[s]->L[w].present ? b->sys[s]->g_list[w] : 0;
+    b->m_list[w] = make_map(b, g);
+    for (size_t s = 0; s < n; ++s) g[s] = b->sys[s]->L[w].present ? 1 : 0;
+    b->m_scan[w] = make_map(b, g);
+    // list build: one group per T, each system with its own grid
+    std::set<int> Ts;
+    for (size_t s = 0; s < n; ++s)
+      if (b->sys[s]->L[w].present) Ts.insert(b->sys[s]->L[w].T);
+    for (int T : Ts) {
+      NBGroup grp;
+      grp.T = T;
+      for (size_t s = 0; s < n; ++s) {
+        const DevList& L = b->sys[s]->L[w];
+        g[s] = (L.present && L.T == T) ? b->sys[s]->g_build[w] : 0;
+      }
+      grp.map = make_map(b, g);
+      b->lb[w].push_back(grp);
+    }
+    // nonbonded: one group per (T, smem); the group's resident blocks are
+    // shared among its systems in proportion to their work units
+    std::set<std::pair<int, int>> keys;
+    for (size_t s = 0; s < n; ++s)
+      if (b->sys[s]->L[w].present) keys.insert({b->sys[s]->L[w].T, (int)b->sys[s]->L[w].use_smem});
+    for (auto key : keys) {
+      NBGroup grp;
+      grp.T = key.first;
+      grp.smem = key.second != 0;
+      double units = 0;
+      for (size_t s = 0; s < n; ++s) {
+        const DevList& L = b->sys[s]->L[w];
+        if (!(L.present && L.T == grp.T && (int)L.use_smem == key.second)) continue;
+        grp.sm = std::max(grp.sm, nb_smem(b->sys[s], L));
+        units += (double)L.nslices * ((L.w_cap + 7) / 8);
+      }
+      int per = 1;
+      for (size_t s = 0; s < n; ++s) {
+        const DevList& L = b->sys[s]->L[w];
+        if (L.present && L.T == grp.T && (int)L.use_smem == key.second) {
+          per = nb_occupancy<R, true>(b->sys[s], L, grp.sm);
+          break;
+        }
+      }
+      const double resident = (double)b->nsm * per;
+      for (size_t s = 0; s < n; ++s) {
+        const DevList& L = b->sys[s]->L[w];
+        if (!(L.present && L.T == grp.T && (int)L.use_smem == key.second)) { g[s] = 0; continue; }
+        const double u = (double)L.nslices * ((L.w_cap + 7) / 8);
+        g[s] = std::max(1, std::min(L.grid_nb, (int)std::lround(resident * u / std::max(units, 1.0))));
+      }
+      grp.map = make_map(b, g);
+      b->nb[w].push_back(grp);
+    }
+  }
+}
+
+enum BatchVariant : unsigned { BV_REBUILD = 1u, BV_MOMENTUM = 2u, BV_SCALE = 4u };
+
+template <typename R>
+void batch_enqueue(ibg_batch* b, unsigned v) {
+  cudaStream_t st = b->st, st2 = b->st2;
+  long long& n = b->launches;
+  k_positions<R, true><<<b->m_pos.grid, 256, 0, st>>>(PosArgs{}, (const PosArgs* const*)b->t_pos, b->m_pos.m(), 1);
+  ++n;
+  // bonded branch
+  CK(cudaEventRecord(b->fork_ev[0], st));
+  CK(cudaStreamWaitEvent(st2, b->fork_ev[0], 0));
+  k_bonded<R, true><<<b->m_bond.grid, 256, 0, st2>>>(BondedArgs<R>{}, (const BondedArgs<R>* const*)b->t_bond,
+                                                     b->m_bond.m());
+  ++n;
+  if (b->any_vs) {
+    k_distribute<R, true><<<b->m_dist.grid, 256, 0, st2>>>(DistArgs<R>{}, (const DistArgs<R>* const*)b->t_dist,
+                                                           b->m_dist.m(), 1);
+    ++n;
+  }
+  CK(cudaEventRecord(b->fork_ev[1], st2));
+  // list rebuild of the systems whose step rebuilds
+  if (v & BV_REBUILD) {
+    for (int w = 0; w < 2; ++w) {
+      if (!b->any_list[w]) continue;
+      const ListArgs* const* t = (const ListArgs* const*)b->t_list[w];
+      const BMap& ml = b->m_list[w];
+      k_regrid<R, true><<<b->m_regrid[w].grid, 256, 0, st>>>(ListArgs{}, t, b->m_regrid[w].m(), 0);
+      k_cell_assign<R, true><<<ml.grid, 256, 0, st>>>(ListArgs{}, t, ml.m(), 0);
+      k_scan_cells<true><<<b->m_scan[w].grid, 1024, 0, st>>>(ListArgs{}, t, b->m_scan[w].m(), 0);
+      k_cell_fill<true><<<ml.grid, 256, 0, st>>>(ListArgs{}, t, ml.m(), 0);
+      k_cell_rank<true><<<ml.grid, 256, 0, st>>>(ListArgs{}, t, ml.m(), 0);
+      k_reslot<R, true><<<ml.grid, 256, 0, st>>>(ListArgs{}, t, ml.m(), 0);
+      k_slot_of<R, true><<<ml.grid, 256, 0, st>>>(ListArgs{}, t, ml.m(), 0);
+      n += 7;
+      for (const NBGroup& grp : b->lb[w]) {
+        switch (grp.T) {
+          case 1: k_list_build<R, 1, true><<<grp.map.grid, 256, 0, st>>>(ListArgs{}, t, grp.map.m(), 0); break;
+          case 2: k_list_build<R, 2, true><<<grp.map.grid, 256, 0, st>>>(ListArgs{}, t, grp.map.m(), 0); break;
+          case 4: k_list_build<R, 4, true><<<grp.map.grid, 256, 0, st>>>(ListArgs{}, t, grp.map.m(), 0); break;
+          default: k_list_build<R, 8, true><<<grp.map.grid, 256, 0, st>>>(ListArgs{}, t, grp.map.m(), 0); break;
+        }
+        ++n;
+      }
+    }
+  }
+  // nonbonded, bead list first
+  for (int w : {1, 0}) {
+    for (const NBGroup& grp : b->nb[w]) {
+      nb_kernel<R, true>(grp.smem, grp.T)<<<grp.map.grid, 256, grp.sm, st>>>(
+          NBArgs<R>{}, (const NBArgs<R>* const*)b->t_nb[w], grp.map.m());
+      ++n;
+    }
+  }
+  for (int w : {1, 0}) {
+    if (!b->any_list[w]) continue;
+    k_nb_collect<R, true><<<b->m_list[w].grid, 256, 0, st>>>(CollectArgs<R>{}, (const CollectArgs<R>* const*)b->t_col[w],
+                                                            b->m_list[w].m());
+    ++n;
+  }
+  if (b->any_vs) {
+    k_distribute<R, true><<<b->m_dist.grid, 256, 0, st>>>(DistArgs<R>{}, (const DistArgs<R>* const*)b->t_dist,
+                                                          b->m_dist.m(), 0);
+    ++n;
+  }
+  CK(cudaStreamWaitEvent(st, b->fork_ev[1], 0));
+  k_move<R, true><<<b->m_move.grid, 256, 0, st>>>(MoveArgs<R>{}, (const MoveArgs<R>* const*)b->t_move, b->m_move.m());
+  ++n;
+  if (v & BV_MOMENTUM) {
+    k_mom_sum<true><<<b->m_move.grid, 256, 0, st>>>(MomArgs{}, (const MomArgs* const*)b->t_mom, b->m_move.m());
+    k_mom_apply<true><<<b->m_move.grid, 256, 0, st>>>(MomArgs{}, (const MomArgs* const*)b->t_mom, b->m_move.m());
+    n += 2;
+  }
+  k_finalize<true><<<b->m_fin.grid, 1024, 0, st>>>(FinalArgs{}, (const FinalArgs* const*)b->t_fin, b->m_fin.m());
+  ++n;
+  if (v & BV_SCALE) {
+    k_scale_positions<R, true><<<b->m_move.grid, 256, 0, st>>>(MoveArgs<R>{}, (const MoveArgs<R>* const*)b->t_move,
+                                                               b->m_move.m());
+    ++n;
+  }
+}
+
+void batch_enqueue_any(ibg_batch* b, unsigned v) {
+  if (b->prec == IBG_PREC_FP32_FIXED) batch_enqueue<float>(b, v);
+  else batch_enqueue<double>(b, v);
+}
+
+// Variant of batch step k: which optional stages some system needs.
+unsigned batch_variant(const ibg_batch* b, const std::vector<int>& from, const std::vector<int>& last, int k) {
+  unsigned v = 0;
+  for (size_t s = 0; s < b->sys.size(); ++s) {
+    const ibg_ctx* c = b->sys[s];
+    const int step = from[s] + 1 + k;
+    if (step > last[s]) continue;
+    if (step % c->nupdate == 0) v |= BV_REBUILD;
+    if (step % c->halt_drift == 0) v |= BV_MOMENTUM;
+    if (c->ensemble == 2 && step % 10 == 0) v |= BV_SCALE;
+  }
+  return v;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ibg_batch_create(ibg_ctx* const* ctxs, int n, ibg_batch** out) {
+  if (!ctxs || n <= 0 || !out) return IBG_E_INVALID;
+  *out = nullptr;
+  auto b = std::make_unique<ibg_batch>();
+  try {
+    CK(cudaGetDevice(&b->dev));
+    CK(cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->dev));
+    std::set<const ibg_ctx*> seen;
+    for (int s = 0; s < n; ++s) {
+      ibg_ctx* c = ctxs[s];
+      if (!c || !c->state_set || c->in_batch || seen.count(c)) return IBG_E_INVALID;
+      if (s > 0 && (c->prec != ctxs[0]->prec || c->dev != ctxs[0]->dev)) return IBG_E_INVALID;
+      seen.insert(c);
+      CK(cudaStreamSynchronize(c->st));
+      b->sys.push_back(c);
+    }
+    b->prec = ctxs[0]->prec;
+    CK(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&b->st2, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; ++k) {
+      CK(cudaEventCreateWithFlags(&b->fork_ev[k], cudaEventDisableTiming));
+      CK(cudaEventCreate(&b->run_ev[k]));
+    }
+    if (b->prec == IBG_PREC_FP32_FIXED) batch_layout<float>(b.get());
+    else batch_layout<double>(b.get());
+    for (ibg_ctx* c : b->sys) c->in_batch = true;
+    CK(cudaDeviceSynchronize());
+  } catch (CudaError& e) {
+    b->owned.free_all();
+    return IBG_E_CUDA;
+  }
+  *out = b.release();
+  return IBG_OK;
+}
+
+int ibg_batch_run(ibg_batch* b, int nsteps, const int* last_step, ibg_obs* last_obs) {
+  if (!b || nsteps < 0) return IBG_E_INVALID;
+  const size_t n = b->sys.size();
+  try {
+    std::vector<int> last(n), from(n);
+    for (size_t s = 0; s < n; ++s) {
+      ibg_ctx* c = b->sys[s];
+      from[s] = c->step_now;
+      last[s] = c->step_now + nsteps;
+      if (last_step) last[s] = std::max(c->step_now, std::min(last[s], last_step[s]));
+    }
+    float total_ms = 0.f;
+    for (int attempt = 0; attempt < 8; ++attempt) {
+      int need = 0;
+      for (size_t s = 0; s < n; ++s) need = std::max(need, last[s] - from[s]);
+      if (need == 0) break;
+      for (size_t s = 0; s < n; ++s) set_step_counter(b->sys[s], from[s], INT_MAX, last[s]);
+      CK(cudaEventRecord(b->run_ev[0], b->st));
+      for (int k = 0; k < need; ++k) {
+        const unsigned v = batch_variant(b, from, last, k);
+        auto it = b->graphs.find(v);
+        if (it == b->graphs.end()) {
+          cudaGraph_t g;
+          CK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+          const long long l0 = b->launches;
+          batch_enqueue_any(b, v);
+          CK(cudaStreamEndCapture(b->st, &g));
+          b->launches_per_variant[v & 7] = b->launches - l0;
+          b->launches = l0;
+          cudaGraphExec_t ge;
+          CK(cudaGraphInstantiate(&ge, g, 0));
+          CK(cudaGraphDestroy(g));
+          it = b->graphs.emplace(v, ge).first;
+        }
+        CK(cudaGraphLaunch(it->second, b->st));
+        b->launches += b->launches_per_variant[v & 7];
+      }
+      CK(cudaEventRecord(b->run_ev[1], b->st));
+      CK(cudaStreamSynchronize(b->st));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, b->run_ev[0], b->run_ev[1]));
+      total_ms += ms;
+      // systems whose list storage overflowed: grow it and repeat from the
+      // step that aborted; the others are done
+      bool again = false;
+      for (size_t s = 0; s < n; ++s) {
+        ibg_ctx* c = b->sys[s];
+        if (grow_lists(c)) {
+          int st = 0;
+          CK(cudaMemcpy(&st, &c->sc->step, sizeof(int), cudaMemcpyDeviceToHost));
+          from[s] = st - 1;
+          again = true;
+        } else {
+          from[s] = last[s];
+        }
+      }
+      if (!again) break;
+    }
+    b->run_ms = total_ms;
+    // every system's status: a failing system does not hide the others'
+    int first_rc = IBG_OK;
+    for (size_t s = 0; s < n; ++s) {
+      ibg_ctx* c = b->sys[s];
+      int rc = IBG_OK;
+      if (from[s] < last[s]) rc = fail(c, IBG_E_CAPACITY, "neighbour-list storage could not be sized");
+      c->step_now = from[s];
+      if (!rc) rc = check_device(c);
+      if (last_obs) {
+        read_obs(c, &last_obs[s]);
+        last_obs[s].status = rc;
+      }
+      if (rc && !first_rc) {
+        first_rc = rc;
+        bfail(b, rc, "system " + std::to_string(s) + ": " + c->err);
+      }
+    }
+    return first_rc;
+  } catch (CudaError& e) {
+    return bfail(b, IBG_E_CUDA, cudaGetErrorString(e.e));
+  }
+}
+
+int ibg_batch_size(const ibg_batch* b) { return b ? (int)b->sys.size() : 0; }
+
+int ibg_batch_get_timing(const ibg_batch* b, double* run_ms, long long* launches) {
+  if (!b) return IBG_E_INVALID;
+  if (run_ms) *run_ms = b->run_ms;
+  if (launches) *launches = b->launches;
+  return IBG_OK;
+}
+
+const char* ibg_batch_last_error(const ibg_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+void ibg_batch_destroy(ibg_batch* b) {
+  if (!b) return;
+  cudaStreamSynchronize(b->st);
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->owned.free_all();
+  for (int k = 0; k < 2; ++k) {
+    if (b->fork_ev[k]) cudaEventDestroy(b->fork_ev[k]);
+    if (b->run_ev[k]) cudaEventDestroy(b->run_ev[k]);
+  }
+  if (b->st2) cudaStreamDestroy(b->st2);
+  if (b->st) cudaStreamDestroy(b->st);
+  for (ibg_ctx* c : b->sys) c->in_batch = false;
+  delete b;
 }
 
 }  // extern "C"

@@ -83,15 +83,6 @@ __device__ __forceinline__ void box_of<double>(const Scalars* sc, double* b, dou
 }
 
 // ------------------------------------------------------------------ per step
-__global__ void k_begin(Scalars* sc, int nupdate, int nmts) {
-  if (sc->abort) return;
-  for (int k = 0; k < 4; ++k) sc->work[k] = 0u;
-  int st = ++sc->step;
-  sc->rebuild = (st % nupdate) == 0;
-  sc->mts_m = nmts > 0 ? st % (3 + nmts) : -1;
-  sc->miu = 1.0;
-}
-
 // Fold into the primary box (SHIFT.f90:37-43): applied to all three
 // components when any one lies outside [-L/2, L/2].
 template <typename R>
@@ -109,8 +100,9 @@ __device__ __forceinline__ void fold3(R* r, const R* b2) {
 }
 
 struct PosArgs {
+  Scalars* sc;
   int natoms, nvirta;
-  int begin, nupdate, nmts;  // begin != 0: also start the step (k_begin)
+  int nupdate, nmts;
   const double* S;     // unwrapped positions (3,NITEMS), FP64 state
   double* Svs;         // VS rows of S (written for the FP64 path and output)
   const int* tbits;    // type | label<<16 per particle
@@ -125,22 +117,37 @@ struct PosArgs {
 
 // SHIFT.f90:36-44 for atoms and VIRTUAL_DEF.f90:67-95 for virtual sites
 // (centre-of-mass sums with all three components reset per site).
-// begin: when set, block 0 first advances the step counter (k_begin's work);
-// the positions do not depend on it.
-template <typename R>
-__global__ void k_positions(PosArgs a, Scalars* sc) {
+// begin: when set, block 0 first starts the step: it advances the step
+// counter and sets this step's flags, or marks the step skipped when the run
+// aborted.  A system that has run its last step (done) is left as it is, so
+// its virtual-site rows keep the values of its last step.
+template <typename R, bool B>
+__global__ void k_positions(__grid_constant__ const PosArgs a0, const PosArgs* const* tab, const BlockMap bm,
+                            int begin) {
   using PT = typename Prec<R>::pos_t;
-  if (a.begin && blockIdx.x == 0 && threadIdx.x == 0 && !sc->abort) {
-    for (int k = 0; k < 4; ++k) sc->work[k] = 0u;
-    const int st = ++sc->step;
-    sc->rebuild = (st % a.nupdate) == 0;
-    sc->mts_m = a.nmts > 0 ? st % (3 + a.nmts) : -1;
-    sc->miu = 1.0;
+  const Blk bk = blk<B>(bm);
+  const PosArgs& a = B ? *tab[bk.sys] : a0;
+  Scalars* sc = a.sc;
+  if (sc->done) {
+    if (begin && bk.b == 0 && threadIdx.x == 0) sc->skip = 1;
+    return;
+  }
+  if (begin && bk.b == 0 && threadIdx.x == 0) {
+    if (sc->abort) {
+      sc->skip = 1;
+    } else {
+      sc->skip = 0;
+      for (int q = 0; q < 4; ++q) sc->work[q] = 0u;
+      const int st = ++sc->step;
+      sc->rebuild = (st % a.nupdate) == 0;
+      sc->mts_m = a.nmts > 0 ? st % (3 + a.nmts) : -1;
+      sc->miu = 1.0;
+    }
   }
   const int n = a.natoms + a.nvirta;
   R b[3], bi[3], b2[3];
   box_of<R>(sc, b, bi, b2);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (int i = bk.b * blockDim.x + threadIdx.x; i < n; i += bk.g * blockDim.x) {
     R s[3];
     if (i < a.natoms) {
 #pragma unroll
@@ -179,6 +186,7 @@ __global__ void k_positions(PosArgs a, Scalars* sc) {
 
 // ------------------------------------------------------------ cell lists
 struct ListArgs {
+  Scalars* sc;
   int n;             // particles in the list
   int which;         // 0 atoms, 1 beads
   int natoms;        // NATOMS (VS-VS exclusion)
@@ -207,11 +215,19 @@ struct ListArgs {
   const int* excl;   // CONNECTED_TO, [i*20 + c], 0-based
 };
 
+// List-rebuild kernels run when the step rebuilds its lists (or always, for
+// the rebuild of ibg_set_state) and the step is not skipped.
+//
 // UPDATE_NEIGHBOURLIST.F90:14-48 / ALLOCATEVAR2.f90:156-180: cells per
-// dimension = INT(BOX/RLIST).
-template <typename R>
-__global__ void k_regrid(ListArgs L, Scalars* sc) {
-  if (threadIdx.x || blockIdx.x) return;
+// dimension = INT(BOX/RLIST).  The grid also clears the cell counters.
+template <typename R, bool B>
+__global__ void k_regrid(__grid_constant__ const ListArgs L0, const ListArgs* const* tab, const BlockMap bm, int always) {
+  const Blk bk = blk<B>(bm);
+  const ListArgs& L = B ? *tab[bk.sys] : L0;
+  Scalars* sc = L.sc;
+  if (sc->skip || !(always || sc->rebuild)) return;
+  for (int c = bk.b * blockDim.x + threadIdx.x; c < L.cell_cap; c += bk.g * blockDim.x) L.cell_count[c] = 0;
+  if (threadIdx.x || bk.b) return;
   int nc[3];
   for (int c = 0; c < 3; ++c) {
     if (sizeof(R) == 4) nc[c] = fint(sc->boxf[c] / L.rlist);
@@ -227,14 +243,18 @@ __global__ void k_regrid(ListArgs L, Scalars* sc) {
 
 // LINKS.f90:192-194.  A component equal to NCELL (coordinate at +L/2 after
 // rounding) would address a cell outside the grid; it is clamped and counted.
-template <typename R>
-__global__ void k_cell_assign(ListArgs L, Scalars* sc) {
+template <typename R, bool B>
+__global__ void k_cell_assign(__grid_constant__ const ListArgs L0, const ListArgs* const* tab, const BlockMap bm, int always) {
   using PT = typename Prec<R>::pos_t;
+  const Blk bk = blk<B>(bm);
+  const ListArgs& L = B ? *tab[bk.sys] : L0;
+  Scalars* sc = L.sc;
+  if (sc->skip || !(always || sc->rebuild)) return;
   const int nx = sc->ncell[L.which][0], ny = sc->ncell[L.which][1], nz = sc->ncell[L.which][2];
   R b[3], bi[3], b2[3];
   box_of<R>(sc, b, bi, b2);
   const PT* pos = (const PT*)L.pos4;
-  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < L.n; a += gridDim.x * blockDim.x) {
+  for (int a = bk.b * blockDim.x + threadIdx.x; a < L.n; a += bk.g * blockDim.x) {
     PT p = pos[L.slot_of[a]];
     R x[3] = {p.x, p.y, p.z};
     int nc[3] = {nx, ny, nz}, k[3];
@@ -252,29 +272,54 @@ __global__ void k_cell_assign(ListArgs L, Scalars* sc) {
   }
 }
 
-// Single-block exclusive scan of m ints (out has m+1 entries); zeroes zero[]
-// (m entries) when given.
-__global__ void k_scan_int(const int* in, int* out, int m, int* zero) {
-  __shared__ int part[1024];
-  const int t = threadIdx.x, T = blockDim.x;
+// Exclusive scan of the cell counts by one block per system (cell_start has
+// cell_cap + 1 entries); clears the fill counters.
+template <bool B>
+__global__ void k_scan_cells(__grid_constant__ const ListArgs L0, const ListArgs* const* tab, const BlockMap bm, int always) {
+  const Blk bk = blk<B>(bm);
+  const ListArgs& L = B ? *tab[bk.sys] : L0;
+  Scalars* sc = L.sc;
+  if (sc->skip || !(always || sc->rebuild)) return;
+  const int* in = L.cell_count;
+  int* out = L.cell_start;
+  int* zero = L.cell_fill;
+  const int m = L.cell_cap;
+  __shared__ int wsum[32];
+  const int t = threadIdx.x, T = blockDim.x, lane = t & 31, warp = t >> 5, nw = (T + 31) >> 5;
   const int chunk = (m + T - 1) / T;
   const int b = t * chunk, e = min(m, b + chunk);
   int s = 0;
   for (int i = b; i < e; ++i) s += in[i];
-  part[t] = s;
+  int v = s;  // inclusive scan of the chunk sums: warps, then warp totals
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += y;
+  }
+  if (lane == 31) wsum[warp] = v;
   __syncthreads();
-  if (t == 0) {
-    int run = 0;
-    for (int i = 0; i < T; ++i) { int v = part[i]; part[i] = run; run += v; }
-    out[m] = run;
+  if (warp == 0) {
+    int w = lane < nw ? wsum[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    wsum[lane] = w;
   }
   __syncthreads();
-  int run = part[t];
-  for (int i = b; i < e; ++i) { int v = in[i]; out[i] = run; run += v; if (zero) zero[i] = 0; }
+  int run = v - s + (warp ? wsum[warp - 1] : 0);
+  if (t == T - 1) out[m] = run + s;
+  for (int i = b; i < e; ++i) { int x = in[i]; out[i] = run; run += x; zero[i] = 0; }
 }
 
-__global__ void k_cell_fill(ListArgs L) {
-  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < L.n; a += gridDim.x * blockDim.x) {
+template <bool B>
+__global__ void k_cell_fill(__grid_constant__ const ListArgs L0, const ListArgs* const* tab, const BlockMap bm, int always) {
+  const Blk bk = blk<B>(bm);
+  const ListArgs& L = B ? *tab[bk.sys] : L0;
+  Scalars* sc = L.sc;
+  if (sc->skip || !(always || sc->rebuild)) return;
+  for (int a = bk.b * blockDim.x + threadIdx.x; a < L.n; a += bk.g * blockDim.x) {
     int c = L.cell_of[a];
     int s = L.cell_start[c] + atomicAdd(&L.cell_fill[c], 1);
     L.sorted_new[s] = a;
@@ -285,8 +330,13 @@ __global__ void k_cell_fill(ListArgs L) {
 // (LINKS.f90:195-196); slots are kept in increasing A so the list build can
 // walk them backwards.  k_cell_fill placed a cell's entries in arbitrary order
 // (atomics); here each entry finds its rank among its cell's entries.
-__global__ void k_cell_rank(ListArgs L, const Scalars* sc) {
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < L.n; s += gridDim.x * blockDim.x) {
+template <bool B>
+__global__ void k_cell_rank(__grid_constant__ const ListArgs L0, const ListArgs* const* tab, const BlockMap bm, int always) {
+  const Blk bk = blk<B>(bm);
+  const ListArgs& L = B ? *tab[bk.sys] : L0;
+  Scalars* sc = L.sc;
+  if (sc->skip || !(always || sc->rebuild)) return;
+  for (int s = bk.b * blockDim.x + threadIdx.x; s < L.n; s += bk.g * blockDim.x) {
     const int a = L.sorted_new[s];
     const int c = L.cell_of[a];
     const int b = L.cell_start[c], e = L.cell_start[c + 1];
@@ -299,10 +349,14 @@ __global__ void k_cell_rank(ListArgs L, const Scalars* sc) {
 // New slot order: positions move to their new slots, and the slot of every
 // entry (and of its global particle) is updated.  Reads the ordered cells from
 // the scratch k_cell_rank wrote; writes the new order to sorted.
-template <typename R>
-__global__ void k_reslot(ListArgs L) {
+template <typename R, bool B>
+__global__ void k_reslot(__grid_constant__ const ListArgs L0, const ListArgs* const* tab, const BlockMap bm, int always) {
   using PT = typename Prec<R>::pos_t;
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < L.n; s += gridDim.x * blockDim.x) {
+  const Blk bk = blk<B>(bm);
+  const ListArgs& L = B ? *tab[bk.sys] : L0;
+  Scalars* sc = L.sc;
+  if (sc->skip || !(always || sc->rebuild)) return;
+  for (int s = bk.b * blockDim.x + threadIdx.x; s < L.n; s += bk.g * blockDim.x) {
     int a = L.slot_of_new[s];
     ((PT*)L.pos4_new)[s] = ((const PT*)L.pos4)[L.slot_of[a]];
     L.sorted[s] = a;
@@ -310,9 +364,19 @@ __global__ void k_reslot(ListArgs L) {
   }
 }
 
-// slot_of from the new order (after k_reslot and the position copy).
-__global__ void k_slot_of(ListArgs L) {
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < L.n; s += gridDim.x * blockDim.x) L.slot_of[L.sorted[s]] = s;
+// slot_of from the new order, and the positions into their new slots (after
+// k_reslot).
+template <typename R, bool B>
+__global__ void k_slot_of(__grid_constant__ const ListArgs L0, const ListArgs* const* tab, const BlockMap bm, int always) {
+  using PT = typename Prec<R>::pos_t;
+  const Blk bk = blk<B>(bm);
+  const ListArgs& L = B ? *tab[bk.sys] : L0;
+  Scalars* sc = L.sc;
+  if (sc->skip || !(always || sc->rebuild)) return;
+  for (int s = bk.b * blockDim.x + threadIdx.x; s < L.n; s += bk.g * blockDim.x) {
+    L.slot_of[L.sorted[s]] = s;
+    ((PT*)L.pos4)[s] = ((const PT*)L.pos4_new)[s];
+  }
 }
 
 // NEW_NEIGHBOUR_WITHLIST.f90:34-123.  T lanes share one slot (particle); a
@@ -326,9 +390,20 @@ __global__ void k_slot_of(ListArgs L) {
 // (g*w_cap + k/T)*32 + (s%P)*T + k%T.  A slice that needs more than w_cap rows
 // records its need and raises the abort flag (the host enlarges the storage
 // and repeats the step).
-template <typename R, int T>
-__global__ void __launch_bounds__(256) k_list_build(ListArgs L, Scalars* sc) {
+// The 13 neighbour cells of the half stencil in MAPS.f90:137-149 order.
+__constant__ int kStencil[13][3] = {{1, 0, 0}, {1, 1, 0},  {0, 1, 0},  {-1, 1, 0}, {1, 0, -1}, {1, 1, -1}, {0, 1, -1},
+                                    {-1, 1, -1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}, {-1, 1, 1}, {0, 0, 1}};
+
+template <typename R, int T, bool B>
+__global__ void __launch_bounds__(256) k_list_build(__grid_constant__ const ListArgs L0, const ListArgs* const* tab, const BlockMap bm, int always) {
   using PT = typename Prec<R>::pos_t;
+  const Blk bk = blk<B>(bm);
+  __shared__ ListArgs s_args;
+  if (B) stage_args(&s_args, tab[bk.sys]);
+  const ListArgs& L = B ? s_args : L0;
+  Scalars* sc = L.sc;
+  if (sc->skip || !(always || sc->rebuild)) return;
+
   constexpr int P = 32 / T;
   const int nx = sc->ncell[L.which][0], ny = sc->ncell[L.which][1], nz = sc->ncell[L.which][2];
   R b[3], bi[3], b2[3];
@@ -339,8 +414,6 @@ __global__ void __launch_bounds__(256) k_list_build(ListArgs L, Scalars* sc) {
   const unsigned gmask = ((1u << T) - 1u) << (grp * T);
   const int nslices = (L.n + P - 1) / P;
   const int cap = L.w_cap * T;  // entries a slot may hold
-  const int off[13][3] = {{1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {-1, 1, 0}, {1, 0, -1}, {1, 1, -1}, {0, 1, -1},
-                          {-1, 1, -1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}, {-1, 1, 1}, {0, 0, 1}};
   for (;;) {
     int g = 0;
     if (lane == 0) g = (int)atomicAdd(&sc->work[2 + L.which], 1u);
@@ -391,7 +464,8 @@ __global__ void __launch_bounds__(256) k_list_build(ListArgs L, Scalars* sc) {
       segment(s - 1, L.cell_start[c0]);
 #pragma unroll 1
       for (int u = 0; u < 13; ++u) {
-        const int jx = (ix + off[u][0] + nx) % nx, jy = (iy + off[u][1] + ny) % ny, jz = (iz + off[u][2] + nz) % nz;
+        const int jx = (ix + kStencil[u][0] + nx) % nx, jy = (iy + kStencil[u][1] + ny) % ny,
+                  jz = (iz + kStencil[u][2] + nz) % nz;
         const int c = jx * nz * ny + jy * nz + jz;
         segment(L.cell_start[c + 1] - 1, L.cell_start[c]);
       }
@@ -407,6 +481,7 @@ __global__ void __launch_bounds__(256) k_list_build(ListArgs L, Scalars* sc) {
       if (rows > L.w_cap) {
         atomicMax(&sc->need_rows[L.which], rows);
         sc->abort = 1;
+        sc->skip = 1;
       }
     }
   }
@@ -415,6 +490,8 @@ __global__ void __launch_bounds__(256) k_list_build(ListArgs L, Scalars* sc) {
 // ------------------------------------------------------------- nonbonded
 template <typename R>
 struct NBArgs {
+  Scalars* sc;
+  int mts;                         // bead list of an MTS run: only steps m = 1..3 evaluate it
   int n, nslices, ntype;
   const void* pos4;
   const int* counts;
@@ -434,9 +511,20 @@ struct NBArgs {
   const R* tx;
   int ntab, nrows;
   R rcutsq;
-  double* part;  // 9 per block: V_NB(1..3), PT11,PT22,PT33,PT12,PT13,PT23
-  int part_stride;
 };
+
+// A nonbonded launch does nothing on a skipped step, and for the bead list
+// of an MTS run on the steps MTS_APPROX extrapolates (MTS_LOOP.f90:100-110).
+template <typename R>
+__device__ __forceinline__ bool nb_idle(const NBArgs<R>& A) {
+  const Scalars* sc = A.sc;
+  if (sc->skip) return true;
+  if (A.mts) {
+    const int m = sc->mts_m;
+    return !(m >= 1 && m <= 3);
+  }
+  return false;
+}
 
 // NONBONDED_FORCE.F90:173-232.  Persistent grid; a warp owns one slice of
 // P = 32/T slots at a time and T lanes walk each slot's list; list reads are
@@ -444,9 +532,16 @@ struct NBArgs {
 // cell-ordered array.  i-forces are summed in registers and reduced exactly
 // over the slot's lanes (integer shuffles); j-forces are 64-bit integer
 // atomics.  Tables are staged in shared memory when SMEM.
-template <typename R, bool SMEM, int T>
-__global__ void __launch_bounds__(256, 4) k_nonbonded(NBArgs<R> A, Scalars* sc) {
+template <typename R, bool SMEM, int T, bool B>
+__global__ void __launch_bounds__(256, 4) k_nonbonded(__grid_constant__ const NBArgs<R> A0, const NBArgs<R>* const* tab,
+                                                      const BlockMap bm) {
   using P = Prec<R>;
+  const Blk bk = blk<B>(bm);
+  __shared__ NBArgs<R> s_args;
+  if (B) stage_args(&s_args, tab[bk.sys]);
+  const NBArgs<R>& A = B ? s_args : A0;
+  Scalars* sc = A.sc;
+  if (nb_idle(A)) return;
   using PT = typename P::pos_t;
   using reg_t = typename P::reg_t;
   constexpr int PS = 32 / T;
@@ -482,7 +577,7 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded(NBArgs<R> A, Scalars* sc) 
 #pragma unroll
   for (int k = 0; k < 9; ++k) acc[k] = 0.0;
   unsigned err = 0;
-  const bool run = !sc->abort;
+  const bool run = true;
   // work unit = up to ROWS rows of 32 entries of one slice; units are taken
   // dynamically so that warps finish within one unit of each other
   constexpr int ROWS = 8;
@@ -578,7 +673,7 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded(NBArgs<R> A, Scalars* sc) 
   double out[9];
   block_sum<9>(acc, red, out);
   if (threadIdx.x == 0)
-    for (int k = 0; k < 9; ++k) A.part[k * A.part_stride + blockIdx.x] = out[k];
+    for (int k = 0; k < 9; ++k) atomicAdd((double*)&sc->nbacc[A.work][k], out[k]);
 }
 
 // round(v * 2^32) for |v| < 2^31 with integer operations only (the
@@ -597,21 +692,45 @@ __device__ __forceinline__ long long f2fix(float v) {
   return (u >> 31) ? -mag : mag;
 }
 
+// round(v * 2^S) as a 64-bit integer with integer operations only; values of
+// magnitude 2^(63-S) and above (and Inf/NaN) raise EB_FIXED and count as 0.
+template <int S>
+__device__ __forceinline__ long long fixq(float v, unsigned& err) {
+  const unsigned u = __float_as_uint(v);
+  const int e = (int)((u >> 23) & 0xffu);
+  const long long m = (long long)((u & 0x7fffffu) | 0x800000u);
+  const int sh = e - 150 + S;
+  long long mag;
+  if (sh > 39) { err |= EB_FIXED; mag = 0; }
+  else if (sh >= 0) mag = m << sh;
+  else if (sh > -25) mag = (m + (1LL << (-sh - 1))) >> (-sh);
+  else mag = 0;
+  return (u >> 31) ? -mag : mag;
+}
+
 // NONBONDED_FORCE.F90:173-232, FP32 force path.  Same structure as
 // k_nonbonded (slices of P = 32/T slots, T lanes per slot, dynamic units of
 // ROWS list rows).  The arithmetic is REAL*4 as in the reference, with
 // cheaper equivalents where only the force value (not a bit pattern) is
 // compared: minimum image by compare-and-select, r from rsqrt, the table row
 // and interpolation weight from a precomputed 1/bin, float-to-fixed on the
-// integer units.  Energies and virials are summed in FP32 over one unit and
-// then in FP64 in a per-lane shared-memory slot (a fixed order, so the sums are
-// reproducible).
-template <bool SMEM, int T>
-__global__ void __launch_bounds__(256, 4) k_nonbonded_f32(NBArgs<float> A, Scalars* sc) {
+// integer units.  Energies and virials are summed in FP32 over one unit, then
+// as 64-bit fixed point (2^-24) per lane and per block, and added to the
+// system's accumulators: integer sums do not depend on which warp took which
+// unit, so they are reproducible and the same alone or in a batch.
+template <bool SMEM, int T, bool B>
+__global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ const NBArgs<float> A0,
+                                                          const NBArgs<float>* const* tab, const BlockMap bm) {
   constexpr int PS = 32 / T;
   constexpr int ROWS = 8;
+  const Blk bk = blk<B>(bm);
+  __shared__ NBArgs<float> s_args;
+  if (B) stage_args(&s_args, tab[bk.sys]);
+  const NBArgs<float>& A = B ? s_args : A0;
+  Scalars* sc = A.sc;
+  if (nb_idle(A)) return;
   extern __shared__ unsigned char smem_raw[];
-  double* lacc = (double*)smem_raw;  // [9][blockDim.x] per-lane sums
+  long long* lacc = (long long*)smem_raw;  // [9][blockDim.x] per-lane sums
   const int* ltab = A.ltab;
   const int* toff = A.toff;
   const int* tndat = A.tndat;
@@ -634,14 +753,14 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(NBArgs<float> A, Scala
       ltab = s_ltab; toff = s_toff; tndat = s_ndat; tinv = s_inv; tfp = s_fp; tx = s_x;
     }
   }
-  for (int k = 0; k < 9; ++k) lacc[k * blockDim.x + threadIdx.x] = 0.0;
+  for (int k = 0; k < 9; ++k) lacc[k * blockDim.x + threadIdx.x] = 0;
   __syncthreads();
   const float bx = sc->boxf[0], by = sc->boxf[1], bz = sc->boxf[2];
   const float hx = sc->box2f[0], hy = sc->box2f[1], hz = sc->box2f[2];
   const float4* pos = (const float4*)A.pos4;
   const int lane = threadIdx.x & 31, grp = lane / T, q = lane % T;
   unsigned err = 0;
-  const bool run = !sc->abort;
+  const bool run = true;
   const int U = (A.w_cap + ROWS - 1) / ROWS;
   const int nunits = A.nslices * U;
   for (;;) {
@@ -720,21 +839,19 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(NBArgs<float> A, Scala
       atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)s + 1], (unsigned long long)fi1);
       atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)s + 2], (unsigned long long)fi2);
     }
-    double* la = lacc + threadIdx.x;
-    la[0] += (double)e[0];
-    la[blockDim.x] += (double)e[1];
-    la[2 * blockDim.x] += (double)e[2];
+    long long* la = lacc + threadIdx.x;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) la[(3 + k) * blockDim.x] += (double)vir[k];
+    for (int k = 0; k < 3; ++k) la[k * blockDim.x] += fixq<24>(e[k], err);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) la[(3 + k) * blockDim.x] += fixq<24>(vir[k], err);
   }
   if (err) atomicOr(&sc->err, err);
-  double acc[9];
+  long long acc[9];
   for (int k = 0; k < 9; ++k) acc[k] = lacc[k * blockDim.x + threadIdx.x];
   __syncthreads();
-  double out[9];
-  block_sum<9>(acc, lacc, out);
-  if (threadIdx.x == 0)
-    for (int k = 0; k < 9; ++k) A.part[k * A.part_stride + blockIdx.x] = out[k];
+  block_sum_i64<9>(acc, lacc);
+  if (threadIdx.x < 9 && lacc[threadIdx.x] != 0)
+    atomicAdd(&sc->nbacc[A.work][threadIdx.x], (unsigned long long)lacc[threadIdx.x]);
 }
 
 // Per-slot forces of both lists into the global-order nonbonded force
@@ -743,6 +860,7 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(NBArgs<float> A, Scala
 // MTS_LOOP.f90:176).  The slot buffer is cleared for the next step.
 template <typename R>
 struct CollectArgs {
+  Scalars* sc;
   int n;                         // slots in this list
   int mts;                       // 1 for the bead list of an MTS run
   const int* sorted;             // slot -> A
@@ -752,13 +870,17 @@ struct CollectArgs {
   typename Prec<R>::acc_t* mtsf; // [3][n][3] by A
 };
 
-template <typename R>
-__global__ void k_nb_collect(CollectArgs<R> C, Scalars* sc) {
+template <typename R, bool B>
+__global__ void k_nb_collect(__grid_constant__ const CollectArgs<R> C0, const CollectArgs<R>* const* tab,
+                             const BlockMap bm) {
   using P = Prec<R>;
-  if (sc->abort) return;
+  const Blk bk = blk<B>(bm);
+  const CollectArgs<R>& C = B ? *tab[bk.sys] : C0;
+  Scalars* sc = C.sc;
+  if (sc->skip) return;
   const int m = sc->mts_m;
   const bool explicit_step = !C.mts || (m >= 1 && m <= 3);
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < C.n; s += gridDim.x * blockDim.x) {
+  for (int s = bk.b * blockDim.x + threadIdx.x; s < C.n; s += bk.g * blockDim.x) {
     const int a = C.sorted[s];
     const int gi = C.idx[a];
     if (explicit_step) {
@@ -781,13 +903,32 @@ __global__ void k_nb_collect(CollectArgs<R> C, Scalars* sc) {
   }
 }
 
-// DISTRIBUTE_VSFORCE.f90:27-37: F(atom) += F(vs) * VIRT_MASSCOEFF; F(vs) = 0.
 template <typename R>
-__global__ void k_distribute(typename Prec<R>::acc_t* F, int natoms, int nvirta, const int* vnum, const int* vmem,
-                             const float* vcoef, Scalars* sc) {
+struct DistArgs {
+  Scalars* sc;
+  typename Prec<R>::acc_t* F[2];  // nonbonded / bonded forces (3,NITEMS)
+  int natoms, nvirta;
+  const int* vnum;
+  const int* vmem;
+  const float* vcoef;
+};
+
+// DISTRIBUTE_VSFORCE.f90:27-37: F(atom) += F(vs) * VIRT_MASSCOEFF; F(vs) = 0,
+// on the nonbonded (which = 0) or bonded (which = 1) forces.
+template <typename R, bool B>
+__global__ void k_distribute(__grid_constant__ const DistArgs<R> D0, const DistArgs<R>* const* tab, const BlockMap bm,
+                             int which) {
   using P = Prec<R>;
-  if (sc->abort) return;
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nvirta; v += gridDim.x * blockDim.x) {
+  const Blk bk = blk<B>(bm);
+  const DistArgs<R>& D = B ? *tab[bk.sys] : D0;
+  Scalars* sc = D.sc;
+  if (sc->skip) return;
+  typename P::acc_t* F = D.F[which];
+  const int natoms = D.natoms, nvirta = D.nvirta;
+  const int* vnum = D.vnum;
+  const int* vmem = D.vmem;
+  const float* vcoef = D.vcoef;
+  for (int v = bk.b * blockDim.x + threadIdx.x; v < nvirta; v += bk.g * blockDim.x) {
     const size_t vs = (size_t)(natoms + v);
     double f[3];
 #pragma unroll
@@ -807,6 +948,7 @@ __global__ void k_distribute(typename Prec<R>::acc_t* F, int natoms, int nvirta,
 // --------------------------------------------------------------- bonded
 template <typename A>
 struct BondedArgs {
+  Scalars* sc;
   const double* su;                // unwrapped positions (3,NITEMS), FP64
   typename Prec<A>::acc_t* fb;     // bonded forces (3,NITEMS)
   int nb, na, nt, no;
@@ -846,9 +988,13 @@ __device__ __forceinline__ void addf(typename Prec<A>::acc_t* F, int i, const do
 // trans dihedrals amplifies REAL*4 rounding (about 1e-5 of the largest force
 // in a strained chain), while the terms are few; the forces are summed in the
 // path's accumulator (64-bit fixed point on the FP32 path).
-template <typename A>
-__global__ void __launch_bounds__(256) k_bonded(BondedArgs<A> B, Scalars* sc) {
+template <typename A, bool BA>
+__global__ void __launch_bounds__(256) k_bonded(__grid_constant__ const BondedArgs<A> B0, const BondedArgs<A>* const* tab,
+                                                const BlockMap bm) {
   using R = double;
+  const Blk bk = blk<BA>(bm);
+  const BondedArgs<A>& B = BA ? *tab[bk.sys] : B0;
+  Scalars* sc = B.sc;
   __shared__ double red[12 * 8];
   double acc[12];
 #pragma unroll
@@ -856,9 +1002,9 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs<A> B, Scalars* sc) {
   unsigned long long overext = 0;
   unsigned* err = &sc->err;
   const R* S = B.su;
-  const int total = sc->abort ? 0 : B.nb + B.na + B.nt + B.no;
+  const int total = sc->skip ? 0 : B.nb + B.na + B.nt + B.no;
   auto pos = [&](int i, R* o) { o[0] = S[3 * (size_t)i]; o[1] = S[3 * (size_t)i + 1]; o[2] = S[3 * (size_t)i + 2]; };
-  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < total; u += gridDim.x * blockDim.x) {
+  for (int u = bk.b * blockDim.x + threadIdx.x; u < total; u += bk.g * blockDim.x) {
     if (u < B.nb) {  // -------------------------------- bond
       const int4 e = B.bonds[u];
       R ri[3], rj[3], d[3];
@@ -1091,17 +1237,18 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs<A> B, Scalars* sc) {
   double out[12];
   block_sum<12>(acc, red, out);
   if (threadIdx.x == 0)
-    for (int k = 0; k < 12; ++k) B.part[k * B.part_stride + blockIdx.x] = out[k];
+    for (int k = 0; k < 12; ++k) B.part[k * B.part_stride + bk.b] = out[k];
 }
 
 // ------------------------------------------------------------ integration
 template <typename R>
 struct MoveArgs {
+  Scalars* sc;
   int natoms;
   double* S;  // (3,NATOMS) unwrapped, FP64 state
   double* V;  // (3,NATOMS)
-  const typename Prec<R>::acc_t* fnb;
-  const typename Prec<R>::acc_t* fb;
+  typename Prec<R>::acc_t* fnb;
+  typename Prec<R>::acc_t* fb;
   const int* tbits;         // label in bits 16.. (1 atom, 2 bead)
   const double* mass;       // per particle
   const double* invmass;    // per particle
@@ -1113,24 +1260,33 @@ struct MoveArgs {
 
 // MOVE.F90:81-129 (leap-frog with Berendsen factors per class) and the
 // bonded virial sum of NEW_FORCE.F90:73-80, which uses the positions before
-// the update.  Partials: PTK(6) atoms, PTK(6) beads, bonded virial(6).
-template <typename R>
-__global__ void __launch_bounds__(256) k_move(MoveArgs<R> M, Scalars* sc) {
+// the update.  Partials: PTK(6) atoms, PTK(6) beads, bonded virial(6).  The
+// bonded forces are folded into the nonbonded array (fnb becomes the total
+// force FXYZ of the step) and cleared for the next step.
+template <typename R, bool B>
+__global__ void __launch_bounds__(256) k_move(__grid_constant__ const MoveArgs<R> M0, const MoveArgs<R>* const* tab,
+                                              const BlockMap bm) {
   using P = Prec<R>;
+  const Blk bk = blk<B>(bm);
+  const MoveArgs<R>& M = B ? *tab[bk.sys] : M0;
+  Scalars* sc = M.sc;
   __shared__ double red[18 * 8];
   double acc[18];
 #pragma unroll
   for (int k = 0; k < 18; ++k) acc[k] = 0.0;
   const double lam0 = sc->lam[0], lam1 = sc->lam[1];
-  const int nrun = sc->abort ? 0 : M.natoms;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrun; i += gridDim.x * blockDim.x) {
+  const int nrun = sc->skip ? 0 : M.natoms;
+  for (int i = bk.b * blockDim.x + threadIdx.x; i < nrun; i += bk.g * blockDim.x) {
     double s[3], v[3], fb[3], f[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       s[c] = M.S[3 * (size_t)i + c];
       v[c] = M.V[3 * (size_t)i + c];
-      fb[c] = P::get(M.fb[3 * (size_t)i + c]);
-      f[c] = P::get(M.fnb[3 * (size_t)i + c]) + fb[c];
+      const typename P::acc_t qb = M.fb[3 * (size_t)i + c], qn = M.fnb[3 * (size_t)i + c];
+      fb[c] = P::get(qb);
+      f[c] = P::get(qn) + fb[c];
+      M.fnb[3 * (size_t)i + c] = qn + qb;
+      M.fb[3 * (size_t)i + c] = 0;
     }
     acc[12] += fb[0] * s[0];
     acc[13] += fb[1] * s[1];
@@ -1161,7 +1317,7 @@ __global__ void __launch_bounds__(256) k_move(MoveArgs<R> M, Scalars* sc) {
   double out[18];
   block_sum<18>(acc, red, out);
   if (threadIdx.x == 0)
-    for (int k = 0; k < 18; ++k) M.part[k * M.part_stride + blockIdx.x] = out[k];
+    for (int k = 0; k < 18; ++k) M.part[k * M.part_stride + bk.b] = out[k];
 }
 
 // Initial kinetic energies (main.F90:179-195).  Partials: EK atoms, EK beads.
@@ -1177,47 +1333,73 @@ __global__ void k_kinetic(int natoms, const double* V, const int* tbits, const d
   if (threadIdx.x == 0) { part[blockIdx.x] = out[0]; part[stride + blockIdx.x] = out[1]; }
 }
 
-// MOMENTUM.f90:14-29 in FP64: partial sums of m v, then the removal.
-__global__ void k_mom_sum(int natoms, const double* V, const double* mass, double* part, int stride) {
+struct MomArgs {
+  Scalars* sc;
+  int natoms, halt_drift;
+  double* V;
+  const double* mass;
+  const double* invmass;
+  double* part;  // 3 per block, nblocks blocks
+  int nblocks;
+};
+
+// MOMENTUM.f90:14-29 in FP64 on steps that are multiples of HALT_DRIFT
+// (NEW_LOOP.F90:108-114): partial sums of m v, then the removal.
+template <bool B>
+__global__ void k_mom_sum(__grid_constant__ const MomArgs A0, const MomArgs* const* tab, const BlockMap bm) {
+  const Blk bk = blk<B>(bm);
+  const MomArgs& A = B ? *tab[bk.sys] : A0;
+  const Scalars* sc = A.sc;
+  if (sc->skip || sc->step % A.halt_drift != 0) return;
   __shared__ double red[3 * 8];
   double acc[3] = {0.0, 0.0, 0.0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < natoms; i += gridDim.x * blockDim.x)
-    for (int c = 0; c < 3; ++c) acc[c] += V[3 * (size_t)i + c] * mass[i];
+  for (int i = bk.b * blockDim.x + threadIdx.x; i < A.natoms; i += bk.g * blockDim.x)
+    for (int c = 0; c < 3; ++c) acc[c] += A.V[3 * (size_t)i + c] * A.mass[i];
   double out[3];
   block_sum<3>(acc, red, out);
   if (threadIdx.x == 0)
-    for (int c = 0; c < 3; ++c) part[c * stride + blockIdx.x] = out[c];
+    for (int c = 0; c < 3; ++c) A.part[c * A.nblocks + bk.b] = out[c];
 }
 
-__global__ void k_mom_apply(int natoms, double* V, const double* invmass, const double* part, int stride, int nblocks,
-                            const Scalars* sc) {
+template <bool B>
+__global__ void k_mom_apply(__grid_constant__ const MomArgs A0, const MomArgs* const* tab, const BlockMap bm) {
+  const Blk bk = blk<B>(bm);
+  const MomArgs& A = B ? *tab[bk.sys] : A0;
+  const Scalars* sc = A.sc;
+  if (sc->skip || sc->step % A.halt_drift != 0) return;
   __shared__ double tot[3];
-  if (sc->abort) return;
   if (threadIdx.x < 32) {
     for (int c = 0; c < 3; ++c) {
       double s = 0.0;
-      for (int b = threadIdx.x; b < nblocks; b += 32) s += part[c * stride + b];
+      for (int b = threadIdx.x; b < A.nblocks; b += 32) s += A.part[c * A.nblocks + b];
       s = warp_sum(s);
-      if (threadIdx.x == 0) tot[c] = s / (double)natoms;
+      if (threadIdx.x == 0) tot[c] = s / (double)A.natoms;
     }
   }
   __syncthreads();
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < natoms; i += gridDim.x * blockDim.x)
-    for (int c = 0; c < 3; ++c) V[3 * (size_t)i + c] -= tot[c] * invmass[i];
+  for (int i = bk.b * blockDim.x + threadIdx.x; i < A.natoms; i += bk.g * blockDim.x)
+    for (int c = 0; c < 3; ++c) A.V[3 * (size_t)i + c] -= tot[c] * A.invmass[i];
 }
 
-// SCALEBP.f90:259-261: positions scaled with the box.
-__global__ void k_scale_positions(int natoms, double* S, const Scalars* sc) {
-  if (sc->abort) return;
+// SCALEBP.f90:259-261: positions scaled with the box on the steps the
+// barostat changed it.
+template <typename R, bool B>
+__global__ void k_scale_positions(__grid_constant__ const MoveArgs<R> M0, const MoveArgs<R>* const* tab,
+                                  const BlockMap bm) {
+  const Blk bk = blk<B>(bm);
+  const MoveArgs<R>& M = B ? *tab[bk.sys] : M0;
+  const Scalars* sc = M.sc;
+  if (sc->skip) return;
   const double miu = sc->miu;
   if (miu == 1.0) return;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < natoms; i += gridDim.x * blockDim.x)
-    for (int c = 0; c < 3; ++c) S[3 * (size_t)i + c] *= miu;
+  for (int i = bk.b * blockDim.x + threadIdx.x; i < M.natoms; i += bk.g * blockDim.x)
+    for (int c = 0; c < 3; ++c) M.S[3 * (size_t)i + c] *= miu;
 }
 
 // ------------------------------------------------------------- reductions
 struct FinalArgs {
-  const double* p_nb[2]; int g_nb;   // nonbonded partials of the atom / bead list (9 x g_nb)
+  Scalars* sc;
+  int fixed;                         // nonbonded accumulators in fixed point (FP32 path)
   const double* p_b; int g_b;        // bonded partials (12 x g_b)
   const double* p_mv; int g_mv;      // move partials (18 x g_mv)
   int mts;                           // MTS run
@@ -1235,17 +1417,26 @@ __device__ double wsum(const double* p, int g) {
 
 // Deterministic reduction of all partials into the observables, the MTS
 // auxiliary history (MTS_SAVEAUXS / MTS_LOADAUXS), the thermostat factors of
-// the next step and the barostat window (SCALEBP.f90:240-263).
-__global__ void k_finalize(FinalArgs F, Scalars* sc) {
+// the next step and the barostat window (SCALEBP.f90:240-263).  The
+// nonbonded accumulators are read and cleared for the next step.
+template <bool B>
+__global__ void k_finalize(__grid_constant__ const FinalArgs F0, const FinalArgs* const* tab, const BlockMap bm) {
+  const Blk bk = blk<B>(bm);
+  const FinalArgs& F = B ? *tab[bk.sys] : F0;
+  Scalars* sc = F.sc;
   __shared__ double q[64];
-  if (sc->abort) return;
+  if (sc->skip) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   // q[0..8] atom NB, q[9..17] bead NB, q[18..29] bonded, q[30..47] move
-  for (int k = warp; k < 48; k += nw) {
+  if (threadIdx.x < 18) {
+    unsigned long long* p = &sc->nbacc[threadIdx.x / 9][threadIdx.x % 9];
+    const unsigned long long v = *p;
+    q[threadIdx.x] = F.fixed ? (double)(long long)v * kEnInv : __longlong_as_double((long long)v);
+    *p = 0ull;
+  }
+  for (int k = 18 + warp; k < 48; k += nw) {
     double v;
-    if (k < 9) v = F.p_nb[0] ? wsum(F.p_nb[0] + (size_t)k * F.g_nb, F.g_nb) : 0.0;
-    else if (k < 18) v = F.p_nb[1] ? wsum(F.p_nb[1] + (size_t)(k - 9) * F.g_nb, F.g_nb) : 0.0;
-    else if (k < 30) v = wsum(F.p_b + (size_t)(k - 18) * F.g_b, F.g_b);
+    if (k < 30) v = wsum(F.p_b + (size_t)(k - 18) * F.g_b, F.g_b);
     else v = wsum(F.p_mv + (size_t)(k - 30) * F.g_mv, F.g_mv);
     if (lane == 0) q[k] = v;
   }
@@ -1312,6 +1503,7 @@ __global__ void k_finalize(FinalArgs F, Scalars* sc) {
       }
     }
   }
+  sc->done = sc->step >= sc->stop_at;
   for (int c = 0; c < 6; ++c) o.pt[c] = pt[c];
   for (int c = 0; c < 3; ++c) o.box[c] = sc->box[c];
   o.bond_overext = (long long)sc->bond_overext;

@@ -32,8 +32,15 @@ EXPORTS = [
     "ibg_setup_array_i", "ibg_setup_array_f", "ibg_setup_free",
     "ibg_create", "ibg_set_state", "ibg_step", "ibg_forces", "ibg_run", "ibg_get_state",
     "ibg_get_state_f64", "ibg_get_neighbour_list", "ibg_get_exclusions", "ibg_set_timing",
-    "ibg_get_timing", "ibg_last_error", "ibg_destroy", "ibg_version", "ibg_set_l2_flush", "ibg_set_device", "ibg_set_list_rows", "ibg_nonbonded_static",
+    "ibg_get_timing", "ibg_last_error", "ibg_destroy", "ibg_version", "ibg_set_l2_flush", "ibg_set_device",
+    "ibg_set_list_rows", "ibg_nonbonded_static",
+    "ibg_batch_create", "ibg_batch_run", "ibg_batch_size", "ibg_batch_get_timing", "ibg_batch_last_error",
+    "ibg_batch_destroy", "ibg_device_bytes", "ibg_estimate_bytes",
+    "ibg_server_create", "ibg_server_submit", "ibg_server_wait", "ibg_server_drain", "ibg_server_result",
+    "ibg_server_job_error", "ibg_server_get_stats", "ibg_server_destroy",
 ]
+
+IBG_JOB_QUEUED, IBG_JOB_RUNNING, IBG_JOB_DONE, IBG_JOB_FAILED = 0, 1, 2, 3
 
 
 _I, _F, _PI, _PF = ctypes.c_int, ctypes.c_float, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)
@@ -62,6 +69,16 @@ class IbgDesc(ctypes.Structure):
         + [("ld_vs", _I), ("vs_maxatoms", _I), ("vitype", _PI), ("virt_center", _PI), ("virt_numatoms", _PI),
            ("virt_atm_ind", _PI), ("virt_invmass", _PF), ("virt_masscoeff", _PF)]
     )
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_longlong) for k in ("submitted", "done", "failed", "running", "queued")] + \
+               [(k, ctypes.c_double) for k in ("p50_s", "p99_s", "mean_s", "span_s", "jobs_per_s")] + \
+               [("atom_steps", ctypes.c_longlong), ("atom_steps_per_s", ctypes.c_double), ("gpu_s", ctypes.c_double)] + \
+               [(k, ctypes.c_longlong) for k in ("ticks", "batch_builds", "peak_jobs", "peak_bytes", "budget_bytes")]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class IbgObs(ctypes.Structure):
@@ -138,6 +155,23 @@ def lib(build_if_missing: bool = True):
         "ibg_nonbonded_static": (ctypes.c_int, [ctypes.c_int, ctypes.c_int] + [vp] * 5 + [ctypes.c_int, vp, ctypes.c_int, vp,
                                                 ctypes.c_int, ctypes.c_int] + [vp] * 5 + [vp, ctypes.c_float, vp, vp, vp,
                                                                                         cp, ctypes.c_int]),
+        "ibg_batch_create": (ctypes.c_int, [pvp, ctypes.c_int, pvp]),
+        "ibg_batch_run": (ctypes.c_int, [vp, ctypes.c_int, ip, ctypes.POINTER(IbgObs)]),
+        "ibg_batch_size": (ctypes.c_int, [vp]),
+        "ibg_batch_get_timing": (ctypes.c_int, [vp, dp, ctypes.POINTER(ctypes.c_longlong)]),
+        "ibg_batch_last_error": (cp, [vp]),
+        "ibg_batch_destroy": (None, [vp]),
+        "ibg_device_bytes": (ctypes.c_longlong, [vp]),
+        "ibg_estimate_bytes": (ctypes.c_longlong, [vp, ctypes.c_int, fp]),
+        "ibg_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                             pvp]),
+        "ibg_server_submit": (ctypes.c_int, [vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]),
+        "ibg_server_wait": (ctypes.c_int, [vp, ctypes.c_longlong, ctypes.c_double]),
+        "ibg_server_drain": (ctypes.c_int, [vp, ctypes.c_double]),
+        "ibg_server_result": (ctypes.c_int, [vp, ctypes.c_longlong, fp, fp, ctypes.POINTER(IbgObs), dp]),
+        "ibg_server_job_error": (cp, [vp, ctypes.c_longlong]),
+        "ibg_server_get_stats": (ctypes.c_int, [vp, ctypes.POINTER(ServerStats)]),
+        "ibg_server_destroy": (None, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -319,6 +353,107 @@ class System:
     def close(self):
         if getattr(self, "_h", None):
             lib().ibg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Batch:
+    """Systems stepped together, one launch per stage (``ibg_batch``).
+
+    Holds references to its ``System`` objects so that they outlive it."""
+
+    def __init__(self, systems):
+        self.systems = list(systems)
+        arr = (ctypes.c_void_p * len(self.systems))(*[x._h.value for x in self.systems])
+        h = ctypes.c_void_p()
+        rc = lib().ibg_batch_create(arr, len(self.systems), ctypes.byref(h))
+        if rc != 0:
+            raise IbiscoError(rc, "ibg_batch_create failed")
+        self._h = h
+
+    def run(self, nsteps: int, last_step=None, observe: bool = False):
+        n = len(self.systems)
+        last = None
+        if last_step is not None:
+            last = np.ascontiguousarray(last_step, np.int32)
+        obs = (IbgObs * n)() if observe else None
+        rc = lib().ibg_batch_run(self._h, int(nsteps), _ip(last) if last is not None else None, obs)
+        if rc != 0:
+            raise IbiscoError(rc, lib().ibg_batch_last_error(self._h).decode())
+        return [obs[k].as_dict() for k in range(n)] if observe else None
+
+    def timing(self) -> dict:
+        ms = ctypes.c_double()
+        n = ctypes.c_longlong()
+        lib().ibg_batch_get_timing(self._h, ctypes.byref(ms), ctypes.byref(n))
+        return {"run_ms": ms.value, "launches": n.value}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ibg_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Server:
+    """Continuous-batching service of simulation jobs on one GPU (``ibg_server``)."""
+
+    def __init__(self, device: int = 0, precision: int = IBG_PREC_FP32_FIXED, hbm_budget: int = 0,
+                 max_jobs: int = 64, tick_steps: int = 100):
+        h = ctypes.c_void_p()
+        rc = lib().ibg_server_create(int(device), int(precision), int(hbm_budget), int(max_jobs), int(tick_steps),
+                                     ctypes.byref(h))
+        if rc != 0:
+            raise IbiscoError(rc, "ibg_server_create failed")
+        self._h = h
+        self._shapes = {}
+
+    def submit(self, directory: str, nsteps: int) -> int:
+        """Read a system directory (the reference's input files) and queue it."""
+        h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        rc = lib().ibg_setup_read(directory.encode(), ctypes.byref(h), err, 512)
+        if rc != 0:
+            raise IbiscoError(rc, err.value.decode())
+        d = IbgDesc.from_address(lib().ibg_setup_desc(h))
+        shape = (d.nitems, d.natoms)
+        job = ctypes.c_longlong()
+        rc = lib().ibg_server_submit(self._h, h, int(nsteps), ctypes.byref(job))
+        if rc != 0:
+            lib().ibg_setup_free(h)
+            raise IbiscoError(rc, "ibg_server_submit failed")
+        self._shapes[job.value] = shape
+        return job.value
+
+    def wait(self, job: int, timeout_s: float = -1.0) -> int:
+        return lib().ibg_server_wait(self._h, int(job), float(timeout_s))
+
+    def drain(self, timeout_s: float = -1.0) -> bool:
+        return lib().ibg_server_drain(self._h, float(timeout_s)) == 0
+
+    def result(self, job: int) -> dict:
+        nitems, natoms = self._shapes[job]
+        s = np.zeros((nitems, 3), np.float32)
+        v = np.zeros((natoms, 3), np.float32)
+        o = IbgObs()
+        t = (ctypes.c_double * 3)()
+        rc = lib().ibg_server_result(self._h, int(job), _fp(s), _fp(v), ctypes.byref(o), t)
+        if rc != 0:
+            raise IbiscoError(rc, lib().ibg_server_job_error(self._h, int(job)).decode())
+        return {"sxyz": s, "vxyz": v, "obs": o.as_dict(), "queued_s": t[0], "run_s": t[1], "latency_s": t[2]}
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        lib().ibg_server_get_stats(self._h, ctypes.byref(st))
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ibg_server_destroy(self._h)
             self._h = None
 
     def __del__(self):

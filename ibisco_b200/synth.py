@@ -504,3 +504,67 @@ def feature_mix(seed=7, nmol=6, ensemble="NVT", nmts=0, non_bonded=4, temp=400.0
         nb_tabs=nb_tabs,
         oop_tabs=[((3, 1, 2, 1), oop_t), ((3, 1, 1, 2), oop_t)],
         virtual=virt, virtbonds=vb, virtangles=va)
+
+
+# ------------------------------------------------------------ served jobs
+def serpentine_lattice(m):
+    """The m^3 sites of a cubic lattice in an order where consecutive sites
+    are nearest neighbours (boustrophedon in x, then y, then z)."""
+    pts = []
+    for z in range(m):
+        ys = range(m) if z % 2 == 0 else range(m - 1, -1, -1)
+        for j, y in enumerate(ys):
+            xs = range(m) if (z * m + j) % 2 == 0 else range(m - 1, -1, -1)
+            for x in xs:
+                pts.append((x, y, z))
+    return np.asarray(pts, float)
+
+
+def serving_job(seed, n_target, rho=8.0, nsteps=2000, temp=300.0, amp=0.5):
+    """One job of a served stream: bead-spring chains of 10-100 beads with 1-3
+    bead types, placed along a serpentine path through a cubic lattice of
+    spacing rho^(-1/3) (bonds at their rest length, no overlaps), each type
+    pair with its own LJ table plus a seeded smooth perturbation of 5 Fourier
+    modes (amplitudes up to amp kJ/mol).  rc 1.0 nm, list 1.2 nm every 10 steps,
+    NVT at temp, dt 10 fs."""
+    rng = np.random.default_rng(seed)
+    nper = int(rng.integers(10, 101))
+    nchains = max(1, int(round(n_target / nper)))
+    n = nchains * nper
+    a = rho ** (-1.0 / 3.0)
+    m = int(np.ceil(n ** (1.0 / 3.0)))
+    box = m * a
+    pos = serpentine_lattice(m)[:n] * a - 0.5 * box + 0.5 * a
+    pos += rng.normal(scale=0.01, size=pos.shape)
+    ntypes = int(rng.integers(1, 4))
+    types = list(range(1, ntypes + 1))
+    itype = np.array([1 + (k % ntypes) for ch in range(nchains) for k in range(nper)])
+    mass = 0.072
+    vel = maxwell_boltzmann(rng, [mass] * n, temp)
+    bond_t = harmonic_bond_table("bond.tab", a, 5.0e3, 1.0, 0.001)
+    nb = []
+    for i in types:
+        for j in types:
+            if i <= j:
+                amps = rng.uniform(-amp, amp, size=5) / 5.0
+                nb.append(((i, j), perturbed_lj_table(f"nb{i}{j}", 0.47, 3.5, 1.0, 0.002, amps)))
+    control = dict(ensemble="NVT", temperature=temp, pressure=101.3, atoms=n, num_of_time_steps=nsteps,
+                   time_step=0.010, temperature_coupling_time="0.1D0", pressure_coupling_time="5.0D0",
+                   isothermal_compressibility="1.0D-6", virtual_sites=0, mts=0, bead_cutoff=1.0,
+                   bead_neighbour_list_cutoff=1.2, non_bonded_bead=4, cutoff=1.0, neighbour_list_cutoff=1.2,
+                   update_neighbour_list=10, trajectory=nsteps, halt_drift=nsteps + 1, non_bonded=4,
+                   initialize_velocities="N")
+    return SystemSpec(control=control, types=[(f"C{t}", mass, "A") for t in types], pos=pos, vel=vel,
+                      itype=itype, bonds=chain_bonds(nchains, nper), molecules=[("chain", nper)] * nchains,
+                      box=(box, box, box), bond_tabs=[((i, j), bond_t) for i in types for j in types if i <= j],
+                      nb_tabs=nb)
+
+
+def job_stream(njobs, seed=5, nmin=500, nmax=50000, rate=20.0):
+    """Sizes log-uniform in [nmin, nmax] and Poisson arrival times (jobs/s) of
+    a served stream: [(arrival_s, n_target, job_seed)]."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(nmin), np.log(nmax), size=njobs)).astype(int)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=njobs))
+    arrivals -= arrivals[0]
+    return [(float(t), int(nn), int(seed * 100003 + k)) for k, (t, nn) in enumerate(zip(arrivals, sizes))]

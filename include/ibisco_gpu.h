@@ -202,6 +202,12 @@ int ibg_set_l2_flush(ibg_ctx* c, long long bytes);
    (the same path a growing system takes).  stage_ms[7] of ibg_get_timing
    counts the growths. */
 int ibg_set_list_rows(ibg_ctx* c, int rows);
+/* Device memory a context holds (bytes), and an estimate made before creating
+   one from its descriptor and box; the estimate includes the Verlet-list
+   storage the first list build will need, with margin.  A serving loop admits
+   systems by these figures. */
+long long ibg_device_bytes(const ibg_ctx* c);
+long long ibg_estimate_bytes(const ibg_desc* d, int precision, const float* box);
 /* Select the CUDA device of the calling thread for subsequent ibg_create. */
 int ibg_set_device(int device);
 const char* ibg_last_error(const ibg_ctx* c);
@@ -209,6 +215,34 @@ void ibg_destroy(ibg_ctx* c);
 
 /* Library version string. */
 const char* ibg_version(void);
+
+/* ---------------------------------------------------------------- batch --
+ * Many independent systems stepped together on one GPU.  A batch packs its
+ * systems into one kernel launch per stage (blocks are mapped to systems) and
+ * replays the whole batch step as one CUDA graph.  This is the form in which
+ * many small or mid-size systems, such as iterative Boltzmann inversion trial
+ * runs each with its own tables, fill the GPU.  Every system keeps its own
+ * step counter, list schedule, MTS phase, thermostat and barostat, and its
+ * results are bitwise the same as when it runs alone.
+ *
+ * ibg_batch_create: contexts of one device and precision, each after
+ *   ibg_set_state and in no other batch.  The batch refers to the contexts;
+ *   destroy it before any of them.  Contexts stay usable on their own between
+ *   batch runs (ibg_run, ibg_get_state, ...).
+ * ibg_batch_run: advances every system by nsteps steps from its own last step
+ *   (the step of its last ibg_run/ibg_step or batch run; 0 after
+ *   ibg_set_state), or only up to last_step[s] when last_step is given.
+ *   last_obs (may be NULL) receives, per system, the observables of the last
+ *   step it ran.
+ * ibg_batch_get_timing: device milliseconds of the last ibg_batch_run (CUDA
+ *   events on the batch's stream) and kernels launched by the batch so far. */
+typedef struct ibg_batch ibg_batch;
+int ibg_batch_create(ibg_ctx* const* ctxs, int n, ibg_batch** out);
+int ibg_batch_run(ibg_batch* b, int nsteps, const int* last_step, ibg_obs* last_obs);
+int ibg_batch_size(const ibg_batch* b);
+int ibg_batch_get_timing(const ibg_batch* b, double* run_ms, long long* launches);
+const char* ibg_batch_last_error(const ibg_batch* b);
+void ibg_batch_destroy(ibg_batch* b);
 
 /* ---------------------------------------------------- no-allocation path --
  * ibg_nonbonded_static: the nonbonded forces, energies and virial of one
@@ -239,6 +273,51 @@ int ibg_nonbonded_static(int nitems, int n, const float* rxyz, const int* itype,
                          const float* nbond_force, const float* nbond_pot, const float* binnb,
                          const int* ndatnb, const float* box, float rcutsq, double* fxyz, double* sums,
                          void* stream, char* err, int errlen);
+
+/* -------------------------------------------------------------- serving --
+ * A service of simulation jobs on one GPU with continuous batching.  Jobs are
+ * submitted from any host thread; one service thread admits them in order
+ * while the job-slot count and the device-memory budget allow (estimated with
+ * ibg_estimate_bytes, accounted with ibg_device_bytes), keeps their state,
+ * lists and tables resident, steps all admitted jobs together as one batch,
+ * tick_steps steps per tick, each up to its own step count, and retires
+ * finished jobs between ticks (final state to host memory, device memory
+ * freed).  Jobs that arrive while others run join at the next tick.  A job's
+ * result is bitwise the same as the same system run alone with ibg_run.
+ *
+ * ibg_server_create: hbm_budget <= 0 takes 80 % of the free device memory.
+ * ibg_server_submit: the server takes ownership of the setup (it frees it) and
+ *   runs steps 1..nsteps from the setup's initial state.
+ * ibg_server_wait: blocks until the job is done or failed (timeout_s < 0: no
+ *   limit) and returns its state (IBG_JOB_*).
+ * ibg_server_result: SXYZ(3,NITEMS) and VXYZ(3,NATOMS) after the last step,
+ *   its observables, and times[3] = seconds queued, seconds from admission to
+ *   completion, latency (submission to completion); any pointer may be NULL.
+ * ibg_server_get_stats: counts, latency percentiles over completed jobs, jobs/s and
+ *   atom-steps/s over the span from the first submission to the last
+ *   completion, GPU time of the ticks, and peak residency. */
+#define IBG_JOB_QUEUED 0
+#define IBG_JOB_RUNNING 1
+#define IBG_JOB_DONE 2
+#define IBG_JOB_FAILED 3
+typedef struct ibg_server ibg_server;
+typedef struct ibg_server_stats {
+  long long submitted, done, failed, running, queued;
+  double p50_s, p99_s, mean_s, span_s, jobs_per_s;
+  long long atom_steps;
+  double atom_steps_per_s, gpu_s;
+  long long ticks, batch_builds;
+  long long peak_jobs, peak_bytes, budget_bytes;
+} ibg_server_stats;
+int ibg_server_create(int device, int precision, long long hbm_budget, int max_jobs, int tick_steps,
+                      ibg_server** out);
+int ibg_server_submit(ibg_server* s, ibg_setup* setup, int nsteps, long long* job);
+int ibg_server_wait(ibg_server* s, long long job, double timeout_s);
+int ibg_server_drain(ibg_server* s, double timeout_s);
+int ibg_server_result(ibg_server* s, long long job, float* sxyz, float* vxyz, ibg_obs* last_obs, double* times);
+const char* ibg_server_job_error(ibg_server* s, long long job);
+int ibg_server_get_stats(ibg_server* s, ibg_server_stats* out);
+void ibg_server_destroy(ibg_server* s);
 
 #ifdef __cplusplus
 }
