@@ -161,6 +161,7 @@ struct ibg_ctx {
   SysArgs<double> ad;
   void* dargs = nullptr;  // device copy of af or ad
   int g_list[2] = {1, 1}, g_regrid[2] = {1, 1}, g_build[2] = {1, 1}, g_dist = 1;
+  int nb_blocks_per_sm = 0;  // tuning: resident nonbonded blocks per SM (0: all that fit)
   ObsD* ring = nullptr;
   int ring_cap = 0;
   double *p_b = nullptr, *p_mv = nullptr, *p_mom = nullptr;
@@ -304,7 +305,9 @@ void build_list(ibg_ctx* c, const ibg_desc* d, int which) {
   const size_t rs = rsize(c);
   L.smem = 9 * 256 * sizeof(double) + rs * 3 * (size_t)L.nrows + 2 * rs * L.ntab +
            sizeof(int) * ((size_t)NT * NT + 2 * L.ntab + 1) + 64;
-  L.use_smem = L.smem <= 200 * 1024;
+  // launch defaults (ibg_set_tuning / ibg_autotune change them): the FP32
+  // kernel reads its tables through L1, the FP64 kernel stages them
+  L.use_smem = c->prec != IBG_PREC_FP32_FIXED && L.smem <= 200 * 1024;
 }
 
 void alloc_cells(ibg_ctx* c, DevList& L, const float* box) {
@@ -534,8 +537,9 @@ int nb_occupancy(const ibg_ctx* c, const DevList& L, size_t sm) {
 
 template <typename R>
 void nb_configure(ibg_ctx* c, DevList& L) {
-  const int per = nb_occupancy<R, false>(c, L, nb_smem(c, L));
+  int per = nb_occupancy<R, false>(c, L, nb_smem(c, L));
   nb_occupancy<R, true>(c, L, nb_smem(c, L));
+  if (c->nb_blocks_per_sm > 0) per = std::min(per, c->nb_blocks_per_sm);
   const long long units = (long long)L.nslices * 4;
   L.grid_nb = (int)std::max<long long>(1, std::min<long long>((long long)c->nsm * per, (units + 7) / 8));
 }
@@ -776,6 +780,90 @@ int ibg_set_list_rows(ibg_ctx* c, int rows) {
     return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
   }
   return IBG_OK;
+}
+
+int ibg_get_tuning(const ibg_ctx* c, ibg_tuning* t) {
+  if (!c || !t) return IBG_E_INVALID;
+  const DevList& L = c->L[c->L[0].present ? 0 : 1];
+  t->nb_tables_smem = L.use_smem ? 1 : 0;
+  t->nb_blocks_per_sm = c->nb_blocks_per_sm;
+  return IBG_OK;
+}
+
+int ibg_set_tuning(ibg_ctx* c, const ibg_tuning* t) {
+  if (!c || !t || t->nb_blocks_per_sm < 0) return IBG_E_INVALID;
+  if (c->in_batch) return fail(c, IBG_E_INVALID, "the context is in a batch");
+  try {
+    c->nb_blocks_per_sm = t->nb_blocks_per_sm;
+    for (auto& L : c->L) {
+      if (!L.present) continue;
+      L.use_smem = t->nb_tables_smem != 0 && L.smem <= 200 * 1024;
+      if (c->prec == IBG_PREC_FP32_FIXED) nb_configure<float>(c, L);
+      else nb_configure<double>(c, L);
+    }
+    refresh_args(c);
+    for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+    c->graphs.clear();
+  } catch (CudaError& e) {
+    return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
+  }
+  return IBG_OK;
+}
+
+int ibg_autotune(ibg_ctx* c, int reps, ibg_tuning* best, double* us, int ncand) {
+  if (!c || reps <= 0) return IBG_E_INVALID;
+  if (!c->state_set) return fail(c, IBG_E_INVALID, "ibg_set_state has not been called");
+  if (c->in_batch) return fail(c, IBG_E_INVALID, "the context is in a batch");
+  std::vector<ibg_tuning> cand;
+  for (int smem : {0, 1})
+    for (int per : {0, 3, 2}) cand.push_back(ibg_tuning{smem, per});
+  ibg_tuning keep;
+  ibg_get_tuning(c, &keep);
+  int win = -1;
+  double win_us = 0.0;
+  try {
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (size_t k = 0; k < cand.size(); ++k) {
+      int rc = ibg_set_tuning(c, &cand[k]);
+      if (rc) return rc;
+      float ms = 0.f;
+      for (int r = 0; r <= reps; ++r) {  // the first launch warms up
+        CK(cudaMemsetAsync(c->sc->work, 0, sizeof(c->sc->work), c->st));
+        if (r == 1) CK(cudaEventRecord(e0, c->st));
+        for (auto& L : c->L) {
+          if (!L.present) continue;
+          if (c->prec == IBG_PREC_FP32_FIXED) enq_nonbonded<float>(c, L);
+          else enq_nonbonded<double>(c, L);
+        }
+      }
+      CK(cudaEventRecord(e1, c->st));
+      CK(cudaEventSynchronize(e1));
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      const double t = 1000.0 * ms / reps;
+      if (us && (int)k < ncand) us[k] = t;
+      if (win < 0 || t < win_us) { win = (int)k; win_us = t; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // the timing launches summed forces and energies: clear them
+    for (auto& L : c->L)
+      if (L.present) CK(cudaMemset(L.fsort, 0, accsize(c) * 3 * (size_t)L.n));
+    CK(cudaMemset(c->sc->nbacc, 0, sizeof(c->sc->nbacc)));
+    CK(cudaMemset(c->sc->work, 0, sizeof(c->sc->work)));
+    unsigned bits = 0;
+    CK(cudaMemcpy(&bits, &c->sc->err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (bits) {
+      ibg_set_tuning(c, &keep);
+      return check_device(c);
+    }
+  } catch (CudaError& e) {
+    return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
+  }
+  int rc = ibg_set_tuning(c, &cand[win]);
+  if (best) *best = cand[win];
+  return rc ? rc : (int)cand.size();
 }
 
 int ibg_set_l2_flush(ibg_ctx* c, long long bytes) {

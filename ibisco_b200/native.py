@@ -38,6 +38,7 @@ EXPORTS = [
     "ibg_batch_destroy", "ibg_device_bytes", "ibg_estimate_bytes",
     "ibg_server_create", "ibg_server_submit", "ibg_server_wait", "ibg_server_drain", "ibg_server_result",
     "ibg_server_job_error", "ibg_server_get_stats", "ibg_server_destroy",
+    "ibg_get_tuning", "ibg_set_tuning", "ibg_autotune",
 ]
 
 IBG_JOB_QUEUED, IBG_JOB_RUNNING, IBG_JOB_DONE, IBG_JOB_FAILED = 0, 1, 2, 3
@@ -69,6 +70,13 @@ class IbgDesc(ctypes.Structure):
         + [("ld_vs", _I), ("vs_maxatoms", _I), ("vitype", _PI), ("virt_center", _PI), ("virt_numatoms", _PI),
            ("virt_atm_ind", _PI), ("virt_invmass", _PF), ("virt_masscoeff", _PF)]
     )
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("nb_tables_smem", ctypes.c_int), ("nb_blocks_per_sm", ctypes.c_int)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class ServerStats(ctypes.Structure):
@@ -161,6 +169,9 @@ def lib(build_if_missing: bool = True):
         "ibg_batch_get_timing": (ctypes.c_int, [vp, dp, ctypes.POINTER(ctypes.c_longlong)]),
         "ibg_batch_last_error": (cp, [vp]),
         "ibg_batch_destroy": (None, [vp]),
+        "ibg_get_tuning": (ctypes.c_int, [vp, ctypes.POINTER(Tuning)]),
+        "ibg_set_tuning": (ctypes.c_int, [vp, ctypes.POINTER(Tuning)]),
+        "ibg_autotune": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(Tuning), dp, ctypes.c_int]),
         "ibg_device_bytes": (ctypes.c_longlong, [vp]),
         "ibg_estimate_bytes": (ctypes.c_longlong, [vp, ctypes.c_int, fp]),
         "ibg_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
@@ -343,6 +354,26 @@ class System:
         return {"list_ms": ms[0], "nonbonded_ms": ms[1], "bonded_ms": ms[2], "integrate_ms": ms[3],
                 "other_ms": ms[4], "run_ms": ms[5], "nonbonded_launches": int(ms[6]), "list_growths": int(ms[7]),
                 "launches": n.value}
+
+    def tuning(self) -> dict:
+        t = Tuning()
+        self._check(lib().ibg_get_tuning(self._h, ctypes.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, nb_tables_smem: int = 0, nb_blocks_per_sm: int = 0):
+        t = Tuning(nb_tables_smem, nb_blocks_per_sm)
+        self._check(lib().ibg_set_tuning(self._h, ctypes.byref(t)))
+
+    def autotune(self, reps: int = 20):
+        """Time the candidate tunings of the nonbonded kernel and keep the
+        fastest; returns (best, [(candidate, us per launch)])."""
+        best = Tuning()
+        us = (ctypes.c_double * 16)()
+        n = lib().ibg_autotune(self._h, int(reps), ctypes.byref(best), us, 16)
+        if n < 0:
+            self._check(n)
+        cands = [(sm, per) for sm in (0, 1) for per in (0, 3, 2)]
+        return best.as_dict(), [(c, us[k]) for k, c in enumerate(cands[:n])]
 
     def set_timing(self, on: bool):
         self._check(lib().ibg_set_timing(self._h, 1 if on else 0))

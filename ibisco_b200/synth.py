@@ -148,6 +148,18 @@ def lj_table(fname, sigma, eps, rmax, dr, vcap=1.0e20):
     return Tab(fname, r, v)
 
 
+def shifted_force_lj_table(fname, sigma, eps, rc, dr):
+    """LJ 12-6 with its value and slope shifted to zero at the cutoff rc, so
+    that the energy is continuous and conserved to the integrator's order."""
+    t = lj_table(fname, sigma, eps, rc, dr)
+    sr6 = (sigma / rc) ** 6
+    vc = 4.0 * eps * (sr6 * sr6 - sr6)
+    dvc = 4.0 * eps * (-12.0 * sr6 * sr6 + 6.0 * sr6) / rc
+    v = t.v - vc - (t.x - rc) * dvc
+    v[0] = v[1]
+    return Tab(fname, t.x, v)
+
+
 def perturbed_lj_table(fname, sigma, eps, rmax, dr, amps):
     t = lj_table(fname, sigma, eps, rmax, dr)
     r = t.x
@@ -334,7 +346,7 @@ def _all_torsion_keys(types):
 
 
 # ------------------------------------------------------------------ configs
-def lj_fluid(n=4000, rho=8.0, seed=1, nsteps=1000, dmin=0.3):
+def lj_fluid(n=4000, rho=8.0, seed=1, nsteps=1000, dmin=0.3, shifted=False, dt=0.010):
     """Single-type LJ bead fluid: uniform positions rejected below dmin, LJ
     sigma 0.47 nm.  (With dmin 0.3 nm the first steps at dt 10 fs meet pair
     forces beyond the fixed-point range; a larger dmin avoids that.)"""
@@ -344,14 +356,15 @@ def lj_fluid(n=4000, rho=8.0, seed=1, nsteps=1000, dmin=0.3):
     mass = 0.072
     vel = maxwell_boltzmann(rng, [mass] * n, 300.0)
     control = dict(ensemble="NVE", temperature=300, pressure=101.3, atoms=n, num_of_time_steps=nsteps,
-                   time_step=0.010, temperature_coupling_time="0.1D0", pressure_coupling_time="5.0D0",
+                   time_step=dt, temperature_coupling_time="0.1D0", pressure_coupling_time="5.0D0",
                    isothermal_compressibility="1.0D-6", virtual_sites=0, mts=0, bead_cutoff=1.2,
                    bead_neighbour_list_cutoff=1.4, non_bonded_bead=4, cutoff=1.2, neighbour_list_cutoff=1.4,
                    update_neighbour_list=10, trajectory=nsteps, halt_drift=nsteps + 1, non_bonded=4,
                    initialize_velocities="N")
     return SystemSpec(control=control, types=[("CG", mass, "A")], pos=pos, vel=vel, itype=np.ones(n, int),
                       bonds=[[] for _ in range(n)], molecules=[("bead", 1)] * n, box=(box, box, box),
-                      nb_tabs=[((1, 1), lj_table("nb11", 0.47, 3.5, 1.2, 0.002))])
+                      nb_tabs=[((1, 1), (shifted_force_lj_table if shifted else lj_table)("nb11", 0.47, 3.5, 1.2,
+                                                                                          0.002))])
 
 
 def polymer_melt(nchains=400, nper=100, rho=20.0, ntypes=3, seed=2, nsteps=5000, temp=500.0, dt=0.001,

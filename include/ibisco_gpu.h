@@ -202,6 +202,24 @@ int ibg_set_l2_flush(ibg_ctx* c, long long bytes);
    (the same path a growing system takes).  stage_ms[7] of ibg_get_timing
    counts the growths. */
 int ibg_set_list_rows(ibg_ctx* c, int rows);
+/* Launch tuning of the nonbonded kernel: nb_tables_smem stages the tables in
+   shared memory per block (1) or reads them through L1 (0; the FP32 default,
+   the FP64 path stages them); nb_blocks_per_sm limits the resident blocks per
+   SM (0: all that fit).  Forces and trajectories do not depend on the tuning
+   (integer force sums); on the FP32 path nonbonded energies and virials are
+   summed per work unit before their exact fixed-point sum, so they do not
+   depend on it either.  Set it before a batch is made of the context.
+   ibg_autotune: times each candidate tuning on the context's current lists
+   (reps launches each, CUDA events), keeps the fastest, writes it to best and
+   the microseconds per launch of candidate k to us[k] (k < ncand); returns the
+   number of candidates.  It leaves the system's state unchanged. */
+typedef struct ibg_tuning {
+  int nb_tables_smem;
+  int nb_blocks_per_sm;
+} ibg_tuning;
+int ibg_get_tuning(const ibg_ctx* c, ibg_tuning* t);
+int ibg_set_tuning(ibg_ctx* c, const ibg_tuning* t);
+int ibg_autotune(ibg_ctx* c, int reps, ibg_tuning* best, double* us, int ncand);
 /* Device memory a context holds (bytes), and an estimate made before creating
    one from its descriptor and box; the estimate includes the Verlet-list
    storage the first list build will need, with margin.  A serving loop admits

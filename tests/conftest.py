@@ -47,6 +47,7 @@ def sysdir(tmp_path_factory):
     made = {}
     builders = {
         "fluid": lambda: synth.lj_fluid(n=1500, seed=11, nsteps=50, dmin=0.42),
+        "fluid_sf": lambda: synth.lj_fluid(n=1500, seed=11, nsteps=2000, dmin=0.42, shifted=True, dt=0.005),
         "melt": lambda: synth.polymer_melt(nchains=24, nper=40, seed=12, nsteps=50),
         "mix4": lambda: synth.feature_mix(seed=7, non_bonded=4),
         "mix5_mts": lambda: synth.feature_mix(seed=8, non_bonded=5, nmts=3),

@@ -66,10 +66,12 @@ def energies(obs):
     return np.array([obs[k] for k in sorted(keys)])
 
 
+@pytest.mark.parametrize("smem", [0, 1], ids=["tables_l1", "tables_smem"])
 @pytest.mark.parametrize("name", SYSTEMS)
-def test_forces_fp32_fixed_against_fp64_oracle(sysdir, name):
+def test_forces_fp32_fixed_against_fp64_oracle(sysdir, name, smem):
     d = sysdir(name)
     _, g = make(d, native.IBG_PREC_FP32_FIXED)
+    g.set_tuning(nb_tables_smem=smem)
     o = oracle_init(d, 1)
     og = g.forces(1)
     o.forces(1, 1)
@@ -208,3 +210,22 @@ def test_too_few_cells_is_reported(sysdir, tmp_path):
     with pytest.raises(native.IbiscoError) as e:
         g.set_state()
     assert e.value.code == -6
+
+
+def test_tuning_changes_no_trajectory(sysdir):
+    """Forces are exact integer sums and FP32 energies are summed per work unit,
+    so every launch tuning gives the same trajectory and observables;
+    autotuning times candidates without touching the state."""
+    d = sysdir("mix5_mts")
+    _, a = make(d, native.IBG_PREC_FP32_FIXED)
+    _, b = make(d, native.IBG_PREC_FP32_FIXED)
+    _, c = make(d, native.IBG_PREC_FP32_FIXED)
+    best, cands = a.autotune(reps=3)
+    assert len(cands) >= 2 and all(us > 0 for _, us in cands)
+    assert a.tuning() == best
+    c.set_tuning(nb_tables_smem=1 - best["nb_tables_smem"], nb_blocks_per_sm=2)
+    oa, ob, oc = a.run(1, 20, observe=True), b.run(1, 20, observe=True), c.run(1, 20, observe=True)
+    sa, sb, sc = a.state64(), b.state64(), c.state64()
+    for k in ("sxyz", "vxyz", "fxyz"):
+        assert np.array_equal(sa[k], sb[k]) and np.array_equal(sb[k], sc[k])
+    assert oa == ob == oc

@@ -1,0 +1,53 @@
+"""NVE energy drift of the FP32/fixed-point path against the reference.
+
+An LJ fluid with a shifted-force table (1,500 beads, dt 5 fs, list rebuilt
+every 10 steps) runs 2,000 NVE steps on the GPU and in the oracle.  With the
+potential and force continuous at the cutoff, the drift of the total energy
+(kinetic plus every potential term) is set by the integrator and the
+arithmetic, not by pairs crossing the cutoff.  The reference computes in
+REAL*4, so its drift is the bar: the GPU's drift -- the slope of a linear fit
+over steps 100..2000 times the steps, relative to the mean energy -- stays
+within the REAL*4 oracle's (25 % margin: one short chaotic run).  The change
+between the means of the first and last 100 steps is printed beside it; it
+follows the slow energy fluctuations of each trajectory rather than a drift
+(it ranks the REAL*4 run below the FP64 one), so it is not a criterion.
+"""
+import numpy as np
+import pytest
+
+from ibisco_b200 import native
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+NSTEPS = 2000
+
+
+def etot(o):
+    return sum(v for k, v in o.items() if k.startswith(("EK", "V_")))
+
+
+def drift(e):
+    e = np.asarray(e)[100:]
+    scale = abs(e.mean())
+    slope = np.polyfit(np.arange(len(e)), e, 1)[0]
+    return abs(slope) * len(e) / scale, abs(e[-100:].mean() - e[:100].mean()) / scale
+
+
+def test_nve_drift_within_reference(sysdir):
+    d = sysdir("fluid_sf")
+    g = native.System(native.Setup(d), native.IBG_PREC_FP32_FIXED)
+    g.set_state()
+    gpu = drift([etot(o) for o in g.run(1, NSTEPS, observe=True)])
+    ref = {}
+    for prec in (0, 1):
+        o = Oracle(d, threads=8)
+        o.init(prec)
+        e = []
+        for st in range(1, NSTEPS + 1):
+            o.step(st, prec)
+            e.append(etot(o.obs(prec)))
+        ref[prec] = drift(e)
+    print(f"NVE drift over {NSTEPS} steps (fitted, windowed): GPU FP32/fixed {gpu}, "
+          f"oracle REAL*4 {ref[0]}, oracle FP64 {ref[1]}")
+    assert gpu[0] <= 1.25 * ref[0][0]
