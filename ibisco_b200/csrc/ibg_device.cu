@@ -103,6 +103,7 @@ struct DevList {
   size_t pos_bytes = 0;
   // tables of this list
   int *ltab = nullptr, *toff = nullptr, *tndat = nullptr;
+  int4* ptab = nullptr;  // per type pair: first row, NDAT, 1/bin bits, table present
   void *tbin = nullptr, *tinv = nullptr, *tfp = nullptr, *tx = nullptr;
   int ntab = 0, nrows = 0;
   size_t smem = 0;
@@ -299,12 +300,23 @@ void build_list(ibg_ctx* c, const ibg_desc* d, int which) {
     std::vector<float> f1(fp.begin(), fp.end()), x1(xx.begin(), xx.end()), b1(bin.begin(), bin.end()), i1(bin.size());
     for (size_t k = 0; k < bin.size(); ++k) i1[k] = (float)(1.0 / (double)(float)bin[k]);
     L.tfp = dupload(f1, o); L.tx = dupload(x1, o); L.tbin = dupload(b1, o); L.tinv = dupload(i1, o);
+    std::vector<int4> pt((size_t)NT * NT);
+    for (size_t k = 0; k < pt.size(); ++k) {
+      const int t = ltab[k];
+      float inv = t >= 0 ? i1[t] : 0.f;
+      int ib;
+      std::memcpy(&ib, &inv, sizeof(int));
+      pt[k] = t >= 0 ? make_int4(toff[t], tnd[t], ib, 1) : make_int4(0, 0, 0, 0);
+    }
+    L.ptab = dupload(pt, o);
   } else {
     L.tfp = dupload(fp, o); L.tx = dupload(xx, o); L.tbin = dupload(bin, o);
   }
   const size_t rs = rsize(c);
-  L.smem = 9 * 256 * sizeof(double) + rs * 3 * (size_t)L.nrows + 2 * rs * L.ntab +
-           sizeof(int) * ((size_t)NT * NT + 2 * L.ntab + 1) + 64;
+  L.smem = c->prec == IBG_PREC_FP32_FIXED
+               ? 9 * 256 * sizeof(double) + sizeof(int4) * (size_t)NT * NT + 12 * (size_t)L.nrows + 64
+               : 9 * 256 * sizeof(double) + rs * 3 * (size_t)L.nrows + 2 * rs * L.ntab +
+                     sizeof(int) * ((size_t)NT * NT + 2 * L.ntab + 1) + 64;
   // launch defaults (ibg_set_tuning / ibg_autotune change them): the FP32
   // kernel reads its tables through L1, the FP64 kernel stages them
   L.use_smem = c->prec != IBG_PREC_FP32_FIXED && L.smem <= 200 * 1024;
@@ -378,6 +390,7 @@ void make_args(ibg_ctx* c) {
     a.sc = sc;
     a.n = L.n; a.which = w; a.natoms = c->natoms; a.hybrid = c->ibrdescr == 0; a.maxnab = c->maxnab;
     a.cell_cap = L.cell_cap;
+    a.nslices = L.nslices;
     a.rlist = L.rlist; a.rlistsq = L.rlistsq; a.rlistd = (double)L.rlist; a.rlistsqd = (double)L.rlist * (double)L.rlist;
     a.idx = L.idx; a.cell_of = L.cell_of; a.cell_count = L.cell_count; a.cell_start = L.cell_start;
     a.cell_fill = L.cell_fill;
@@ -392,7 +405,7 @@ void make_args(ibg_ctx* c) {
     n.w_cap = L.w_cap; n.work = w;
     n.fsort = (acc_t*)L.fsort;
     n.ltab = L.ltab; n.toff = L.toff; n.tndat = L.tndat; n.tbin = (const R*)L.tbin; n.tinv = (const R*)L.tinv;
-    n.tfp = (const R*)L.tfp; n.tx = (const R*)L.tx;
+    n.tfp = (const R*)L.tfp; n.tx = (const R*)L.tx; n.ptab = L.ptab;
     n.ntab = L.ntab; n.nrows = L.nrows; n.rcutsq = (R)L.rcutsq;
     CollectArgs<R>& k = A.col[w];
     k.sc = sc; k.n = L.n; k.mts = (w == 1 && c->nmts > 0); k.sorted = L.sorted; k.idx = L.idx;
@@ -1087,7 +1100,7 @@ int ibg_create(const ibg_desc* d, int precision, ibg_ctx** out) {
       DevList& L = c->L[w];
       if (!L.present) continue;
       c->g_list[w] = grid_for(c.get(), L.n);
-      c->g_build[w] = std::max(1, std::min(L.nslices / 8 + 1, c->nsm * 8));
+      c->g_build[w] = std::max(1, std::min((L.n + 7) / 8, c->nsm * 8));
     }
     c->g_dist = grid_for(c.get(), std::max(1, c->nvirta));
     c->g_b = grid_for(c.get(), (long long)c->nb + c->na + c->nt + c->no, 4);

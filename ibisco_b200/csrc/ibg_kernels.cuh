@@ -193,6 +193,7 @@ struct ListArgs {
   int hybrid;        // IBRDESCR == 0
   int maxnab;        // reference STOP threshold
   int cell_cap;      // capacity of the cell arrays
+  int nslices;       // slices of the list storage
   float rlist, rlistsq;
   double rlistd, rlistsqd;
   const int* idx;    // INDEX_LIST, 0-based global ids
@@ -227,6 +228,7 @@ __global__ void k_regrid(__grid_constant__ const ListArgs L0, const ListArgs* co
   Scalars* sc = L.sc;
   if (sc->skip || !(always || sc->rebuild)) return;
   for (int c = bk.b * blockDim.x + threadIdx.x; c < L.cell_cap; c += bk.g * blockDim.x) L.cell_count[c] = 0;
+  for (int g = bk.b * blockDim.x + threadIdx.x; g < L.nslices; g += bk.g * blockDim.x) L.slice_w[g] = 0;
   if (threadIdx.x || bk.b) return;
   int nc[3];
   for (int c = 0; c < 3; ++c) {
@@ -379,15 +381,18 @@ __global__ void k_slot_of(__grid_constant__ const ListArgs L0, const ListArgs* c
   }
 }
 
-// NEW_NEIGHBOUR_WITHLIST.f90:34-123.  T lanes share one slot (particle); a
-// warp takes one slice of P = 32/T consecutive slots at a time (dynamic
-// scheduling).  Candidates are visited in the reference's order -- the
-// particle's own cell below it (decreasing A), then the 13 cells of the
-// MAPS.f90:137-149 stencil, each by decreasing A -- T at a time; a ballot over
-// the slot's lanes keeps accepted candidates in that order.  The distance test
-// runs first and the exclusion scan only for candidates inside RLIST (the
-// accepted set is the same).  Entry k of slot s (slice g) is stored at
-// (g*w_cap + k/T)*32 + (s%P)*T + k%T.  A slice that needs more than w_cap rows
+// NEW_NEIGHBOUR_WITHLIST.f90:34-123.  A warp builds one particle's list at a
+// time (slots taken dynamically).  Candidates are visited in the reference's
+// order -- the particle's own cell below it (decreasing A), then the 13 cells
+// of the MAPS.f90:137-149 stencil, each by decreasing A -- 32 at a time, one
+// per lane (consecutive slots: coalesced loads); a ballot and a prefix count
+// keep the accepted ones in that order.  The distance test runs first and the
+// exclusion test only for candidates inside RLIST (the accepted set is the
+// same); exclusions are compared as slots of this list, and a virtual site is
+// recognised by its label in the position's w, so no candidate's global id is
+// loaded.  The list is stored in the nonbonded kernel's layout: T lanes per
+// slot, slices of P = 32/T slots, entry k of slot s (slice g) at
+// (g*w_cap + k/T)*32 + (s%P)*T + k%T.  A slot that needs more than w_cap rows
 // records its need and raises the abort flag (the host enlarges the storage
 // and repeats the step).
 // The 13 neighbour cells of the half stencil in MAPS.f90:137-149 order.
@@ -395,7 +400,8 @@ __constant__ int kStencil[13][3] = {{1, 0, 0}, {1, 1, 0},  {0, 1, 0},  {-1, 1, 0
                                     {-1, 1, -1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}, {-1, 1, 1}, {0, 0, 1}};
 
 template <typename R, int T, bool B>
-__global__ void __launch_bounds__(256) k_list_build(__grid_constant__ const ListArgs L0, const ListArgs* const* tab, const BlockMap bm, int always) {
+__global__ void __launch_bounds__(256) k_list_build(__grid_constant__ const ListArgs L0, const ListArgs* const* tab,
+                                                    const BlockMap bm, int always) {
   using PT = typename Prec<R>::pos_t;
   const Blk bk = blk<B>(bm);
   __shared__ ListArgs s_args;
@@ -403,87 +409,88 @@ __global__ void __launch_bounds__(256) k_list_build(__grid_constant__ const List
   const ListArgs& L = B ? s_args : L0;
   Scalars* sc = L.sc;
   if (sc->skip || !(always || sc->rebuild)) return;
-
   constexpr int P = 32 / T;
+  __shared__ int s_exs[8][20];  // each warp's particle's exclusions, as slots of this list
   const int nx = sc->ncell[L.which][0], ny = sc->ncell[L.which][1], nz = sc->ncell[L.which][2];
   R b[3], bi[3], b2[3];
   box_of<R>(sc, b, bi, b2);
   const R rlsq = sizeof(R) == 4 ? (R)L.rlistsq : (R)L.rlistsqd;
   const PT* pos = (const PT*)L.pos4;
-  const int lane = threadIdx.x & 31, grp = lane / T, q = lane % T;
-  const unsigned gmask = ((1u << T) - 1u) << (grp * T);
-  const int nslices = (L.n + P - 1) / P;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned below = (1u << lane) - 1u;
   const int cap = L.w_cap * T;  // entries a slot may hold
+  int* exs = s_exs[warp];
   for (;;) {
-    int g = 0;
-    if (lane == 0) g = (int)atomicAdd(&sc->work[2 + L.which], 1u);
-    g = __shfl_sync(0xffffffffu, g, 0);
-    if (g >= nslices) break;
-    const int s = g * P + grp;
-    const bool valid = s < L.n;
-    const long long base = (long long)g * L.w_cap * 32;
-    int cnt = 0;
-    if (valid) {
-      const int a = L.sorted[s];
-      const int i = L.idx[a];
-      const PT pi = pos[s];
-      const int ne = L.excl_n[i];
-      const int* ex = L.excl + (size_t)i * 20;
-      const bool i_vs = L.hybrid && i >= L.natoms;
-      const int c0 = L.cell_of[a];
-      const int ix = c0 / (nz * ny), iy = (c0 / nz) % ny, iz = c0 % nz;
-      // candidates t = hi, hi-1, ..., lo
-      auto segment = [&](int hi, int lo) {
-        for (int t0 = hi; t0 >= lo; t0 -= T) {
-          const int t = t0 - q;
-          bool ok = false;
-          if (t >= lo) {
-            const PT pj = pos[t];
-            R d0 = pi.x - pj.x, d1 = pi.y - pj.y, d2 = pi.z - pj.z;
-            d0 = d0 - r_round(d0 * bi[0]) * b[0];
-            d1 = d1 - r_round(d1 * bi[1]) * b[1];
-            d2 = d2 - r_round(d2 * bi[2]) * b[2];
-            R r2 = d0 * d0;
-            r2 = r2 + d1 * d1;
-            r2 = r2 + d2 * d2;
-            if (r2 < rlsq) {
-              const int j = L.idx[L.sorted[t]];
-              ok = !(i_vs && j >= L.natoms);
-              for (int e = 0; e < ne && ok; ++e)
-                if (ex[e] == j) ok = false;
-            }
-          }
-          const unsigned bits = (__ballot_sync(gmask, ok) >> (grp * T)) & ((1u << T) - 1u);
-          if (ok) {
-            const int k = cnt + __popc(bits & ((1u << q) - 1u));
-            if (k < cap) L.entries[base + (long long)(k / T) * 32 + grp * T + (k % T)] = t;
-          }
-          cnt += __popc(bits);
-        }
-      };
-      segment(s - 1, L.cell_start[c0]);
-#pragma unroll 1
-      for (int u = 0; u < 13; ++u) {
-        const int jx = (ix + kStencil[u][0] + nx) % nx, jy = (iy + kStencil[u][1] + ny) % ny,
-                  jz = (iz + kStencil[u][2] + nz) % nz;
-        const int c = jx * nz * ny + jy * nz + jz;
-        segment(L.cell_start[c + 1] - 1, L.cell_start[c]);
-      }
-      if (q == 0) {
-        L.counts[s] = cnt;
-        if (cnt >= L.maxnab) atomicOr(&sc->err, EB_LIST_OVERFLOW);
-      }
+    int s = 0;
+    if (lane == 0) s = (int)atomicAdd(&sc->work[2 + L.which], 1u);
+    s = __shfl_sync(0xffffffffu, s, 0);
+    if (s >= L.n) break;
+    const int g = s / P;
+    const long long base = (long long)g * L.w_cap * 32 + (s % P) * T;
+    const int a = L.sorted[s];
+    const int i = L.idx[a];
+    const PT pi = pos[s];
+    const int ne = L.excl_n[i];
+    if (lane < ne) {
+      const int gs = L.gslot[L.excl[(size_t)i * 20 + lane]];
+      exs[lane] = (gs & 1) == L.which ? gs >> 1 : -1;
     }
-    const int w = __reduce_max_sync(0xffffffffu, valid ? cnt : 0);
+    __syncwarp();
+    const bool i_vs = L.hybrid && i >= L.natoms;
+    const int c0 = L.cell_of[a];
+    const int ix = c0 / (nz * ny), iy = (c0 / nz) % ny, iz = c0 % nz;
+    int cnt = 0;
+    // minimum image by compare and select.  It equals d - ANINT(d/L)*L for
+    // |d| < L/2 (ANINT = 0) and for |d| > L/2 away from the rounding of d/L
+    // to 1/2 (both subtract L the same way); where they can differ, |d| is
+    // within rounding of L/2, beyond RLIST <= L/3 either way.  So the accepted
+    // set is bit for bit the reference's.
+    auto segment = [&](int hi, int lo) {  // candidates hi, hi-1, ..., lo
+      for (int t0 = hi; t0 >= lo; t0 -= 32) {
+        const int t = t0 - lane;
+        bool ok = false;
+        if (t >= lo) {
+          const PT pj = pos[t];
+          R d0 = pi.x - pj.x, d1 = pi.y - pj.y, d2 = pi.z - pj.z;
+          d0 = d0 > b2[0] ? d0 - b[0] : (d0 < -b2[0] ? d0 + b[0] : d0);
+          d1 = d1 > b2[1] ? d1 - b[1] : (d1 < -b2[1] ? d1 + b[1] : d1);
+          d2 = d2 > b2[2] ? d2 - b[2] : (d2 < -b2[2] ? d2 + b[2] : d2);
+          R r2 = d0 * d0;
+          r2 = r2 + d1 * d1;
+          r2 = r2 + d2 * d2;
+          if (r2 < rlsq) {
+            ok = !(i_vs && (Prec<R>::bits(pj.w) >> 16) == 3);
+            for (int e = 0; e < ne; ++e) ok &= exs[e] != t;
+          }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, ok);
+        if (ok) {
+          const int k = cnt + __popc(m & below);
+          if (k < cap) ((int*)L.entries)[base + (long long)(k / T) * 32 + (k % T)] = t;
+        }
+        cnt += __popc(m);
+      }
+    };
+    segment(s - 1, L.cell_start[c0]);
+#pragma unroll 1
+    for (int u = 0; u < 13; ++u) {
+      const int jx = (ix + kStencil[u][0] + nx) % nx, jy = (iy + kStencil[u][1] + ny) % ny,
+                jz = (iz + kStencil[u][2] + nz) % nz;
+      const int c = jx * nz * ny + jy * nz + jz;
+      segment(L.cell_start[c + 1] - 1, L.cell_start[c]);
+    }
     if (lane == 0) {
-      const int rows = (w + T - 1) / T;
-      L.slice_w[g] = rows;
+      L.counts[s] = cnt;
+      if (cnt >= L.maxnab) atomicOr(&sc->err, EB_LIST_OVERFLOW);
+      const int rows = (cnt + T - 1) / T;
+      atomicMax(&L.slice_w[g], rows);
       if (rows > L.w_cap) {
         atomicMax(&sc->need_rows[L.which], rows);
         sc->abort = 1;
         sc->skip = 1;
       }
     }
+    __syncwarp();  // exs is rewritten for the next particle
   }
 }
 
@@ -507,6 +514,7 @@ struct NBArgs {
   const int* tndat;
   const R* tbin;
   const R* tinv; // 1/bin per table (FP32 force kernel)
+  const int4* ptab;  // FP32 kernel: per type pair {first row, NDAT, 1/bin bits, 1 if a table}
   const R* tfp;  // 2 per row
   const R* tx;
   int ntab, nrows;
@@ -731,32 +739,25 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
   if (nb_idle(A)) return;
   extern __shared__ unsigned char smem_raw[];
   long long* lacc = (long long*)smem_raw;  // [9][blockDim.x] per-lane sums
-  const int* ltab = A.ltab;
-  const int* toff = A.toff;
-  const int* tndat = A.tndat;
-  const float* tinv = A.tinv;
+  // per type pair {first row, last row index, 1/bin bits, has a table}
+  const int4* ptab = A.ptab;
   const float2* tfp = (const float2*)A.tfp;
   const float* tx = A.tx;
   {
     unsigned char* p = smem_raw + 9 * 256 * sizeof(double);
     if (SMEM) {
+      int4* s_ptab = (int4*)p;       p += sizeof(int4) * A.ntype * A.ntype;
       float2* s_fp = (float2*)p;     p += sizeof(float2) * A.nrows;
-      float* s_x = (float*)p;        p += sizeof(float) * A.nrows;
-      float* s_inv = (float*)p;      p += sizeof(float) * A.ntab;
-      int* s_ltab = (int*)p;         p += sizeof(int) * A.ntype * A.ntype;
-      int* s_toff = (int*)p;         p += sizeof(int) * (A.ntab + 1);
-      int* s_ndat = (int*)p;
+      float* s_x = (float*)p;
       for (int k = threadIdx.x; k < A.nrows; k += blockDim.x) { s_fp[k] = ((const float2*)A.tfp)[k]; s_x[k] = A.tx[k]; }
-      for (int k = threadIdx.x; k < A.ntab; k += blockDim.x) { s_inv[k] = A.tinv[k]; s_ndat[k] = A.tndat[k]; }
-      for (int k = threadIdx.x; k < A.ntype * A.ntype; k += blockDim.x) s_ltab[k] = A.ltab[k];
-      for (int k = threadIdx.x; k <= A.ntab; k += blockDim.x) s_toff[k] = A.toff[k];
-      ltab = s_ltab; toff = s_toff; tndat = s_ndat; tinv = s_inv; tfp = s_fp; tx = s_x;
+      for (int k = threadIdx.x; k < A.ntype * A.ntype; k += blockDim.x) s_ptab[k] = A.ptab[k];
+      ptab = s_ptab; tfp = s_fp; tx = s_x;
     }
   }
   for (int k = 0; k < 9; ++k) lacc[k * blockDim.x + threadIdx.x] = 0;
   __syncthreads();
   const float bx = sc->boxf[0], by = sc->boxf[1], bz = sc->boxf[2];
-  const float hx = sc->box2f[0], hy = sc->box2f[1], hz = sc->box2f[2];
+  const float ix = sc->boxinvf[0], iy = sc->boxinvf[1], iz = sc->boxinvf[2];
   const float4* pos = (const float4*)A.pos4;
   const int lane = threadIdx.x & 31, grp = lane / T, q = lane % T;
   unsigned err = 0;
@@ -783,30 +784,39 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
     long long fi0 = 0, fi1 = 0, fi2 = 0;
     float e[3] = {0.f, 0.f, 0.f}, vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     auto pair = [&](int t, const float4& pj) {
+      // minimum image d - rint(d/L) L (the pair is beyond the cutoff wherever
+      // this and ANINT could choose differently, |d| ~ L/2)
       float d0 = pi.x - pj.x, d1 = pi.y - pj.y, d2 = pi.z - pj.z;
-      d0 = d0 > hx ? d0 - bx : (d0 < -hx ? d0 + bx : d0);
-      d1 = d1 > hy ? d1 - by : (d1 < -hy ? d1 + by : d1);
-      d2 = d2 > hz ? d2 - bz : (d2 < -hz ? d2 + bz : d2);
+      d0 = __fmaf_rn(-rintf(d0 * ix), bx, d0);
+      d1 = __fmaf_rn(-rintf(d1 * iy), by, d1);
+      d2 = __fmaf_rn(-rintf(d2 * iz), bz, d2);
       const float r2 = __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, d0 * d0));
       if (!(r2 < A.rcutsq)) return;
       const int wj = __float_as_int(pj.w);
       const int tj = wj & 0xffff, lj = wj >> 16;
-      const int tab = ltab[ti * A.ntype + tj];
-      if (tab < 0) { err |= EB_MISSING_TABLE; return; }
+      const int4 pt = ptab[ti * A.ntype + tj];
+      if (!pt.w) { err |= EB_MISSING_TABLE; return; }
       const float r = r2 * rsqrtf(r2);
-      const float ib = tinv[tab];
+      const float ib = __int_as_float(pt.z);
       const int ni = (int)(r * ib);
-      if (ni > tndat[tab]) { err |= EB_TABLE_RANGE; return; }
-      const int row = toff[tab] + ni;
+      if (ni > pt.y) { err |= EB_TABLE_RANGE; return; }
+      const int row = pt.x + ni;
       const float alpha = (r - tx[row]) * ib;
       const float2 a0 = tfp[row], a1 = tfp[row + 1];
       const float fij = __fmaf_rn(a1.x - a0.x, alpha, a0.x);
       const float vij = __fmaf_rn(a1.y - a0.y, alpha, a0.y);
-      const int slot = li == 1 ? 0 : (li == 2 ? (lj == 2 ? 1 : (lj == 3 ? 2 : 3)) : (li == 3 ? 2 : 3));
-      if (slot < 3) e[slot] += vij;
+      // V_NB(1) atom pairs, V_NB(2) bead-bead, V_NB(3) pairs with a virtual site
+      const bool lab3 = li == 3 || lj == 3;
+      e[0] += li == 1 ? vij : 0.f;
+      e[1] += (li == 2 && lj == 2) ? vij : 0.f;
+      e[2] += (li != 1 && lab3) ? vij : 0.f;
+      // |f component| <= |fij| r (to rounding): one test keeps every
+      // component in range
+      if (!(fabsf(fij) * r < 0.99f * kFixMax)) { err |= EB_FIXED; return; }
       const float fx = fij * d0, fy = fij * d1, fz = fij * d2;
-      if (!(fabsf(fx) < kFixMax && fabsf(fy) < kFixMax && fabsf(fz) < kFixMax)) { err |= EB_FIXED; return; }
-      const long long qx = f2fix(fx), qy = f2fix(fy), qz = f2fix(fz);
+      // round(f * 2^32): the scaling is exact, the conversion rounds to nearest
+      const long long qx = __float2ll_rn(fx * kFixScale), qy = __float2ll_rn(fy * kFixScale),
+                      qz = __float2ll_rn(fz * kFixScale);
       fi0 += qx; fi1 += qy; fi2 += qz;
       atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 0], (unsigned long long)(-qx));
       atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 1], (unsigned long long)(-qy));
