@@ -387,12 +387,21 @@ def run_b200(args, world, rank, local, pg):
         # stage over all of them (ibg_batch); device time, state resident
         batched = None
         if prec == native.IBG_PREC_FP32_FIXED and args.batch > 1:
-            systems = []
-            for _ in range(args.batch):
-                gb = native.System(setup, native.IBG_PREC_FP32_FIXED)
-                gb.set_state(s0, v0, b0)
-                gb.set_tuning(**tuned)
-                systems.append(gb)
+            def make_systems():
+                out = []
+                for _ in range(args.batch):
+                    gb = native.System(setup, native.IBG_PREC_FP32_FIXED)
+                    gb.set_state(s0, v0, b0)
+                    out.append(gb)
+                return out
+
+            # the batch's own launch tuning (it can differ from one system's)
+            base = dict(nb_tables_smem=0, nb_blocks_per_sm=0, nb_chunk=0)
+            cands = [base] + ([tuned] if tuned != base else [])
+            btuned, btimes = native.tune_batch(make_systems, cands, steps=100)
+            systems = make_systems()
+            for gb in systems:
+                gb.set_tuning(**btuned)
             bat = native.Batch(systems)
             bat.run(args.warmup)
             barrier(pg)
@@ -400,7 +409,7 @@ def run_b200(args, world, rank, local, pg):
                 bat.run(args.steps)
             bms = reduce_max(pg, bat.timing()["run_ms"])
             bval = world * args.batch * n * args.steps / (bms / 1000.0)
-            batched = {"systems": args.batch, "value": bval, "unit": "atom-steps/s",
+            batched = {"systems": args.batch, "value": bval, "unit": "atom-steps/s", "tuning": btuned,
                        "ms_per_step": bms / args.steps, "particles_per_step": args.batch * n,
                        "l2": "not flushed; the batch's working set exceeds the 126 MB L2",
                        "clocks": clk_b.summary()}

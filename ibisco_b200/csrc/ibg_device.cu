@@ -163,6 +163,7 @@ struct ibg_ctx {
   void* dargs = nullptr;  // device copy of af or ad
   int g_list[2] = {1, 1}, g_regrid[2] = {1, 1}, g_build[2] = {1, 1}, g_dist = 1;
   int nb_blocks_per_sm = 0;  // tuning: resident nonbonded blocks per SM (0: all that fit)
+  int nb_chunk = 0;          // tuning (FP32): work units per block chunk (0: per warp)
   ObsD* ring = nullptr;
   int ring_cap = 0;
   double *p_b = nullptr, *p_mv = nullptr, *p_mom = nullptr;
@@ -405,7 +406,7 @@ void make_args(ibg_ctx* c) {
     n.w_cap = L.w_cap; n.work = w;
     n.fsort = (acc_t*)L.fsort;
     n.ltab = L.ltab; n.toff = L.toff; n.tndat = L.tndat; n.tbin = (const R*)L.tbin; n.tinv = (const R*)L.tinv;
-    n.tfp = (const R*)L.tfp; n.tx = (const R*)L.tx; n.ptab = L.ptab;
+    n.tfp = (const R*)L.tfp; n.tx = (const R*)L.tx; n.ptab = L.ptab; n.chunk = c->nb_chunk;
     n.ntab = L.ntab; n.nrows = L.nrows; n.rcutsq = (R)L.rcutsq;
     CollectArgs<R>& k = A.col[w];
     k.sc = sc; k.n = L.n; k.mts = (w == 1 && c->nmts > 0); k.sorted = L.sorted; k.idx = L.idx;
@@ -800,14 +801,16 @@ int ibg_get_tuning(const ibg_ctx* c, ibg_tuning* t) {
   const DevList& L = c->L[c->L[0].present ? 0 : 1];
   t->nb_tables_smem = L.use_smem ? 1 : 0;
   t->nb_blocks_per_sm = c->nb_blocks_per_sm;
+  t->nb_chunk = c->nb_chunk;
   return IBG_OK;
 }
 
 int ibg_set_tuning(ibg_ctx* c, const ibg_tuning* t) {
-  if (!c || !t || t->nb_blocks_per_sm < 0) return IBG_E_INVALID;
+  if (!c || !t || t->nb_blocks_per_sm < 0 || t->nb_chunk < 0) return IBG_E_INVALID;
   if (c->in_batch) return fail(c, IBG_E_INVALID, "the context is in a batch");
   try {
     c->nb_blocks_per_sm = t->nb_blocks_per_sm;
+    c->nb_chunk = c->prec == IBG_PREC_FP32_FIXED ? t->nb_chunk : 0;
     for (auto& L : c->L) {
       if (!L.present) continue;
       L.use_smem = t->nb_tables_smem != 0 && L.smem <= 200 * 1024;
@@ -828,8 +831,14 @@ int ibg_autotune(ibg_ctx* c, int reps, ibg_tuning* best, double* us, int ncand) 
   if (!c->state_set) return fail(c, IBG_E_INVALID, "ibg_set_state has not been called");
   if (c->in_batch) return fail(c, IBG_E_INVALID, "the context is in a batch");
   std::vector<ibg_tuning> cand;
-  for (int smem : {0, 1})
-    for (int per : {0, 3, 2}) cand.push_back(ibg_tuning{smem, per});
+  if (c->prec == IBG_PREC_FP32_FIXED) {
+    for (int chunk : {0, 48, 96})
+      for (int smem : {0, 1})
+        for (int per : {0, 3}) cand.push_back(ibg_tuning{smem, per, chunk});
+  } else {
+    for (int smem : {0, 1})
+      for (int per : {0, 3, 2}) cand.push_back(ibg_tuning{smem, per, 0});
+  }
   ibg_tuning keep;
   ibg_get_tuning(c, &keep);
   int win = -1;

@@ -515,6 +515,7 @@ struct NBArgs {
   const R* tbin;
   const R* tinv; // 1/bin per table (FP32 force kernel)
   const int4* ptab;  // FP32 kernel: per type pair {first row, NDAT, 1/bin bits, 1 if a table}
+  int chunk;         // FP32 kernel: work units per block chunk (0: each warp takes units alone)
   const R* tfp;  // 2 per row
   const R* tx;
   int ntab, nrows;
@@ -764,15 +765,11 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
   const bool run = true;
   const int U = (A.w_cap + ROWS - 1) / ROWS;
   const int nunits = A.nslices * U;
-  for (;;) {
-    int u = 0;
-    if (lane == 0) u = run ? (int)atomicAdd(&sc->work[A.work], 1u) : nunits;
-    u = __shfl_sync(0xffffffffu, u, 0);
-    if (u >= nunits) break;
+  auto unit = [&](int u) {
     const int g = u / U;
     const int r0 = (u - g * U) * ROWS;
     const int w = min(A.slice_w[g], A.w_cap);
-    if (r0 >= w) continue;
+    if (r0 >= w) return;
     const int r1 = min(w, r0 + ROWS);
     const int s = g * PS + grp;
     const bool valid = s < A.n;
@@ -854,6 +851,39 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
     for (int k = 0; k < 3; ++k) la[k * blockDim.x] += fixq<24>(e[k], err);
 #pragma unroll
     for (int k = 0; k < 6; ++k) la[(3 + k) * blockDim.x] += fixq<24>(vir[k], err);
+  };
+  if (A.chunk > 0) {
+    // chunks of consecutive units (neighbouring slices) per block, handed out
+    // to its warps through a shared counter: the block's warps gather from
+    // one region of space and share it in L1
+    __shared__ int s_chunk, s_next;
+    const int nchunks = (nunits + A.chunk - 1) / A.chunk;
+    for (;;) {
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        s_chunk = run ? (int)atomicAdd(&sc->work[A.work], 1u) : nchunks;
+        s_next = 0;
+      }
+      __syncthreads();
+      const int ch = s_chunk;
+      if (ch >= nchunks) break;
+      const int u0 = ch * A.chunk, u1 = min(nunits, u0 + A.chunk);
+      for (;;) {
+        int k = 0;
+        if (lane == 0) k = atomicAdd(&s_next, 1);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        if (u0 + k >= u1) break;
+        unit(u0 + k);
+      }
+    }
+  } else {
+    for (;;) {
+      int u = 0;
+      if (lane == 0) u = run ? (int)atomicAdd(&sc->work[A.work], 1u) : nunits;
+      u = __shfl_sync(0xffffffffu, u, 0);
+      if (u >= nunits) break;
+      unit(u);
+    }
   }
   if (err) atomicOr(&sc->err, err);
   long long acc[9];

@@ -73,7 +73,7 @@ class IbgDesc(ctypes.Structure):
 
 
 class Tuning(ctypes.Structure):
-    _fields_ = [("nb_tables_smem", ctypes.c_int), ("nb_blocks_per_sm", ctypes.c_int)]
+    _fields_ = [("nb_tables_smem", ctypes.c_int), ("nb_blocks_per_sm", ctypes.c_int), ("nb_chunk", ctypes.c_int)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -360,8 +360,8 @@ class System:
         self._check(lib().ibg_get_tuning(self._h, ctypes.byref(t)))
         return t.as_dict()
 
-    def set_tuning(self, nb_tables_smem: int = 0, nb_blocks_per_sm: int = 0):
-        t = Tuning(nb_tables_smem, nb_blocks_per_sm)
+    def set_tuning(self, nb_tables_smem: int = 0, nb_blocks_per_sm: int = 0, nb_chunk: int = 0):
+        t = Tuning(nb_tables_smem, nb_blocks_per_sm, nb_chunk)
         self._check(lib().ibg_set_tuning(self._h, ctypes.byref(t)))
 
     def autotune(self, reps: int = 20):
@@ -372,7 +372,10 @@ class System:
         n = lib().ibg_autotune(self._h, int(reps), ctypes.byref(best), us, 16)
         if n < 0:
             self._check(n)
-        cands = [(sm, per) for sm in (0, 1) for per in (0, 3, 2)]
+        if self.precision == IBG_PREC_FP32_FIXED:
+            cands = [(sm, per, ch) for ch in (0, 48, 96) for sm in (0, 1) for per in (0, 3)]
+        else:
+            cands = [(sm, per, 0) for sm in (0, 1) for per in (0, 3, 2)]
         return best.as_dict(), [(c, us[k]) for k, c in enumerate(cands[:n])]
 
     def set_timing(self, on: bool):
@@ -489,3 +492,23 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+def tune_batch(make_systems, candidates, steps: int = 100):
+    """Pick the launch tuning of a batch by timing: for each candidate tuning
+    (a dict for System.set_tuning), make the systems (make_systems() returns
+    fresh Systems after set_state), apply it, run `steps` batch steps and keep
+    the fastest.  Returns (best tuning, [(tuning, us per batch step)])."""
+    times = []
+    for tun in candidates:
+        systems = make_systems()
+        for x in systems:
+            x.set_tuning(**tun)
+        b = Batch(systems)
+        b.run(10)
+        b.run(steps)
+        times.append((tun, 1000.0 * b.timing()["run_ms"] / steps))
+        b.close()
+        for x in systems:
+            x.close()
+    return min(times, key=lambda t: t[1])[0], times

@@ -205,7 +205,10 @@ int ibg_set_list_rows(ibg_ctx* c, int rows);
 /* Launch tuning of the nonbonded kernel: nb_tables_smem stages the tables in
    shared memory per block (1) or reads them through L1 (0; the FP32 default,
    the FP64 path stages them); nb_blocks_per_sm limits the resident blocks per
-   SM (0: all that fit).  Forces and trajectories do not depend on the tuning
+   SM (0: all that fit); nb_chunk (FP32 path): a block takes chunks of this
+   many consecutive work units (neighbouring slices) and shares them among its
+   warps, so they gather from one region of space (0: every warp takes units
+   alone).  Forces and trajectories do not depend on the tuning
    (integer force sums); on the FP32 path nonbonded energies and virials are
    summed per work unit before their exact fixed-point sum, so they do not
    depend on it either.  Set it before a batch is made of the context.
@@ -216,6 +219,7 @@ int ibg_set_list_rows(ibg_ctx* c, int rows);
 typedef struct ibg_tuning {
   int nb_tables_smem;
   int nb_blocks_per_sm;
+  int nb_chunk;
 } ibg_tuning;
 int ibg_get_tuning(const ibg_ctx* c, ibg_tuning* t);
 int ibg_set_tuning(ibg_ctx* c, const ibg_tuning* t);

@@ -223,7 +223,8 @@ def test_tuning_changes_no_trajectory(sysdir):
     best, cands = a.autotune(reps=3)
     assert len(cands) >= 2 and all(us > 0 for _, us in cands)
     assert a.tuning() == best
-    c.set_tuning(nb_tables_smem=1 - best["nb_tables_smem"], nb_blocks_per_sm=2)
+    c.set_tuning(nb_tables_smem=1 - best["nb_tables_smem"], nb_blocks_per_sm=2,
+                 nb_chunk=16 if best["nb_chunk"] == 0 else 0)
     oa, ob, oc = a.run(1, 20, observe=True), b.run(1, 20, observe=True), c.run(1, 20, observe=True)
     sa, sb, sc = a.state64(), b.state64(), c.state64()
     for k in ("sxyz", "vxyz", "fxyz"):
