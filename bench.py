@@ -313,8 +313,14 @@ def run_b200(args, world, rank, local, pg):
         prec = native.IBG_PREC_FP64_PLAIN if args.precision == "fp64" else native.IBG_PREC_FP32_FIXED
         g = native.System(setup, prec)
         g.set_state(s0, v0, b0)
-        # launch tuning of the nonbonded kernel, picked by timing (state unchanged)
-        tuned, tune_cands = g.autotune(reps=20)
+        # launch tuning of the nonbonded kernel, picked by timing (state
+        # unchanged), or fixed by --tuning (profiling runs)
+        if args.tuning:
+            sm, per, ch = (int(x) for x in args.tuning.split(","))
+            tuned, tune_cands = dict(nb_tables_smem=sm, nb_blocks_per_sm=per, nb_chunk=ch), []
+            g.set_tuning(**tuned)
+        else:
+            tuned, tune_cands = g.autotune(reps=20)
         flush = 256 << 20
         g.set_l2_flush(flush)
         # ---- warm-up (captures the CUDA graphs) and device-timed region
@@ -375,7 +381,8 @@ def run_b200(args, world, rank, local, pg):
         if prec == native.IBG_PREC_FP32_FIXED and not args.no_fp64:
             g64 = native.System(setup, native.IBG_PREC_FP64_PLAIN)
             g64.set_state(s0, v0, b0)
-            g64.autotune(reps=10)  # the comparison path gets its own best launch tuning
+            if not args.tuning:
+                g64.autotune(reps=10)  # the comparison path gets its own best launch tuning
             g64.set_l2_flush(flush)
             g64.run(1, args.warmup)
             g64.run(1 + args.warmup, args.steps)
@@ -460,6 +467,8 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--batch", type=int, default=8, help="systems in the batched leg (0 or 1: no batched leg)")
     ap.add_argument("--serve-jobs", type=int, default=48, help="jobs of the served stream (0: no serving leg)")
+    ap.add_argument("--tuning", default="", help="fixed nonbonded tuning 'tables_smem,blocks_per_sm,chunk' "
+                                                  "instead of the autotuner (for profiling)")
     ap.add_argument("--serve-steps", type=int, default=2000)
     ap.add_argument("--serve-tick", type=int, default=100)
     args = ap.parse_args()
