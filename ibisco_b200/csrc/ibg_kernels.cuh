@@ -1076,7 +1076,8 @@ __global__ void __launch_bounds__(256) k_bonded(__grid_constant__ const BondedAr
       for (int c = 0; c < 3; ++c) { ij[c] = ri[c] - rj[c]; kj[c] = rk[c] - rj[c]; }
       const R rij = r_sqrt((ij[0] * ij[0] + ij[1] * ij[1]) + ij[2] * ij[2]);
       const R rkj = r_sqrt((kj[0] * kj[0] + kj[1] * kj[1]) + kj[2] * kj[2]);
-      const R ct = ((ij[0] * kj[0] + ij[1] * kj[1]) + ij[2] * kj[2]) / rij / rkj;
+      R ct = ((ij[0] * kj[0] + ij[1] * kj[1]) + ij[2] * kj[2]) / rij / rkj;
+      ct = ct > (R)1 ? (R)1 : (ct < (R)-1 ? (R)-1 : ct);  // rounding of a straight angle (the oracle clamps too)
       const R theta = r_acos(ct) * (R)B.r2d;
       R m[3];
       m[0] = -(ij[1] * kj[2] - ij[2] * kj[1]);

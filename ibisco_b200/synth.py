@@ -397,18 +397,43 @@ def polymer_melt(nchains=400, nper=100, rho=20.0, ntypes=3, seed=2, nsteps=5000,
                  for a in types for b in types if a <= b])
 
 
-def cg_melt(nchains=10000, nper=200, rho=8.0, seed=4, nsteps=2000):
-    """Large CG melt for the roofline study: 10,000 chains x 200 beads (2,000,000) by default."""
-    spec = polymer_melt(nchains=nchains, nper=nper, rho=rho, ntypes=4, seed=seed, nsteps=nsteps, temp=300.0,
-                        dt=0.010, rcut=1.4, rlist=1.6, mass=0.072, bond=0.47, theta0=120.0)
-    types = [1, 2, 3, 4]
-    spec.bond_tabs = [((a, b), harmonic_bond_table("bond.tab", 0.47, 5.0e3, 0.9, 0.0009)) for a in types for b in types
-                      if a <= b]
-    spec.torsion_tabs = []
-    spec.nb_tabs = [((a, b), lj_table(f"nb{a}{b}", 0.45 + 0.01 * (a + b), 2.0, 1.4, 0.001)) for a in types for b in types
-                    if a <= b]
-    spec.control["non_bonded"] = 4
-    return spec
+def cg_melt(nchains=10000, nper=200, rho=8.0, seed=4, nsteps=2000, ntypes=4):
+    """Large CG melt for the roofline study: 10,000 chains x 200 beads (2,000,000)
+    by default, 4 bead types by position along the chain, at number density rho.
+    The chains follow a serpentine path through a cubic lattice of spacing
+    rho^(-1/3) (bonds at their rest length, no overlaps), so the set-up is
+    vectorised and fast at any size.  Harmonic bond (rest length = spacing) and
+    angle (150 deg, weak) tables; the 10 type-pair LJ tables are tabulated on a
+    0.001 nm grid to the 1.4 nm cutoff (list 1.6 nm, rebuilt every 10 steps);
+    NVT 300 K, dt 10 fs."""
+    rng = np.random.default_rng(seed)
+    n = nchains * nper
+    a = rho ** (-1.0 / 3.0)
+    m = int(np.ceil(n ** (1.0 / 3.0)))
+    box = m * a
+    pos = serpentine_lattice(m)[:n] * a - 0.5 * box + 0.5 * a
+    # alternate z offsets bend the chains along x
+    pos[:, 2] += 0.1 * a * (np.arange(n) % 2 - 0.5)
+    pos += rng.normal(scale=0.01, size=pos.shape)
+    types = list(range(1, ntypes + 1))
+    itype = np.tile(1 + np.arange(nper) % ntypes, nchains)
+    mass = 0.072
+    vel = maxwell_boltzmann(rng, np.full(n, mass), 300.0)
+    control = dict(ensemble="NVT", temperature=300.0, pressure=101.3, atoms=n, num_of_time_steps=nsteps,
+                   time_step=0.010, temperature_coupling_time="0.1D0", pressure_coupling_time="5.0D0",
+                   isothermal_compressibility="1.0D-6", virtual_sites=0, mts=0, bead_cutoff=1.4,
+                   bead_neighbour_list_cutoff=1.6, non_bonded_bead=4, cutoff=1.4, neighbour_list_cutoff=1.6,
+                   update_neighbour_list=10, trajectory=nsteps, halt_drift=nsteps + 1, non_bonded=4,
+                   initialize_velocities="N")
+    bond_t = harmonic_bond_table("bond.tab", a, 5.0e3, 1.0, 0.001)
+    ang_t = harmonic_angle_table("ang.tab", 150.0, 10.0)
+    return SystemSpec(
+        control=control, types=[(f"C{t}", mass, "A") for t in types], pos=pos, vel=vel, itype=itype,
+        bonds=chain_bonds(nchains, nper), molecules=[("chain", nper)] * nchains, box=(box, box, box),
+        bond_tabs=[((i, j), bond_t) for i in types for j in types if i <= j],
+        angle_tabs=[(k, ang_t) for k in _all_angle_keys(types)],
+        nb_tabs=[((i, j), lj_table(f"nb{i}{j}", 0.42 + 0.01 * (i + j), 2.0, 1.4, 0.001)) for i in types for j in types
+                 if i <= j])
 
 
 def feature_mix(seed=7, nmol=6, ensemble="NVT", nmts=0, non_bonded=4, temp=400.0):
@@ -517,6 +542,112 @@ def feature_mix(seed=7, nmol=6, ensemble="NVT", nmts=0, non_bonded=4, temp=400.0
         nb_tabs=nb_tabs,
         oop_tabs=[((3, 1, 2, 1), oop_t), ((3, 1, 1, 2), oop_t)],
         virtual=virt, virtbonds=vb, virtangles=va)
+
+
+def hybrid_melt(n_atomistic=100, n_cg=100, nmono=20, seed=3, nsteps=10000, nmts=9, temp=300.0):
+    """Hybrid atomistic/CG melt with centre-of-mass virtual sites and MTS.
+
+    n_atomistic chains of nmono monomers, each monomer 4 backbone carbons in a
+    112-degree zig-zag with 2 hydrogens per carbon (12 atoms, label A) and one
+    virtual site at its centre of mass; n_cg chains of nmono explicit CG beads
+    (label B), one per monomer.  Chains run straight along x on a 0.65 nm grid
+    in y and z; the box is one chain length plus a gap in x.  Atom-atom tables
+    (C, H) to 1.0 nm (list 1.2 nm), bead/site tables to 1.4 nm (list 1.6 nm) as a
+    smooth seeded IBI-like potential: LJ plus Fourier modes.  The reference
+    pairs atoms only with atoms, and beads with beads and sites, but never sites
+    with sites, so the CG chains are what the site tables act on.  MTS evaluates
+    the CG nonbonded forces on 3 of every 3 + nmts steps; bonded terms and atom
+    nonbonded run every step.  Berendsen NVT, dt 1 fs."""
+    rng = np.random.default_rng(seed)
+    bond, theta = 0.155, np.radians(112.0)
+    dx, dy = bond * np.sin(theta / 2), bond * np.cos(theta / 2)   # zig-zag step along x, offset in y
+    mono_len = 4 * dx
+    cg_bond = mono_len / np.sin(np.radians(75.0))
+    cg_dy = cg_bond * np.cos(np.radians(75.0))
+    grid = 0.65
+    nrow = n_atomistic + n_cg
+    ny = int(np.ceil(np.sqrt(nrow)))
+    nz = int(np.ceil(nrow / ny))
+    box = (nmono * mono_len + 0.5, ny * grid, nz * grid)
+    types = [("C", 0.012, "A"), ("H", 0.001008, "A"), ("B", 0.170, "B"), ("V", 0.170, "B")]
+    pos, itype, bonds, mols, virt = [], [], [], [], []
+    alpha = np.radians(54.75)
+    for ch in range(n_atomistic):
+        y0 = -0.5 * box[1] + (ch % ny + 0.5) * grid
+        z0 = -0.5 * box[2] + (ch // ny + 0.5) * grid
+        first = len(pos)
+        nc = 4 * nmono
+        cids = []
+        for k in range(nc):
+            cids.append(len(pos))
+            pos.append((-0.5 * box[0] + 0.25 + k * dx, y0 + (k % 2) * dy, z0))
+            itype.append(1)
+            bonds.append([])
+        for k in range(nc):
+            c = np.array(pos[cids[k]])
+            away = np.array([0.0, -1.0 if k % 2 == 0 else 1.0, 0.0])
+            for sgn in (1.0, -1.0):
+                h = c + bond * 0.7 * (np.cos(alpha) * away + sgn * np.sin(alpha) * np.array([0.0, 0.0, 1.0]))
+                hid = len(pos)
+                pos.append(tuple(h))
+                itype.append(2)
+                bonds.append([cids[k] + 1])
+                bonds[cids[k]].append(hid + 1)
+        for k in range(nc - 1):
+            bonds[cids[k]].append(cids[k + 1] + 1)
+            bonds[cids[k + 1]].append(cids[k] + 1)
+        # molecule = chain; a site per monomer at the centre of mass of its 12 atoms
+        mols.append(("achain", len(pos) - first))
+        for m in range(nmono):
+            members = []
+            for k in range(4 * m, 4 * m + 4):
+                members.append(cids[k] + 1)
+                members.extend(b for b in bonds[cids[k]] if itype[b - 1] == 2)
+            virt.append((4, sorted(members), 0))
+    # the reference lists a particle's bonded partners in coordinate-file order
+    for ch in range(n_cg):
+        row = n_atomistic + ch
+        y0 = -0.5 * box[1] + (row % ny + 0.5) * grid
+        z0 = -0.5 * box[2] + (row // ny + 0.5) * grid
+        first = len(pos)
+        for m in range(nmono):  # a 150-degree zig-zag (a straight angle has no plane)
+            pos.append((-0.5 * box[0] + 0.25 + (m + 0.5) * mono_len, y0 + (m % 2) * cg_dy, z0))
+            itype.append(3)
+            nb = []
+            if m > 0:
+                nb.append(first + m)
+            if m < nmono - 1:
+                nb.append(first + m + 2)
+            bonds.append(nb)
+        mols.append(("cgchain", nmono))
+    pos = np.array(pos)
+    natoms = len(pos)
+    masses = [types[t - 1][1] for t in itype]
+    vel = maxwell_boltzmann(rng, masses, temp)
+    control = dict(ensemble="NVT", temperature=temp, pressure=101.3, atoms=natoms, num_of_time_steps=nsteps,
+                   time_step=0.001, temperature_coupling_time="0.1D0", pressure_coupling_time="1.0D0",
+                   isothermal_compressibility="4.5D-5", virtual_sites=len(virt), mts=nmts, bead_cutoff=1.4,
+                   bead_neighbour_list_cutoff=1.6, non_bonded_bead=4, cutoff=1.0, neighbour_list_cutoff=1.2,
+                   update_neighbour_list=10, trajectory=nsteps, halt_drift=nsteps + 1, non_bonded=4,
+                   initialize_velocities="N")
+    cc = harmonic_bond_table("bcc.tab", bond, 2.5e5, 0.6, 0.0003)
+    ch_t = harmonic_bond_table("bch.tab", bond * 0.7, 2.5e5, 0.6, 0.0003)
+    bb = harmonic_bond_table("bbb.tab", cg_bond, 5.0e3, 1.2, 0.001)
+    ang = harmonic_angle_table("ang.tab", 112.0, 400.0)
+    ang_cg = harmonic_angle_table("angcg.tab", 150.0, 20.0)
+    tor = cosine_torsion_table("tors.tab", 5.0)
+    sig = {(1, 1): 0.34, (1, 2): 0.29, (2, 2): 0.24}
+    eps = {(1, 1): 0.35, (1, 2): 0.15, (2, 2): 0.06}
+    nb = [(k, lj_table(f"nba{k[0]}{k[1]}", sig[k], eps[k], 1.0, 0.002)) for k in sorted(sig)]
+    for k in ((3, 3), (3, 4), (4, 4)):
+        amps = rng.uniform(-0.5, 0.5, size=5) / 5.0
+        nb.append((k, perturbed_lj_table(f"nbc{k[0]}{k[1]}", 0.5, 1.0, 1.4, 0.002, amps)))
+    return SystemSpec(
+        control=control, types=types, pos=pos, vel=vel, itype=np.array(itype), bonds=bonds, molecules=mols,
+        box=box, bond_tabs=[((1, 1), cc), ((1, 2), ch_t), ((3, 3), bb)],
+        angle_tabs=[((1, 1, 1), ang), ((1, 1, 2), ang), ((2, 1, 2), ang), ((3, 3, 3), ang_cg)],
+        torsion_tabs=[((1, 1, 1, 1), tor)],
+        nb_tabs=nb, virtual=virt)
 
 
 # ------------------------------------------------------------ served jobs

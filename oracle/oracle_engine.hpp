@@ -407,6 +407,11 @@ struct Engine {
           R rij = std::sqrt((ij[0] * ij[0] + ij[1] * ij[1]) + ij[2] * ij[2]);
           R rkj = std::sqrt((kj[0] * kj[0] + kj[1] * kj[1]) + kj[2] * kj[2]);
           R ct = ((ij[0] * kj[0] + ij[1] * kj[1]) + ij[2] * kj[2]) / rij / rkj;
+          // ANGLES.inc:20-21 takes ACOS(CT) unclamped; rounding can put |CT| of a
+          // straight angle just above 1, where the reference's result is NaN.  The
+          // restatement clamps there, as TORSIONS.inc:93-96 does for its cosine.
+          if (ct > (R)1) ct = (R)1;
+          if (ct < (R)-1) ct = (R)-1;
           R theta = std::acos(ct) * (R)s->R2D;
           R m[3];
           m[0] = -(ij[1] * kj[2] - ij[2] * kj[1]);
@@ -422,7 +427,8 @@ struct Engine {
           ss[1] = -(-m[0] * kj[2] + m[2] * kj[0]) / rkj;
           ss[2] = -(m[0] * kj[1] - m[1] * kj[0]) / rkj;
           int k = fint(theta / bend.bin[TIJK]);
-          if (k < 0 || k + 1 >= bend.w) { ++tor_err; continue; }  // NaN or >180 deg: outside the table
+          // NaN or beyond the table (ANGLES.inc:43-49 reads row NI alone at 180 deg)
+          if (k < 0 || k >= bend.w || (k + 1 >= bend.w && theta != (R)180.0)) { ++tor_err; continue; }
           R fijk, vijk;
           if (theta == (R)180.0) {
             fijk = bend.Fo(TIJK, k); vijk = bend.P(TIJK, k);

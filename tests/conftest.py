@@ -53,6 +53,7 @@ def sysdir(tmp_path_factory):
         "mix5_mts": lambda: synth.feature_mix(seed=8, non_bonded=5, nmts=3),
         "mix_npt": lambda: synth.feature_mix(seed=9, ensemble="NPT"),
         "mix_nve": lambda: synth.feature_mix(seed=10, ensemble="NVE"),
+        "hybrid": lambda: synth.hybrid_melt(n_atomistic=32, n_cg=32, nmono=20, seed=13, nsteps=100),
     }
 
     def get(name):

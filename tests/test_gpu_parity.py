@@ -22,7 +22,7 @@ FORCE_TOL = 1e-5     # FP32/fixed vs FP64, max-norm relative
 ENERGY_TOL = 1e-5
 FP64_TOL = 1e-9      # FP64 path vs FP64 oracle
 
-SYSTEMS = ["fluid", "melt", "mix4", "mix5_mts", "mix_npt", "mix_nve"]
+SYSTEMS = ["fluid", "melt", "mix4", "mix5_mts", "mix_npt", "mix_nve", "hybrid"]
 
 
 def make(d, prec):
