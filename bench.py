@@ -58,8 +58,8 @@ WORKLOADS = {
     "fluid4k": "single-type LJ fluid: 4,000 beads, rho 8/nm^3, rc 1.2 nm, list 1.4 nm every 10 steps, NVE, dt 10 fs",
     "melt2m": "CG melt: 10,000 chains x 200 beads (2,000,000), 4 types, bond/angle tables, 10 LJ tables "
               "rc 1.4 nm, list 1.6 nm every 10 steps, NVT 300 K, dt 10 fs",
-    "hybrid": "hybrid melt: 100 atomistic chains x 20 monomers x 12 atoms (24,000) with a centre-of-mass "
-              "virtual site per monomer (2,000) and 100 CG chains x 20 beads (2,000); atom tables rc 1.0 nm, "
+    "hybrid": "hybrid melt: 200 atomistic chains x 20 monomers x 12 atoms (48,000) with a centre-of-mass "
+              "virtual site per monomer (4,000) and 200 CG chains x 20 beads (4,000); atom tables rc 1.0 nm, "
               "bead/site tables rc 1.4 nm, MTS 9 (CG nonbonded on 3 of 12 steps), NVT 300 K, dt 1 fs",
 }
 
@@ -74,7 +74,7 @@ def make_workload(name: str, directory: str):
     elif name == "melt2m":
         spec = synth.cg_melt()
     elif name == "hybrid":
-        spec = synth.hybrid_melt()
+        spec = synth.hybrid_melt(n_atomistic=200, n_cg=200)
     else:
         raise SystemExit(f"unknown workload {name}")
     synth.write_system(spec, directory)
@@ -144,13 +144,14 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel_summary: str):
-    """Per-launch DRAM bytes of the nonbonded kernel from the committed ncu
-    summary (a 'dram_bytes_per_launch: <n>' line), scaled later to this run."""
-    p = os.path.join(ROOT, "profiles", kernel_summary)
+def ncu_traffic(workload: str):
+    """DRAM bytes (read + write) per nonbonded launch of this workload, from
+    its committed ncu summary (a 'dram_bytes_per_launch: <n>' line), or None
+    where no capture of this workload exists."""
+    p = os.path.join(ROOT, "profiles", f"nonbonded_{workload}.md")
     if not os.path.exists(p):
         return None
-    m = re.search(r"dram_bytes_per_particle:\s*([0-9.eE+]+)", open(p).read())
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
     return float(m.group(1)) if m else None
 
 
@@ -301,6 +302,28 @@ def reduce_sum(pg, x: float) -> float:
     return float(t.item())
 
 
+TUNING_KEYS = ("nb_tables_smem", "nb_blocks_per_sm", "nb_chunk", "nb_rows")
+
+
+def pick_tuning(native, g, setup, prec, state, flush, reps=20, top=6):
+    """Launch tuning of the nonbonded kernel: rank the candidates by their
+    launches alone (ibg_autotune, L2 flushed before each), then time whole
+    steps of the `top` fastest on fresh systems and apply the fastest to g.
+    Returns (tuning, [(candidate, us per launch)], [(candidate, us per step)])."""
+    _, cands = g.autotune(reps=reps)
+    best = [dict(zip(TUNING_KEYS, c)) for c, _ in sorted(cands, key=lambda t: t[1])[:top]]
+
+    def make_one():
+        x = native.System(setup, prec)
+        x.set_state(*state)
+        return x
+
+    n = state[0].shape[0]
+    tuned, steps = native.tune_steps(make_one, best, steps=100 if n < 500000 else 20, l2_flush=flush)
+    g.set_tuning(**tuned)
+    return tuned, cands, steps
+
+
 def run_b200(args, world, rank, local, pg):
     import ctypes
 
@@ -320,14 +343,14 @@ def run_b200(args, world, rank, local, pg):
         g.set_state(s0, v0, b0)
         # launch tuning of the nonbonded kernel, picked by timing (state
         # unchanged), or fixed by --tuning (profiling runs)
-        if args.tuning:
-            sm, per, ch = (int(x) for x in args.tuning.split(","))
-            tuned, tune_cands = dict(nb_tables_smem=sm, nb_blocks_per_sm=per, nb_chunk=ch), []
-            g.set_tuning(**tuned)
-        else:
-            tuned, tune_cands = g.autotune(reps=20)
         flush = 256 << 20
         g.set_l2_flush(flush)
+        if args.tuning:
+            vals = [int(x) for x in args.tuning.split(",")]
+            g.set_tuning(**dict(zip(TUNING_KEYS, vals)))
+            tuned, tune_cands, tune_steps = g.tuning(), [], []
+        else:
+            tuned, tune_cands, tune_steps = pick_tuning(native, g, setup, prec, (s0, v0, b0), flush)
         # ---- warm-up (captures the CUDA graphs) and device-timed region
         g.run(1, args.warmup)
         barrier(pg)
@@ -346,17 +369,26 @@ def run_b200(args, world, rank, local, pg):
         g.run(1 + args.warmup + args.steps, k_roof)
         t2 = g.timing()
         g.set_timing(False)
-        _, nn = g.neighbour_list(0)
-        pairs = float(nn.sum())
-        nb_launch_s = t2["nonbonded_ms"] / max(1, t2["nonbonded_launches"]) / 1000.0
-        bytes_launch = 16.0 * n + 4.0 * pairs
+        # algorithmic bytes of every nonbonded launch of the pass: 16 B of own
+        # position per particle of the list plus 4 B per listed pair
+        lists = {}
+        for w in (0, 1):
+            nn = g.neighbour_counts(w)
+            if len(nn):
+                lists[w] = (len(nn), float(nn.sum()))
+        nlaunch = {1: t2["nonbonded_bead_launches"]}
+        nlaunch[0] = t2["nonbonded_launches"] - nlaunch[1]
+        nb_bytes = sum(nlaunch[w] * (16.0 * nw + 4.0 * pw) for w, (nw, pw) in lists.items())
+        nb_count = max(1, t2["nonbonded_launches"])
+        nb_launch_s = t2["nonbonded_ms"] / nb_count / 1000.0
+        bytes_launch = nb_bytes / nb_count
         peak, peak_kind = measured_peak()
         achieved = bytes_launch / nb_launch_s / 1e9
-        tr = ncu_traffic("nonbonded_melt40k.md")
         roof = {"bound": "hbm", "kernel": "k_nonbonded", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": (tr * n if tr else None),
+                "frac": achieved / peak, "traffic": ncu_traffic(args.workload),
                 "peak_kind": peak_kind, "launch_us": nb_launch_s * 1e6,
-                "algorithmic_bytes_per_launch": bytes_launch, "mean_half_list": pairs / n}
+                "algorithmic_bytes_per_launch": bytes_launch,
+                "mean_half_list": {("atom", "bead")[w]: pw / nw for w, (nw, pw) in lists.items()}}
         stage = {k: t2[k] / k_roof for k in ("list_ms", "nonbonded_ms", "bonded_ms", "integrate_ms", "other_ms")}
         # ---- end to end through the C ABI with host buffers
         sp = np.ascontiguousarray(s0, np.float32)
@@ -386,9 +418,9 @@ def run_b200(args, world, rank, local, pg):
         if prec == native.IBG_PREC_FP32_FIXED and not args.no_fp64:
             g64 = native.System(setup, native.IBG_PREC_FP64_PLAIN)
             g64.set_state(s0, v0, b0)
-            if not args.tuning:
-                g64.autotune(reps=10)  # the comparison path gets its own best launch tuning
             g64.set_l2_flush(flush)
+            if not args.tuning:  # the comparison path gets its own best launch tuning
+                pick_tuning(native, g64, setup, native.IBG_PREC_FP64_PLAIN, (s0, v0, b0), flush, reps=10)
             g64.run(1, args.warmup)
             g64.run(1 + args.warmup, args.steps)
             ms64 = reduce_max(pg, g64.timing()["run_ms"])
@@ -408,8 +440,11 @@ def run_b200(args, world, rank, local, pg):
                 return out
 
             # the batch's own launch tuning (it can differ from one system's)
-            base = dict(nb_tables_smem=0, nb_blocks_per_sm=0, nb_chunk=0)
-            cands = [base] + ([tuned] if tuned != base else [])
+            cands = []
+            for cand in [tuned] + [dict(nb_tables_smem=0, nb_blocks_per_sm=0, nb_chunk=ch, nb_rows=rows)
+                                   for rows in (8, 16) for ch in (0, 24, 48)]:
+                if cand not in cands:
+                    cands.append(cand)
             btuned, btimes = native.tune_batch(make_systems, cands, steps=100)
             systems = make_systems()
             for gb in systems:
@@ -451,7 +486,8 @@ def run_b200(args, world, rank, local, pg):
                            "l2": "flushed before every step (256 MiB write, outside the timed interval)"},
                 "ns_per_day": steps_per_s * dt_ps * 1e-3 * 86400.0,
                 "roofline": roof, "stage_ms_per_step": stage,
-                "tuning": {"nonbonded": tuned, "candidates_us": [[list(c), u] for c, u in tune_cands]},
+                "tuning": {"nonbonded": tuned, "candidates_us": [[list(c), u] for c, u in tune_cands],
+                           "steps_us": [[t, u] for t, u in tune_steps]},
                 "cpu_baseline": cpu, "e2e": e2e, "fp64_plain": fp64, "batched": batched, "serving": serving,
                 "gpu_launches": launches,
                 "clocks": clk.summary(),
@@ -472,7 +508,7 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--batch", type=int, default=8, help="systems in the batched leg (0 or 1: no batched leg)")
     ap.add_argument("--serve-jobs", type=int, default=48, help="jobs of the served stream (0: no serving leg)")
-    ap.add_argument("--tuning", default="", help="fixed nonbonded tuning 'tables_smem,blocks_per_sm,chunk' "
+    ap.add_argument("--tuning", default="", help="fixed nonbonded tuning 'tables_smem,blocks_per_sm,chunk[,rows]' "
                                                   "instead of the autotuner (for profiling)")
     ap.add_argument("--serve-steps", type=int, default=2000)
     ap.add_argument("--serve-tick", type=int, default=100)

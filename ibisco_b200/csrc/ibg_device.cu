@@ -164,6 +164,7 @@ struct ibg_ctx {
   int g_list[2] = {1, 1}, g_regrid[2] = {1, 1}, g_build[2] = {1, 1}, g_dist = 1;
   int nb_blocks_per_sm = 0;  // tuning: resident nonbonded blocks per SM (0: all that fit)
   int nb_chunk = 0;          // tuning (FP32): work units per block chunk (0: per warp)
+  int nb_rows = 16;          // tuning: list rows per nonbonded work unit (8 or 16)
   ObsD* ring = nullptr;
   int ring_cap = 0;
   double *p_b = nullptr, *p_mv = nullptr, *p_mom = nullptr;
@@ -177,7 +178,7 @@ struct ibg_ctx {
   long long launches_per_variant[32] = {0};
   // timing: stage events (timing mode, direct launches) and whole-run events
   bool timing = false;
-  double stage_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double stage_ms[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   std::vector<std::pair<cudaEvent_t, int>> marks;  // event, stage that starts there
   cudaEvent_t run_ev[2] = {nullptr, nullptr};
   long long launches = 0;
@@ -360,7 +361,6 @@ void collect_marks(ibg_ctx* c) {
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, c->marks[k].first, c->marks[k + 1].first));
     c->stage_ms[stg] += ms;
-    if (stg == 1) c->stage_ms[6] += 0;  // counted at launch
   }
   for (auto& m : c->marks) cudaEventDestroy(m.first);
   c->marks.clear();
@@ -407,6 +407,7 @@ void make_args(ibg_ctx* c) {
     n.fsort = (acc_t*)L.fsort;
     n.ltab = L.ltab; n.toff = L.toff; n.tndat = L.tndat; n.tbin = (const R*)L.tbin; n.tinv = (const R*)L.tinv;
     n.tfp = (const R*)L.tfp; n.tx = (const R*)L.tx; n.ptab = L.ptab; n.chunk = c->nb_chunk;
+    n.rows = c->nb_rows;
     n.ntab = L.ntab; n.nrows = L.nrows; n.rcutsq = (R)L.rcutsq;
     CollectArgs<R>& k = A.col[w];
     k.sc = sc; k.n = L.n; k.mts = (w == 1 && c->nmts > 0); k.sorted = L.sorted; k.idx = L.idx;
@@ -632,7 +633,11 @@ void enqueue_step(ibg_ctx* c, unsigned v) {
   // nonbonded: MTS runs the bead list first (MTS_LOOP.f90:100-116); sums are
   // order independent, so one sequence serves both loops
   mark(c, 1);
-  if (c->L[1].present && !(v & V_MTS_APPROX)) { enq_nonbonded<R>(c, c->L[1]); c->stage_ms[6] += c->timing; }
+  if (c->L[1].present && !(v & V_MTS_APPROX)) {
+    enq_nonbonded<R>(c, c->L[1]);
+    c->stage_ms[6] += c->timing;
+    c->stage_ms[8] += c->timing;
+  }
   if (c->L[0].present) { enq_nonbonded<R>(c, c->L[0]); c->stage_ms[6] += c->timing; }
   mark(c, 4);
   if (c->L[1].present) enq_collect<R>(c, c->L[1]);
@@ -802,15 +807,18 @@ int ibg_get_tuning(const ibg_ctx* c, ibg_tuning* t) {
   t->nb_tables_smem = L.use_smem ? 1 : 0;
   t->nb_blocks_per_sm = c->nb_blocks_per_sm;
   t->nb_chunk = c->nb_chunk;
+  t->nb_rows = c->nb_rows;
   return IBG_OK;
 }
 
 int ibg_set_tuning(ibg_ctx* c, const ibg_tuning* t) {
   if (!c || !t || t->nb_blocks_per_sm < 0 || t->nb_chunk < 0) return IBG_E_INVALID;
+  if (t->nb_rows != 0 && t->nb_rows != 8 && t->nb_rows != 16) return IBG_E_INVALID;
   if (c->in_batch) return fail(c, IBG_E_INVALID, "the context is in a batch");
   try {
     c->nb_blocks_per_sm = t->nb_blocks_per_sm;
     c->nb_chunk = c->prec == IBG_PREC_FP32_FIXED ? t->nb_chunk : 0;
+    c->nb_rows = t->nb_rows ? t->nb_rows : 16;
     for (auto& L : c->L) {
       if (!L.present) continue;
       L.use_smem = t->nb_tables_smem != 0 && L.smem <= 200 * 1024;
@@ -826,49 +834,71 @@ int ibg_set_tuning(ibg_ctx* c, const ibg_tuning* t) {
   return IBG_OK;
 }
 
-int ibg_autotune(ibg_ctx* c, int reps, ibg_tuning* best, double* us, int ncand) {
+int ibg_autotune(ibg_ctx* c, int reps, ibg_tuning* best, ibg_tuning* cand_out, double* us, int ncand) {
   if (!c || reps <= 0) return IBG_E_INVALID;
   if (!c->state_set) return fail(c, IBG_E_INVALID, "ibg_set_state has not been called");
   if (c->in_batch) return fail(c, IBG_E_INVALID, "the context is in a batch");
   std::vector<ibg_tuning> cand;
   if (c->prec == IBG_PREC_FP32_FIXED) {
-    for (int chunk : {0, 48, 96})
-      for (int smem : {0, 1})
-        for (int per : {0, 3}) cand.push_back(ibg_tuning{smem, per, chunk});
+    for (int rows : {8, 16})
+      for (int chunk : {0, 12, 24, 48, 96})
+        for (int smem : {0, 1})
+          for (int per : {0, 3}) cand.push_back(ibg_tuning{smem, per, chunk, rows});
   } else {
-    for (int smem : {0, 1})
-      for (int per : {0, 3, 2}) cand.push_back(ibg_tuning{smem, per, 0});
+    for (int rows : {8, 16})
+      for (int smem : {0, 1})
+        for (int per : {0, 3, 2}) cand.push_back(ibg_tuning{smem, per, 0, rows});
   }
   ibg_tuning keep;
   ibg_get_tuning(c, &keep);
   int win = -1;
   double win_us = 0.0;
+  std::vector<cudaEvent_t> ev(2 * (size_t)reps, nullptr);
+  auto drop_events = [&] {
+    for (auto& e : ev)
+      if (e) {
+        cudaEventDestroy(e);
+        e = nullptr;
+      }
+  };
   try {
-    cudaEvent_t e0, e1;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    // with an L2 flush set, every timed launch starts from a flushed L2 as the
+    // nonbonded launch of a timed step does; only the launches are timed
+    const bool flush = c->flush_bytes > 0;
+    if (flush && !c->flush_buf) CK(cudaMalloc(&c->flush_buf, c->flush_bytes));
     for (size_t k = 0; k < cand.size(); ++k) {
       int rc = ibg_set_tuning(c, &cand[k]);
-      if (rc) return rc;
-      float ms = 0.f;
+      if (rc) {
+        drop_events();
+        return rc;
+      }
       for (int r = 0; r <= reps; ++r) {  // the first launch warms up
         CK(cudaMemsetAsync(c->sc->work, 0, sizeof(c->sc->work), c->st));
-        if (r == 1) CK(cudaEventRecord(e0, c->st));
+        if (flush) CK(cudaMemsetAsync(c->flush_buf, r & 0xff, c->flush_bytes, c->st));
+        if (r > 0) CK(cudaEventRecord(ev[2 * (r - 1)], c->st));
         for (auto& L : c->L) {
           if (!L.present) continue;
           if (c->prec == IBG_PREC_FP32_FIXED) enq_nonbonded<float>(c, L);
           else enq_nonbonded<double>(c, L);
         }
+        if (r > 0) CK(cudaEventRecord(ev[2 * (r - 1) + 1], c->st));
       }
-      CK(cudaEventRecord(e1, c->st));
-      CK(cudaEventSynchronize(e1));
-      CK(cudaEventElapsedTime(&ms, e0, e1));
+      CK(cudaEventSynchronize(ev.back()));
+      double ms = 0.0;
+      for (int r = 0; r < reps; ++r) {
+        float m = 0.f;
+        CK(cudaEventElapsedTime(&m, ev[2 * r], ev[2 * r + 1]));
+        ms += m;
+      }
       const double t = 1000.0 * ms / reps;
-      if (us && (int)k < ncand) us[k] = t;
+      if ((int)k < ncand) {
+        if (us) us[k] = t;
+        if (cand_out) cand_out[k] = cand[k];
+      }
       if (win < 0 || t < win_us) { win = (int)k; win_us = t; }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    drop_events();
     // the timing launches summed forces and energies: clear them
     for (auto& L : c->L)
       if (L.present) CK(cudaMemset(L.fsort, 0, accsize(c) * 3 * (size_t)L.n));
@@ -881,6 +911,7 @@ int ibg_autotune(ibg_ctx* c, int reps, ibg_tuning* best, double* us, int ncand) 
       return check_device(c);
     }
   } catch (CudaError& e) {
+    drop_events();
     return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
   }
   int rc = ibg_set_tuning(c, &cand[win]);
@@ -1109,7 +1140,7 @@ int ibg_create(const ibg_desc* d, int precision, ibg_ctx** out) {
       DevList& L = c->L[w];
       if (!L.present) continue;
       c->g_list[w] = grid_for(c.get(), L.n);
-      c->g_build[w] = std::max(1, std::min((L.n + 7) / 8, c->nsm * 8));
+      c->g_build[w] = std::max(1, std::min((L.n + 15) / 16, c->nsm * 4));  // blocks take cells
     }
     c->g_dist = grid_for(c.get(), std::max(1, c->nvirta));
     c->g_b = grid_for(c.get(), (long long)c->nb + c->na + c->nt + c->no, 4);
@@ -1425,7 +1456,7 @@ int ibg_get_neighbour_list(ibg_ctx* c, int which, int* list, int maxnab, int* nn
     CK(cudaMemcpy(counts.data(), L.counts, sizeof(int) * L.n, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(sorted.data(), L.sorted, sizeof(int) * L.n, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(idx.data(), L.idx, sizeof(int) * L.n, cudaMemcpyDeviceToHost));
-    std::vector<int> e((size_t)L.nslices * 32 * L.w_cap);
+    std::vector<int> e(list ? (size_t)L.nslices * 32 * L.w_cap : 0);
     if (!e.empty()) CK(cudaMemcpy(e.data(), L.entries, sizeof(int) * e.size(), cudaMemcpyDeviceToHost));
     const int T = L.T, P = 32 / L.T;
     for (int s = 0; s < L.n; ++s) {
@@ -1478,7 +1509,7 @@ int ibg_set_timing(ibg_ctx* c, int on) {
 int ibg_get_timing(ibg_ctx* c, double* stage_ms, int nstage, long long* launches) {
   if (!c) return IBG_E_INVALID;
   c->stage_ms[7] = (double)c->list_growths;
-  for (int k = 0; k < nstage && k < 8; ++k) stage_ms[k] = c->stage_ms[k];
+  for (int k = 0; k < nstage && k < 9; ++k) stage_ms[k] = c->stage_ms[k];
   if (launches) *launches = c->launches;
   return IBG_OK;
 }

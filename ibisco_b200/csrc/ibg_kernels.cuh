@@ -381,28 +381,42 @@ __global__ void k_slot_of(__grid_constant__ const ListArgs L0, const ListArgs* c
   }
 }
 
-// NEW_NEIGHBOUR_WITHLIST.f90:34-123.  A warp builds one particle's list at a
-// time (slots taken dynamically).  Candidates are visited in the reference's
-// order -- the particle's own cell below it (decreasing A), then the 13 cells
-// of the MAPS.f90:137-149 stencil, each by decreasing A -- 32 at a time, one
-// per lane (consecutive slots: coalesced loads); a ballot and a prefix count
-// keep the accepted ones in that order.  The distance test runs first and the
-// exclusion test only for candidates inside RLIST (the accepted set is the
-// same); exclusions are compared as slots of this list, and a virtual site is
-// recognised by its label in the position's w, so no candidate's global id is
-// loaded.  The list is stored in the nonbonded kernel's layout: T lanes per
-// slot, slices of P = 32/T slots, entry k of slot s (slice g) at
-// (g*w_cap + k/T)*32 + (s%P)*T + k%T.  A slot that needs more than w_cap rows
-// records its need and raises the abort flag (the host enlarges the storage
-// and repeats the step).
+// NEW_NEIGHBOUR_WITHLIST.f90:34-123.  A block builds the lists of one cell's
+// particles at a time (cells taken dynamically).  The candidates of the cell --
+// its own slots, then the slots of the 13 cells of the MAPS.f90:137-149
+// stencil, each run by decreasing A -- are staged once in shared memory, in
+// that order, with their slot numbers; every particle of the cell then reads
+// them from there.  A warp builds one particle's list: its candidates are the
+// staged ones from just below its own slot to the end, which is the
+// reference's order (its own cell below it by decreasing A, then the stencil
+// cells), visited 32 at a time, one per lane; a ballot and a prefix count keep
+// the accepted ones in that order.  A cell whose candidates do not fit the
+// staging buffer reads them from global memory instead (same order).  The
+// distance test runs first and the exclusion test only for candidates inside
+// RLIST (the accepted set is the same); exclusions are compared as slots of
+// this list, and a virtual site is recognised by its label in the position's
+// w, so no candidate's global id is loaded.  The list is stored in the
+// nonbonded kernel's layout: T lanes per slot, slices of P = 32/T slots, entry
+// k of slot s (slice g) at (g*w_cap + k/T)*32 + (s%P)*T + k%T.  A slot that
+// needs more than w_cap rows records its need and raises the abort flag (the
+// host enlarges the storage and repeats the step).
 // The 13 neighbour cells of the half stencil in MAPS.f90:137-149 order.
 __constant__ int kStencil[13][3] = {{1, 0, 0}, {1, 1, 0},  {0, 1, 0},  {-1, 1, 0}, {1, 0, -1}, {1, 1, -1}, {0, 1, -1},
                                     {-1, 1, -1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}, {-1, 1, 1}, {0, 0, 1}};
 
+// Candidates one block stages (positions and slots): 2,304 in FP32 (about 160
+// particles per cell), 1,152 in FP64, within 48 KB of static shared memory.
+template <typename R>
+struct ListStage {
+  static constexpr int cap = sizeof(R) == 4 ? 2304 : 1152;
+};
+
 template <typename R, int T, bool B>
-__global__ void __launch_bounds__(256) k_list_build(__grid_constant__ const ListArgs L0, const ListArgs* const* tab,
-                                                    const BlockMap bm, int always) {
+__global__ void __launch_bounds__(256, 4) k_list_build(__grid_constant__ const ListArgs L0, const ListArgs* const* tab,
+                                                       const BlockMap bm, int always) {
   using PT = typename Prec<R>::pos_t;
+  constexpr int kCap = ListStage<R>::cap;
+  constexpr int kWarps = 8;  // blockDim.x = 256
   const Blk bk = blk<B>(bm);
   __shared__ ListArgs s_args;
   if (B) stage_args(&s_args, tab[bk.sys]);
@@ -410,8 +424,13 @@ __global__ void __launch_bounds__(256) k_list_build(__grid_constant__ const List
   Scalars* sc = L.sc;
   if (sc->skip || !(always || sc->rebuild)) return;
   constexpr int P = 32 / T;
-  __shared__ int s_exs[8][20];  // each warp's particle's exclusions, as slots of this list
+  __shared__ PT s_pos[kCap];
+  __shared__ int s_slot[kCap];
+  __shared__ int s_hi[14], s_pre[15];  // run u: slots s_hi[u] down, staged from s_pre[u]
+  __shared__ int s_exs[kWarps][20];    // each warp's particle's exclusions, as slots of this list
+  __shared__ int s_cell;
   const int nx = sc->ncell[L.which][0], ny = sc->ncell[L.which][1], nz = sc->ncell[L.which][2];
+  const int ncells = nx * ny * nz;
   R b[3], bi[3], b2[3];
   box_of<R>(sc, b, bi, b2);
   const R rlsq = sizeof(R) == 4 ? (R)L.rlistsq : (R)L.rlistsqd;
@@ -421,36 +440,95 @@ __global__ void __launch_bounds__(256) k_list_build(__grid_constant__ const List
   const int cap = L.w_cap * T;  // entries a slot may hold
   int* exs = s_exs[warp];
   for (;;) {
-    int s = 0;
-    if (lane == 0) s = (int)atomicAdd(&sc->work[2 + L.which], 1u);
-    s = __shfl_sync(0xffffffffu, s, 0);
-    if (s >= L.n) break;
-    const int g = s / P;
-    const long long base = (long long)g * L.w_cap * 32 + (s % P) * T;
-    const int a = L.sorted[s];
-    const int i = L.idx[a];
-    const PT pi = pos[s];
-    const int ne = L.excl_n[i];
-    if (lane < ne) {
-      const int gs = L.gslot[L.excl[(size_t)i * 20 + lane]];
-      exs[lane] = (gs & 1) == L.which ? gs >> 1 : -1;
+    __syncthreads();  // the previous cell's staging is no longer read
+    if (threadIdx.x == 0) s_cell = (int)atomicAdd(&sc->work[2 + L.which], 1u);
+    __syncthreads();
+    const int c0 = s_cell;
+    if (c0 >= ncells) break;
+    const int first = L.cell_start[c0], last = L.cell_start[c0 + 1];
+    if (first == last) continue;
+    if (warp == 0) {
+      // run 0: the own cell from its last slot down; runs 1..13: the stencil
+      // cells, each from its last slot down; exclusive prefix of the lengths
+      int hi = 0, len = 0;
+      if (lane == 0) {
+        hi = last - 1;
+        len = last - first;
+      } else if (lane < 14) {
+        const int ix = c0 / (nz * ny), iy = (c0 / nz) % ny, iz = c0 % nz;
+        const int jx = (ix + kStencil[lane - 1][0] + nx) % nx, jy = (iy + kStencil[lane - 1][1] + ny) % ny,
+                  jz = (iz + kStencil[lane - 1][2] + nz) % nz;
+        const int c = jx * nz * ny + jy * nz + jz;
+        const int lo = L.cell_start[c];
+        hi = L.cell_start[c + 1] - 1;
+        len = hi - lo + 1;
+      }
+      int incl = len;
+#pragma unroll
+      for (int o = 1; o < 16; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (lane < 14) {
+        s_hi[lane] = hi;
+        s_pre[lane] = incl - len;
+      }
+      if (lane == 13) s_pre[14] = incl;
     }
-    __syncwarp();
-    const bool i_vs = L.hybrid && i >= L.natoms;
-    const int c0 = L.cell_of[a];
-    const int ix = c0 / (nz * ny), iy = (c0 / nz) % ny, iz = c0 % nz;
-    int cnt = 0;
-    // minimum image by compare and select.  It equals d - ANINT(d/L)*L for
-    // |d| < L/2 (ANINT = 0) and for |d| > L/2 away from the rounding of d/L
-    // to 1/2 (both subtract L the same way); where they can differ, |d| is
-    // within rounding of L/2, beyond RLIST <= L/3 either way.  So the accepted
-    // set is bit for bit the reference's.
-    auto segment = [&](int hi, int lo) {  // candidates hi, hi-1, ..., lo
-      for (int t0 = hi; t0 >= lo; t0 -= 32) {
-        const int t = t0 - lane;
+    __syncthreads();
+    const int total = s_pre[14];
+    // run of staged index v: the largest u with s_pre[u] <= v (that run is
+    // not empty)
+    auto slot_at = [&](int v) {
+      int lo = 0, hi = 13;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s_pre[mid] <= v) lo = mid;
+        else hi = mid - 1;
+      }
+      return s_hi[lo] - (v - s_pre[lo]);
+    };
+    const bool staged = total <= kCap;
+    if (staged) {
+      for (int v = threadIdx.x; v < total; v += blockDim.x) {
+        const int t = slot_at(v);
+        s_slot[v] = t;
+        s_pos[v] = pos[t];
+      }
+    }
+    __syncthreads();
+    for (int s = first + warp; s < last; s += kWarps) {
+      const int g = s / P;
+      const long long base = (long long)g * L.w_cap * 32 + (s % P) * T;
+      const int a = L.sorted[s];
+      const int i = L.idx[a];
+      const PT pi = staged ? s_pos[last - 1 - s] : pos[s];
+      const int ne = L.excl_n[i];
+      if (lane < ne) {
+        const int gs = L.gslot[L.excl[(size_t)i * 20 + lane]];
+        exs[lane] = (gs & 1) == L.which ? gs >> 1 : -1;
+      }
+      __syncwarp();
+      const bool i_vs = L.hybrid && i >= L.natoms;
+      int cnt = 0;
+      // minimum image by compare and select.  It equals d - ANINT(d/L)*L for
+      // |d| < L/2 (ANINT = 0) and for |d| > L/2 away from the rounding of d/L
+      // to 1/2 (both subtract L the same way); where they can differ, |d| is
+      // within rounding of L/2, beyond RLIST <= L/3 either way.  So the
+      // accepted set is bit for bit the reference's.
+      for (int v0 = last - s; v0 < total; v0 += 32) {
+        const int v = v0 + lane;
         bool ok = false;
-        if (t >= lo) {
-          const PT pj = pos[t];
+        int t = -1;
+        if (v < total) {
+          PT pj;
+          if (staged) {
+            t = s_slot[v];
+            pj = s_pos[v];
+          } else {
+            t = slot_at(v);
+            pj = pos[t];
+          }
           R d0 = pi.x - pj.x, d1 = pi.y - pj.y, d2 = pi.z - pj.z;
           d0 = d0 > b2[0] ? d0 - b[0] : (d0 < -b2[0] ? d0 + b[0] : d0);
           d1 = d1 > b2[1] ? d1 - b[1] : (d1 < -b2[1] ? d1 + b[1] : d1);
@@ -470,31 +548,27 @@ __global__ void __launch_bounds__(256) k_list_build(__grid_constant__ const List
         }
         cnt += __popc(m);
       }
-    };
-    segment(s - 1, L.cell_start[c0]);
-#pragma unroll 1
-    for (int u = 0; u < 13; ++u) {
-      const int jx = (ix + kStencil[u][0] + nx) % nx, jy = (iy + kStencil[u][1] + ny) % ny,
-                jz = (iz + kStencil[u][2] + nz) % nz;
-      const int c = jx * nz * ny + jy * nz + jz;
-      segment(L.cell_start[c + 1] - 1, L.cell_start[c]);
-    }
-    if (lane == 0) {
-      L.counts[s] = cnt;
-      if (cnt >= L.maxnab) atomicOr(&sc->err, EB_LIST_OVERFLOW);
-      const int rows = (cnt + T - 1) / T;
-      atomicMax(&L.slice_w[g], rows);
-      if (rows > L.w_cap) {
-        atomicMax(&sc->need_rows[L.which], rows);
-        sc->abort = 1;
-        sc->skip = 1;
+      if (lane == 0) {
+        L.counts[s] = cnt;
+        if (cnt >= L.maxnab) atomicOr(&sc->err, EB_LIST_OVERFLOW);
+        const int rows = (cnt + T - 1) / T;
+        atomicMax(&L.slice_w[g], rows);
+        if (rows > L.w_cap) {
+          atomicMax(&sc->need_rows[L.which], rows);
+          sc->abort = 1;
+          sc->skip = 1;
+        }
       }
+      __syncwarp();  // exs is rewritten for the next particle
     }
-    __syncwarp();  // exs is rewritten for the next particle
   }
 }
 
 // ------------------------------------------------------------- nonbonded
+// FP32 nonbonded energies and virials are summed in FP32 over this many list
+// rows of a slice, then in fixed point.
+constexpr int kEnergyRows = 8;
+
 template <typename R>
 struct NBArgs {
   Scalars* sc;
@@ -516,6 +590,7 @@ struct NBArgs {
   const R* tinv; // 1/bin per table (FP32 force kernel)
   const int4* ptab;  // FP32 kernel: per type pair {first row, NDAT, 1/bin bits, 1 if a table}
   int chunk;         // FP32 kernel: work units per block chunk (0: each warp takes units alone)
+  int rows;          // list rows per work unit, a multiple of kEnergyRows
   const R* tfp;  // 2 per row
   const R* tx;
   int ntab, nrows;
@@ -589,7 +664,7 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded(__grid_constant__ const NB
   const bool run = true;
   // work unit = up to ROWS rows of 32 entries of one slice; units are taken
   // dynamically so that warps finish within one unit of each other
-  constexpr int ROWS = 8;
+  const int ROWS = A.rows;
   const int U = (A.w_cap + ROWS - 1) / ROWS;
   const int nunits = A.nslices * U;
   for (;;) {
@@ -685,53 +760,31 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded(__grid_constant__ const NB
     for (int k = 0; k < 9; ++k) atomicAdd((double*)&sc->nbacc[A.work][k], out[k]);
 }
 
-// round(v * 2^32) for |v| < 2^31 with integer operations only (the
-// conversion unit is the busiest pipe of the pair loop).  Rounds half away
-// from zero in magnitude; exact antisymmetry between i and j is kept because
-// one conversion serves both.
-__device__ __forceinline__ long long f2fix(float v) {
-  const unsigned u = __float_as_uint(v);
-  const int e = (int)((u >> 23) & 0xffu);
-  const long long m = (long long)((u & 0x7fffffu) | 0x800000u);
-  const int sh = e - 118;  // v * 2^32 = m * 2^(e - 150 + 32)
-  long long mag;
-  if (sh >= 0) mag = m << min(sh, 39);
-  else if (sh > -25) mag = (m + (1LL << (-sh - 1))) >> (-sh);
-  else mag = 0;
-  return (u >> 31) ? -mag : mag;
-}
-
-// round(v * 2^S) as a 64-bit integer with integer operations only; values of
-// magnitude 2^(63-S) and above (and Inf/NaN) raise EB_FIXED and count as 0.
+// round(v * 2^S) to the nearest 64-bit integer: the scaling by a power of two
+// is exact and the conversion rounds to nearest.  Values of magnitude
+// 2^(63-S) and above (and Inf/NaN) raise EB_FIXED and count as 0.
 template <int S>
 __device__ __forceinline__ long long fixq(float v, unsigned& err) {
-  const unsigned u = __float_as_uint(v);
-  const int e = (int)((u >> 23) & 0xffu);
-  const long long m = (long long)((u & 0x7fffffu) | 0x800000u);
-  const int sh = e - 150 + S;
-  long long mag;
-  if (sh > 39) { err |= EB_FIXED; mag = 0; }
-  else if (sh >= 0) mag = m << sh;
-  else if (sh > -25) mag = (m + (1LL << (-sh - 1))) >> (-sh);
-  else mag = 0;
-  return (u >> 31) ? -mag : mag;
+  const float s = v * (float)(1ull << S);
+  if (!(fabsf(s) < 0x1p63f)) { err |= EB_FIXED; return 0; }
+  return __float2ll_rn(s);
 }
 
 // NONBONDED_FORCE.F90:173-232, FP32 force path.  Same structure as
 // k_nonbonded (slices of P = 32/T slots, T lanes per slot, dynamic units of
-// ROWS list rows).  The arithmetic is REAL*4 as in the reference, with
+// `rows` list rows).  The arithmetic is REAL*4 as in the reference, with
 // cheaper equivalents where only the force value (not a bit pattern) is
-// compared: minimum image by compare-and-select, r from rsqrt, the table row
-// and interpolation weight from a precomputed 1/bin, float-to-fixed on the
-// integer units.  Energies and virials are summed in FP32 over one unit, then
-// as 64-bit fixed point (2^-24) per lane and per block, and added to the
-// system's accumulators: integer sums do not depend on which warp took which
-// unit, so they are reproducible and the same alone or in a batch.
+// compared: minimum image as d - rint(d/L) L, r from rsqrt, the table row
+// and interpolation weight from a precomputed 1/bin, float-to-fixed by the
+// hardware conversion of the exactly scaled value.  Energies and virials are
+// summed in FP32 over kEnergyRows list rows, then as 64-bit fixed point
+// (2^-24) per lane and per block, and added to the system's accumulators:
+// integer sums depend neither on which warp took which unit nor on the rows
+// per unit, so they are reproducible and the same alone or in a batch.
 template <bool SMEM, int T, bool B>
 __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ const NBArgs<float> A0,
                                                           const NBArgs<float>* const* tab, const BlockMap bm) {
   constexpr int PS = 32 / T;
-  constexpr int ROWS = 8;
   const Blk bk = blk<B>(bm);
   __shared__ NBArgs<float> s_args;
   if (B) stage_args(&s_args, tab[bk.sys]);
@@ -763,14 +816,17 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
   const int lane = threadIdx.x & 31, grp = lane / T, q = lane % T;
   unsigned err = 0;
   const bool run = true;
-  const int U = (A.w_cap + ROWS - 1) / ROWS;
+  // a work unit is `rows` list rows of one slice (a multiple of kEnergyRows)
+  const int rows = A.rows;
+  const int U = (A.w_cap + rows - 1) / rows;
   const int nunits = A.nslices * U;
+  long long* la = lacc + threadIdx.x;
   auto unit = [&](int u) {
     const int g = u / U;
-    const int r0 = (u - g * U) * ROWS;
+    const int r0 = (u - g * U) * rows;
     const int w = min(A.slice_w[g], A.w_cap);
     if (r0 >= w) return;
-    const int r1 = min(w, r0 + ROWS);
+    const int r1 = min(w, r0 + rows);
     const int s = g * PS + grp;
     const bool valid = s < A.n;
     const int cnt = valid ? A.counts[s] : 0;
@@ -779,61 +835,71 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
     const int wi = __float_as_int(pi.w);
     const int ti = wi & 0xffff, li = wi >> 16;
     long long fi0 = 0, fi1 = 0, fi2 = 0;
-    float e[3] = {0.f, 0.f, 0.f}, vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    auto pair = [&](int t, const float4& pj) {
-      // minimum image d - rint(d/L) L (the pair is beyond the cutoff wherever
-      // this and ANINT could choose differently, |d| ~ L/2)
-      float d0 = pi.x - pj.x, d1 = pi.y - pj.y, d2 = pi.z - pj.z;
-      d0 = __fmaf_rn(-rintf(d0 * ix), bx, d0);
-      d1 = __fmaf_rn(-rintf(d1 * iy), by, d1);
-      d2 = __fmaf_rn(-rintf(d2 * iz), bz, d2);
-      const float r2 = __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, d0 * d0));
-      if (!(r2 < A.rcutsq)) return;
-      const int wj = __float_as_int(pj.w);
-      const int tj = wj & 0xffff, lj = wj >> 16;
-      const int4 pt = ptab[ti * A.ntype + tj];
-      if (!pt.w) { err |= EB_MISSING_TABLE; return; }
-      const float r = r2 * rsqrtf(r2);
-      const float ib = __int_as_float(pt.z);
-      const int ni = (int)(r * ib);
-      if (ni > pt.y) { err |= EB_TABLE_RANGE; return; }
-      const int row = pt.x + ni;
-      const float alpha = (r - tx[row]) * ib;
-      const float2 a0 = tfp[row], a1 = tfp[row + 1];
-      const float fij = __fmaf_rn(a1.x - a0.x, alpha, a0.x);
-      const float vij = __fmaf_rn(a1.y - a0.y, alpha, a0.y);
-      // V_NB(1) atom pairs, V_NB(2) bead-bead, V_NB(3) pairs with a virtual site
-      const bool lab3 = li == 3 || lj == 3;
-      e[0] += li == 1 ? vij : 0.f;
-      e[1] += (li == 2 && lj == 2) ? vij : 0.f;
-      e[2] += (li != 1 && lab3) ? vij : 0.f;
-      // |f component| <= |fij| r (to rounding): one test keeps every
-      // component in range
-      if (!(fabsf(fij) * r < 0.99f * kFixMax)) { err |= EB_FIXED; return; }
-      const float fx = fij * d0, fy = fij * d1, fz = fij * d2;
-      // round(f * 2^32): the scaling is exact, the conversion rounds to nearest
-      const long long qx = __float2ll_rn(fx * kFixScale), qy = __float2ll_rn(fy * kFixScale),
-                      qz = __float2ll_rn(fz * kFixScale);
-      fi0 += qx; fi1 += qy; fi2 += qz;
-      atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 0], (unsigned long long)(-qx));
-      atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 1], (unsigned long long)(-qy));
-      atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 2], (unsigned long long)(-qz));
-      vir[0] = __fmaf_rn(fx, d0, vir[0]);
-      vir[1] = __fmaf_rn(fy, d1, vir[1]);
-      vir[2] = __fmaf_rn(fz, d2, vir[2]);
-      vir[3] = __fmaf_rn(fy, d0, vir[3]);
-      vir[4] = __fmaf_rn(fz, d0, vir[4]);
-      vir[5] = __fmaf_rn(fz, d1, vir[5]);
-    };
-    for (int it = r0; it < r1; it += 2) {
-      const bool v0 = it * T + q < cnt;
-      const bool v1 = it + 1 < r1 && (it + 1) * T + q < cnt;
-      const int t0 = v0 ? ent[it * 32] : 0;
-      const int t1 = v1 ? ent[(it + 1) * 32] : 0;
-      const float4 p0 = pos[t0];
-      const float4 p1 = pos[t1];
-      if (v0) pair(t0, p0);
-      if (v1) pair(t1, p1);
+    // energies and virials: FP32 over kEnergyRows rows (aligned to multiples of
+    // kEnergyRows), then fixed point, so that their sums depend neither on the
+    // rows per unit nor on which warp took which unit
+    for (int b0 = r0; b0 < r1; b0 += kEnergyRows) {
+      const int b1 = min(r1, b0 + kEnergyRows);
+      float e[3] = {0.f, 0.f, 0.f}, vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      auto pair = [&](int t, const float4& pj) {
+        // minimum image d - rint(d/L) L (the pair is beyond the cutoff wherever
+        // this and ANINT could choose differently, |d| ~ L/2)
+        float d0 = pi.x - pj.x, d1 = pi.y - pj.y, d2 = pi.z - pj.z;
+        d0 = __fmaf_rn(-rintf(d0 * ix), bx, d0);
+        d1 = __fmaf_rn(-rintf(d1 * iy), by, d1);
+        d2 = __fmaf_rn(-rintf(d2 * iz), bz, d2);
+        const float r2 = __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, d0 * d0));
+        if (!(r2 < A.rcutsq)) return;
+        const int wj = __float_as_int(pj.w);
+        const int tj = wj & 0xffff, lj = wj >> 16;
+        const int4 pt = ptab[ti * A.ntype + tj];
+        if (!pt.w) { err |= EB_MISSING_TABLE; return; }
+        const float r = r2 * rsqrtf(r2);
+        const float ib = __int_as_float(pt.z);
+        const int ni = (int)(r * ib);
+        if (ni > pt.y) { err |= EB_TABLE_RANGE; return; }
+        const int row = pt.x + ni;
+        const float alpha = (r - tx[row]) * ib;
+        const float2 a0 = tfp[row], a1 = tfp[row + 1];
+        const float fij = __fmaf_rn(a1.x - a0.x, alpha, a0.x);
+        const float vij = __fmaf_rn(a1.y - a0.y, alpha, a0.y);
+        // V_NB(1) atom pairs, V_NB(2) bead-bead, V_NB(3) pairs with a virtual site
+        const bool lab3 = li == 3 || lj == 3;
+        e[0] += li == 1 ? vij : 0.f;
+        e[1] += (li == 2 && lj == 2) ? vij : 0.f;
+        e[2] += (li != 1 && lab3) ? vij : 0.f;
+        // |f component| <= |fij| r (to rounding): one test keeps every
+        // component in range
+        if (!(fabsf(fij) * r < 0.99f * kFixMax)) { err |= EB_FIXED; return; }
+        const float fx = fij * d0, fy = fij * d1, fz = fij * d2;
+        // round(f * 2^32): the scaling is exact, the conversion rounds to nearest
+        const long long qx = __float2ll_rn(fx * kFixScale), qy = __float2ll_rn(fy * kFixScale),
+                        qz = __float2ll_rn(fz * kFixScale);
+        fi0 += qx; fi1 += qy; fi2 += qz;
+        atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 0], (unsigned long long)(-qx));
+        atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 1], (unsigned long long)(-qy));
+        atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 2], (unsigned long long)(-qz));
+        vir[0] = __fmaf_rn(fx, d0, vir[0]);
+        vir[1] = __fmaf_rn(fy, d1, vir[1]);
+        vir[2] = __fmaf_rn(fz, d2, vir[2]);
+        vir[3] = __fmaf_rn(fy, d0, vir[3]);
+        vir[4] = __fmaf_rn(fz, d0, vir[4]);
+        vir[5] = __fmaf_rn(fz, d1, vir[5]);
+      };
+      for (int it = b0; it < b1; it += 2) {
+        const bool v0 = it * T + q < cnt;
+        const bool v1 = it + 1 < b1 && (it + 1) * T + q < cnt;
+        const int t0 = v0 ? ent[it * 32] : 0;
+        const int t1 = v1 ? ent[(it + 1) * 32] : 0;
+        const float4 p0 = pos[t0];
+        const float4 p1 = pos[t1];
+        if (v0) pair(t0, p0);
+        if (v1) pair(t1, p1);
+      }
+#pragma unroll
+      for (int k = 0; k < 3; ++k) la[k * blockDim.x] += fixq<24>(e[k], err);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) la[(3 + k) * blockDim.x] += fixq<24>(vir[k], err);
     }
 #pragma unroll
     for (int o = T / 2; o > 0; o >>= 1) {
@@ -846,11 +912,6 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
       atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)s + 1], (unsigned long long)fi1);
       atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)s + 2], (unsigned long long)fi2);
     }
-    long long* la = lacc + threadIdx.x;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) la[k * blockDim.x] += fixq<24>(e[k], err);
-#pragma unroll
-    for (int k = 0; k < 6; ++k) la[(3 + k) * blockDim.x] += fixq<24>(vir[k], err);
   };
   if (A.chunk > 0) {
     // chunks of consecutive units (neighbouring slices) per block, handed out

@@ -73,7 +73,8 @@ class IbgDesc(ctypes.Structure):
 
 
 class Tuning(ctypes.Structure):
-    _fields_ = [("nb_tables_smem", ctypes.c_int), ("nb_blocks_per_sm", ctypes.c_int), ("nb_chunk", ctypes.c_int)]
+    _fields_ = [("nb_tables_smem", ctypes.c_int), ("nb_blocks_per_sm", ctypes.c_int), ("nb_chunk", ctypes.c_int),
+                ("nb_rows", ctypes.c_int)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -171,7 +172,8 @@ def lib(build_if_missing: bool = True):
         "ibg_batch_destroy": (None, [vp]),
         "ibg_get_tuning": (ctypes.c_int, [vp, ctypes.POINTER(Tuning)]),
         "ibg_set_tuning": (ctypes.c_int, [vp, ctypes.POINTER(Tuning)]),
-        "ibg_autotune": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(Tuning), dp, ctypes.c_int]),
+        "ibg_autotune": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(Tuning), ctypes.POINTER(Tuning), dp,
+                                         ctypes.c_int]),
         "ibg_device_bytes": (ctypes.c_longlong, [vp]),
         "ibg_estimate_bytes": (ctypes.c_longlong, [vp, ctypes.c_int, fp]),
         "ibg_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
@@ -340,6 +342,15 @@ class System:
             self._check(rc)
         return lst[:n], nn[:n]
 
+    def neighbour_counts(self, which: int) -> np.ndarray:
+        """NNEBS of list `which` (0 atoms, 1 beads) alone."""
+        n = len(self.setup.array("ATOM")) if which == 0 else len(self.setup.array("BEAD"))
+        nn = np.zeros(max(n, 1), np.int32)
+        rc = lib().ibg_get_neighbour_list(self._h, which, None, 0, _ip(nn))
+        if rc < 0:
+            self._check(rc)
+        return nn[:n]
+
     def exclusions(self):
         n = self.nitems
         c = np.zeros(n, np.int32)
@@ -348,35 +359,34 @@ class System:
         return c, t
 
     def timing(self) -> dict:
-        ms = (ctypes.c_double * 8)()
+        ms = (ctypes.c_double * 9)()
         n = ctypes.c_longlong()
-        lib().ibg_get_timing(self._h, ms, 8, ctypes.byref(n))
+        lib().ibg_get_timing(self._h, ms, 9, ctypes.byref(n))
         return {"list_ms": ms[0], "nonbonded_ms": ms[1], "bonded_ms": ms[2], "integrate_ms": ms[3],
                 "other_ms": ms[4], "run_ms": ms[5], "nonbonded_launches": int(ms[6]), "list_growths": int(ms[7]),
-                "launches": n.value}
+                "nonbonded_bead_launches": int(ms[8]), "launches": n.value}
 
     def tuning(self) -> dict:
         t = Tuning()
         self._check(lib().ibg_get_tuning(self._h, ctypes.byref(t)))
         return t.as_dict()
 
-    def set_tuning(self, nb_tables_smem: int = 0, nb_blocks_per_sm: int = 0, nb_chunk: int = 0):
-        t = Tuning(nb_tables_smem, nb_blocks_per_sm, nb_chunk)
+    def set_tuning(self, nb_tables_smem: int = 0, nb_blocks_per_sm: int = 0, nb_chunk: int = 0, nb_rows: int = 0):
+        t = Tuning(nb_tables_smem, nb_blocks_per_sm, nb_chunk, nb_rows)
         self._check(lib().ibg_set_tuning(self._h, ctypes.byref(t)))
 
     def autotune(self, reps: int = 20):
         """Time the candidate tunings of the nonbonded kernel and keep the
         fastest; returns (best, [(candidate, us per launch)])."""
         best = Tuning()
-        us = (ctypes.c_double * 16)()
-        n = lib().ibg_autotune(self._h, int(reps), ctypes.byref(best), us, 16)
+        cap = 64
+        cand = (Tuning * cap)()
+        us = (ctypes.c_double * cap)()
+        n = lib().ibg_autotune(self._h, int(reps), ctypes.byref(best), cand, us, cap)
         if n < 0:
             self._check(n)
-        if self.precision == IBG_PREC_FP32_FIXED:
-            cands = [(sm, per, ch) for ch in (0, 48, 96) for sm in (0, 1) for per in (0, 3)]
-        else:
-            cands = [(sm, per, 0) for sm in (0, 1) for per in (0, 3, 2)]
-        return best.as_dict(), [(c, us[k]) for k, c in enumerate(cands[:n])]
+        return best.as_dict(), [((c.nb_tables_smem, c.nb_blocks_per_sm, c.nb_chunk, c.nb_rows), us[k])
+                                for k, c in enumerate(cand[:min(n, cap)])]
 
     def set_timing(self, on: bool):
         self._check(lib().ibg_set_timing(self._h, 1 if on else 0))
@@ -492,6 +502,27 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+def tune_steps(make_system, candidates, steps: int = 100, l2_flush: int = 0):
+    """Pick one system's launch tuning by whole steps: for each candidate
+    tuning (a dict for System.set_tuning), make the system (make_system()
+    returns a fresh System after set_state), apply it, run 10 + `steps` steps
+    (with the L2 flushed before each, if l2_flush > 0) and keep the fastest.
+    The list build, positions and bonded kernels of a step leave the L2 in the
+    state the nonbonded kernel meets, which timing its launches alone does not
+    reproduce.  Returns (best tuning, [(tuning, us per step)])."""
+    times = []
+    for tun in candidates:
+        g = make_system()
+        g.set_tuning(**tun)
+        if l2_flush:
+            g.set_l2_flush(l2_flush)
+        g.run(1, 10)
+        g.run(11, steps)
+        times.append((tun, 1000.0 * g.timing()["run_ms"] / steps))
+        g.close()
+    return min(times, key=lambda t: t[1])[0], times
 
 
 def tune_batch(make_systems, candidates, steps: int = 100):

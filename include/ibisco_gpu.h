@@ -187,8 +187,9 @@ int ibg_get_exclusions(ibg_ctx* c, int* connections, int* connected_to);
    With timing on (ibg_set_timing(c,1): direct launches, no graph replay),
    stage_ms[0..4] accumulate the time of the list build, nonbonded, bonded,
    integration/reduction and remaining kernels since ibg_set_timing, and
-   stage_ms[6] counts the nonbonded launches; stage_ms[7] counts the growths of
-   the Verlet-list storage.  launches = kernels enqueued by this context so
+   stage_ms[6] counts the nonbonded launches, stage_ms[8] those of them that
+   ran the bead list; stage_ms[7] counts the growths of the Verlet-list
+   storage (nstage <= 9).  launches = kernels enqueued by this context so
    far. */
 int ibg_set_timing(ibg_ctx* c, int on);
 int ibg_get_timing(ibg_ctx* c, double* stage_ms, int nstage, long long* launches);
@@ -208,22 +209,26 @@ int ibg_set_list_rows(ibg_ctx* c, int rows);
    SM (0: all that fit); nb_chunk (FP32 path): a block takes chunks of this
    many consecutive work units (neighbouring slices) and shares them among its
    warps, so they gather from one region of space (0: every warp takes units
-   alone).  Forces and trajectories do not depend on the tuning
+   alone); nb_rows: list rows per work unit, 8 or 16 (0: 16).  Forces and
+   trajectories do not depend on the tuning
    (integer force sums); on the FP32 path nonbonded energies and virials are
    summed per work unit before their exact fixed-point sum, so they do not
    depend on it either.  Set it before a batch is made of the context.
    ibg_autotune: times each candidate tuning on the context's current lists
-   (reps launches each, CUDA events), keeps the fastest, writes it to best and
-   the microseconds per launch of candidate k to us[k] (k < ncand); returns the
-   number of candidates.  It leaves the system's state unchanged. */
+   (reps launches each, CUDA events; with an L2 flush set by ibg_set_l2_flush,
+   each launch starts from a flushed L2, as a timed step does), keeps the
+   fastest, writes it to best, and candidate k and its microseconds per launch
+   to cand[k] and us[k] (k < ncand; either may be NULL); returns the number of
+   candidates.  It leaves the system's state unchanged. */
 typedef struct ibg_tuning {
   int nb_tables_smem;
   int nb_blocks_per_sm;
   int nb_chunk;
+  int nb_rows;
 } ibg_tuning;
 int ibg_get_tuning(const ibg_ctx* c, ibg_tuning* t);
 int ibg_set_tuning(ibg_ctx* c, const ibg_tuning* t);
-int ibg_autotune(ibg_ctx* c, int reps, ibg_tuning* best, double* us, int ncand);
+int ibg_autotune(ibg_ctx* c, int reps, ibg_tuning* best, ibg_tuning* cand, double* us, int ncand);
 /* Device memory a context holds (bytes), and an estimate made before creating
    one from its descriptor and box; the estimate includes the Verlet-list
    storage the first list build will need, with margin.  A serving loop admits

@@ -54,6 +54,8 @@ def sysdir(tmp_path_factory):
         "mix_npt": lambda: synth.feature_mix(seed=9, ensemble="NPT"),
         "mix_nve": lambda: synth.feature_mix(seed=10, ensemble="NVE"),
         "hybrid": lambda: synth.hybrid_melt(n_atomistic=32, n_cg=32, nmono=20, seed=13, nsteps=100),
+        # 3x3x3 cells of ~220 particles: ~3,100 list candidates per cell
+        "dense": lambda: synth.lj_fluid(n=6000, rho=45.0, seed=14, nsteps=10, dmin=0.12),
     }
 
     def get(name):

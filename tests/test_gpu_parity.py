@@ -52,6 +52,22 @@ def test_neighbour_lists_match_reference_order(sysdir, name):
         np.testing.assert_array_equal(lg, lo)
 
 
+@pytest.mark.parametrize("prec", [0, 1], ids=["fp32", "fp64"])
+@pytest.mark.parametrize("name", ["melt", "dense"])
+def test_neighbour_lists_staged_and_unstaged_cells(sysdir, name, prec):
+    """The list build stages a cell's candidates in shared memory when they
+    fit (2,304 in FP32, 1,152 in FP64) and reads them from global memory
+    otherwise; the dense fluid takes the second way on both paths.  Each
+    path's lists equal the oracle's at its own precision."""
+    d = sysdir(name)
+    _, g = make(d, native.IBG_PREC_FP32_FIXED if prec == 0 else native.IBG_PREC_FP64_PLAIN)
+    o = oracle_init(d, prec)
+    lg, ng = g.neighbour_list(0)
+    lo, no = o.neighbour_list(0, prec)
+    np.testing.assert_array_equal(ng, no)
+    np.testing.assert_array_equal(lg, lo)
+
+
 @pytest.mark.parametrize("name", ["mix4", "mix5_mts"])
 def test_exclusions_on_device(sysdir, name):
     d = sysdir(name)
@@ -224,7 +240,7 @@ def test_tuning_changes_no_trajectory(sysdir):
     assert len(cands) >= 2 and all(us > 0 for _, us in cands)
     assert a.tuning() == best
     c.set_tuning(nb_tables_smem=1 - best["nb_tables_smem"], nb_blocks_per_sm=2,
-                 nb_chunk=16 if best["nb_chunk"] == 0 else 0)
+                 nb_chunk=16 if best["nb_chunk"] == 0 else 0, nb_rows=8 if best["nb_rows"] == 16 else 16)
     oa, ob, oc = a.run(1, 20, observe=True), b.run(1, 20, observe=True), c.run(1, 20, observe=True)
     sa, sb, sc = a.state64(), b.state64(), c.state64()
     for k in ("sxyz", "vxyz", "fxyz"):
