@@ -58,9 +58,12 @@ WORKLOADS = {
     "fluid4k": "single-type LJ fluid: 4,000 beads, rho 8/nm^3, rc 1.2 nm, list 1.4 nm every 10 steps, NVE, dt 10 fs",
     "melt2m": "CG melt: 10,000 chains x 200 beads (2,000,000), 4 types, bond/angle tables, 10 LJ tables "
               "rc 1.4 nm, list 1.6 nm every 10 steps, NVT 300 K, dt 10 fs",
-    "hybrid": "hybrid melt: 200 atomistic chains x 20 monomers x 12 atoms (48,000) with a centre-of-mass "
-              "virtual site per monomer (4,000) and 200 CG chains x 20 beads (4,000); atom tables rc 1.0 nm, "
-              "bead/site tables rc 1.4 nm, MTS 9 (CG nonbonded on 3 of 12 steps), NVT 300 K, dt 1 fs",
+    "hybrid3a": "hybrid melt as specified: 200 atomistic chains x 20 monomers x 12 atoms (48,000) with a "
+                "centre-of-mass virtual site per monomer (4,000); atom tables rc 1.0 nm, site tables rc 1.4 nm "
+                "(no pair reaches them: sites pair with neither atoms nor sites), MTS 9, NVT 300 K, dt 1 fs",
+    "hybrid3b": "hybrid melt with a CG half: 100 atomistic chains x 20 monomers x 12 atoms (24,000) with a "
+                "centre-of-mass virtual site per monomer (2,000) and 100 CG chains x 20 beads (2,000); atom tables "
+                "rc 1.0 nm, bead/site tables rc 1.4 nm, MTS 9 (CG nonbonded on 3 of 12 steps), NVT 300 K, dt 1 fs",
 }
 
 
@@ -73,8 +76,10 @@ def make_workload(name: str, directory: str):
         spec = synth.lj_fluid(n=4000, seed=1)
     elif name == "melt2m":
         spec = synth.cg_melt()
-    elif name == "hybrid":
-        spec = synth.hybrid_melt(n_atomistic=200, n_cg=200)
+    elif name == "hybrid3a":
+        spec = synth.hybrid_melt(n_atomistic=200, n_cg=0)
+    elif name == "hybrid3b":
+        spec = synth.hybrid_melt(n_atomistic=100, n_cg=100)
     else:
         raise SystemExit(f"unknown workload {name}")
     synth.write_system(spec, directory)

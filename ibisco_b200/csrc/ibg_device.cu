@@ -158,6 +158,7 @@ struct ibg_ctx {
   float *tb_bin = nullptr, *ta_bin = nullptr, *tt_bin = nullptr, *to_bin = nullptr;
   DevList L[2];
   Scalars* sc = nullptr;
+  Scalars* hsc = nullptr;    // pinned host copy of *sc, read back once per run
   SysArgs<float> af;
   SysArgs<double> ad;
   void* dargs = nullptr;  // device copy of af or ad
@@ -686,18 +687,27 @@ void enqueue(ibg_ctx* c, unsigned v) {
 
 // The system runs steps step_before+1 .. last; observables of step k go to
 // ring slot k - base.
-void set_step_counter(ibg_ctx* c, int step_before, int base, int last) {
-  const int skip_stop[3] = {0, last, step_before >= last ? 1 : 0};  // skip, stop_at, done
-  CK(cudaMemcpyAsync(&c->sc->step, &step_before, sizeof(int), cudaMemcpyHostToDevice, c->st));
-  CK(cudaMemcpyAsync(&c->sc->ring_base, &base, sizeof(int), cudaMemcpyHostToDevice, c->st));
-  CK(cudaMemcpyAsync(&c->sc->skip, skip_stop, sizeof(skip_stop), cudaMemcpyHostToDevice, c->st));
-  CK(cudaStreamSynchronize(c->st));
+// Step counter, ring base and step limit for the next run, in stream order
+// on the context's stream (sync: also wait for it, for launches on another
+// stream).
+void set_step_counter(ibg_ctx* c, int step_before, int base, int last, bool sync) {
+  k_set_counter<<<1, 1, 0, c->st>>>(c->sc, step_before, base, last);
+  CK(cudaGetLastError());
+  ++c->launches;
+  if (sync) CK(cudaStreamSynchronize(c->st));
 }
+
+int check_bits(ibg_ctx* c, unsigned bits);
 
 int check_device(ibg_ctx* c) {
   unsigned bits = 0;
   CK(cudaMemcpyAsync(&bits, &c->sc->err, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
+  return check_bits(c, bits);
+}
+
+// Error bits read from the device: clear them there and report.
+int check_bits(ibg_ctx* c, unsigned bits) {
   if (bits) {
     unsigned zero = 0;
     CK(cudaMemcpy(&c->sc->err, &zero, sizeof(unsigned), cudaMemcpyHostToDevice));
@@ -1133,6 +1143,8 @@ int ibg_create(const ibg_desc* d, int precision, ibg_ctx** out) {
     // grids and partial sums
     for (auto& L : c->L) {
       if (!L.present) continue;
+      // the list build tags a staged candidate's slot with its cell run in bits 27..30
+      if (L.n > kSlotMask) return fail(nullptr, IBG_E_CAPACITY, "");
       if (precision == IBG_PREC_FP32_FIXED) nb_configure<float>(c.get(), L);
       else nb_configure<double>(c.get(), L);
     }
@@ -1150,6 +1162,7 @@ int ibg_create(const ibg_desc* d, int precision, ibg_ctx** out) {
     c->p_mv = dalloc<double>(18 * (size_t)c->g_mv, o);
     c->p_mom = dalloc<double>(3 * (size_t)c->g_mv, o);
     c->sc = dalloc<Scalars>(1, o);
+    CK(cudaHostAlloc(&c->hsc, sizeof(Scalars), cudaHostAllocDefault));
     c->ring_cap = 1;
     c->ring = nullptr;
     refresh_args(c.get());
@@ -1257,7 +1270,7 @@ static int run_steps(ibg_ctx* c, int first, int nsteps, ibg_obs* per_step, bool 
     int done = 0;
     float run_ms_total = 0.f;
     for (int attempt = 0; attempt < 8 && done < nsteps; ++attempt) {
-      set_step_counter(c, first + done - 1, first, first + nsteps - 1);
+      set_step_counter(c, first + done - 1, first, first + nsteps - 1, false);
       if (c->flush_bytes) {
         if (!c->flush_buf) CK(cudaMalloc(&c->flush_buf, c->flush_bytes));
         while ((int)c->step_ev.size() < 2 * nsteps) {
@@ -1302,6 +1315,8 @@ static int run_steps(ibg_ctx* c, int first, int nsteps, ibg_obs* per_step, bool 
         if (flush) CK(cudaEventRecord(c->step_ev[2 * k + 1], c->st));
       }
       CK(cudaEventRecord(c->run_ev[1], c->st));
+      // one read-back per run: step, abort and error flags, observables
+      CK(cudaMemcpyAsync(c->hsc, c->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, c->st));
       collect_marks(c);
       CK(cudaStreamSynchronize(c->st));
       float ms = 0.f;
@@ -1315,10 +1330,8 @@ static int run_steps(ibg_ctx* c, int first, int nsteps, ibg_obs* per_step, bool 
         }
       }
       run_ms_total += ms;
-      if (grow_lists(c)) {
-        int st = 0;  // the step that aborted did not complete
-        CK(cudaMemcpy(&st, &c->sc->step, sizeof(int), cudaMemcpyDeviceToHost));
-        done = st - first;
+      if (c->hsc->abort && grow_lists(c)) {
+        done = c->hsc->step - first;  // the step that aborted did not complete
         continue;
       }
       done = nsteps;
@@ -1326,7 +1339,7 @@ static int run_steps(ibg_ctx* c, int first, int nsteps, ibg_obs* per_step, bool 
     c->stage_ms[5] = run_ms_total;
     c->step_now = first + done - 1;
     if (done < nsteps) return fail(c, IBG_E_CAPACITY, "neighbour-list storage could not be sized");
-    int rc = check_device(c);
+    int rc = check_bits(c, c->hsc->err);
     if (rc) return rc;
     if (per_step) {
       std::vector<ObsD> h(nsteps);
@@ -1342,22 +1355,14 @@ static int run_steps(ibg_ctx* c, int first, int nsteps, ibg_obs* per_step, bool 
 int ibg_step(ibg_ctx* c, int step, ibg_obs* out) {
   int rc = run_steps(c, step, 1, nullptr, false, true);
   if (rc) return rc;
-  try {
-    read_obs(c, out);
-  } catch (CudaError& e) {
-    return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
-  }
+  if (out) obs_to_c(c->hsc->obs, out);  // read back by run_steps
   return IBG_OK;
 }
 
 int ibg_forces(ibg_ctx* c, int step, ibg_obs* out) {
   int rc = run_steps(c, step, 1, nullptr, true, false);
   if (rc) return rc;
-  try {
-    read_obs(c, out);
-  } catch (CudaError& e) {
-    return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
-  }
+  if (out) obs_to_c(c->hsc->obs, out);
   return IBG_OK;
 }
 
@@ -1523,6 +1528,7 @@ void ibg_destroy(ibg_ctx* c) {
     if (e) cudaEventDestroy(e);
   for (auto* e : c->step_ev) cudaEventDestroy(e);
   if (c->flush_buf) cudaFree(c->flush_buf);
+  if (c->hsc) cudaFreeHost(c->hsc);
   for (auto* e : c->fork_ev)
     if (e) cudaEventDestroy(e);
   if (c->st2) cudaStreamDestroy(c->st2);
@@ -1851,7 +1857,7 @@ int ibg_batch_run(ibg_batch* b, int nsteps, const int* last_step, ibg_obs* last_
       int need = 0;
       for (size_t s = 0; s < n; ++s) need = std::max(need, last[s] - from[s]);
       if (need == 0) break;
-      for (size_t s = 0; s < n; ++s) set_step_counter(b->sys[s], from[s], INT_MAX, last[s]);
+      for (size_t s = 0; s < n; ++s) set_step_counter(b->sys[s], from[s], INT_MAX, last[s], true);
       CK(cudaEventRecord(b->run_ev[0], b->st));
       for (int k = 0; k < need; ++k) {
         const unsigned v = batch_variant(b, from, last, k);

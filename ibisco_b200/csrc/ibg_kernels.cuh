@@ -406,6 +406,9 @@ __constant__ int kStencil[13][3] = {{1, 0, 0}, {1, 1, 0},  {0, 1, 0},  {-1, 1, 0
 
 // Candidates one block stages (positions and slots): 2,304 in FP32 (about 160
 // particles per cell), 1,152 in FP64, within 48 KB of static shared memory.
+// A staged slot carries its run (0..13) in bits 27..30, so lists hold fewer
+// than 2^27 particles.
+constexpr int kSlotMask = (1 << 27) - 1;
 template <typename R>
 struct ListStage {
   static constexpr int cap = sizeof(R) == 4 ? 2304 : 1152;
@@ -425,8 +428,9 @@ __global__ void __launch_bounds__(256, 4) k_list_build(__grid_constant__ const L
   if (sc->skip || !(always || sc->rebuild)) return;
   constexpr int P = 32 / T;
   __shared__ PT s_pos[kCap];
-  __shared__ int s_slot[kCap];
+  __shared__ int s_slot[kCap];          // slot | run << 27
   __shared__ int s_hi[14], s_pre[15];  // run u: slots s_hi[u] down, staged from s_pre[u]
+  __shared__ R s_sh[14][3];            // run u: periodic image shift, 0 or +-L per axis
   __shared__ int s_exs[kWarps][20];    // each warp's particle's exclusions, as slots of this list
   __shared__ int s_cell;
   const int nx = sc->ncell[L.which][0], ny = sc->ncell[L.which][1], nz = sc->ncell[L.which][2];
@@ -451,14 +455,20 @@ __global__ void __launch_bounds__(256, 4) k_list_build(__grid_constant__ const L
       // run 0: the own cell from its last slot down; runs 1..13: the stencil
       // cells, each from its last slot down; exclusive prefix of the lengths
       int hi = 0, len = 0;
+      int w[3] = {0, 0, 0};  // the neighbour cell wraps past the box's +L/2 (1) or -L/2 (-1) face
       if (lane == 0) {
         hi = last - 1;
         len = last - first;
       } else if (lane < 14) {
-        const int ix = c0 / (nz * ny), iy = (c0 / nz) % ny, iz = c0 % nz;
-        const int jx = (ix + kStencil[lane - 1][0] + nx) % nx, jy = (iy + kStencil[lane - 1][1] + ny) % ny,
-                  jz = (iz + kStencil[lane - 1][2] + nz) % nz;
-        const int c = jx * nz * ny + jy * nz + jz;
+        const int ic[3] = {c0 / (nz * ny), (c0 / nz) % ny, c0 % nz}, nc[3] = {nx, ny, nz};
+        int jc[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const int j = ic[q] + kStencil[lane - 1][q];
+          w[q] = j >= nc[q] ? 1 : (j < 0 ? -1 : 0);
+          jc[q] = j - w[q] * nc[q];
+        }
+        const int c = jc[0] * nz * ny + jc[1] * nz + jc[2];
         const int lo = L.cell_start[c];
         hi = L.cell_start[c + 1] - 1;
         len = hi - lo + 1;
@@ -472,13 +482,15 @@ __global__ void __launch_bounds__(256, 4) k_list_build(__grid_constant__ const L
       if (lane < 14) {
         s_hi[lane] = hi;
         s_pre[lane] = incl - len;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) s_sh[lane][q] = w[q] > 0 ? b[q] : (w[q] < 0 ? -b[q] : (R)0);
       }
       if (lane == 13) s_pre[14] = incl;
     }
     __syncthreads();
     const int total = s_pre[14];
-    // run of staged index v: the largest u with s_pre[u] <= v (that run is
-    // not empty)
+    // staged index v -> slot | run << 27, the run being the largest u with
+    // s_pre[u] <= v (that run is not empty)
     auto slot_at = [&](int v) {
       int lo = 0, hi = 13;
       while (lo < hi) {
@@ -486,14 +498,14 @@ __global__ void __launch_bounds__(256, 4) k_list_build(__grid_constant__ const L
         if (s_pre[mid] <= v) lo = mid;
         else hi = mid - 1;
       }
-      return s_hi[lo] - (v - s_pre[lo]);
+      return (s_hi[lo] - (v - s_pre[lo])) | (lo << 27);
     };
     const bool staged = total <= kCap;
     if (staged) {
       for (int v = threadIdx.x; v < total; v += blockDim.x) {
-        const int t = slot_at(v);
-        s_slot[v] = t;
-        s_pos[v] = pos[t];
+        const int tu = slot_at(v);
+        s_slot[v] = tu;
+        s_pos[v] = pos[tu & kSlotMask];
       }
     }
     __syncthreads();
@@ -509,37 +521,43 @@ __global__ void __launch_bounds__(256, 4) k_list_build(__grid_constant__ const L
         exs[lane] = (gs & 1) == L.which ? gs >> 1 : -1;
       }
       __syncwarp();
+      // the first four exclusions in registers (a bead of a chain has four
+      // 1-2 and 1-3 partners), the rest from shared memory
+      const int e0 = ne > 0 ? exs[0] : -1, e1 = ne > 1 ? exs[1] : -1, e2 = ne > 2 ? exs[2] : -1,
+                e3 = ne > 3 ? exs[3] : -1;
       const bool i_vs = L.hybrid && i >= L.natoms;
       int cnt = 0;
-      // minimum image by compare and select.  It equals d - ANINT(d/L)*L for
-      // |d| < L/2 (ANINT = 0) and for |d| > L/2 away from the rounding of d/L
-      // to 1/2 (both subtract L the same way); where they can differ, |d| is
-      // within rounding of L/2, beyond RLIST <= L/3 either way.  So the
-      // accepted set is bit for bit the reference's.
+      // minimum image: d - s with s the run's image shift.  For a pair inside
+      // RLIST <= L/3 that shift is the nearest image, so s = ANINT(d/L)*L
+      // exactly and d - s is the reference's d - ANINT(d/L)*L bit for bit;
+      // with any other shift the distance is above RLIST either way.
       for (int v0 = last - s; v0 < total; v0 += 32) {
         const int v = v0 + lane;
         bool ok = false;
         int t = -1;
         if (v < total) {
           PT pj;
+          int tu;
           if (staged) {
-            t = s_slot[v];
+            tu = s_slot[v];
             pj = s_pos[v];
           } else {
-            t = slot_at(v);
-            pj = pos[t];
+            tu = slot_at(v);
+            pj = pos[tu & kSlotMask];
           }
+          t = tu & kSlotMask;
+          const R* sh = s_sh[tu >> 27];
           R d0 = pi.x - pj.x, d1 = pi.y - pj.y, d2 = pi.z - pj.z;
-          d0 = d0 > b2[0] ? d0 - b[0] : (d0 < -b2[0] ? d0 + b[0] : d0);
-          d1 = d1 > b2[1] ? d1 - b[1] : (d1 < -b2[1] ? d1 + b[1] : d1);
-          d2 = d2 > b2[2] ? d2 - b[2] : (d2 < -b2[2] ? d2 + b[2] : d2);
+          d0 = d0 - sh[0];
+          d1 = d1 - sh[1];
+          d2 = d2 - sh[2];
           R r2 = d0 * d0;
           r2 = r2 + d1 * d1;
           r2 = r2 + d2 * d2;
-          if (r2 < rlsq) {
-            ok = !(i_vs && (Prec<R>::bits(pj.w) >> 16) == 3);
-            for (int e = 0; e < ne; ++e) ok &= exs[e] != t;
-          }
+          ok = r2 < rlsq && !(i_vs && (Prec<R>::bits(pj.w) >> 16) == 3) && t != e0 && t != e1 && t != e2 &&
+               t != e3;
+          if (ok && ne > 4)
+            for (int e = 4; e < ne; ++e) ok &= exs[e] != t;
         }
         const unsigned m = __ballot_sync(0xffffffffu, ok);
         if (ok) {
@@ -1616,6 +1634,15 @@ __global__ void k_finalize(__grid_constant__ const FinalArgs F0, const FinalArgs
     int slot = sc->step - sc->ring_base;
     if (slot >= 0 && slot < F.ring_cap) F.ring[slot] = o;
   }
+}
+
+// Step counter, observable ring base and step limit of the next run.
+__global__ void k_set_counter(Scalars* sc, int step_before, int ring_base, int last) {
+  sc->step = step_before;
+  sc->ring_base = ring_base;
+  sc->skip = 0;
+  sc->stop_at = last;
+  sc->done = step_before >= last ? 1 : 0;
 }
 
 // Initial temperatures and Berendsen factors (main.F90:174-195).
