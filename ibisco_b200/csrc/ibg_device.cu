@@ -1154,7 +1154,7 @@ int ibg_create(const ibg_desc* d, int precision, ibg_ctx** out) {
       c->g_list[w] = grid_for(c.get(), L.n);
       c->g_build[w] = std::max(1, std::min((L.n + 15) / 16, c->nsm * 4));  // blocks take cells
     }
-    c->g_dist = grid_for(c.get(), std::max(1, c->nvirta));
+    c->g_dist = grid_for(c.get(), 16LL * std::max(1, c->nvirta));  // 16 lanes per site
     c->g_b = grid_for(c.get(), (long long)c->nb + c->na + c->nt + c->no, 4);
     c->g_mv = grid_for(c.get(), NA, 4);
     c->g_pos = grid_for(c.get(), N, 8);

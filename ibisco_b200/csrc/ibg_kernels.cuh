@@ -144,43 +144,63 @@ __global__ void k_positions(__grid_constant__ const PosArgs a0, const PosArgs* c
       sc->miu = 1.0;
     }
   }
-  const int n = a.natoms + a.nvirta;
   R b[3], bi[3], b2[3];
   box_of<R>(sc, b, bi, b2);
-  for (int i = bk.b * blockDim.x + threadIdx.x; i < n; i += bk.g * blockDim.x) {
-    R s[3];
-    if (i < a.natoms) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) s[c] = (R)a.S[3 * (size_t)i + c];
-    } else {
-      int v = i - a.natoms;
-      int ctr = a.vcenter[v];
-      if (ctr >= 0) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) s[c] = (R)a.S[3 * (size_t)ctr + c];
-      } else {
-        R acc[3] = {0, 0, 0};
-        int nm = a.vnum[v];
-        for (int k = 0; k < nm; ++k) {
-          int m = a.vmem[v * 15 + k];
-          R mm = (R)a.vmass[v * 15 + k];
-#pragma unroll
-          for (int c = 0; c < 3; ++c) acc[c] = acc[c] + mm * (R)a.S[3 * (size_t)m + c];
-        }
-        R inv = (R)a.vinv[v];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) s[c] = acc[c] * inv;
-      }
-#pragma unroll
-      for (int c = 0; c < 3; ++c) a.Svs[3 * (size_t)v + c] = (double)s[c];
-    }
+  auto store = [&](int i, const R* s) {
     R r[3] = {s[0], s[1], s[2]};
     fold3<R>(r, b2);
-    int g = a.gslot[i];
+    const int g = a.gslot[i];
     PT p;
     p.x = r[0]; p.y = r[1]; p.z = r[2];
     p.w = Prec<R>::tbits(a.tbits[i]);
     ((PT*)a.pos4[g & 1])[g >> 1] = p;
+  };
+  for (int i = bk.b * blockDim.x + threadIdx.x; i < a.natoms; i += bk.g * blockDim.x) {
+    R s[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) s[c] = (R)a.S[3 * (size_t)i + c];
+    store(i, s);
+  }
+  // VIRTUAL_DEF.f90:67-95: 16 lanes per site (half a warp), lane k holding
+  // member k's mass-weighted position; the sum runs over the members in
+  // order (0 + p0 + p1 + ...), as the reference's loop does.  The loop over
+  // sites is uniform within a warp, so its shuffles see all 32 lanes.
+  const int hl = threadIdx.x & 15;
+  const int w0 = (bk.b * blockDim.x + threadIdx.x) >> 5, nw = (bk.g * blockDim.x) >> 5;
+  for (int w = w0; 2 * w < a.nvirta; w += nw) {
+    const int v = 2 * w + ((threadIdx.x >> 4) & 1);
+    const bool valid = v < a.nvirta;
+    const int ctr = valid ? a.vcenter[v] : 0;
+    const int nm = valid && ctr < 0 ? a.vnum[v] : 0;
+    R pm[3] = {0, 0, 0};
+    if (hl < nm) {
+      const int m = a.vmem[v * 15 + hl];
+      const R mm = (R)a.vmass[v * 15 + hl];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) pm[c] = mm * (R)a.S[3 * (size_t)m + c];
+    }
+    R acc[3] = {0, 0, 0};
+#pragma unroll
+    for (int q = 0; q < 15; ++q) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const R x = __shfl_sync(0xffffffffu, pm[c], q, 16);
+        if (q < nm) acc[c] = acc[c] + x;
+      }
+    }
+    if (!valid || hl != 0) continue;
+    R s[3];
+    if (ctr >= 0) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) s[c] = (R)a.S[3 * (size_t)ctr + c];
+    } else {
+      const R inv = (R)a.vinv[v];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) s[c] = acc[c] * inv;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) a.Svs[3 * (size_t)v + c] = (double)s[c];
+    store(a.natoms + v, s);
   }
 }
 
@@ -1047,20 +1067,25 @@ __global__ void k_distribute(__grid_constant__ const DistArgs<R> D0, const DistA
   const int* vnum = D.vnum;
   const int* vmem = D.vmem;
   const float* vcoef = D.vcoef;
-  for (int v = bk.b * blockDim.x + threadIdx.x; v < nvirta; v += bk.g * blockDim.x) {
+  // 16 lanes per site (half a warp), one member each (VIRT_NUMATOMS <= 15)
+  const int hl = threadIdx.x & 15;
+  const unsigned half = 0xffffu << (threadIdx.x & 16);
+  const int h0 = (bk.b * blockDim.x + threadIdx.x) >> 4, nh = (bk.g * blockDim.x) >> 4;
+  for (int v = h0; v < nvirta; v += nh) {
     const size_t vs = (size_t)(natoms + v);
     double f[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) f[c] = P::get(F[3 * vs + c]);
-    const int nm = vnum[v];
-    for (int k = 0; k < nm; ++k) {
-      const int j = vmem[v * 15 + k];
-      const double cf = (double)vcoef[v * 15 + k];
+    if (hl < vnum[v]) {
+      const int j = vmem[v * 15 + hl];
+      const double cf = (double)vcoef[v * 15 + hl];
 #pragma unroll
       for (int c = 0; c < 3; ++c) P::add(&F[3 * (size_t)j + c], P::from_double(f[c] * cf, &sc->err));
     }
+    __syncwarp(half);  // the site's 16 lanes have read F(vs)
+    if (hl == 0)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) F[3 * vs + c] = 0;
+      for (int c = 0; c < 3; ++c) F[3 * vs + c] = 0;
   }
 }
 
