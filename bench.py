@@ -310,6 +310,36 @@ def reduce_sum(pg, x: float) -> float:
 TUNING_KEYS = ("nb_tables_smem", "nb_blocks_per_sm", "nb_chunk", "nb_rows")
 
 
+def precision_report(native, setup, state):
+    """Error of the FP32/fixed-point path against the plain FP64 GPU path on
+    the same state: the force stage of step 1 on both paths (ibg_forces),
+    max-norm relative error of the total force over particles, and the
+    relative error of each nonzero energy and virial term."""
+    out = {}
+    for name, prec in (("fp32", native.IBG_PREC_FP32_FIXED), ("fp64", native.IBG_PREC_FP64_PLAIN)):
+        g = native.System(setup, prec)
+        g.set_state(*state)
+        obs = g.forces(1)
+        out[name] = (obs, g.state64()["fxyz"])
+        g.close()
+    (o32, f32), (o64, f64) = out["fp32"], out["fp64"]
+    ferr = float(np.abs(f32 - f64).max() / np.abs(f64).max())
+    terms = {}
+    for k, v64 in o64.items():
+        if k.startswith(("V_", "PT")) and abs(v64) > 0:
+            terms[k] = abs(o32[k] - v64) / abs(v64)
+    return {"reference": "plain FP64 GPU path, same state, force stage of step 1",
+            "force_max_rel_err": ferr, "force_tolerance": 1e-5,
+            "energy_virial_rel_err_max": max(terms.values()) if terms else 0.0,
+            "energy_virial_rel_err": terms,
+            "choices": {"displacements": "32-bit box fractions from the FP64 state, wrapped integer difference",
+                        "pair_math": "FP32 table interpolation and rsqrt",
+                        "cutoff": "FP32 r^2; pairs within 1e-6 of rc^2 decided from the FP64 state",
+                        "force_sums": "int64 fixed point, 2^-32 per pair contribution (exact, order-independent sums)",
+                        "energy_virial_sums": "FP32 over 8 list rows, then int64 fixed point at 2^-24",
+                        "integration": "FP64 (positions, velocities, momentum removal, thermostat, barostat)"}}
+
+
 def pick_tuning(native, g, setup, prec, state, flush, reps=20, top=6):
     """Launch tuning of the nonbonded kernel: rank the candidates by their
     launches alone (ibg_autotune, L2 flushed before each), then time whole
@@ -418,6 +448,10 @@ def run_b200(args, world, rank, local, pg):
         d2h = ctypes.sizeof(native.IbgObs) + (3 * out["s"].nbytes + vo.nbytes) / k_e2e
         e2e = {"value": world * n * k_e2e / e2e_s, "unit": "atom-steps/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h}
+        # ---- error of the FP32/fixed-point path against the plain FP64 path
+        precision = None
+        if prec == native.IBG_PREC_FP32_FIXED and not args.no_fp64:
+            precision = precision_report(native, setup, (s0, v0, b0))
         # ---- plain FP64 path, same workload and timing
         fp64 = None
         if prec == native.IBG_PREC_FP32_FIXED and not args.no_fp64:
@@ -493,7 +527,8 @@ def run_b200(args, world, rank, local, pg):
                 "roofline": roof, "stage_ms_per_step": stage,
                 "tuning": {"nonbonded": tuned, "candidates_us": [[list(c), u] for c, u in tune_cands],
                            "steps_us": [[t, u] for t, u in tune_steps]},
-                "cpu_baseline": cpu, "e2e": e2e, "fp64_plain": fp64, "batched": batched, "serving": serving,
+                "cpu_baseline": cpu, "e2e": e2e, "fp64_plain": fp64, "precision_vs_fp64": precision,
+                "batched": batched, "serving": serving,
                 "gpu_launches": launches,
                 "clocks": clk.summary(),
             }

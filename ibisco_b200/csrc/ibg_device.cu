@@ -100,6 +100,9 @@ struct DevList {
   int *sorted = nullptr, *sorted_new = nullptr, *slot_of = nullptr, *slot_of_new = nullptr;
   int *counts = nullptr, *slice_w = nullptr, *entries = nullptr;
   void *pos4 = nullptr, *pos4_new = nullptr, *fsort = nullptr, *mtsf = nullptr;
+  int4 *posq = nullptr, *posq_new = nullptr;  // FP32 path: positions as box fractions
+  int2* near = nullptr;                       // FP32 path: pairs at the cutoff (k_nb_near)
+  int near_cap = 0;
   size_t pos_bytes = 0;
   // tables of this list
   int *ltab = nullptr, *toff = nullptr, *tndat = nullptr;
@@ -259,6 +262,13 @@ void build_list(ibg_ctx* c, const ibg_desc* d, int which) {
   L.pos_bytes = possize(c) * L.n;
   L.pos4 = dalloc<unsigned char>(L.pos_bytes, o);
   L.pos4_new = dalloc<unsigned char>(L.pos_bytes, o);
+  if (c->prec == IBG_PREC_FP32_FIXED) {
+    L.posq = dalloc<int4>(L.n, o);
+    L.posq_new = dalloc<int4>(L.n, o);
+    // about 16 pairs a step sit this close to the cutoff on 40,000 beads
+    L.near_cap = std::max(4096, L.n / 32);
+    L.near = dalloc<int2>(L.near_cap, o);
+  }
   L.fsort = dalloc<unsigned char>(accsize(c) * 3 * L.n, o);
   if (which == 1 && c->nmts > 0) L.mtsf = dalloc<unsigned char>(accsize(c) * 9 * L.n, o);
   L.cell_cap = 0;  // sized in ibg_set_state once the box is known
@@ -385,6 +395,7 @@ void make_args(ibg_ctx* c) {
   p.sc = sc; p.natoms = c->natoms; p.nvirta = c->nvirta; p.nupdate = c->nupdate; p.nmts = c->nmts;
   p.S = c->S; p.Svs = c->S + 3 * (size_t)c->natoms; p.tbits = c->tbits; p.gslot = c->gslot;
   p.pos4[0] = c->L[0].pos4; p.pos4[1] = c->L[1].pos4;
+  p.posq[0] = c->L[0].posq; p.posq[1] = c->L[1].posq;
   p.vcenter = c->vcenter; p.vnum = c->vnum; p.vmem = c->vmem; p.vmass = c->vmass; p.vinv = c->vinv;
   for (int w = 0; w < 2; ++w) {
     DevList& L = c->L[w];
@@ -398,18 +409,23 @@ void make_args(ibg_ctx* c) {
     a.cell_fill = L.cell_fill;
     a.sorted = L.sorted; a.sorted_new = L.sorted_new; a.slot_of = L.slot_of; a.slot_of_new = L.slot_of_new;
     a.gslot = c->gslot; a.pos4 = L.pos4; a.pos4_new = L.pos4_new;
+    a.posq = L.posq; a.posq_new = L.posq_new;
     a.counts = L.counts; a.slice_w = L.slice_w; a.entries = L.entries; a.w_cap = L.w_cap;
     a.excl_n = c->excl_n; a.excl = c->excl;
     NBArgs<R>& n = A.nb[w];
     n.sc = sc; n.mts = (w == 1 && c->nmts > 0);
     n.n = L.n; n.nslices = L.nslices; n.ntype = c->ntype;
-    n.pos4 = L.pos4; n.counts = L.counts; n.slice_w = L.slice_w; n.entries = L.entries;
+    n.pos4 = L.pos4; n.posq = L.posq; n.counts = L.counts; n.slice_w = L.slice_w; n.entries = L.entries;
     n.w_cap = L.w_cap; n.work = w;
     n.fsort = (acc_t*)L.fsort;
     n.ltab = L.ltab; n.toff = L.toff; n.tndat = L.tndat; n.tbin = (const R*)L.tbin; n.tinv = (const R*)L.tinv;
     n.tfp = (const R*)L.tfp; n.tx = (const R*)L.tx; n.ptab = L.ptab; n.chunk = c->nb_chunk;
     n.rows = c->nb_rows;
     n.ntab = L.ntab; n.nrows = L.nrows; n.rcutsq = (R)L.rcutsq;
+    n.rcut_lo = L.rcutsq * (1.0f - 1e-6f);
+    n.rcut_hi = L.rcutsq * (1.0f + 1e-6f);
+    n.near = L.near; n.near_cap = L.near_cap;
+    n.sorted = L.sorted; n.idx = L.idx; n.S = c->S; n.natoms = c->natoms;
     CollectArgs<R>& k = A.col[w];
     k.sc = sc; k.n = L.n; k.mts = (w == 1 && c->nmts > 0); k.sorted = L.sorted; k.idx = L.idx;
     k.fsort = (acc_t*)L.fsort; k.fnb = (acc_t*)c->fnb; k.mtsf = (acc_t*)L.mtsf;
@@ -564,6 +580,10 @@ template <typename R>
 void enq_nonbonded(ibg_ctx* c, DevList& L) {
   nb_kernel<R, false>(L.use_smem, L.T)<<<L.grid_nb, 256, nb_smem(c, L), c->st>>>(args<R>(c).nb[L.which], nullptr, kOne);
   ++c->launches;
+  if (c->prec == IBG_PREC_FP32_FIXED) {
+    k_nb_near<false><<<1, 256, 0, c->st>>>(args<float>(c).nb[L.which], nullptr, kOne);
+    ++c->launches;
+  }
 }
 
 template <typename R>
@@ -968,6 +988,7 @@ long long ibg_estimate_bytes(const ibg_desc* d, int precision, const float* box)
     const double half = (double)n / vol * (2.0 / 3.0) * 3.14159265358979 * rl * rl * rl;
     const double rows = (half * 1.25 + 8.0) * 1.25 + 2.0;  // growth margin and slice padding
     b += (double)n * (7 * 4 + 2 * pos + 3 * acc + rows * 4);
+    if (precision == IBG_PREC_FP32_FIXED) b += (double)n * 32 + 8.0 * std::max(4096, n / 32);  // box fractions, cutoff pairs
     if (w == 1 && d->nmts > 0) b += (double)n * 9 * acc;
     const double cells = (box[0] * 1.25 / rl + 2) * (box[1] * 1.25 / rl + 2) * (box[2] * 1.25 / rl + 2);
     b += cells * 12;
@@ -1747,11 +1768,17 @@ void batch_enqueue(ibg_batch* b, unsigned v) {
       }
     }
   }
-  // nonbonded, bead list first
+  // nonbonded, bead list first; the FP32 path's pairs at the cutoff after
+  // each list (one block per system with the list, as the cell scan)
   for (int w : {1, 0}) {
     for (const NBGroup& grp : b->nb[w]) {
       nb_kernel<R, true>(grp.smem, grp.T)<<<grp.map.grid, 256, grp.sm, st>>>(
           NBArgs<R>{}, (const NBArgs<R>* const*)b->t_nb[w], grp.map.m());
+      ++n;
+    }
+    if (b->prec == IBG_PREC_FP32_FIXED && b->any_list[w]) {
+      k_nb_near<true><<<b->m_scan[w].grid, 256, 0, st>>>(NBArgs<float>{}, (const NBArgs<float>* const*)b->t_nb[w],
+                                                         b->m_scan[w].m());
       ++n;
     }
   }

@@ -99,6 +99,22 @@ __device__ __forceinline__ void fold3(R* r, const R* b2) {
   }
 }
 
+// A position as 32-bit fractions of the box per axis: round(x/L * 2^32)
+// modulo 2^32, in FP64.  The wrapped difference of two of them, read as a
+// signed integer, is the nearest-image displacement in units of L/2^32, exact
+// to one unit (L/2^32: 3e-9 nm for a 12.6 nm box), whatever the particles'
+// distance from the box centre.
+__device__ __forceinline__ int4 box_fraction(const double* x, const double* boxinv, int w) {
+  int q[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    double t = x[c] * boxinv[c];
+    t -= floor(t + 0.5);
+    q[c] = (int)(unsigned)(long long)llrint(t * 4294967296.0);
+  }
+  return make_int4(q[0], q[1], q[2], w);
+}
+
 struct PosArgs {
   Scalars* sc;
   int natoms, nvirta;
@@ -108,6 +124,7 @@ struct PosArgs {
   const int* tbits;    // type | label<<16 per particle
   const int* gslot;    // slot*2 + list per particle
   void* pos4[2];       // per-list wrapped positions, slot order
+  int4* posq[2];       // FP32 path: per-list positions as 32-bit fractions of the box, slot order
   const int* vcenter;  // VIRT_CENTER (0-based atom id or -1 for COM)
   const int* vnum;     // members per VS
   const int* vmem;     // members, [v*15 + k], 0-based
@@ -146,7 +163,8 @@ __global__ void k_positions(__grid_constant__ const PosArgs a0, const PosArgs* c
   }
   R b[3], bi[3], b2[3];
   box_of<R>(sc, b, bi, b2);
-  auto store = [&](int i, const R* s) {
+  // sd: the position in FP64 for the fixed-point copy (FP32 path)
+  auto store = [&](int i, const R* s, const double* sd) {
     R r[3] = {s[0], s[1], s[2]};
     fold3<R>(r, b2);
     const int g = a.gslot[i];
@@ -154,12 +172,17 @@ __global__ void k_positions(__grid_constant__ const PosArgs a0, const PosArgs* c
     p.x = r[0]; p.y = r[1]; p.z = r[2];
     p.w = Prec<R>::tbits(a.tbits[i]);
     ((PT*)a.pos4[g & 1])[g >> 1] = p;
+    if (a.posq[g & 1]) a.posq[g & 1][g >> 1] = box_fraction(sd, sc->boxinv, a.tbits[i]);
   };
   for (int i = bk.b * blockDim.x + threadIdx.x; i < a.natoms; i += bk.g * blockDim.x) {
     R s[3];
+    double sd[3];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) s[c] = (R)a.S[3 * (size_t)i + c];
-    store(i, s);
+    for (int c = 0; c < 3; ++c) {
+      sd[c] = a.S[3 * (size_t)i + c];
+      s[c] = (R)sd[c];
+    }
+    store(i, s, sd);
   }
   // VIRTUAL_DEF.f90:67-95: 16 lanes per site (half a warp), lane k holding
   // member k's mass-weighted position; the sum runs over the members in
@@ -198,9 +221,13 @@ __global__ void k_positions(__grid_constant__ const PosArgs a0, const PosArgs* c
 #pragma unroll
       for (int c = 0; c < 3; ++c) s[c] = acc[c] * inv;
     }
+    double sd[3];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) a.Svs[3 * (size_t)v + c] = (double)s[c];
-    store(a.natoms + v, s);
+    for (int c = 0; c < 3; ++c) {
+      sd[c] = (double)s[c];
+      a.Svs[3 * (size_t)v + c] = sd[c];
+    }
+    store(a.natoms + v, s, sd);
   }
 }
 
@@ -228,6 +255,8 @@ struct ListArgs {
   int* gslot;        // [NITEMS]
   void* pos4;        // [n]
   void* pos4_new;    // [n]
+  int4* posq;        // [n] FP32 path: fixed-point positions (box fractions), or null
+  int4* posq_new;    // [n]
   int* counts;       // [n] per slot
   int* slice_w;      // [nslices] rows of 32 entries used by each slice
   int* entries;      // list storage: slice g owns rows [g*w_cap, (g+1)*w_cap) of 32 entries
@@ -381,6 +410,7 @@ __global__ void k_reslot(__grid_constant__ const ListArgs L0, const ListArgs* co
   for (int s = bk.b * blockDim.x + threadIdx.x; s < L.n; s += bk.g * blockDim.x) {
     int a = L.slot_of_new[s];
     ((PT*)L.pos4_new)[s] = ((const PT*)L.pos4)[L.slot_of[a]];
+    if (L.posq) L.posq_new[s] = L.posq[L.slot_of[a]];
     L.sorted[s] = a;
     L.gslot[L.idx[a]] = s * 2 + L.which;
   }
@@ -398,6 +428,7 @@ __global__ void k_slot_of(__grid_constant__ const ListArgs L0, const ListArgs* c
   for (int s = bk.b * blockDim.x + threadIdx.x; s < L.n; s += bk.g * blockDim.x) {
     L.slot_of[L.sorted[s]] = s;
     ((PT*)L.pos4)[s] = ((const PT*)L.pos4_new)[s];
+    if (L.posq) L.posq[s] = L.posq_new[s];
   }
 }
 
@@ -613,6 +644,7 @@ struct NBArgs {
   int mts;                         // bead list of an MTS run: only steps m = 1..3 evaluate it
   int n, nslices, ntype;
   const void* pos4;
+  const int4* posq;                // FP32 kernel: positions as box fractions
   const int* counts;
   const int* slice_w;
   const int* entries;
@@ -629,6 +661,16 @@ struct NBArgs {
   const int4* ptab;  // FP32 kernel: per type pair {first row, NDAT, 1/bin bits, 1 if a table}
   int chunk;         // FP32 kernel: work units per block chunk (0: each warp takes units alone)
   int rows;          // list rows per work unit, a multiple of kEnergyRows
+  // FP32 kernel: pairs whose r^2 lies within a relative 1e-6 of the cutoff
+  // are left to k_nb_near, which decides them as the FP64 path does from the
+  // FP64 state (slot -> A -> global id)
+  float rcut_lo, rcut_hi;
+  int2* near;          // (i slot, j slot) of those pairs
+  int near_cap;
+  const int* sorted;
+  const int* idx;
+  const double* S;
+  int natoms;
   const R* tfp;  // 2 per row
   const R* tx;
   int ntab, nrows;
@@ -812,9 +854,11 @@ __device__ __forceinline__ long long fixq(float v, unsigned& err) {
 // k_nonbonded (slices of P = 32/T slots, T lanes per slot, dynamic units of
 // `rows` list rows).  The arithmetic is REAL*4 as in the reference, with
 // cheaper equivalents where only the force value (not a bit pattern) is
-// compared: minimum image as d - rint(d/L) L, r from rsqrt, the table row
-// and interpolation weight from a precomputed 1/bin, float-to-fixed by the
-// hardware conversion of the exactly scaled value.  Energies and virials are
+// compared: positions as 32-bit box fractions, whose wrapped difference is
+// the nearest-image displacement at full precision anywhere in the box (a
+// REAL*4 coordinate near the box edge carries only 24 bits), r from rsqrt,
+// the table row and interpolation weight from a precomputed 1/bin,
+// float-to-fixed by the hardware conversion of the exactly scaled value.  Energies and virials are
 // summed in FP32 over kEnergyRows list rows, then as 64-bit fixed point
 // (2^-24) per lane and per block, and added to the system's accumulators:
 // integer sums depend neither on which warp took which unit nor on the rows
@@ -848,9 +892,9 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
   }
   for (int k = 0; k < 9; ++k) lacc[k * blockDim.x + threadIdx.x] = 0;
   __syncthreads();
-  const float bx = sc->boxf[0], by = sc->boxf[1], bz = sc->boxf[2];
-  const float ix = sc->boxinvf[0], iy = sc->boxinvf[1], iz = sc->boxinvf[2];
-  const float4* pos = (const float4*)A.pos4;
+  // displacement unit per axis: L / 2^32
+  const float ux = (float)(sc->box[0] * 0x1p-32), uy = (float)(sc->box[1] * 0x1p-32), uz = (float)(sc->box[2] * 0x1p-32);
+  const int4* pos = A.posq;
   const int lane = threadIdx.x & 31, grp = lane / T, q = lane % T;
   unsigned err = 0;
   const bool run = true;
@@ -869,8 +913,8 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
     const bool valid = s < A.n;
     const int cnt = valid ? A.counts[s] : 0;
     const int* ent = A.entries + (long long)g * A.w_cap * 32 + lane;
-    const float4 pi = valid ? pos[s] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const int wi = __float_as_int(pi.w);
+    const int4 pi = valid ? pos[s] : make_int4(0, 0, 0, 0);
+    const int wi = pi.w;
     const int ti = wi & 0xffff, li = wi >> 16;
     long long fi0 = 0, fi1 = 0, fi2 = 0;
     // energies and virials: FP32 over kEnergyRows rows (aligned to multiples of
@@ -879,16 +923,21 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
     for (int b0 = r0; b0 < r1; b0 += kEnergyRows) {
       const int b1 = min(r1, b0 + kEnergyRows);
       float e[3] = {0.f, 0.f, 0.f}, vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      auto pair = [&](int t, const float4& pj) {
-        // minimum image d - rint(d/L) L (the pair is beyond the cutoff wherever
-        // this and ANINT could choose differently, |d| ~ L/2)
-        float d0 = pi.x - pj.x, d1 = pi.y - pj.y, d2 = pi.z - pj.z;
-        d0 = __fmaf_rn(-rintf(d0 * ix), bx, d0);
-        d1 = __fmaf_rn(-rintf(d1 * iy), by, d1);
-        d2 = __fmaf_rn(-rintf(d2 * iz), bz, d2);
+      auto pair = [&](int t, const int4& pj) {
+        // nearest image: the wrapped difference of the box fractions (it and
+        // ANINT could choose differently only at |d| = L/2, beyond the cutoff)
+        const float d0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * ux;
+        const float d1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * uy;
+        const float d2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * uz;
         const float r2 = __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, d0 * d0));
-        if (!(r2 < A.rcutsq)) return;
-        const int wj = __float_as_int(pj.w);
+        if (!(r2 < A.rcut_hi)) return;
+        if (r2 > A.rcut_lo) {  // at the cutoff: k_nb_near decides and computes it
+          const unsigned k = atomicAdd(&sc->near_n[A.work], 1u);
+          if (k < (unsigned)A.near_cap) A.near[k] = make_int2(s, t);
+          else err |= EB_CAPACITY;
+          return;
+        }
+        const int wj = pj.w;
         const int tj = wj & 0xffff, lj = wj >> 16;
         const int4 pt = ptab[ti * A.ntype + tj];
         if (!pt.w) { err |= EB_MISSING_TABLE; return; }
@@ -929,8 +978,8 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
         const bool v1 = it + 1 < b1 && (it + 1) * T + q < cnt;
         const int t0 = v0 ? ent[it * 32] : 0;
         const int t1 = v1 ? ent[(it + 1) * 32] : 0;
-        const float4 p0 = pos[t0];
-        const float4 p1 = pos[t1];
+        const int4 p0 = pos[t0];
+        const int4 p1 = pos[t1];
         if (v0) pair(t0, p0);
         if (v1) pair(t1, p1);
       }
@@ -991,6 +1040,107 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
   block_sum_i64<9>(acc, lacc);
   if (threadIdx.x < 9 && lacc[threadIdx.x] != 0)
     atomicAdd(&sc->nbacc[A.work][threadIdx.x], (unsigned long long)lacc[threadIdx.x]);
+}
+
+// Whether the pair of slots s, t (FP32 r^2 = r2) lies inside the cutoff as
+// the FP64 path decides it: the same fold of the FP64 state into the box
+// (SHIFT), nearest image and sum of squares as k_positions<double> and
+// k_nonbonded<double>.  FP32 rounding of r^2 (a relative ~5e-7) would
+// otherwise take pairs that sit at the cutoff in or out against that path,
+// each a jump of F(rc) r_c in the force (1.3e-5 of the largest force on the
+// 40,000-bead melt).  A pair with a virtual site keeps the FP32 decision: its
+// FP64 position is not kept on this path.
+__device__ bool inside_as_fp64(const NBArgs<float>& A, const Scalars* sc, int s, int t, float r2) {
+  const int gi = A.idx[A.sorted[s]], gj = A.idx[A.sorted[t]];
+  if (gi >= A.natoms || gj >= A.natoms) return r2 < A.rcutsq;
+  double b[3], bi[3], b2[3];
+  box_of<double>(sc, b, bi, b2);
+  double ri[3], rj[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    ri[c] = A.S[3 * (size_t)gi + c];
+    rj[c] = A.S[3 * (size_t)gj + c];
+  }
+  fold3<double>(ri, b2);
+  fold3<double>(rj, b2);
+  double d[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    d[c] = ri[c] - rj[c];
+    d[c] = d[c] - r_round(d[c] * bi[c]) * b[c];
+  }
+  double q = d[0] * d[0];
+  q = q + d[1] * d[1];
+  q = q + d[2] * d[2];
+  return q < (double)A.rcutsq;
+}
+
+// The pairs the FP32 kernel left at the cutoff: each is decided as the FP64
+// path decides it (inside_as_fp64) and, when inside, computed with the FP32
+// kernel's pair arithmetic; its energy and virial terms go to the system's
+// fixed-point sums one pair at a time.  One block per system and list; the
+// block clears the list's pair count for the next launch.
+template <bool B>
+__global__ void __launch_bounds__(256) k_nb_near(__grid_constant__ const NBArgs<float> A0,
+                                                 const NBArgs<float>* const* tab, const BlockMap bm) {
+  const Blk bk = blk<B>(bm);
+  const NBArgs<float>& A = B ? *tab[bk.sys] : A0;
+  Scalars* sc = A.sc;
+  if (nb_idle(A)) return;
+  __shared__ long long red[32 + 9 * 8];  // block_sum_i64: 32 results + 9 per warp
+  const unsigned n = min(sc->near_n[A.work], (unsigned)A.near_cap);
+  const float ux = (float)(sc->box[0] * 0x1p-32), uy = (float)(sc->box[1] * 0x1p-32), uz = (float)(sc->box[2] * 0x1p-32);
+  unsigned err = 0;
+  long long acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (unsigned k = threadIdx.x; k < n; k += blockDim.x) {
+    const int s = A.near[k].x, t = A.near[k].y;
+    const int4 pi = A.posq[s], pj = A.posq[t];
+    const float d0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * ux;
+    const float d1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * uy;
+    const float d2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * uz;
+    const float r2 = __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, d0 * d0));
+    if (!inside_as_fp64(A, sc, s, t, r2)) continue;
+    const int ti = pi.w & 0xffff, li = pi.w >> 16, tj = pj.w & 0xffff, lj = pj.w >> 16;
+    const int4 pt = A.ptab[ti * A.ntype + tj];
+    if (!pt.w) { err |= EB_MISSING_TABLE; continue; }
+    const float r = r2 * rsqrtf(r2);
+    const float ib = __int_as_float(pt.z);
+    const int ni = (int)(r * ib);
+    if (ni > pt.y) { err |= EB_TABLE_RANGE; continue; }
+    const int row = pt.x + ni;
+    const float alpha = (r - A.tx[row]) * ib;
+    const float2 a0 = ((const float2*)A.tfp)[row], a1 = ((const float2*)A.tfp)[row + 1];
+    const float fij = __fmaf_rn(a1.x - a0.x, alpha, a0.x);
+    const float vij = __fmaf_rn(a1.y - a0.y, alpha, a0.y);
+    if (!(fabsf(fij) * r < 0.99f * kFixMax)) { err |= EB_FIXED; continue; }
+    const float fx = fij * d0, fy = fij * d1, fz = fij * d2;
+    const long long qx = __float2ll_rn(fx * kFixScale), qy = __float2ll_rn(fy * kFixScale),
+                    qz = __float2ll_rn(fz * kFixScale);
+    unsigned long long* fs = (unsigned long long*)A.fsort;
+    atomicAdd(fs + 3 * (size_t)s + 0, (unsigned long long)qx);
+    atomicAdd(fs + 3 * (size_t)s + 1, (unsigned long long)qy);
+    atomicAdd(fs + 3 * (size_t)s + 2, (unsigned long long)qz);
+    atomicAdd(fs + 3 * (size_t)t + 0, (unsigned long long)(-qx));
+    atomicAdd(fs + 3 * (size_t)t + 1, (unsigned long long)(-qy));
+    atomicAdd(fs + 3 * (size_t)t + 2, (unsigned long long)(-qz));
+    const bool lab3 = li == 3 || lj == 3;
+    const long long qe = fixq<24>(vij, err);
+    if (li == 1) acc[0] += qe;
+    if (li == 2 && lj == 2) acc[1] += qe;
+    if (li != 1 && lab3) acc[2] += qe;
+    acc[3] += fixq<24>(fx * d0, err);
+    acc[4] += fixq<24>(fy * d1, err);
+    acc[5] += fixq<24>(fz * d2, err);
+    acc[6] += fixq<24>(fy * d0, err);
+    acc[7] += fixq<24>(fz * d0, err);
+    acc[8] += fixq<24>(fz * d1, err);
+  }
+  if (err) atomicOr(&sc->err, err);
+  block_sum_i64<9>(acc, red);
+  if (threadIdx.x < 9 && red[threadIdx.x] != 0)
+    atomicAdd(&sc->nbacc[A.work][threadIdx.x], (unsigned long long)red[threadIdx.x]);
+  __syncthreads();
+  if (threadIdx.x == 0) sc->near_n[A.work] = 0u;
 }
 
 // Per-slot forces of both lists into the global-order nonbonded force
