@@ -55,7 +55,8 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     "melt40k": "bead-spring melt: 400 chains x 100 beads (40,000), 3 types, bond/angle/torsion tables, "
                "6 LJ tables rc 1.0 nm, list 1.2 nm every 10 steps, NVT 500 K, dt 1 fs",
-    "fluid4k": "single-type LJ fluid: 4,000 beads, rho 8/nm^3, rc 1.2 nm, list 1.4 nm every 10 steps, NVE, dt 10 fs",
+    "fluid4k": "single-type LJ fluid: 4,000 beads, rho 8/nm^3, overlaps rejected below 0.42 nm, rc 1.2 nm, "
+               "list 1.4 nm every 10 steps, NVE, dt 10 fs",
     "melt2m": "CG melt: 10,000 chains x 200 beads (2,000,000), 4 types, bond/angle tables, 10 LJ tables "
               "rc 1.4 nm, list 1.6 nm every 10 steps, NVT 300 K, dt 10 fs",
     "hybrid3a": "hybrid melt as specified: 200 atomistic chains x 20 monomers x 12 atoms (48,000) with a "
@@ -73,7 +74,9 @@ def make_workload(name: str, directory: str):
     if name == "melt40k":
         spec = synth.polymer_melt(nchains=400, nper=100, seed=2)
     elif name == "fluid4k":
-        spec = synth.lj_fluid(n=4000, seed=1)
+        # overlap rejection below 0.42 nm: at 0.3 nm (sigma 0.47 nm, dt 10 fs) the
+        # REAL*4 restatement of the reference itself diverges within 10 steps
+        spec = synth.lj_fluid(n=4000, seed=1, dmin=0.42)
     elif name == "melt2m":
         spec = synth.cg_melt()
     elif name == "hybrid3a":
@@ -324,14 +327,18 @@ def precision_report(native, setup, state):
         g.close()
     (o32, f32), (o64, f64) = out["fp32"], out["fp64"]
     ferr = float(np.abs(f32 - f64).max() / np.abs(f64).max())
-    terms = {}
-    for k, v64 in o64.items():
-        if k.startswith(("V_", "PT")) and abs(v64) > 0:
-            terms[k] = abs(o32[k] - v64) / abs(v64)
+    energies = {k: abs(o32[k] - v) / abs(v) for k, v in o64.items() if k.startswith("V_") and abs(v) > 0}
+    # the virial tensor as a whole, max-norm like the forces: an off-diagonal
+    # term that vanishes by symmetry has no meaningful error of its own
+    pt = [k for k in ("PT11", "PT22", "PT33", "PT12", "PT13", "PT23") if k in o64]
+    w64 = np.array([o64[k] for k in pt])
+    w32 = np.array([o32[k] for k in pt])
+    verr = float(np.abs(w32 - w64).max() / np.abs(w64).max()) if len(pt) and np.abs(w64).max() > 0 else 0.0
     return {"reference": "plain FP64 GPU path, same state, force stage of step 1",
             "force_max_rel_err": ferr, "force_tolerance": 1e-5,
-            "energy_virial_rel_err_max": max(terms.values()) if terms else 0.0,
-            "energy_virial_rel_err": terms,
+            "energy_rel_err_max": max(energies.values()) if energies else 0.0,
+            "energy_rel_err": energies,
+            "virial_max_norm_rel_err": verr,
             "choices": {"displacements": "32-bit box fractions from the FP64 state, wrapped integer difference",
                         "pair_math": "FP32 table interpolation and rsqrt",
                         "cutoff": "FP32 r^2; pairs within 1e-6 of rc^2 decided from the FP64 state",

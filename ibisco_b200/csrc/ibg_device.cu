@@ -101,7 +101,7 @@ struct DevList {
   int *counts = nullptr, *slice_w = nullptr, *entries = nullptr;
   void *pos4 = nullptr, *pos4_new = nullptr, *fsort = nullptr, *mtsf = nullptr;
   int4 *posq = nullptr, *posq_new = nullptr;  // FP32 path: positions as box fractions
-  int2* near = nullptr;                       // FP32 path: pairs at the cutoff (k_nb_near)
+  int4* near = nullptr;                       // FP32 path: pairs at the cutoff (k_nb_near)
   int near_cap = 0;
   size_t pos_bytes = 0;
   // tables of this list
@@ -267,7 +267,7 @@ void build_list(ibg_ctx* c, const ibg_desc* d, int which) {
     L.posq_new = dalloc<int4>(L.n, o);
     // about 16 pairs a step sit this close to the cutoff on 40,000 beads
     L.near_cap = std::max(4096, L.n / 32);
-    L.near = dalloc<int2>(L.near_cap, o);
+    L.near = dalloc<int4>(L.near_cap, o);
   }
   L.fsort = dalloc<unsigned char>(accsize(c) * 3 * L.n, o);
   if (which == 1 && c->nmts > 0) L.mtsf = dalloc<unsigned char>(accsize(c) * 9 * L.n, o);
@@ -988,7 +988,7 @@ long long ibg_estimate_bytes(const ibg_desc* d, int precision, const float* box)
     const double half = (double)n / vol * (2.0 / 3.0) * 3.14159265358979 * rl * rl * rl;
     const double rows = (half * 1.25 + 8.0) * 1.25 + 2.0;  // growth margin and slice padding
     b += (double)n * (7 * 4 + 2 * pos + 3 * acc + rows * 4);
-    if (precision == IBG_PREC_FP32_FIXED) b += (double)n * 32 + 8.0 * std::max(4096, n / 32);  // box fractions, cutoff pairs
+    if (precision == IBG_PREC_FP32_FIXED) b += (double)n * 32 + 16.0 * std::max(4096, n / 32);  // box fractions, cutoff pairs
     if (w == 1 && d->nmts > 0) b += (double)n * 9 * acc;
     const double cells = (box[0] * 1.25 / rl + 2) * (box[1] * 1.25 / rl + 2) * (box[2] * 1.25 / rl + 2);
     b += cells * 12;

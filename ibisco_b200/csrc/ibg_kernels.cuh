@@ -663,9 +663,9 @@ struct NBArgs {
   int rows;          // list rows per work unit, a multiple of kEnergyRows
   // FP32 kernel: pairs whose r^2 lies within a relative 1e-6 of the cutoff
   // are left to k_nb_near, which decides them as the FP64 path does from the
-  // FP64 state (slot -> A -> global id)
+  // FP64 state (global ids from slot -> A -> global id)
   float rcut_lo, rcut_hi;
-  int2* near;          // (i slot, j slot) of those pairs
+  int4* near;          // (i slot, j slot, i global id, j global id) of those pairs
   int near_cap;
   const int* sorted;
   const int* idx;
@@ -933,7 +933,7 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
         if (!(r2 < A.rcut_hi)) return;
         if (r2 > A.rcut_lo) {  // at the cutoff: k_nb_near decides and computes it
           const unsigned k = atomicAdd(&sc->near_n[A.work], 1u);
-          if (k < (unsigned)A.near_cap) A.near[k] = make_int2(s, t);
+          if (k < (unsigned)A.near_cap) A.near[k] = make_int4(s, t, A.idx[A.sorted[s]], A.idx[A.sorted[t]]);
           else err |= EB_CAPACITY;
           return;
         }
@@ -1042,7 +1042,7 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
     atomicAdd(&sc->nbacc[A.work][threadIdx.x], (unsigned long long)lacc[threadIdx.x]);
 }
 
-// Whether the pair of slots s, t (FP32 r^2 = r2) lies inside the cutoff as
+// Whether the pair of particles gi, gj (FP32 r^2 = r2) lies inside the cutoff as
 // the FP64 path decides it: the same fold of the FP64 state into the box
 // (SHIFT), nearest image and sum of squares as k_positions<double> and
 // k_nonbonded<double>.  FP32 rounding of r^2 (a relative ~5e-7) would
@@ -1050,8 +1050,7 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
 // each a jump of F(rc) r_c in the force (1.3e-5 of the largest force on the
 // 40,000-bead melt).  A pair with a virtual site keeps the FP32 decision: its
 // FP64 position is not kept on this path.
-__device__ bool inside_as_fp64(const NBArgs<float>& A, const Scalars* sc, int s, int t, float r2) {
-  const int gi = A.idx[A.sorted[s]], gj = A.idx[A.sorted[t]];
+__device__ bool inside_as_fp64(const NBArgs<float>& A, const Scalars* sc, int gi, int gj, float r2) {
   if (gi >= A.natoms || gj >= A.natoms) return r2 < A.rcutsq;
   double b[3], bi[3], b2[3];
   box_of<double>(sc, b, bi, b2);
@@ -1093,13 +1092,14 @@ __global__ void __launch_bounds__(256) k_nb_near(__grid_constant__ const NBArgs<
   unsigned err = 0;
   long long acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (unsigned k = threadIdx.x; k < n; k += blockDim.x) {
-    const int s = A.near[k].x, t = A.near[k].y;
+    const int4 nk = A.near[k];
+    const int s = nk.x, t = nk.y;
     const int4 pi = A.posq[s], pj = A.posq[t];
     const float d0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * ux;
     const float d1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * uy;
     const float d2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * uz;
     const float r2 = __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, d0 * d0));
-    if (!inside_as_fp64(A, sc, s, t, r2)) continue;
+    if (!inside_as_fp64(A, sc, nk.z, nk.w, r2)) continue;
     const int ti = pi.w & 0xffff, li = pi.w >> 16, tj = pj.w & 0xffff, lj = pj.w >> 16;
     const int4 pt = A.ptab[ti * A.ntype + tj];
     if (!pt.w) { err |= EB_MISSING_TABLE; continue; }
