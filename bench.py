@@ -503,6 +503,7 @@ def run_b200(args, world, rank, local, pg):
             bms = reduce_max(pg, bat.timing()["run_ms"])
             bval = world * args.batch * n * args.steps / (bms / 1000.0)
             batched = {"systems": args.batch, "value": bval, "unit": "atom-steps/s", "tuning": btuned,
+                       "candidates_us_per_batch_step": [[t, u] for t, u in btimes],
                        "ms_per_step": bms / args.steps, "particles_per_step": args.batch * n,
                        "l2": "not flushed; the batch's working set exceeds the 126 MB L2",
                        "clocks": clk_b.summary()}
