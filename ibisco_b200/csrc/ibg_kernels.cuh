@@ -959,13 +959,14 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
         // component in range
         if (!(fabsf(fij) * r < 0.99f * kFixMax)) { err |= EB_FIXED; return; }
         const float fx = fij * d0, fy = fij * d1, fz = fij * d2;
-        // round(f * 2^32): the scaling is exact, the conversion rounds to nearest
-        const long long qx = __float2ll_rn(fx * kFixScale), qy = __float2ll_rn(fy * kFixScale),
-                        qz = __float2ll_rn(fz * kFixScale);
-        fi0 += qx; fi1 += qy; fi2 += qz;
-        atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 0], (unsigned long long)(-qx));
-        atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 1], (unsigned long long)(-qy));
-        atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 2], (unsigned long long)(-qz));
+        // j's share, round(-f * 2^32): the scaling is exact and round-to-nearest
+        // is symmetric, so i's share is exactly its negation (subtracted below)
+        const long long qx = __float2ll_rn(fx * -kFixScale), qy = __float2ll_rn(fy * -kFixScale),
+                        qz = __float2ll_rn(fz * -kFixScale);
+        fi0 -= qx; fi1 -= qy; fi2 -= qz;
+        atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 0], (unsigned long long)qx);
+        atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 1], (unsigned long long)qy);
+        atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 2], (unsigned long long)qz);
         vir[0] = __fmaf_rn(fx, d0, vir[0]);
         vir[1] = __fmaf_rn(fy, d1, vir[1]);
         vir[2] = __fmaf_rn(fz, d2, vir[2]);
