@@ -873,7 +873,7 @@ int ibg_autotune(ibg_ctx* c, int reps, ibg_tuning* best, ibg_tuning* cand_out, d
     for (int rows : {8, 16})
       for (int chunk : {0, 12, 24, 48, 96})
         for (int smem : {0, 1})
-          for (int per : {0, 3}) cand.push_back(ibg_tuning{smem, per, chunk, rows});
+          for (int per : {0, 4, 3}) cand.push_back(ibg_tuning{smem, per, chunk, rows});
   } else {
     for (int rows : {8, 16})
       for (int smem : {0, 1})

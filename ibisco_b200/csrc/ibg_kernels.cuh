@@ -864,7 +864,7 @@ __device__ __forceinline__ long long fixq(float v, unsigned& err) {
 // integer sums depend neither on which warp took which unit nor on the rows
 // per unit, so they are reproducible and the same alone or in a batch.
 template <bool SMEM, int T, bool B>
-__global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ const NBArgs<float> A0,
+__global__ void __launch_bounds__(256, B ? 4 : 5) k_nonbonded_f32(__grid_constant__ const NBArgs<float> A0,
                                                           const NBArgs<float>* const* tab, const BlockMap bm) {
   constexpr int PS = 32 / T;
   const Blk bk = blk<B>(bm);
