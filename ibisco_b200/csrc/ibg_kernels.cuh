@@ -1705,9 +1705,20 @@ struct FinalArgs {
   ObsD* ring; int ring_cap;
 };
 
+// Sum of g partials by one warp: each lane adds its own in increasing order
+// (p[lane], p[lane+32], ...), then the lanes are summed.  Eight loads per lane
+// are issued before they are added, so the warp waits for memory once per
+// eight rather than once per partial; the order of the additions is the same.
 __device__ double wsum(const double* p, int g) {
   double s = 0.0;
-  for (int b = threadIdx.x & 31; b < g; b += 32) s += p[b];
+  for (int b0 = threadIdx.x & 31; b0 < g; b0 += 8 * 32) {
+    double v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = b0 + 32 * k < g ? p[b0 + 32 * k] : 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (b0 + 32 * k < g) s += v[k];
+  }
   return warp_sum(s);
 }
 
