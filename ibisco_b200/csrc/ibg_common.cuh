@@ -62,6 +62,7 @@ struct Scalars {
   int need_rows[2];   // rows of 32 entries a slice of each list needed
   unsigned work[4];   // dynamic work counters: nonbonded atom/bead, list build atom/bead
   unsigned near_n[2];  // pairs at the cutoff left by the FP32 nonbonded kernel, per list
+  int need_near[2];    // pairs at the cutoff a list needed room for (the step is repeated)
   // nonbonded V_NB(1..3) and PT11..PT23 of the atom / bead list: 64-bit fixed
   // point at 2^-24 (FP32 path; order independent) or double (FP64 path)
   unsigned long long nbacc[2][9];

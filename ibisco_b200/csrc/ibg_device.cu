@@ -771,23 +771,39 @@ int grow_lists(ibg_ctx* c) {
   CK(cudaStreamSynchronize(c->st));
   CK(cudaMemcpy(&abort_flag, &c->sc->abort, sizeof(int), cudaMemcpyDeviceToHost));
   if (!abort_flag) return 0;
+  int need_near[2] = {0, 0};
   CK(cudaMemcpy(need, c->sc->need_rows, sizeof(need), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(need_near, c->sc->need_near, sizeof(need_near), cudaMemcpyDeviceToHost));
   for (int w = 0; w < 2; ++w) {
     DevList& L = c->L[w];
-    if (!L.present || need[w] <= L.w_cap) continue;
-    const int cap = need[w] + need[w] / 4 + 2;
-    if (L.entries) c->owned.release(L.entries);
-    L.entries = dalloc<int>((size_t)L.nslices * 32 * cap, c->owned);
-    L.w_cap = cap;
-    ++c->list_growths;
+    if (!L.present) continue;
+    if (need[w] > L.w_cap) {
+      const int cap = need[w] + need[w] / 4 + 2;
+      if (L.entries) c->owned.release(L.entries);
+      L.entries = dalloc<int>((size_t)L.nslices * 32 * cap, c->owned);
+      L.w_cap = cap;
+      ++c->list_growths;
+    }
+    if (need_near[w] > L.near_cap) {  // pairs at the cutoff (FP32 path)
+      const int cap = need_near[w] + need_near[w] / 4 + 64;
+      if (L.near) c->owned.release(L.near);
+      L.near = dalloc<int4>(cap, c->owned);
+      L.near_cap = cap;
+    }
   }
   const int zero[3] = {0, 0, 0};
   CK(cudaMemcpy(&c->sc->abort, zero, sizeof(int), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(&c->sc->skip, zero, sizeof(int), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->sc->need_rows, zero, 2 * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->sc->need_near, zero, 2 * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->sc->near_n, zero, 2 * sizeof(unsigned), cudaMemcpyHostToDevice));
   // the bonded branch of the aborted step may have run (it overlaps the list
-  // build); its forces are recomputed when the step is repeated
+  // build), and so may its nonbonded kernels (a step aborted for the pairs at
+  // the cutoff): their sums are recomputed when the step is repeated
   CK(cudaMemset(c->fb, 0, accsize(c) * 3 * (size_t)c->nitems));
+  for (auto& L : c->L)
+    if (L.present) CK(cudaMemset(L.fsort, 0, accsize(c) * 3 * (size_t)L.n));
+  CK(cudaMemset(c->sc->nbacc, 0, sizeof(c->sc->nbacc)));
   refresh_args(c);
   for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);  // they bake the old pointers
   c->graphs.clear();

@@ -934,8 +934,7 @@ __global__ void __launch_bounds__(256, B ? 4 : 5) k_nonbonded_f32(__grid_constan
         if (r2 > A.rcut_lo) {  // at the cutoff: k_nb_near decides and computes it
           const unsigned k = atomicAdd(&sc->near_n[A.work], 1u);
           if (k < (unsigned)A.near_cap) A.near[k] = make_int4(s, t, A.idx[A.sorted[s]], A.idx[A.sorted[t]]);
-          else err |= EB_CAPACITY;
-          return;
+          return;  // beyond the buffer: k_nb_near has the step repeated with a larger one
         }
         const int wj = pj.w;
         const int tj = wj & 0xffff, lj = wj >> 16;
@@ -1079,7 +1078,8 @@ __device__ bool inside_as_fp64(const NBArgs<float>& A, const Scalars* sc, int gi
 // path decides it (inside_as_fp64) and, when inside, computed with the FP32
 // kernel's pair arithmetic; its energy and virial terms go to the system's
 // fixed-point sums one pair at a time.  One block per system and list; the
-// block clears the list's pair count for the next launch.
+// block clears the list's pair count for the next launch.  When more pairs came
+// than the buffer holds, the step is aborted and repeated with a larger one.
 template <bool B>
 __global__ void __launch_bounds__(256) k_nb_near(__grid_constant__ const NBArgs<float> A0,
                                                  const NBArgs<float>* const* tab, const BlockMap bm) {
@@ -1088,7 +1088,19 @@ __global__ void __launch_bounds__(256) k_nb_near(__grid_constant__ const NBArgs<
   Scalars* sc = A.sc;
   if (nb_idle(A)) return;
   __shared__ long long red[32 + 9 * 8];  // block_sum_i64: 32 results + 9 per warp
-  const unsigned n = min(sc->near_n[A.work], (unsigned)A.near_cap);
+  const unsigned n = sc->near_n[A.work];
+  if (n > (unsigned)A.near_cap) {
+    // the pairs did not fit: record the need and abort the step, which the
+    // host repeats with a larger buffer (as for the Verlet-list storage)
+    __syncthreads();  // every thread has read the count
+    if (threadIdx.x == 0) {
+      sc->need_near[A.work] = (int)n;
+      sc->near_n[A.work] = 0u;
+      sc->abort = 1;
+      sc->skip = 1;
+    }
+    return;
+  }
   const float ux = (float)(sc->box[0] * 0x1p-32), uy = (float)(sc->box[1] * 0x1p-32), uz = (float)(sc->box[2] * 0x1p-32);
   unsigned err = 0;
   long long acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};

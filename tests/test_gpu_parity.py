@@ -128,6 +128,31 @@ def test_forces_fp32_fixed_against_fp64_path_in_a_large_box(tmp_path):
         assert abs(o32[k] - o64[k]) <= ENERGY_TOL * abs(o64[k]), k
 
 
+def test_cutoff_pairs_beyond_their_buffer_repeat_the_step(tmp_path):
+    """A simple cubic lattice (20^3 beads, spacing 0.5 nm, cutoff 1.0 nm) puts
+    24,000 pairs exactly at the cutoff, far more than the FP32 kernel's first
+    buffer for them holds (4,096).  The step is aborted, the buffer grows and
+    the step is repeated: the run completes and its energies match the FP64
+    path's, which decides those pairs the same way (outside)."""
+    from ibisco_b200 import synth
+
+    spec = synth.lj_fluid(n=8000, rho=8.0, seed=21, nsteps=10, dmin=0.42)
+    L = spec.box[0]
+    k = np.arange(20)
+    spec.pos = np.stack(np.meshgrid(k, k, k, indexing="ij"), -1).reshape(-1, 3) * (L / 20) - L / 2
+    spec.control = dict(spec.control, cutoff=1.0, bead_cutoff=1.0)
+    d = str(tmp_path / "lattice")
+    synth.write_system(spec, d)
+    s = native.Setup(d)
+    out = {}
+    for prec in (native.IBG_PREC_FP32_FIXED, native.IBG_PREC_FP64_PLAIN):
+        g = native.System(s, prec)
+        g.set_state()
+        out[prec] = g.run(1, 3, observe=True)
+    for o32, o64 in zip(out[native.IBG_PREC_FP32_FIXED], out[native.IBG_PREC_FP64_PLAIN]):
+        assert abs(o32["V_NB1"] - o64["V_NB1"]) <= ENERGY_TOL * abs(o64["V_NB1"])
+
+
 @pytest.mark.parametrize("name", SYSTEMS)
 def test_forces_fp64_path_against_fp64_oracle(sysdir, name):
     d = sysdir(name)
