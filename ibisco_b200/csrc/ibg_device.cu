@@ -167,7 +167,7 @@ struct ibg_ctx {
   void* dargs = nullptr;  // device copy of af or ad
   int g_list[2] = {1, 1}, g_regrid[2] = {1, 1}, g_build[2] = {1, 1}, g_dist = 1;
   int nb_blocks_per_sm = 0;  // tuning: resident nonbonded blocks per SM (0: all that fit)
-  int nb_chunk = 0;          // tuning (FP32): work units per block chunk (0: per warp)
+  int nb_chunk = 0;          // tuning (FP32): 256ths of the units taken dynamically after the block ranges (0: all, per warp)
   int nb_rows = 16;          // tuning: list rows per nonbonded work unit (8 or 16)
   ObsD* ring = nullptr;
   int ring_cap = 0;

@@ -659,7 +659,7 @@ struct NBArgs {
   const R* tbin;
   const R* tinv; // 1/bin per table (FP32 force kernel)
   const int4* ptab;  // FP32 kernel: per type pair {first row, NDAT, 1/bin bits, 1 if a table}
-  int chunk;         // FP32 kernel: work units per block chunk (0: each warp takes units alone)
+  int chunk;         // FP32 kernel: 256ths of the units taken dynamically after the blocks' own ranges (0: all, per warp)
   int rows;          // list rows per work unit, a multiple of kEnergyRows
   // FP32 kernel: pairs whose r^2 lies within a relative 1e-6 of the cutoff
   // are left to k_nb_near, which decides them as the FP64 path does from the
@@ -1001,28 +1001,30 @@ __global__ void __launch_bounds__(256, B ? 4 : 5) k_nonbonded_f32(__grid_constan
     }
   };
   if (A.chunk > 0) {
-    // chunks of consecutive units (neighbouring slices) per block, handed out
-    // to its warps through a shared counter: the block's warps gather from
-    // one region of space and share it in L1
-    __shared__ int s_chunk, s_next;
-    const int nchunks = (nunits + A.chunk - 1) / A.chunk;
+    // each block a contiguous range of units (neighbouring slices), its warps
+    // taking them through a shared counter, so they gather from one region of
+    // space and share it in L1, with no barrier between them; the last
+    // chunk/256 of the units are taken from the global counter by whichever
+    // warps finish their block's range first
+    __shared__ int s_next;
+    if (threadIdx.x == 0) s_next = 0;
+    __syncthreads();
+    const int tail = (int)((long long)nunits * min(A.chunk, 256) / 256);
+    const int nstat = nunits - tail;
+    const int lo = (int)((long long)nstat * bk.b / bk.g), hi = (int)((long long)nstat * (bk.b + 1) / bk.g);
     for (;;) {
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        s_chunk = run ? (int)atomicAdd(&sc->work[A.work], 1u) : nchunks;
-        s_next = 0;
-      }
-      __syncthreads();
-      const int ch = s_chunk;
-      if (ch >= nchunks) break;
-      const int u0 = ch * A.chunk, u1 = min(nunits, u0 + A.chunk);
-      for (;;) {
-        int k = 0;
-        if (lane == 0) k = atomicAdd(&s_next, 1);
-        k = __shfl_sync(0xffffffffu, k, 0);
-        if (u0 + k >= u1) break;
-        unit(u0 + k);
-      }
+      int k = 0;
+      if (lane == 0) k = atomicAdd(&s_next, 1);
+      k = __shfl_sync(0xffffffffu, k, 0);
+      if (lo + k >= hi) break;
+      unit(lo + k);
+    }
+    for (;;) {
+      int u = 0;
+      if (lane == 0) u = nstat + (int)atomicAdd(&sc->work[A.work], 1u);
+      u = __shfl_sync(0xffffffffu, u, 0);
+      if (u >= nunits) break;
+      unit(u);
     }
   } else {
     for (;;) {

@@ -206,14 +206,15 @@ int ibg_set_list_rows(ibg_ctx* c, int rows);
 /* Launch tuning of the nonbonded kernel: nb_tables_smem stages the tables in
    shared memory per block (1) or reads them through L1 (0; the FP32 default,
    the FP64 path stages them); nb_blocks_per_sm limits the resident blocks per
-   SM (0: all that fit); nb_chunk (FP32 path): a block takes chunks of this
-   many consecutive work units (neighbouring slices) and shares them among its
-   warps, so they gather from one region of space (0: every warp takes units
-   alone); nb_rows: list rows per work unit, 8 or 16 (0: 16).  Forces and
-   trajectories do not depend on the tuning
-   (integer force sums); on the FP32 path nonbonded energies and virials are
-   summed per work unit before their exact fixed-point sum, so they do not
-   depend on it either.  Set it before a batch is made of the context.
+   SM (0: all that fit); nb_chunk (FP32 path): each block works through its
+   own contiguous range of work units (neighbouring slices), so its warps
+   gather from one region of space, and the last nb_chunk/256 of the units are
+   taken dynamically by whichever warps finish first (0: every warp takes
+   units alone, dynamically); nb_rows: list rows per work unit, 8 or 16 (0:
+   16).  Forces and trajectories do not depend on the tuning (integer force
+   sums); on the FP32 path nonbonded energies and virials are summed in groups
+   of 8 list rows before their exact fixed-point sum, so they do not depend on
+   it either.  Set it before a batch is made of the context.
    ibg_autotune: times each candidate tuning on the context's current lists
    (reps launches each, CUDA events; with an L2 flush set by ibg_set_l2_flush,
    each launch starts from a flushed L2, as a timed step does), keeps the
