@@ -163,16 +163,20 @@ __global__ void k_positions(__grid_constant__ const PosArgs a0, const PosArgs* c
   }
   R b[3], bi[3], b2[3];
   box_of<R>(sc, b, bi, b2);
-  // sd: the position in FP64 for the fixed-point copy (FP32 path)
+  const double boxinv[3] = {sc->boxinv[0], sc->boxinv[1], sc->boxinv[2]};
+  // sd: the position in FP64 for the fixed-point copy (FP32 path).  The slot
+  // and label are loaded before the first store (the arrays may alias as far
+  // as the compiler knows, and a load after a store would wait for it).
   auto store = [&](int i, const R* s, const double* sd) {
+    const int g = a.gslot[i];
+    const int tb = a.tbits[i];
     R r[3] = {s[0], s[1], s[2]};
     fold3<R>(r, b2);
-    const int g = a.gslot[i];
     PT p;
     p.x = r[0]; p.y = r[1]; p.z = r[2];
-    p.w = Prec<R>::tbits(a.tbits[i]);
+    p.w = Prec<R>::tbits(tb);
     ((PT*)a.pos4[g & 1])[g >> 1] = p;
-    if (a.posq[g & 1]) a.posq[g & 1][g >> 1] = box_fraction(sd, sc->boxinv, a.tbits[i]);
+    if (a.posq[g & 1]) a.posq[g & 1][g >> 1] = box_fraction(sd, boxinv, tb);
   };
   for (int i = bk.b * blockDim.x + threadIdx.x; i < a.natoms; i += bk.g * blockDim.x) {
     R s[3];
@@ -1188,21 +1192,28 @@ __global__ void k_nb_collect(__grid_constant__ const CollectArgs<R> C0, const Co
     const int a = C.sorted[s];
     const int gi = C.idx[a];
     if (explicit_step) {
+      // all three loads before the first store (the arrays may alias as far
+      // as the compiler knows)
+      typename P::acc_t v[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) v[c] = C.fsort[3 * (size_t)s + c];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        typename P::acc_t v = C.fsort[3 * (size_t)s + c];
-        C.fnb[3 * (size_t)gi + c] = v;
-        if (C.mts) C.mtsf[((size_t)(m - 1) * C.n + a) * 3 + c] = v;
+        C.fnb[3 * (size_t)gi + c] = v[c];
+        if (C.mts) C.mtsf[((size_t)(m - 1) * C.n + a) * 3 + c] = v[c];
         C.fsort[3 * (size_t)s + c] = 0;
       }
     } else {
       const double coef = (double)(m - 3) * 0.5;
+      double f3[3], f1[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        double f3 = P::get(C.mtsf[((size_t)2 * C.n + a) * 3 + c]);
-        double f1 = P::get(C.mtsf[((size_t)0 * C.n + a) * 3 + c]);
-        C.fnb[3 * (size_t)gi + c] = (typename P::acc_t)P::from_double(f3 + coef * (f3 - f1), &sc->err);
+        f3[c] = P::get(C.mtsf[((size_t)2 * C.n + a) * 3 + c]);
+        f1[c] = P::get(C.mtsf[((size_t)0 * C.n + a) * 3 + c]);
       }
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        C.fnb[3 * (size_t)gi + c] = (typename P::acc_t)P::from_double(f3[c] + coef * (f3[c] - f1[c]), &sc->err);
     }
   }
 }
@@ -1587,15 +1598,26 @@ __global__ void __launch_bounds__(256) k_move(__grid_constant__ const MoveArgs<R
   const double lam0 = sc->lam[0], lam1 = sc->lam[1];
   const int nrun = sc->skip ? 0 : M.natoms;
   for (int i = bk.b * blockDim.x + threadIdx.x; i < nrun; i += bk.g * blockDim.x) {
+    // every load of the particle is issued before its first store: the
+    // arrays may alias as far as the compiler knows, so a store between two
+    // loads would make each wait for the one before
     double s[3], v[3], fb[3], f[3];
+    typename P::acc_t qb[3], qn[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       s[c] = M.S[3 * (size_t)i + c];
       v[c] = M.V[3 * (size_t)i + c];
-      const typename P::acc_t qb = M.fb[3 * (size_t)i + c], qn = M.fnb[3 * (size_t)i + c];
-      fb[c] = P::get(qb);
-      f[c] = P::get(qn) + fb[c];
-      M.fnb[3 * (size_t)i + c] = qn + qb;
+      qb[c] = M.fb[3 * (size_t)i + c];
+      qn[c] = M.fnb[3 * (size_t)i + c];
+    }
+    int tb = 0;
+    double m = 0.0, im = 0.0;
+    if (M.update) { tb = M.tbits[i]; m = M.mass[i]; im = M.invmass[i]; }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      fb[c] = P::get(qb[c]);
+      f[c] = P::get(qn[c]) + fb[c];
+      M.fnb[3 * (size_t)i + c] = qn[c] + qb[c];
       M.fb[3 * (size_t)i + c] = 0;
     }
     acc[12] += fb[0] * s[0];
@@ -1605,9 +1627,8 @@ __global__ void __launch_bounds__(256) k_move(__grid_constant__ const MoveArgs<R
     acc[16] += fb[2] * s[0];
     acc[17] += fb[2] * s[1];
     if (!M.update) continue;
-    const int cls = (M.tbits[i] >> 16) == 2 ? 1 : 0;
+    const int cls = (tb >> 16) == 2 ? 1 : 0;
     const double lam = cls ? lam1 : lam0;
-    const double m = M.mass[i], im = M.invmass[i];
     double vt[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
