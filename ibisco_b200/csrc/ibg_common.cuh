@@ -83,6 +83,14 @@ struct BlockMap {
 struct Blk {
   int sys, b, g;
 };
+
+// Programmatic dependent launch.  A kernel launched with programmatic stream
+// serialization may start while the kernel before it in the stream still
+// runs; pdl_wait() returns once that kernel has completed and its writes are
+// visible (at once when the launch was an ordinary one).  pdl_trigger() lets
+// the next kernel's launch begin before this one ends.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 template <bool B>
 __device__ __forceinline__ Blk blk(const BlockMap& m) {
   if (!B) return Blk{0, (int)blockIdx.x, (int)gridDim.x};

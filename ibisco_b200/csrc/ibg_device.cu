@@ -182,6 +182,9 @@ struct ibg_ctx {
   long long launches_per_variant[32] = {0};
   // timing: stage events (timing mode, direct launches) and whole-run events
   bool timing = false;
+  // programmatic dependent launches in the step (off while the autotuner
+  // times single launches between memsets and events)
+  bool pdl = true;
   double stage_ms[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   std::vector<std::pair<cudaEvent_t, int>> marks;  // event, stage that starts there
   cudaEvent_t run_ev[2] = {nullptr, nullptr};
@@ -577,20 +580,39 @@ void nb_configure(ibg_ctx* c, DevList& L) {
   L.grid_nb = (int)std::max<long long>(1, std::min<long long>((long long)c->nsm * per, (units + 7) / 8));
 }
 
+// A launch on the context's stream with programmatic stream serialization:
+// the kernel may start while the one before it still runs and waits for it
+// in pdl_wait(), so that its launch overlaps the other's tail.  Kernels
+// launched this way call pdl_wait() before anything else.  Timing mode, which
+// separates the stages with events, launches them in the ordinary way.
+template <typename... KArgs, typename... Args>
+void launch_pdl(ibg_ctx* c, void (*k)(KArgs...), int grid, int block, size_t smem, const Args&... a) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = c->st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = (c->pdl && !c->timing) ? 1 : 0;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  CK(cudaLaunchKernelEx(&cfg, k, a...));
+  ++c->launches;
+}
+
 template <typename R>
 void enq_nonbonded(ibg_ctx* c, DevList& L) {
-  nb_kernel<R, false>(L.use_smem, L.T)<<<L.grid_nb, 256, nb_smem(c, L), c->st>>>(args<R>(c).nb[L.which], nullptr, kOne);
-  ++c->launches;
-  if (c->prec == IBG_PREC_FP32_FIXED) {
-    k_nb_near<false><<<1, 256, 0, c->st>>>(args<float>(c).nb[L.which], nullptr, kOne);
-    ++c->launches;
-  }
+  launch_pdl(c, nb_kernel<R, false>(L.use_smem, L.T), L.grid_nb, 256, nb_smem(c, L), args<R>(c).nb[L.which],
+             (const NBArgs<R>* const*)nullptr, kOne);
+  if (c->prec == IBG_PREC_FP32_FIXED)
+    launch_pdl(c, k_nb_near<false>, 1, 256, 0, args<float>(c).nb[L.which], (const NBArgs<float>* const*)nullptr, kOne);
 }
 
 template <typename R>
 void enq_collect(ibg_ctx* c, DevList& L) {
-  k_nb_collect<R, false><<<c->g_list[L.which], 256, 0, c->st>>>(args<R>(c).col[L.which], nullptr, kOne);
-  ++c->launches;
+  launch_pdl(c, k_nb_collect<R, false>, c->g_list[L.which], 256, 0, args<R>(c).col[L.which],
+             (const CollectArgs<R>* const*)nullptr, kOne);
 }
 
 template <typename R>
@@ -618,8 +640,7 @@ template <typename R>
 void enq_finalize(ibg_ctx* c, int move) {
   FinalArgs F = args<R>(c).fin;
   F.move = move;
-  k_finalize<false><<<1, 1024, 0, c->st>>>(F, nullptr, kOne);
-  ++c->launches;
+  launch_pdl(c, k_finalize<false>, 1, 1024, 0, F, (const FinalArgs* const*)nullptr, kOne);
 }
 
 // One loop body.  In graph mode the bonded branch (bonded terms and their VS
@@ -901,6 +922,13 @@ int ibg_autotune(ibg_ctx* c, int reps, ibg_tuning* best, ibg_tuning* cand_out, d
   int win = -1;
   double win_us = 0.0;
   std::vector<cudaEvent_t> ev(2 * (size_t)reps, nullptr);
+  // the trial launches run in the ordinary way, each on its own between the
+  // memsets and events; programmatic launches are restored on every return
+  struct PdlOff {
+    ibg_ctx* c;
+    ~PdlOff() { c->pdl = true; }
+  } pdl_off{c};
+  c->pdl = false;
   auto drop_events = [&] {
     for (auto& e : ev)
       if (e) {

@@ -142,6 +142,7 @@ template <typename R, bool B>
 __global__ void k_positions(__grid_constant__ const PosArgs a0, const PosArgs* const* tab, const BlockMap bm,
                             int begin) {
   using PT = typename Prec<R>::pos_t;
+  pdl_trigger();
   const Blk bk = blk<B>(bm);
   const PosArgs& a = B ? *tab[bk.sys] : a0;
   Scalars* sc = a.sc;
@@ -704,6 +705,8 @@ template <typename R, bool SMEM, int T, bool B>
 __global__ void __launch_bounds__(256, 4) k_nonbonded(__grid_constant__ const NBArgs<R> A0, const NBArgs<R>* const* tab,
                                                       const BlockMap bm) {
   using P = Prec<R>;
+  pdl_wait();
+  pdl_trigger();
   const Blk bk = blk<B>(bm);
   __shared__ NBArgs<R> s_args;
   if (B) stage_args(&s_args, tab[bk.sys]);
@@ -871,6 +874,8 @@ template <bool SMEM, int T, bool B>
 __global__ void __launch_bounds__(256, B ? 4 : 5) k_nonbonded_f32(__grid_constant__ const NBArgs<float> A0,
                                                           const NBArgs<float>* const* tab, const BlockMap bm) {
   constexpr int PS = 32 / T;
+  pdl_wait();
+  pdl_trigger();
   const Blk bk = blk<B>(bm);
   __shared__ NBArgs<float> s_args;
   if (B) stage_args(&s_args, tab[bk.sys]);
@@ -1089,6 +1094,8 @@ __device__ bool inside_as_fp64(const NBArgs<float>& A, const Scalars* sc, int gi
 template <bool B>
 __global__ void __launch_bounds__(256) k_nb_near(__grid_constant__ const NBArgs<float> A0,
                                                  const NBArgs<float>* const* tab, const BlockMap bm) {
+  pdl_wait();
+  pdl_trigger();
   const Blk bk = blk<B>(bm);
   const NBArgs<float>& A = B ? *tab[bk.sys] : A0;
   Scalars* sc = A.sc;
@@ -1182,6 +1189,7 @@ template <typename R, bool B>
 __global__ void k_nb_collect(__grid_constant__ const CollectArgs<R> C0, const CollectArgs<R>* const* tab,
                              const BlockMap bm) {
   using P = Prec<R>;
+  pdl_wait();
   const Blk bk = blk<B>(bm);
   const CollectArgs<R>& C = B ? *tab[bk.sys] : C0;
   Scalars* sc = C.sc;
@@ -1588,6 +1596,7 @@ template <typename R, bool B>
 __global__ void __launch_bounds__(256) k_move(__grid_constant__ const MoveArgs<R> M0, const MoveArgs<R>* const* tab,
                                               const BlockMap bm) {
   using P = Prec<R>;
+  pdl_trigger();
   const Blk bk = blk<B>(bm);
   const MoveArgs<R>& M = B ? *tab[bk.sys] : M0;
   Scalars* sc = M.sc;
@@ -1763,6 +1772,7 @@ __device__ double wsum(const double* p, int g) {
 // nonbonded accumulators are read and cleared for the next step.
 template <bool B>
 __global__ void k_finalize(__grid_constant__ const FinalArgs F0, const FinalArgs* const* tab, const BlockMap bm) {
+  pdl_wait();
   const Blk bk = blk<B>(bm);
   const FinalArgs& F = B ? *tab[bk.sys] : F0;
   Scalars* sc = F.sc;
