@@ -476,6 +476,27 @@ void refresh_args(ibg_ctx* c) {
 
 const BlockMap kOne{nullptr, nullptr};
 
+// A launch on the context's stream with programmatic stream serialization:
+// the kernel may start while the one before it still runs and waits for it
+// in pdl_wait(), so that its launch overlaps the other's tail.  Kernels
+// launched this way call pdl_wait() before anything else.  Timing mode, which
+// separates the stages with events, launches them in the ordinary way.
+template <typename... KArgs, typename... Args>
+void launch_pdl(ibg_ctx* c, void (*k)(KArgs...), int grid, int block, size_t smem, const Args&... a) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = c->st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = (c->pdl && !c->timing) ? 1 : 0;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  CK(cudaLaunchKernelEx(&cfg, k, a...));
+  ++c->launches;
+}
+
 template <typename R>
 void enq_positions(ibg_ctx* c, int begin = 0) {
   k_positions<R, false><<<c->g_pos, 256, 0, c->st>>>(args<R>(c).pos, nullptr, kOne, begin);
@@ -488,21 +509,24 @@ void enq_rebuild(ibg_ctx* c, DevList& L, int always) {
   if (!L.present) return;
   const ListArgs& a = args<R>(c).list[L.which];
   const int w = L.which, gn = c->g_list[w];
+  // the first launch may follow a memset (ibg_set_state): an ordinary one;
+  // the rest follow a kernel of the chain
+  using LA = const ListArgs* const*;
   k_regrid<R, false><<<c->g_regrid[w], 256, 0, c->st>>>(a, nullptr, kOne, always);
-  k_cell_assign<R, false><<<gn, 256, 0, c->st>>>(a, nullptr, kOne, always);
-  k_scan_cells<false><<<1, 1024, 0, c->st>>>(a, nullptr, kOne, always);
-  k_cell_fill<false><<<gn, 256, 0, c->st>>>(a, nullptr, kOne, always);
-  k_cell_rank<false><<<gn, 256, 0, c->st>>>(a, nullptr, kOne, always);
-  k_reslot<R, false><<<gn, 256, 0, c->st>>>(a, nullptr, kOne, always);
-  k_slot_of<R, false><<<gn, 256, 0, c->st>>>(a, nullptr, kOne, always);
+  ++c->launches;
+  launch_pdl(c, k_cell_assign<R, false>, gn, 256, 0, a, (LA)nullptr, kOne, always);
+  launch_pdl(c, k_scan_cells<false>, 1, 1024, 0, a, (LA)nullptr, kOne, always);
+  launch_pdl(c, k_cell_fill<false>, gn, 256, 0, a, (LA)nullptr, kOne, always);
+  launch_pdl(c, k_cell_rank<false>, gn, 256, 0, a, (LA)nullptr, kOne, always);
+  launch_pdl(c, k_reslot<R, false>, gn, 256, 0, a, (LA)nullptr, kOne, always);
+  launch_pdl(c, k_slot_of<R, false>, gn, 256, 0, a, (LA)nullptr, kOne, always);
   const int gl = c->g_build[w];
   switch (L.T) {
-    case 1: k_list_build<R, 1, false><<<gl, 256, 0, c->st>>>(a, nullptr, kOne, always); break;
-    case 2: k_list_build<R, 2, false><<<gl, 256, 0, c->st>>>(a, nullptr, kOne, always); break;
-    case 4: k_list_build<R, 4, false><<<gl, 256, 0, c->st>>>(a, nullptr, kOne, always); break;
-    default: k_list_build<R, 8, false><<<gl, 256, 0, c->st>>>(a, nullptr, kOne, always); break;
+    case 1: launch_pdl(c, k_list_build<R, 1, false>, gl, 256, 0, a, (LA)nullptr, kOne, always); break;
+    case 2: launch_pdl(c, k_list_build<R, 2, false>, gl, 256, 0, a, (LA)nullptr, kOne, always); break;
+    case 4: launch_pdl(c, k_list_build<R, 4, false>, gl, 256, 0, a, (LA)nullptr, kOne, always); break;
+    default: launch_pdl(c, k_list_build<R, 8, false>, gl, 256, 0, a, (LA)nullptr, kOne, always); break;
   }
-  c->launches += 8;
 }
 
 template <typename R, bool B>
@@ -580,27 +604,6 @@ void nb_configure(ibg_ctx* c, DevList& L) {
   L.grid_nb = (int)std::max<long long>(1, std::min<long long>((long long)c->nsm * per, (units + 7) / 8));
 }
 
-// A launch on the context's stream with programmatic stream serialization:
-// the kernel may start while the one before it still runs and waits for it
-// in pdl_wait(), so that its launch overlaps the other's tail.  Kernels
-// launched this way call pdl_wait() before anything else.  Timing mode, which
-// separates the stages with events, launches them in the ordinary way.
-template <typename... KArgs, typename... Args>
-void launch_pdl(ibg_ctx* c, void (*k)(KArgs...), int grid, int block, size_t smem, const Args&... a) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)grid);
-  cfg.blockDim = dim3((unsigned)block);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = c->st;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = (c->pdl && !c->timing) ? 1 : 0;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  CK(cudaLaunchKernelEx(&cfg, k, a...));
-  ++c->launches;
-}
-
 template <typename R>
 void enq_nonbonded(ibg_ctx* c, DevList& L) {
   launch_pdl(c, nb_kernel<R, false>(L.use_smem, L.T), L.grid_nb, 256, nb_smem(c, L), args<R>(c).nb[L.which],
@@ -618,8 +621,8 @@ void enq_collect(ibg_ctx* c, DevList& L) {
 template <typename R>
 void enq_distribute(ibg_ctx* c, int which) {
   if (c->nvirta == 0) return;
-  k_distribute<R, false><<<c->g_dist, 256, 0, c->st>>>(args<R>(c).dist, nullptr, kOne, which);
-  ++c->launches;
+  launch_pdl(c, k_distribute<R, false>, c->g_dist, 256, 0, args<R>(c).dist, (const DistArgs<R>* const*)nullptr, kOne,
+             which);
 }
 
 template <typename R>
@@ -632,6 +635,7 @@ template <typename R>
 void enq_move(ibg_ctx* c, int update) {
   MoveArgs<R> M = args<R>(c).move;
   M.update = update;
+  // an ordinary launch: it follows the join with the bonded branch
   k_move<R, false><<<c->g_mv, 256, 0, c->st>>>(M, nullptr, kOne);
   ++c->launches;
 }

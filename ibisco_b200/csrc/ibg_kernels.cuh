@@ -277,6 +277,8 @@ struct ListArgs {
 // dimension = INT(BOX/RLIST).  The grid also clears the cell counters.
 template <typename R, bool B>
 __global__ void k_regrid(__grid_constant__ const ListArgs L0, const ListArgs* const* tab, const BlockMap bm, int always) {
+  pdl_wait();
+  pdl_trigger();
   const Blk bk = blk<B>(bm);
   const ListArgs& L = B ? *tab[bk.sys] : L0;
   Scalars* sc = L.sc;
@@ -301,6 +303,8 @@ __global__ void k_regrid(__grid_constant__ const ListArgs L0, const ListArgs* co
 // rounding) would address a cell outside the grid; it is clamped and counted.
 template <typename R, bool B>
 __global__ void k_cell_assign(__grid_constant__ const ListArgs L0, const ListArgs* const* tab, const BlockMap bm, int always) {
+  pdl_wait();
+  pdl_trigger();
   using PT = typename Prec<R>::pos_t;
   const Blk bk = blk<B>(bm);
   const ListArgs& L = B ? *tab[bk.sys] : L0;
@@ -332,6 +336,8 @@ __global__ void k_cell_assign(__grid_constant__ const ListArgs L0, const ListArg
 // cell_cap + 1 entries); clears the fill counters.
 template <bool B>
 __global__ void k_scan_cells(__grid_constant__ const ListArgs L0, const ListArgs* const* tab, const BlockMap bm, int always) {
+  pdl_wait();
+  pdl_trigger();
   const Blk bk = blk<B>(bm);
   const ListArgs& L = B ? *tab[bk.sys] : L0;
   Scalars* sc = L.sc;
@@ -371,6 +377,8 @@ __global__ void k_scan_cells(__grid_constant__ const ListArgs L0, const ListArgs
 
 template <bool B>
 __global__ void k_cell_fill(__grid_constant__ const ListArgs L0, const ListArgs* const* tab, const BlockMap bm, int always) {
+  pdl_wait();
+  pdl_trigger();
   const Blk bk = blk<B>(bm);
   const ListArgs& L = B ? *tab[bk.sys] : L0;
   Scalars* sc = L.sc;
@@ -388,6 +396,8 @@ __global__ void k_cell_fill(__grid_constant__ const ListArgs L0, const ListArgs*
 // (atomics); here each entry finds its rank among its cell's entries.
 template <bool B>
 __global__ void k_cell_rank(__grid_constant__ const ListArgs L0, const ListArgs* const* tab, const BlockMap bm, int always) {
+  pdl_wait();
+  pdl_trigger();
   const Blk bk = blk<B>(bm);
   const ListArgs& L = B ? *tab[bk.sys] : L0;
   Scalars* sc = L.sc;
@@ -407,6 +417,8 @@ __global__ void k_cell_rank(__grid_constant__ const ListArgs L0, const ListArgs*
 // the scratch k_cell_rank wrote; writes the new order to sorted.
 template <typename R, bool B>
 __global__ void k_reslot(__grid_constant__ const ListArgs L0, const ListArgs* const* tab, const BlockMap bm, int always) {
+  pdl_wait();
+  pdl_trigger();
   using PT = typename Prec<R>::pos_t;
   const Blk bk = blk<B>(bm);
   const ListArgs& L = B ? *tab[bk.sys] : L0;
@@ -425,6 +437,8 @@ __global__ void k_reslot(__grid_constant__ const ListArgs L0, const ListArgs* co
 // k_reslot).
 template <typename R, bool B>
 __global__ void k_slot_of(__grid_constant__ const ListArgs L0, const ListArgs* const* tab, const BlockMap bm, int always) {
+  pdl_wait();
+  pdl_trigger();
   using PT = typename Prec<R>::pos_t;
   const Blk bk = blk<B>(bm);
   const ListArgs& L = B ? *tab[bk.sys] : L0;
@@ -473,6 +487,8 @@ struct ListStage {
 template <typename R, int T, bool B>
 __global__ void __launch_bounds__(256, 4) k_list_build(__grid_constant__ const ListArgs L0, const ListArgs* const* tab,
                                                        const BlockMap bm, int always) {
+  pdl_wait();
+  pdl_trigger();
   using PT = typename Prec<R>::pos_t;
   constexpr int kCap = ListStage<R>::cap;
   constexpr int kWarps = 8;  // blockDim.x = 256
@@ -1241,6 +1257,8 @@ struct DistArgs {
 template <typename R, bool B>
 __global__ void k_distribute(__grid_constant__ const DistArgs<R> D0, const DistArgs<R>* const* tab, const BlockMap bm,
                              int which) {
+  pdl_wait();
+  pdl_trigger();
   using P = Prec<R>;
   const Blk bk = blk<B>(bm);
   const DistArgs<R>& D = B ? *tab[bk.sys] : D0;
@@ -1596,6 +1614,7 @@ template <typename R, bool B>
 __global__ void __launch_bounds__(256) k_move(__grid_constant__ const MoveArgs<R> M0, const MoveArgs<R>* const* tab,
                                               const BlockMap bm) {
   using P = Prec<R>;
+  pdl_wait();
   pdl_trigger();
   const Blk bk = blk<B>(bm);
   const MoveArgs<R>& M = B ? *tab[bk.sys] : M0;
