@@ -482,18 +482,23 @@ const BlockMap kOne{nullptr, nullptr};
 // launched this way call pdl_wait() before anything else.  Timing mode, which
 // separates the stages with events, launches them in the ordinary way.
 template <typename... KArgs, typename... Args>
-void launch_pdl(ibg_ctx* c, void (*k)(KArgs...), int grid, int block, size_t smem, const Args&... a) {
+void launch_on(cudaStream_t st, bool pdl, void (*k)(KArgs...), int grid, int block, size_t smem, const Args&... a) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)grid);
   cfg.blockDim = dim3((unsigned)block);
   cfg.dynamicSmemBytes = smem;
-  cfg.stream = c->st;
+  cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = (c->pdl && !c->timing) ? 1 : 0;
+  at[0].val.programmaticStreamSerializationAllowed = pdl ? 1 : 0;
   cfg.attrs = at;
   cfg.numAttrs = 1;
   CK(cudaLaunchKernelEx(&cfg, k, a...));
+}
+
+template <typename... KArgs, typename... Args>
+void launch_pdl(ibg_ctx* c, void (*k)(KArgs...), int grid, int block, size_t smem, const Args&... a) {
+  launch_on(c->st, c->pdl && !c->timing, k, grid, block, smem, a...);
   ++c->launches;
 }
 
@@ -1786,9 +1791,11 @@ void batch_enqueue(ibg_batch* b, unsigned v) {
   k_bonded<R, true><<<b->m_bond.grid, 256, 0, st2>>>(BondedArgs<R>{}, (const BondedArgs<R>* const*)b->t_bond,
                                                      b->m_bond.m());
   ++n;
+  // launches that follow a kernel of the same stream start by programmatic
+  // dependent launch, as in one system's step
+  using DA = const DistArgs<R>* const*;
   if (b->any_vs) {
-    k_distribute<R, true><<<b->m_dist.grid, 256, 0, st2>>>(DistArgs<R>{}, (const DistArgs<R>* const*)b->t_dist,
-                                                           b->m_dist.m(), 1);
+    launch_on(st2, true, k_distribute<R, true>, b->m_dist.grid, 256, 0, DistArgs<R>{}, (DA)b->t_dist, b->m_dist.m(), 1);
     ++n;
   }
   CK(cudaEventRecord(b->fork_ev[1], st2));
@@ -1799,19 +1806,20 @@ void batch_enqueue(ibg_batch* b, unsigned v) {
       const ListArgs* const* t = (const ListArgs* const*)b->t_list[w];
       const BMap& ml = b->m_list[w];
       k_regrid<R, true><<<b->m_regrid[w].grid, 256, 0, st>>>(ListArgs{}, t, b->m_regrid[w].m(), 0);
-      k_cell_assign<R, true><<<ml.grid, 256, 0, st>>>(ListArgs{}, t, ml.m(), 0);
-      k_scan_cells<true><<<b->m_scan[w].grid, 1024, 0, st>>>(ListArgs{}, t, b->m_scan[w].m(), 0);
-      k_cell_fill<true><<<ml.grid, 256, 0, st>>>(ListArgs{}, t, ml.m(), 0);
-      k_cell_rank<true><<<ml.grid, 256, 0, st>>>(ListArgs{}, t, ml.m(), 0);
-      k_reslot<R, true><<<ml.grid, 256, 0, st>>>(ListArgs{}, t, ml.m(), 0);
-      k_slot_of<R, true><<<ml.grid, 256, 0, st>>>(ListArgs{}, t, ml.m(), 0);
+      launch_on(st, true, k_cell_assign<R, true>, ml.grid, 256, 0, ListArgs{}, t, ml.m(), 0);
+      launch_on(st, true, k_scan_cells<true>, b->m_scan[w].grid, 1024, 0, ListArgs{}, t, b->m_scan[w].m(), 0);
+      launch_on(st, true, k_cell_fill<true>, ml.grid, 256, 0, ListArgs{}, t, ml.m(), 0);
+      launch_on(st, true, k_cell_rank<true>, ml.grid, 256, 0, ListArgs{}, t, ml.m(), 0);
+      launch_on(st, true, k_reslot<R, true>, ml.grid, 256, 0, ListArgs{}, t, ml.m(), 0);
+      launch_on(st, true, k_slot_of<R, true>, ml.grid, 256, 0, ListArgs{}, t, ml.m(), 0);
       n += 7;
       for (const NBGroup& grp : b->lb[w]) {
+        const BlockMap bm = grp.map.m();
         switch (grp.T) {
-          case 1: k_list_build<R, 1, true><<<grp.map.grid, 256, 0, st>>>(ListArgs{}, t, grp.map.m(), 0); break;
-          case 2: k_list_build<R, 2, true><<<grp.map.grid, 256, 0, st>>>(ListArgs{}, t, grp.map.m(), 0); break;
-          case 4: k_list_build<R, 4, true><<<grp.map.grid, 256, 0, st>>>(ListArgs{}, t, grp.map.m(), 0); break;
-          default: k_list_build<R, 8, true><<<grp.map.grid, 256, 0, st>>>(ListArgs{}, t, grp.map.m(), 0); break;
+          case 1: launch_on(st, true, k_list_build<R, 1, true>, grp.map.grid, 256, 0, ListArgs{}, t, bm, 0); break;
+          case 2: launch_on(st, true, k_list_build<R, 2, true>, grp.map.grid, 256, 0, ListArgs{}, t, bm, 0); break;
+          case 4: launch_on(st, true, k_list_build<R, 4, true>, grp.map.grid, 256, 0, ListArgs{}, t, bm, 0); break;
+          default: launch_on(st, true, k_list_build<R, 8, true>, grp.map.grid, 256, 0, ListArgs{}, t, bm, 0); break;
         }
         ++n;
       }
@@ -1821,25 +1829,24 @@ void batch_enqueue(ibg_batch* b, unsigned v) {
   // each list (one block per system with the list, as the cell scan)
   for (int w : {1, 0}) {
     for (const NBGroup& grp : b->nb[w]) {
-      nb_kernel<R, true>(grp.smem, grp.T)<<<grp.map.grid, 256, grp.sm, st>>>(
-          NBArgs<R>{}, (const NBArgs<R>* const*)b->t_nb[w], grp.map.m());
+      launch_on(st, true, nb_kernel<R, true>(grp.smem, grp.T), grp.map.grid, 256, grp.sm, NBArgs<R>{},
+                (const NBArgs<R>* const*)b->t_nb[w], grp.map.m());
       ++n;
     }
     if (b->prec == IBG_PREC_FP32_FIXED && b->any_list[w]) {
-      k_nb_near<true><<<b->m_scan[w].grid, 256, 0, st>>>(NBArgs<float>{}, (const NBArgs<float>* const*)b->t_nb[w],
-                                                         b->m_scan[w].m());
+      launch_on(st, true, k_nb_near<true>, b->m_scan[w].grid, 256, 0, NBArgs<float>{},
+                (const NBArgs<float>* const*)b->t_nb[w], b->m_scan[w].m());
       ++n;
     }
   }
   for (int w : {1, 0}) {
     if (!b->any_list[w]) continue;
-    k_nb_collect<R, true><<<b->m_list[w].grid, 256, 0, st>>>(CollectArgs<R>{}, (const CollectArgs<R>* const*)b->t_col[w],
-                                                            b->m_list[w].m());
+    launch_on(st, true, k_nb_collect<R, true>, b->m_list[w].grid, 256, 0, CollectArgs<R>{},
+              (const CollectArgs<R>* const*)b->t_col[w], b->m_list[w].m());
     ++n;
   }
   if (b->any_vs) {
-    k_distribute<R, true><<<b->m_dist.grid, 256, 0, st>>>(DistArgs<R>{}, (const DistArgs<R>* const*)b->t_dist,
-                                                          b->m_dist.m(), 0);
+    launch_on(st, true, k_distribute<R, true>, b->m_dist.grid, 256, 0, DistArgs<R>{}, (DA)b->t_dist, b->m_dist.m(), 0);
     ++n;
   }
   CK(cudaStreamWaitEvent(st, b->fork_ev[1], 0));
@@ -1850,7 +1857,8 @@ void batch_enqueue(ibg_batch* b, unsigned v) {
     k_mom_apply<true><<<b->m_move.grid, 256, 0, st>>>(MomArgs{}, (const MomArgs* const*)b->t_mom, b->m_move.m());
     n += 2;
   }
-  k_finalize<true><<<b->m_fin.grid, 1024, 0, st>>>(FinalArgs{}, (const FinalArgs* const*)b->t_fin, b->m_fin.m());
+  launch_on(st, true, k_finalize<true>, b->m_fin.grid, 1024, 0, FinalArgs{}, (const FinalArgs* const*)b->t_fin,
+            b->m_fin.m());
   ++n;
   if (v & BV_SCALE) {
     k_scale_positions<R, true><<<b->m_move.grid, 256, 0, st>>>(MoveArgs<R>{}, (const MoveArgs<R>* const*)b->t_move,
