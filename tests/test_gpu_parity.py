@@ -278,6 +278,24 @@ def test_too_few_cells_is_reported(sysdir, tmp_path):
     assert e.value.code == -6
 
 
+@pytest.mark.parametrize("name", ["melt", "mix5_mts", "mix_npt"])
+def test_programmatic_launches_change_no_trajectory(sysdir, name):
+    """A graph-replayed step starts each kernel of a stream by programmatic
+    dependent launch and runs the bonded branch on a second stream; timing
+    mode launches the same kernels in the ordinary way on one stream.  The
+    fixed-point sums make the two trajectories identical bit for bit, list
+    rebuilds included."""
+    d = sysdir(name)
+    _, a = make(d, native.IBG_PREC_FP32_FIXED)
+    _, b = make(d, native.IBG_PREC_FP32_FIXED)
+    b.set_timing(True)
+    oa, ob = a.run(1, 30, observe=True), b.run(1, 30, observe=True)
+    sa, sb = a.state64(), b.state64()
+    for k in ("sxyz", "vxyz", "fxyz"):
+        assert np.array_equal(sa[k], sb[k]), k
+    assert oa == ob
+
+
 def test_tuning_changes_no_trajectory(sysdir):
     """Forces are exact integer sums and FP32 energies are summed per work unit,
     so every launch tuning gives the same trajectory and observables;
