@@ -570,7 +570,7 @@ def main():
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--batch", type=int, default=8, help="systems in the batched leg (0 or 1: no batched leg)")
+    ap.add_argument("--batch", type=int, default=16, help="systems in the batched leg (0 or 1: no batched leg)")
     ap.add_argument("--serve-jobs", type=int, default=48, help="jobs of the served stream (0: no serving leg)")
     ap.add_argument("--tuning", default="", help="fixed nonbonded tuning 'tables_smem,blocks_per_sm,chunk[,rows]' "
                                                   "instead of the autotuner (for profiling)")
