@@ -476,11 +476,11 @@ void refresh_args(ibg_ctx* c) {
 
 const BlockMap kOne{nullptr, nullptr};
 
-// A launch on the context's stream with programmatic stream serialization:
-// the kernel may start while the one before it still runs and waits for it
-// in pdl_wait(), so that its launch overlaps the other's tail.  Kernels
-// launched this way call pdl_wait() before anything else.  Timing mode, which
-// separates the stages with events, launches them in the ordinary way.
+// A launch on stream st, with programmatic stream serialization when pdl is
+// set: the kernel may start while the kernel before it in the stream still
+// runs, and waits for it in pdl_wait(), so that its launch overlaps the
+// other's tail.  Kernels launched this way call pdl_wait() before anything
+// else.
 template <typename... KArgs, typename... Args>
 void launch_on(cudaStream_t st, bool pdl, void (*k)(KArgs...), int grid, int block, size_t smem, const Args&... a) {
   cudaLaunchConfig_t cfg = {};
@@ -496,6 +496,8 @@ void launch_on(cudaStream_t st, bool pdl, void (*k)(KArgs...), int grid, int blo
   CK(cudaLaunchKernelEx(&cfg, k, a...));
 }
 
+// The same on the context's stream.  Timing mode, which separates the stages
+// with events, and the autotuner's trial launches are ordinary launches.
 template <typename... KArgs, typename... Args>
 void launch_pdl(ibg_ctx* c, void (*k)(KArgs...), int grid, int block, size_t smem, const Args&... a) {
   launch_on(c->st, c->pdl && !c->timing, k, grid, block, smem, a...);
