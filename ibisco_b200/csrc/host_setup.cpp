@@ -541,6 +541,27 @@ void ftable(ibg_setup* s) {
   }
 }
 
+// ---------------------------------------------------------------- SCALEV.f90
+// Initial velocity rescale to TEMP_IN (SCALEV.f90:13-26), run at
+// main.F90:168-171 when initialize_velocities is Y.  The reference first
+// calls COMVEL (COMVEL.f90:17-79), whose draw from gfortran's RANDOM_NUMBER
+// cannot be reproduced; the coordinate file's velocities take its place.
+// Kinetic energy and factor in double over REAL*4 terms, velocities rounded
+// back to REAL*4, as the reference does.
+void scalev(ibg_setup* s) {
+  const ibg_desc& d = s->d;
+  double ek = 0.0;
+  for (int i = 0; i < d.natoms; ++i) {
+    const float* v = &s->vxyz[3 * (size_t)i];
+    const float sq = (v[0] * v[0] + v[1] * v[1]) + v[2] * v[2];
+    ek = ek + (double)(s->mass[s->itype[i] - 1] * sq);
+  }
+  ek = 0.5 * ek;
+  const double t = ek * (double)d.mktemp;
+  const double factor = (double)d.temp_in / t;
+  for (size_t k = 0; k < 3 * (size_t)d.natoms; ++k) s->vxyz[k] = (float)(std::sqrt(factor) * (double)s->vxyz[k]);
+}
+
 // ----------------------------------------------------------------- RDCOOR.f90
 bool coordinate(ibg_setup* s, const std::string& dir) {
   Records r;
@@ -840,6 +861,7 @@ bool read_all(ibg_setup* s, const std::string& dir) {
     d.numatoms = d.natoms; d.numbeads = 0; d.ncoarse = 0;
   }
   ftable(s);
+  if (s->restart == 1) scalev(s);  // main.F90:168-171
   d.mktemp_atom = 2.0f / (3.0f * (float)(d.numatoms - 1));  // main.F90:177-178
   d.mktemp_bead = 2.0f / (3.0f * (float)(d.numbeads - 1));
   if (!topology(s, dir)) return false;

@@ -633,6 +633,26 @@ inline void ftable(Setup& s) {
   }
 }
 
+// ---------------------------------------------------------------- SCALEV.f90
+// SCALEV.f90:13-26, called at main.F90:168-171 when initialize_velocities is
+// Y.  The reference calls COMVEL (COMVEL.f90:17-79) first, which draws new
+// velocities from gfortran's RANDOM_NUMBER; that draw is not reproducible, so
+// the coordinate file's velocities stand in for it.  EK and FACTOR are REAL*8,
+// each term MASS*(vx**2+vy**2+vz**2) REAL*4; the scaled velocity is rounded
+// back to REAL*4.
+inline void scalev(Setup& s) {
+  double ek = 0.0;
+  for (int i = 1; i <= s.NATOMS; ++i) {
+    const float* v = &s.VXYZ[3 * (size_t)(i - 1)];
+    const float sq = (v[0] * v[0] + v[1] * v[1]) + v[2] * v[2];
+    ek = ek + (double)(s.MASS[s.ITYPE[i]] * sq);
+  }
+  ek = 0.5 * ek;
+  const double t = ek * (double)s.MKTEMP;
+  const double factor = (double)s.TEMP_IN / t;
+  for (size_t k = 0; k < 3 * (size_t)s.NATOMS; ++k) s.VXYZ[k] = (float)(std::sqrt(factor) * (double)s.VXYZ[k]);
+}
+
 // ---------------------------------------------------------------- SETLIS.f90
 inline bool setlis(Setup& s) {
   const int NI = s.NITEMS, NA_ = s.NATOMS, NT = s.NTYPE;
@@ -804,6 +824,7 @@ inline bool setup_from_dir(Setup& s, const std::string& dir) {
   }
   if (!make_lists(s)) return false;
   ftable(s);
+  if (s.RESTART == 1) scalev(s);  // main.F90:168-171
   // main.F90:177-178
   s.MKTEMP_ATOM = 2.0f / (3.0f * (float)(s.NUMATOMS - 1));
   s.MKTEMP_BEAD = 2.0f / (3.0f * (float)(s.NUMBEADS - 1));

@@ -10,9 +10,9 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 # The reference's own test fixtures (testsuite/atomisticPA, testsuite/hybridPA)
-# are read from the reference tree when it is present; those tests are skipped
-# elsewhere.
-REFERENCE_DIR = os.environ.get("IBISCO_REFERENCE_DIR", "/root/reference")
+# travel with the tests as golden/reference_fixtures.tar.xz (made by
+# golden/pack_reference_fixtures.py), so they run wherever the tests run.
+FIXTURE_ARCHIVE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_fixtures.tar.xz")
 
 
 def pytest_configure(config):
@@ -20,22 +20,28 @@ def pytest_configure(config):
 
 
 def reference_fixture(tmp_root: str, name: str) -> str:
-    """Copy a reference test fixture and add the `mts 0` key that the current
+    """Unpack a reference test fixture and add the `mts 0` key that the current
     RDCONTROL.f90:485-497 requires (the fixtures predate it)."""
-    src = os.path.join(REFERENCE_DIR, "testsuite", name)
-    if not os.path.isdir(src):
-        pytest.skip("reference test fixtures not available")
+    import tarfile
+
     dst = os.path.join(tmp_root, name)
     if not os.path.isdir(dst):
-        shutil.copytree(src, dst)
-        for root, _, files in os.walk(dst):
-            for f in files:
-                os.chmod(os.path.join(root, f), 0o644)
+        with tarfile.open(FIXTURE_ARCHIVE) as tar:
+            members = [m for m in tar.getmembers() if m.name.startswith(name + "/") and m.isfile()]
+            if not members:
+                pytest.skip(f"fixture {name} not in the archive")
+            tar.extractall(tmp_root, members=members, filter="data")
         ctl = os.path.join(dst, "control")
         lines = [l for l in open(ctl).read().splitlines() if l.strip() not in ("end", "END", "End")]
         lines += ["mts                        0", "end"]
         open(ctl, "w").write("\n".join(lines) + "\n")
     return dst
+
+
+def with_control(spec, **keys):
+    """The spec with some control-file keys replaced."""
+    spec.control = dict(spec.control, **keys)
+    return spec
 
 
 @pytest.fixture(scope="session")
@@ -54,6 +60,9 @@ def sysdir(tmp_path_factory):
         "mix_npt": lambda: synth.feature_mix(seed=9, ensemble="NPT"),
         "mix_nve": lambda: synth.feature_mix(seed=10, ensemble="NVE"),
         "hybrid": lambda: synth.hybrid_melt(n_atomistic=32, n_cg=32, nmono=20, seed=13, nsteps=100),
+        # initialize_velocities Y: SCALEV rescales the file's velocities (drawn
+        # at 400 K) to the control file's 350 K
+        "mix_y": lambda: with_control(synth.feature_mix(seed=15), initialize_velocities="Y", temperature=350),
         # 3x3x3 cells of ~220 particles: ~3,100 list candidates per cell
         "dense": lambda: synth.lj_fluid(n=6000, rho=45.0, seed=14, nsteps=10, dmin=0.12),
     }

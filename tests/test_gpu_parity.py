@@ -5,7 +5,8 @@
 * forces and energies of the FP32/fixed-point path within 1e-5 relative
   (max-norm over particles) of the oracle's FP64 engine on the same positions;
 * the FP64 path agrees with the oracle's FP64 engine to 1e-9;
-* short trajectories (NVT, NVE, NPT, MTS) track the FP64 oracle;
+* short trajectories (NVT, NVE, NPT, MTS, and from velocities rescaled by
+  SCALEV when initialize_velocities is Y) track the FP64 oracle;
 * FP32/fixed-point results are bitwise reproducible run to run.
 """
 import numpy as np
@@ -22,7 +23,7 @@ FORCE_TOL = 1e-5     # FP32/fixed vs FP64, max-norm relative
 ENERGY_TOL = 1e-5
 FP64_TOL = 1e-9      # FP64 path vs FP64 oracle
 
-SYSTEMS = ["fluid", "melt", "mix4", "mix5_mts", "mix_npt", "mix_nve", "hybrid"]
+SYSTEMS = ["fluid", "melt", "mix4", "mix5_mts", "mix_npt", "mix_nve", "hybrid", "mix_y"]
 
 
 def make(d, prec):

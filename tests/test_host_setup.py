@@ -65,9 +65,27 @@ def compare_setup(d):
                 np.testing.assert_array_equal(ra, rb, err_msg=f"{name} table {t + 1}")
 
 
-@pytest.mark.parametrize("name", ["fluid", "melt", "mix4", "mix5_mts", "mix_npt"])
+@pytest.mark.parametrize("name", ["fluid", "melt", "mix4", "mix5_mts", "mix_npt", "mix_y"])
 def test_host_setup_matches_oracle(sysdir, name):
     compare_setup(sysdir(name))
+
+
+def test_scalev_rescales_to_the_control_temperature(sysdir):
+    """initialize_velocities Y runs SCALEV (SCALEV.f90:13-26, main.F90:168-171):
+    the velocities (bit for bit the oracle's, above) now carry the control
+    file's temperature, TEMP = EK * MKTEMP = TEMP_IN, to REAL*4 rounding; with
+    N they are the coordinate file's, unscaled."""
+    s = native.Setup(sysdir("mix_y"))
+    assert s.restart == 1
+    o = Oracle(sysdir("mix_y"))
+    v = s.array("VXYZ").reshape(-1, 3).astype(np.float64)
+    m = s.array("MASS").astype(np.float64)[s.array("ITYPE")[: v.shape[0]] - 1]
+    t = 0.5 * float((m[:, None] * v * v).sum()) * float(o.finfo["MKTEMP"])
+    assert abs(t / float(o.finfo["TEMP_IN"]) - 1.0) < 1e-6
+    n = native.Setup(sysdir("mix4"))
+    assert n.restart == 0
+    _, v0, _ = n.initial_state()
+    np.testing.assert_array_equal(v0.ravel()[: len(n.array("VXYZ"))], n.array("VXYZ"))
 
 
 @pytest.mark.parametrize("fixture", ["atomisticPA", "hybridPA"])
