@@ -169,6 +169,7 @@ struct ibg_ctx {
   int nb_blocks_per_sm = 0;  // tuning: resident nonbonded blocks per SM (0: all that fit)
   int nb_chunk = 0;          // tuning (FP32): 256ths of the units taken dynamically after the block ranges (0: all, per warp)
   int nb_rows = 16;          // tuning: list rows per nonbonded work unit (8 or 16)
+  int vs_com_form = IBG_VS_COM_FIXED;  // centre-of-mass virtual sites: fixed or the reference's form
   ObsD* ring = nullptr;
   int ring_cap = 0;
   double *p_b = nullptr, *p_mv = nullptr, *p_mom = nullptr;
@@ -401,6 +402,7 @@ void make_args(ibg_ctx* c) {
   p.pos4[0] = c->L[0].pos4; p.pos4[1] = c->L[1].pos4;
   p.posq[0] = c->L[0].posq; p.posq[1] = c->L[1].posq;
   p.vcenter = c->vcenter; p.vnum = c->vnum; p.vmem = c->vmem; p.vmass = c->vmass; p.vinv = c->vinv;
+  p.com_carry = c->vs_com_form == IBG_VS_COM_REFERENCE;
   for (int w = 0; w < 2; ++w) {
     DevList& L = c->L[w];
     ListArgs& a = A.list[w];
@@ -871,6 +873,21 @@ int ibg_set_list_rows(ibg_ctx* c, int rows) {
       L.entries = dalloc<int>((size_t)L.nslices * 32 * rows, c->owned);
       L.w_cap = rows;
     }
+    refresh_args(c);
+    for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+    c->graphs.clear();
+  } catch (CudaError& e) {
+    return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
+  }
+  return IBG_OK;
+}
+
+int ibg_set_vsite_com(ibg_ctx* c, int form) {
+  if (!c || (form != IBG_VS_COM_FIXED && form != IBG_VS_COM_REFERENCE)) return IBG_E_INVALID;
+  if (c->in_batch) return fail(c, IBG_E_INVALID, "the context is in a batch");
+  try {
+    CK(cudaStreamSynchronize(c->st));
+    c->vs_com_form = form;
     refresh_args(c);
     for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
     c->graphs.clear();

@@ -130,10 +130,12 @@ struct PosArgs {
   const int* vmem;     // members, [v*15 + k], 0-based
   const float* vmass;  // member masses per [v*15 + k]
   const float* vinv;   // VIRT_INVMASS per VS
+  int com_carry;       // 1: the reference's centre-of-mass form (VIRTUAL_DEF.f90:31)
 };
 
-// SHIFT.f90:36-44 for atoms and VIRTUAL_DEF.f90:67-95 for virtual sites
-// (centre-of-mass sums with all three components reset per site).
+// SHIFT.f90:33-45 for atoms and VIRTUAL_DEF.f90:19-47 for virtual sites
+// (centre-of-mass sums with all three components reset per site, or the
+// reference's form, where only the x sum is reset: com_carry).
 // begin: when set, block 0 first starts the step: it advances the step
 // counter and sets this step's flags, or marks the step skipped when the run
 // aborted.  A system that has run its last step (done) is left as it is, so
@@ -189,11 +191,67 @@ __global__ void k_positions(__grid_constant__ const PosArgs a0, const PosArgs* c
     }
     store(i, s, sd);
   }
-  // VIRTUAL_DEF.f90:67-95: 16 lanes per site (half a warp), lane k holding
-  // member k's mass-weighted position; the sum runs over the members in
-  // order (0 + p0 + p1 + ...), as the reference's loop does.  The loop over
-  // sites is uniform within a warp, so its shuffles see all 32 lanes.
   const int hl = threadIdx.x & 15;
+  if (a.com_carry) {
+    // VIRTUAL_DEF.f90:30-39 as the reference runs it: only SUMTOTXYZ(1) is
+    // reset before a centre-of-mass site (:31), so the y and z sums run on
+    // from one such site to the next, from zero at the start of the pass.
+    // The chain is sequential, so one warp of block 0 walks the sites in
+    // order, two at a time: lanes 0-15 hold the members of the first site,
+    // lanes 16-31 those of the second, and every lane adds the broadcast
+    // terms in the reference's order.
+    if (bk.b != 0 || threadIdx.x >= 32) return;
+    R cy = 0, cz = 0;
+    for (int v0 = 0; v0 < a.nvirta; v0 += 2) {
+      const int v = v0 + (threadIdx.x >> 4);
+      const bool valid = v < a.nvirta;
+      const int ctr = valid ? a.vcenter[v] : 0;
+      const int nm = valid && ctr < 0 ? a.vnum[v] : 0;
+      R pm[3] = {0, 0, 0};
+      if (hl < nm) {
+        const int m = a.vmem[v * 15 + hl];
+        const R mm = (R)a.vmass[v * 15 + hl];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) pm[c] = mm * (R)a.S[3 * (size_t)m + c];
+      }
+      for (int h = 0; h < 2 && v0 + h < a.nvirta; ++h) {
+        const int vh = v0 + h;
+        const int ch = __shfl_sync(0xffffffffu, ctr, 16 * h);
+        const int nh = __shfl_sync(0xffffffffu, nm, 16 * h);
+        R s[3];
+        if (ch >= 0) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) s[c] = (R)a.S[3 * (size_t)ch + c];
+        } else {
+          R sx = 0;
+#pragma unroll
+          for (int q = 0; q < 15; ++q) {
+            const R x = __shfl_sync(0xffffffffu, pm[0], 16 * h + q);
+            const R y = __shfl_sync(0xffffffffu, pm[1], 16 * h + q);
+            const R z = __shfl_sync(0xffffffffu, pm[2], 16 * h + q);
+            if (q < nh) { sx = sx + x; cy = cy + y; cz = cz + z; }
+          }
+          const R inv = (R)a.vinv[vh];
+          s[0] = sx * inv; s[1] = cy * inv; s[2] = cz * inv;
+        }
+        if (threadIdx.x == 0) {
+          double sd[3];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            sd[c] = (double)s[c];
+            a.Svs[3 * (size_t)vh + c] = sd[c];
+          }
+          store(a.natoms + vh, s, sd);
+        }
+      }
+    }
+    return;
+  }
+  // VIRTUAL_DEF.f90:30-39 with all three sums reset per site: 16 lanes per
+  // site (half a warp), lane k holding member k's mass-weighted position; the
+  // sum runs over the members in order (0 + p0 + p1 + ...), as the
+  // reference's loop does.  The loop over sites is uniform within a warp, so
+  // its shuffles see all 32 lanes.
   const int w0 = (bk.b * blockDim.x + threadIdx.x) >> 5, nw = (bk.g * blockDim.x) >> 5;
   for (int w = w0; 2 * w < a.nvirta; w += nw) {
     const int v = 2 * w + ((threadIdx.x >> 4) & 1);

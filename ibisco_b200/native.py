@@ -26,6 +26,8 @@ STATUS = {
     -12: "IBG_E_IO", -13: "IBG_E_MEMORY",
 }
 
+STATUS_CODE = {v: k for k, v in STATUS.items()}
+
 # Every entry point the header declares (checked by the CPU tests).
 EXPORTS = [
     "ibg_setup_read", "ibg_setup_desc", "ibg_setup_initial_state", "ibg_setup_control",
@@ -38,10 +40,11 @@ EXPORTS = [
     "ibg_batch_destroy", "ibg_device_bytes", "ibg_estimate_bytes",
     "ibg_server_create", "ibg_server_submit", "ibg_server_wait", "ibg_server_drain", "ibg_server_result",
     "ibg_server_job_error", "ibg_server_get_stats", "ibg_server_destroy",
-    "ibg_get_tuning", "ibg_set_tuning", "ibg_autotune",
+    "ibg_get_tuning", "ibg_set_tuning", "ibg_autotune", "ibg_set_vsite_com",
 ]
 
 IBG_JOB_QUEUED, IBG_JOB_RUNNING, IBG_JOB_DONE, IBG_JOB_FAILED = 0, 1, 2, 3
+IBG_VS_COM_FIXED, IBG_VS_COM_REFERENCE = 0, 1
 
 
 _I, _F, _PI, _PF = ctypes.c_int, ctypes.c_float, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)
@@ -161,6 +164,7 @@ def lib(build_if_missing: bool = True):
         "ibg_set_l2_flush": (ctypes.c_int, [vp, ctypes.c_longlong]),
         "ibg_set_device": (ctypes.c_int, [ctypes.c_int]),
         "ibg_set_list_rows": (ctypes.c_int, [vp, ctypes.c_int]),
+        "ibg_set_vsite_com": (ctypes.c_int, [vp, ctypes.c_int]),
         "ibg_nonbonded_static": (ctypes.c_int, [ctypes.c_int, ctypes.c_int] + [vp] * 5 + [ctypes.c_int, vp, ctypes.c_int, vp,
                                                 ctypes.c_int, ctypes.c_int] + [vp] * 5 + [vp, ctypes.c_float, vp, vp, vp,
                                                                                         cp, ctypes.c_int]),
@@ -370,6 +374,12 @@ class System:
         t = Tuning()
         self._check(lib().ibg_get_tuning(self._h, ctypes.byref(t)))
         return t.as_dict()
+
+    def set_vsite_com(self, form: int):
+        """Centre-of-mass virtual sites: IBG_VS_COM_FIXED (each site its centre
+        of mass) or IBG_VS_COM_REFERENCE (VIRTUAL_DEF.f90:31 resets only the x
+        sum).  Call before set_state."""
+        self._check(lib().ibg_set_vsite_com(self._h, int(form)))
 
     def set_tuning(self, nb_tables_smem: int = 0, nb_blocks_per_sm: int = 0, nb_chunk: int = 0, nb_rows: int = 0):
         t = Tuning(nb_tables_smem, nb_blocks_per_sm, nb_chunk, nb_rows)

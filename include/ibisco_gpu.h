@@ -230,6 +230,18 @@ typedef struct ibg_tuning {
 int ibg_get_tuning(const ibg_ctx* c, ibg_tuning* t);
 int ibg_set_tuning(ibg_ctx* c, const ibg_tuning* t);
 int ibg_autotune(ibg_ctx* c, int reps, ibg_tuning* best, ibg_tuning* cand, double* us, int ncand);
+/* Centre-of-mass virtual sites (VIRT_CENTER = 0).  VIRTUAL_DEF.f90:30-39 sums
+   MASS*SXYZ over a site's members, but before each site resets only the x
+   component of its sum (VIRTUAL_DEF.f90:31); the y and z sums run on from one
+   such site to the next within a pass.  IBG_VS_COM_FIXED (the default)
+   resets all three, giving each site its centre of mass; IBG_VS_COM_REFERENCE
+   reproduces the reference's running y and z sums (one warp walks the sites
+   in order, so it is slow on many sites).  Centre-atom sites are the same in
+   both.  Set it before ibg_set_state and before a batch is made of the
+   context. */
+#define IBG_VS_COM_FIXED 0
+#define IBG_VS_COM_REFERENCE 1
+int ibg_set_vsite_com(ibg_ctx* c, int form);
 /* Device memory a context holds (bytes), and an estimate made before creating
    one from its descriptor and box; the estimate includes the Verlet-list
    storage the first list build will need, with margin.  A serving loop admits
@@ -276,13 +288,13 @@ void ibg_batch_destroy(ibg_batch* b);
  * ibg_nonbonded_static: the nonbonded forces, energies and virial of one
  * particle list, for callers that cannot allocate device memory at the time
  * they need them (a host whose device memory all belongs to its own
- * allocator, a call recorded into a CUDA graph, a loop that must not let
- * cudaMalloc/cudaFree synchronise the device).  It has no counterpart in the
- * reference: it is NONBONDED_FORCE on the reference's own arrays, offered
- * without a context.  Every pointer except box, err and stream is device
- * memory owned by the caller, in the reference's layout and 1-based ids:
- * rxyz(3,nitems) wrapped positions, itype/type_label(nitems) (3 for virtual
- * sites), index_list(n), list(maxnab,n), nnebs(nitems), inbondt(ntype,ntype),
+ * allocator, a loop that must not let cudaMalloc/cudaFree synchronise the
+ * device).  It has no counterpart in the reference: it is NONBONDED_FORCE on
+ * the reference's own arrays, offered without a context.  Every pointer
+ * except box, err and stream is device memory owned by the caller, in the
+ * reference's layout and 1-based ids: rxyz(3,nitems) wrapped positions,
+ * itype/type_label(nitems) (3 for virtual sites), index_list(n),
+ * list(maxnab,n), nnebs(nitems), inbondt(ntype,ntype),
  * rnbond/nbond_force/nbond_pot(ld_nb,nnbtype), binnb/ndatnb(nnbtype).
  * Outputs: fxyz(3,nitems) in FP64 (the forces of this list alone) and sums[9]
  * = V_NB(1..3), PT11, PT22, PT33, PT12, PT13, PT23 (not divided by the volume).
@@ -291,8 +303,13 @@ void ibg_batch_destroy(ibg_batch* b);
  * The first call on a device looks up that array's address with the device
  * current, so make it before any stream capture.  All calls share the array:
  * calls that overlap on the GPU (other streams, other host threads) race.
- * The call is synchronous on `stream` (a cudaStream_t, may be NULL) and allocates
- * nothing.  err (may be NULL) receives a message. */
+ * The call waits for `stream` (a cudaStream_t, may be NULL) before it returns,
+ * to read its error word, and allocates nothing.  ntype, nnbtype >= 1 and
+ * ld_nb >= 2 (IBG_E_INVALID otherwise); a particle type outside 1..ntype or an
+ * INBONDT entry outside 1..nnbtype on a pair inside the cutoff returns
+ * IBG_E_MISSING_TABLE, a table row whose successor lies beyond ld_nb or beyond
+ * NDATNB+1 IBG_E_TABLE_RANGE, an id outside 1..nitems in index_list or list
+ * IBG_E_INVALID.  err (may be NULL) receives a message. */
 #define IBG_STATIC_MAX_PARTICLES 262144
 #define IBG_STATIC_MAX_BLOCKS 1024
 int ibg_nonbonded_static(int nitems, int n, const float* rxyz, const int* itype, const int* type_label,
