@@ -7,6 +7,7 @@ as text (it is not imported: it needs MDAnalysis and nose) and writes the
 numbers as JSON so the oracle tests do not depend on the reference tree.
 
 Usage:  python tests/golden/extract_goldens.py [path/to/testsuite/tests.py]
+        (default: testsuite/tests.py under $IBISCO_REFERENCE_DIR)
 """
 import ast
 import json
@@ -14,7 +15,6 @@ import os
 import re
 import sys
 
-DEFAULT = "/root/reference/testsuite/tests.py"
 
 
 def extract(path: str) -> dict:
@@ -34,7 +34,12 @@ def extract(path: str) -> dict:
 
 
 if __name__ == "__main__":
-    path = sys.argv[1] if len(sys.argv) > 1 else DEFAULT
+    if len(sys.argv) > 1:
+        path = sys.argv[1]
+    elif os.environ.get("IBISCO_REFERENCE_DIR"):
+        path = os.path.join(os.environ["IBISCO_REFERENCE_DIR"], "testsuite", "tests.py")
+    else:
+        raise SystemExit("give testsuite/tests.py as an argument or the reference tree in IBISCO_REFERENCE_DIR")
     data = extract(path)
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_goldens.json")
     with open(dst, "w") as f:
