@@ -16,6 +16,7 @@ enum : unsigned {
   EB_TABLE_RANGE = 1u << 5,    // nonbonded distance beyond its table
   EB_MISSING_TABLE = 1u << 6,  // listed pair without a nonbonded table
   EB_CAPACITY = 1u << 7,       // neighbour-list / cell storage exhausted
+  EB_BAD_INDEX = 1u << 8,      // a caller's particle id outside 1..NITEMS
 };
 
 // 64-bit fixed-point force accumulation: value * 2^32, two's complement in

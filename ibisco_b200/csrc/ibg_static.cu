@@ -2,19 +2,22 @@
 //
 // Some callers cannot allocate device memory when they need the forces: a
 // host that already owns every byte of device memory through its own
-// allocator (a Fortran or framework memory pool), code that records the call
-// into a CUDA graph where cudaMalloc is not allowed, or a loop that must not
+// allocator (a Fortran or framework memory pool), or a loop that must not
 // stall the device (cudaMalloc and cudaFree can synchronise it).  This entry
 // point serves them: the caller passes its device arrays in and out, and the
 // scratch the computation needs -- the 64-bit fixed-point force sums and the
 // per-block energy/virial partial sums -- lives in one file-scope
 // __device__ array of fixed size that every GPU loading the library holds
-// until the process exits.
+// until the process exits.  The call reads its error word back and waits for
+// its stream before it returns.
 //
-// The computation is NONBONDED_FORCE.F90:173-232 on the reference's own data
+// The computation is NONBONDED_FORCE.F90:45-104 on the reference's own data
 // layout (INDEX_LIST, LIST(MAXNAB,N), NNEBS, the nonbonded tables after
 // FTABLE), in REAL*4 with the reference's operation order, summed in the same
-// fixed point as the context path.
+// fixed point as the context path.  Particle types, table numbers and table
+// rows are checked before they index anything: a type outside 1..NTYPE or a
+// table number outside 1..NNBTYPE counts as a missing table, a row whose
+// successor lies beyond the caller's table column as out of range.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -38,7 +41,7 @@ std::mutex g_mu;
 void* g_ptr[64] = {nullptr};
 
 struct StaticArgs {
-  int nitems, n, maxnab, ntype, ld_nb;
+  int nitems, n, maxnab, ntype, nnbtype, ld_nb;
   const float* rxyz;
   const int* itype;
   const int* type_label;
@@ -80,13 +83,16 @@ __global__ void __launch_bounds__(256) k_static_pairs(StaticArgs a) {
   for (int k = 0; k < 9; ++k) acc[k] = 0.0;
   for (int A = blockIdx.x * blockDim.x + threadIdx.x; A < a.n; A += gridDim.x * blockDim.x) {
     const int i = a.index_list[A] - 1;
+    if (i < 0 || i >= a.nitems) { atomicOr(a.err, ibg::EB_BAD_INDEX); continue; }
     const float rx = a.rxyz[3 * i], ry = a.rxyz[3 * i + 1], rz = a.rxyz[3 * i + 2];
     const int ti = a.itype[i];
     const int li = a.type_label[i];
+    const bool ti_ok = ti >= 1 && ti <= a.ntype;
     long long f0 = 0, f1 = 0, f2 = 0;
     const int cnt = min(a.nnebs[i], a.maxnab);
     for (int k = 0; k < cnt; ++k) {
       const int j = a.list[(long long)A * a.maxnab + k] - 1;
+      if (j < 0 || j >= a.nitems) { atomicOr(a.err, ibg::EB_BAD_INDEX); continue; }
       float d0 = rx - a.rxyz[3 * j], d1 = ry - a.rxyz[3 * j + 1], d2 = rz - a.rxyz[3 * j + 2];
       d0 = __fsub_rn(d0, __fmul_rn(roundf(__fmul_rn(d0, a.boxinv[0])), a.box[0]));
       d1 = __fsub_rn(d1, __fmul_rn(roundf(__fmul_rn(d1, a.boxinv[1])), a.box[1]));
@@ -94,12 +100,13 @@ __global__ void __launch_bounds__(256) k_static_pairs(StaticArgs a) {
       const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)), __fmul_rn(d2, d2));
       if (!(r2 < a.rcutsq)) continue;
       const int tj = a.itype[j];
+      if (!ti_ok || tj < 1 || tj > a.ntype) { atomicOr(a.err, ibg::EB_MISSING_TABLE); continue; }
       const int tab = a.inbondt[(ti - 1) + a.ntype * (tj - 1)];
-      if (tab < 1) { atomicOr(a.err, ibg::EB_MISSING_TABLE); continue; }
+      if (tab < 1 || tab > a.nnbtype) { atomicOr(a.err, ibg::EB_MISSING_TABLE); continue; }
       const float r = __fsqrt_rn(r2);
       const float bin = a.binnb[tab - 1];
       const int ni = (int)__fdiv_rn(r, bin);
-      if (ni < 0 || ni > a.ndatnb[tab - 1]) { atomicOr(a.err, ibg::EB_TABLE_RANGE); continue; }
+      if (ni < 0 || ni > a.ndatnb[tab - 1] || ni + 1 >= a.ld_nb) { atomicOr(a.err, ibg::EB_TABLE_RANGE); continue; }
       const long long row = (long long)a.ld_nb * (tab - 1) + ni;
       const float alpha = __fdiv_rn(__fsub_rn(r, a.rnbond[row]), bin);
       const float one_a = __fsub_rn(1.0f, alpha);
@@ -160,8 +167,8 @@ extern "C" int ibg_nonbonded_static(int nitems, int n, const float* rxyz, const 
                                     const float* nbond_force, const float* nbond_pot, const float* binnb,
                                     const int* ndatnb, const float* box, float rcutsq, double* fxyz, double* sums,
                                     void* stream, char* err, int errlen) {
-  (void)nnbtype;
-  if (nitems < 1 || n < 0 || n > nitems || maxnab < 1 || !rxyz || !itype || !type_label || !index_list || !nnebs ||
+  if (nitems < 1 || n < 0 || n > nitems || maxnab < 1 || ntype < 1 || nnbtype < 1 || ld_nb < 2 || !rxyz ||
+      !itype || !type_label || !index_list || !nnebs ||
       !inbondt || !rnbond || !nbond_force || !nbond_pot || !binnb || !ndatnb || !box || !fxyz || !sums ||
       (n > 0 && !list)) {
     msg(err, errlen, "ibg_nonbonded_static: invalid argument");
@@ -194,7 +201,7 @@ extern "C" int ibg_nonbonded_static(int nitems, int n, const float* rxyz, const 
   }
   cudaStream_t st = (cudaStream_t)stream;
   StaticArgs a;
-  a.nitems = nitems; a.n = n; a.maxnab = maxnab; a.ntype = ntype; a.ld_nb = ld_nb;
+  a.nitems = nitems; a.n = n; a.maxnab = maxnab; a.ntype = ntype; a.nnbtype = nnbtype; a.ld_nb = ld_nb;
   a.rxyz = rxyz; a.itype = itype; a.type_label = type_label; a.index_list = index_list; a.list = list;
   a.nnebs = nnebs; a.inbondt = inbondt; a.rnbond = rnbond; a.nbond_force = nbond_force; a.nbond_pot = nbond_pot;
   a.binnb = binnb; a.ndatnb = ndatnb; a.rcutsq = rcutsq;
@@ -217,6 +224,7 @@ extern "C" int ibg_nonbonded_static(int nitems, int n, const float* rxyz, const 
   if (bits & ibg::EB_FIXED) { msg(err, errlen, "force outside the 64-bit fixed-point range"); return IBG_E_FIXED_OVERFLOW; }
   if (bits & ibg::EB_MISSING_TABLE) { msg(err, errlen, "listed pair without a nonbonded table"); return IBG_E_MISSING_TABLE; }
   if (bits & ibg::EB_TABLE_RANGE) { msg(err, errlen, "nonbonded distance beyond its table"); return IBG_E_TABLE_RANGE; }
+  if (bits & ibg::EB_BAD_INDEX) { msg(err, errlen, "particle id outside 1..nitems in index_list or list"); return IBG_E_INVALID; }
   msg(err, errlen, "");
   return IBG_OK;
 }

@@ -57,6 +57,19 @@ static void register_arrays(OrcHandle* h) {
   Fv("ANGLE_OOP", s.oop.x); Fv("OOP_POT", s.oop.pot); Fv("OOP_FORCE", s.oop.force); Fv("BINO", s.oop.bin);
 }
 
+template <typename E>
+static int nonbonded_list(E& e, const orc::Setup& st, int which, double* fxyz, double* sums) {
+  using R = decltype(e.PT11);
+  e.zero_force_stage();
+  if (which == 0) e.nonbonded_force(st.ATOM, st.NUMATOMS, e.la, (R)st.RCUTSQ_ATOM);
+  else e.nonbonded_force(st.BEAD, st.NCOARSE, e.lb, (R)st.RCUTSQ_BEAD);
+  for (size_t k = 0; k < e.F.size(); ++k) fxyz[k] = (double)e.F[k];
+  const double v[9] = {e.V_NB[0], e.V_NB[1], e.V_NB[2], (double)e.PT11, (double)e.PT22, (double)e.PT33,
+                       (double)e.PT12, (double)e.PT13, (double)e.PT23};
+  for (int k = 0; k < 9; ++k) sums[k] = v[k];
+  return e.err;
+}
+
 extern "C" {
 
 void* orc_open(const char* dir, int nthreads, char* errbuf, int errlen) {
@@ -173,6 +186,14 @@ int orc_run(void* p, int prec, int first, int nsteps) {
 int orc_forces(void* p, int prec, int step) {
   auto* h = static_cast<OrcHandle*>(p);
   ENG(h, prec, { e.force_stage(step); return e.err; });
+}
+// NONBONDED_FORCE.F90 on one list alone (which: 0 atom list, 1 bead list) at
+// the current positions: forces (3,NITEMS) and sums[9] = V_NB(1..3), PT11,
+// PT22, PT33, PT12, PT13, PT23 (not divided by the volume).  It replaces the
+// engine's force arrays; call orc_forces or orc_step to rebuild them.
+int orc_nonbonded_list(void* p, int prec, int which, double* fxyz, double* sums) {
+  auto* h = static_cast<OrcHandle*>(p);
+  return prec == 0 ? nonbonded_list(h->ef, h->s, which, fxyz, sums) : nonbonded_list(h->ed, h->s, which, fxyz, sums);
 }
 const char* orc_error(void* p, int prec) {
   auto* h = static_cast<OrcHandle*>(p);

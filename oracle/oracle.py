@@ -65,6 +65,7 @@ def lib():
         L.orc_error.argtypes = [vp, ctypes.c_int]
         L.orc_get_state.argtypes = [vp, ctypes.c_int, dp, dp, dp, dp]
         L.orc_get_obs.argtypes = [vp, ctypes.c_int, dp]
+        L.orc_nonbonded_list.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, dp]
         L.orc_get_list.argtypes = [vp, ctypes.c_int, ctypes.c_int, ip, ctypes.c_int, ip]
         _lib = L
     return _lib
@@ -146,6 +147,17 @@ class Oracle:
 
     def forces(self, step: int, prec: int = 0):
         self._check(lib().orc_forces(self._h, prec, int(step)), prec)
+
+    def nonbonded_list(self, which: int, prec: int = 0):
+        """NONBONDED_FORCE.F90 on list `which` alone: forces (NITEMS,3) and
+        V_NB(1..3), PT11, PT22, PT33, PT12, PT13, PT23 (not divided by the
+        volume).  The engine's force arrays are replaced."""
+        ni = self.info["NITEMS"]
+        f = np.zeros(3 * ni)
+        sums = np.zeros(9)
+        dp = ctypes.c_double
+        self._check(lib().orc_nonbonded_list(self._h, prec, int(which), _ptr(f, dp), _ptr(sums, dp)), prec)
+        return f.reshape(ni, 3), sums
 
     def state(self, prec: int = 0):
         ni, na = self.info["NITEMS"], self.info["NATOMS"]
