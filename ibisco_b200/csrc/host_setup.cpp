@@ -734,7 +734,7 @@ bool topology(ibg_setup* s, const std::string& dir) {
       }
     }
   }
-  if (d.ibrdescr == 0) {  // RDVIRTANGLES.f90:112-120 (optional file)
+  if (d.ibrdescr == 0) {  // RDVIRTANGLES.f90:35-50 (optional file)
     Records r;
     if (r.load(dir + "/virtangles")) {
       std::vector<std::string> v;
@@ -850,7 +850,7 @@ bool read_all(ibg_setup* s, const std::string& dir) {
   ibg_desc& d = s->d;
   if (d.ibrdescr == 0) {
     if (!virtual_sites(s, dir)) return false;
-    for (int i = 1; i <= d.natoms; ++i)  // MAKE_LISTS.f90:242-255
+    for (int i = 1; i <= d.natoms; ++i)  // MAKE_LISTS.f90:46-60
       (s->type_label[i - 1] == 1 ? s->atom : s->bead).push_back(i);
     d.numatoms = (int)s->atom.size();
     d.numbeads = (int)s->bead.size();

@@ -46,13 +46,13 @@ struct Scalars {
   double box[3], boxinv[3], box2[3];  // FP64 box (integration, FP64 path)
   float boxf[3], boxinvf[3], box2f[3];  // REAL*4 box (FP32 path geometry)
   int ncell[2][3];   // cell grid of the atom / bead list
-  double lam[2];     // Berendsen factors for atoms / beads (MOVE.F90:73-79)
+  double lam[2];     // Berendsen factors for atoms / beads (MOVE.F90:32-38)
   double temp_atom, temp_bead;
   double miu;        // SCALEBP factor of this step (1 if none)
   // MTS history (module_MTS.f90): V_NB(label) and PT11..PT13 for m=1..3
   double mts_vnb[3][3];
   double mts_pt[6][3];
-  // SCALEBP running window (SCALEBP.f90:240-243)
+  // SCALEBP running window (SCALEBP.f90:18-21)
   int iavp, pad1;
   double sp[10];
   unsigned err;

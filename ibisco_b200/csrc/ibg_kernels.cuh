@@ -331,7 +331,7 @@ struct ListArgs {
 // List-rebuild kernels run when the step rebuilds its lists (or always, for
 // the rebuild of ibg_set_state) and the step is not skipped.
 //
-// UPDATE_NEIGHBOURLIST.F90:14-48 / ALLOCATEVAR2.f90:156-180: cells per
+// UPDATE_NEIGHBOURLIST.F90:14-48 / ALLOCATEVAR2.f90:19-42: cells per
 // dimension = INT(BOX/RLIST).  The grid also clears the cell counters.
 template <typename R, bool B>
 __global__ void k_regrid(__grid_constant__ const ListArgs L0, const ListArgs* const* tab, const BlockMap bm, int always) {
@@ -357,7 +357,7 @@ __global__ void k_regrid(__grid_constant__ const ListArgs L0, const ListArgs* co
   for (int c = 0; c < 3; ++c) sc->ncell[L.which][c] = nc[c];
 }
 
-// LINKS.f90:192-194.  A component equal to NCELL (coordinate at +L/2 after
+// LINKS.f90:16-18.  A component equal to NCELL (coordinate at +L/2 after
 // rounding) would address a cell outside the grid; it is clamped and counted.
 template <typename R, bool B>
 __global__ void k_cell_assign(__grid_constant__ const ListArgs L0, const ListArgs* const* tab, const BlockMap bm, int always) {
@@ -449,7 +449,7 @@ __global__ void k_cell_fill(__grid_constant__ const ListArgs L0, const ListArgs*
 }
 
 // Within a cell the reference's linked list visits entries by decreasing A
-// (LINKS.f90:195-196); slots are kept in increasing A so the list build can
+// (LINKS.f90:19-20); slots are kept in increasing A so the list build can
 // walk them backwards.  k_cell_fill placed a cell's entries in arbitrary order
 // (atomics); here each entry finds its rank among its cell's entries.
 template <bool B>
@@ -511,7 +511,7 @@ __global__ void k_slot_of(__grid_constant__ const ListArgs L0, const ListArgs* c
 
 // NEW_NEIGHBOUR_WITHLIST.f90:34-123.  A block builds the lists of one cell's
 // particles at a time (cells taken dynamically).  The candidates of the cell --
-// its own slots, then the slots of the 13 cells of the MAPS.f90:137-149
+// its own slots, then the slots of the 13 cells of the MAPS.f90:39-51
 // stencil, each run by decreasing A -- are staged once in shared memory, in
 // that order, with their slot numbers; every particle of the cell then reads
 // them from there.  A warp builds one particle's list: its candidates are the
@@ -528,7 +528,7 @@ __global__ void k_slot_of(__grid_constant__ const ListArgs L0, const ListArgs* c
 // k of slot s (slice g) at (g*w_cap + k/T)*32 + (s%P)*T + k%T.  A slot that
 // needs more than w_cap rows records its need and raises the abort flag (the
 // host enlarges the storage and repeats the step).
-// The 13 neighbour cells of the half stencil in MAPS.f90:137-149 order.
+// The 13 neighbour cells of the half stencil in MAPS.f90:39-51 order.
 __constant__ int kStencil[13][3] = {{1, 0, 0}, {1, 1, 0},  {0, 1, 0},  {-1, 1, 0}, {1, 0, -1}, {1, 1, -1}, {0, 1, -1},
                                     {-1, 1, -1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}, {-1, 1, 1}, {0, 0, 1}};
 
@@ -769,7 +769,7 @@ __device__ __forceinline__ bool nb_idle(const NBArgs<R>& A) {
   return false;
 }
 
-// NONBONDED_FORCE.F90:173-232.  Persistent grid; a warp owns one slice of
+// NONBONDED_FORCE.F90:45-104.  Persistent grid; a warp owns one slice of
 // P = 32/T slots at a time and T lanes walk each slot's list; list reads are
 // coalesced 128-byte rows, neighbour positions are float4 gathers from the
 // cell-ordered array.  i-forces are summed in registers and reduced exactly
@@ -931,7 +931,7 @@ __device__ __forceinline__ long long fixq(float v, unsigned& err) {
   return __float2ll_rn(s);
 }
 
-// NONBONDED_FORCE.F90:173-232, FP32 force path.  Same structure as
+// NONBONDED_FORCE.F90:45-104, FP32 force path.  Same structure as
 // k_nonbonded (slices of P = 32/T slots, T lanes per slot, dynamic units of
 // `rows` list rows).  The arithmetic is REAL*4 as in the reference, with
 // cheaper equivalents where only the force value (not a bit pattern) is
@@ -1374,7 +1374,7 @@ struct BondedArgs {
 
 template <typename R>
 __device__ __forceinline__ R lerp_mixed(R y0, R y1, R alpha) {
-  // y0*(1.0D0-alpha) + alpha*y1 with the FP64 promotion of BONDS.inc:141-145
+  // y0*(1.0D0-alpha) + alpha*y1 with the FP64 promotion of BONDS.inc:36-40
   return (R)((double)y0 * (1.0 - (double)alpha) + (double)(alpha * y1));
 }
 
@@ -1663,7 +1663,7 @@ struct MoveArgs {
   int part_stride;
 };
 
-// MOVE.F90:81-129 (leap-frog with Berendsen factors per class) and the
+// MOVE.F90:32-88 (leap-frog with Berendsen factors per class) and the
 // bonded virial sum of NEW_FORCE.F90:73-80, which uses the positions before
 // the update.  Partials: PTK(6) atoms, PTK(6) beads, bonded virial(6).  The
 // bonded forces are folded into the nonbonded array (fnb becomes the total
@@ -1798,7 +1798,7 @@ __global__ void k_mom_apply(__grid_constant__ const MomArgs A0, const MomArgs* c
     for (int c = 0; c < 3; ++c) A.V[3 * (size_t)i + c] -= tot[c] * A.invmass[i];
 }
 
-// SCALEBP.f90:259-261: positions scaled with the box on the steps the
+// SCALEBP.f90:37-39: positions scaled with the box on the steps the
 // barostat changed it.
 template <typename R, bool B>
 __global__ void k_scale_positions(__grid_constant__ const MoveArgs<R> M0, const MoveArgs<R>* const* tab,
@@ -1845,7 +1845,7 @@ __device__ double wsum(const double* p, int g) {
 
 // Deterministic reduction of all partials into the observables, the MTS
 // auxiliary history (MTS_SAVEAUXS / MTS_LOADAUXS), the thermostat factors of
-// the next step and the barostat window (SCALEBP.f90:240-263).  The
+// the next step and the barostat window (SCALEBP.f90:18-41).  The
 // nonbonded accumulators are read and cleared for the next step.
 template <bool B>
 __global__ void k_finalize(__grid_constant__ const FinalArgs F0, const FinalArgs* const* tab, const BlockMap bm) {
@@ -1896,7 +1896,7 @@ __global__ void k_finalize(__grid_constant__ const FinalArgs F0, const FinalArgs
   double pt[6];
   for (int c = 0; c < 6; ++c) pt[c] = q[3 + c] + bead_pt[c] + q[42 + c];
   if (F.move) {
-    // MOVE.F90:131-156
+    // MOVE.F90:90-115
     for (int c = 0; c < 6; ++c) pt[c] += q[30 + c] + q[36 + c];
     o.ek[0] = 0.5 * (q[30] + q[31] + q[32]);
     o.ek[1] = 0.5 * (q[36] + q[37] + q[38]);
@@ -1907,11 +1907,11 @@ __global__ void k_finalize(__grid_constant__ const FinalArgs F0, const FinalArgs
     sc->temp_bead = o.temp_bead;
     const double vol = sc->box[0] * sc->box[1] * sc->box[2];
     for (int c = 0; c < 6; ++c) pt[c] /= vol;
-    if (F.ensemble == 1 || F.ensemble == 2) {  // MOVE.F90:73-79, for the next step
+    if (F.ensemble == 1 || F.ensemble == 2) {  // MOVE.F90:32-38, for the next step
       sc->lam[0] = sqrt(1.0 + F.fac * ((F.temp_in / o.temp_atom) - 1.0));
       sc->lam[1] = sqrt(1.0 + F.fac * ((F.temp_in / o.temp_bead) - 1.0));
     }
-    if (F.ensemble == 2) {  // SCALEBP.f90:240-263
+    if (F.ensemble == 2) {  // SCALEBP.f90:18-41
       sc->iavp = sc->iavp + 1;
       if (sc->iavp > 10) sc->iavp -= 10;
       sc->sp[sc->iavp - 1] = (pt[0] + pt[1] + pt[2]) / 3.0;

@@ -23,7 +23,7 @@ extern "C" {
 #define IBG_E_INVALID (-1)        /* bad argument or descriptor                          */
 #define IBG_E_LIST_OVERFLOW (-2)  /* NEW_NEIGHBOUR_WITHLIST.f90:72,113 'LIST TOO SMALL'  */
 #define IBG_E_TORSION_TABLE (-3)  /* TORSIONS.inc:105-109 entry not in torsion table     */
-#define IBG_E_OOP_RANGE (-4)      /* OUTOFPLANES.inc:214-252 angle outside its table     */
+#define IBG_E_OOP_RANGE (-4)      /* OUTOFPLANES.inc:62-100 angle outside its table     */
 #define IBG_E_FIXED_OVERFLOW (-5) /* a force left the 64-bit fixed-point range           */
 #define IBG_E_CELL_GRID (-6)      /* fewer than 3 cells per dimension (MAPS.f90 stencil) */
 #define IBG_E_CUDA (-7)           /* CUDA runtime failure                                */

@@ -22,7 +22,7 @@ enum OrcErr {
   ORC_OK = 0,
   ORC_E_LIST_OVERFLOW = -2,   // NEW_NEIGHBOUR_WITHLIST.f90:72,113
   ORC_E_TORSION_TABLE = -3,   // TORSIONS.inc:105-109
-  ORC_E_OOP_RANGE = -4,       // OUTOFPLANES.inc:214-252
+  ORC_E_OOP_RANGE = -4,       // OUTOFPLANES.inc:62-100
   ORC_E_CELL_GRID = -6,       // MAPS.f90 needs >= 3 cells per dimension
   ORC_E_TABLE_RANGE = -9,     // nonbonded lookup beyond the table
   ORC_E_MISSING_TABLE = -10,  // a listed pair has no nonbonded table
@@ -43,7 +43,7 @@ struct Engine {
   using D = double;
   Setup* s = nullptr;
   int nthreads = 1;
-  bool com_fix = true;  // VIRTUAL_DEF.f90:79 zeroes only the x sum; see com_bug below
+  bool com_fix = true;  // VIRTUAL_DEF.f90:31 zeroes only the x sum; see com_bug below
   int err = 0;
   std::string errmsg;
   int NI_ = 0, NA_ = 0;
@@ -283,7 +283,7 @@ struct Engine {
     }
   }
 
-  // ------------------------------------------------ NONBONDED_FORCE.F90:173-232
+  // ------------------------------------------------ NONBONDED_FORCE.F90:45-104
   void nonbonded_force(const std::vector<int>& idx, int n, NList& L, R rcutsq) {
     const int T = nthreads;
     std::vector<double> vnb((size_t)3 * T, 0.0);
@@ -354,7 +354,7 @@ struct Engine {
     if (bad_range) fail(ORC_E_TABLE_RANGE, "nonbonded distance beyond its table");
   }
 
-  // ------------------------------------------------- BONDED_FORCE.F90:67-99
+  // ------------------------------------------------- BONDED_FORCE.F90:38-99
   void bonded_force() {
     const int T = nthreads;
     std::vector<double> vb((size_t)12 * T, 0.0);
@@ -688,7 +688,7 @@ struct Engine {
     bonded_virial();
   }
 
-  // ------------------------------------------------------------ MOVE.F90:63-156
+  // ------------------------------------------------------------ MOVE.F90:9-118
   void move() {
     R k11[2] = {0, 0}, k22[2] = {0, 0}, k33[2] = {0, 0}, k12[2] = {0, 0}, k23[2] = {0, 0}, k13[2] = {0, 0};
     R lam[2];

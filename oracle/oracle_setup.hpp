@@ -812,7 +812,7 @@ inline bool setup_from_dir(Setup& s, const std::string& dir) {
   if (!rdcontrol(s, dir)) return false;
   if (!rdinteract(s, dir)) return false;
   if (!rdcoor(s, dir)) return false;
-  // ALLOCATEVAR2.f90:156-180
+  // ALLOCATEVAR2.f90:19-42
   s.NCELLX_ATOM = (int)(s.BOX[0] / s.RLIST_ATOM);
   s.NCELLY_ATOM = (int)(s.BOX[1] / s.RLIST_ATOM);
   s.NCELLZ_ATOM = (int)(s.BOX[2] / s.RLIST_ATOM);
