@@ -91,58 +91,123 @@ def make_workload(name: str, directory: str):
 
 
 class Clocks:
-    """nvidia-smi samples (200 ms) during the timed region."""
+    """SM clock and clock-event reasons of this rank's GPU, polled through
+    NVML every 5 ms from a thread (read-only queries), or with nvidia-smi at
+    200 ms where NVML cannot be loaded.  mark(True)/mark(False) bracket the
+    timed region; summary() reports the samples inside it and, beside them,
+    those of the whole window the sampler ran (warm-up and timed region),
+    which a short timed region needs for a median under load."""
 
     FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, gpu: int):
         self.gpu = gpu
+        self.samples = []      # (t, sm_mhz, reasons)
+        self.max_mhz = None
+        self.marks = [None, None]
+        self._stop = threading.Event()
+        self.t = None
         self.proc = None
-        self.lines = []
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        try:
+            p = torch.cuda.get_device_properties(self.gpu)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(
+                f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0")
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+
+    def _poll_nvml(self, nv, h):
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        while not self._stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((time.perf_counter(), float(mhz), {k for k, b in bits.items() if r & b}))
+            except Exception:
+                pass
+            self._stop.wait(0.005)
+
+    def _read_smi(self):
+        for line in self.proc.stdout:
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                mhz, self.max_mhz = float(p[1]), float(p[2])
+            except ValueError:
+                continue
+            self.samples.append((time.perf_counter(), mhz,
+                                 {n for k, n in enumerate(self.NAMES) if p[5 + k].lower() == "active"}))
 
     def __enter__(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.source = "nvml, 5 ms"
+            self.t = threading.Thread(target=self._poll_nvml, args=(nv, h), daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            pass
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
                  "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            self.source = "nvidia-smi, 200 ms"
+            self.t = threading.Thread(target=self._read_smi, daemon=True)
             self.t.start()
         except OSError:
             self.proc = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def mark(self, begin: bool):
+        self.marks[0 if begin else 1] = time.perf_counter()
 
     def __exit__(self, *a):
+        self._stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        if self.t:
             self.t.join(timeout=2)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in self.lines:
-            p = [x.strip() for x in l.split(",")]
-            if len(p) < 9:
-                continue
-            try:
-                sm.append(float(p[1]))
-                mx = float(p[2])
-            except ValueError:
-                continue
-            for k, n in enumerate(names):
-                if p[5 + k].lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        def stats(rows):
+            sm = [r[1] for r in rows]
+            return (float(np.median(sm)) if sm else None), sorted(set().union(*[r[2] for r in rows])), len(rows)
+
+        b, e = self.marks
+        timed = [r for r in self.samples if b is not None and e is not None and b <= r[0] <= e]
+        sm_t, rs_t, n_t = stats(timed)
+        sm_w, rs_w, n_w = stats(self.samples)
+        out = {"sm_mhz": sm_t if n_t else sm_w, "sm_max_mhz": self.max_mhz, "reasons": sorted(set(rs_t) | set(rs_w)),
+               "samples": n_t, "window_samples": n_w, "window_sm_mhz": sm_w, "source": self.source}
+        if self.samples:
+            out["window_s"] = self.samples[-1][0] - self.samples[0][0]
+        return out
+
+
+def workload_config(args, n: int) -> dict:
+    """The workload as both arms name it (the same dict on the reference arm)."""
+    cfg = {"workload": args.workload, "description": WORKLOADS[args.workload], "particles": n}
+    if args.vs_com == "reference":
+        cfg["virtual_sites"] = "reference centre-of-mass form (VIRTUAL_DEF.f90:31 resets only the x sum)"
+    return cfg
 
 
 def measured_peak():
@@ -170,7 +235,7 @@ def cpu_baseline(directory: str, n_particles: int, budget_s: float = 20.0, max_s
     from oracle import oracle as orc
 
     threads = os.cpu_count() or 1
-    o = orc.Oracle(directory, threads=threads)
+    o = orc.Oracle(directory, threads=threads, com_fix=VS_COM["form"] != "reference")
     o.init(0)
     o.step(1, 0)
     t0 = time.perf_counter()
@@ -226,7 +291,7 @@ def run_reference(args, world, rank, pg):
         from oracle import oracle as orc
 
         threads = os.cpu_count() or 1
-        o = orc.Oracle(d, threads=threads)
+        o = orc.Oracle(d, threads=threads, com_fix=VS_COM["form"] != "reference")
         n = o.info["NATOMS"]
         o.init(0)
         for k in range(min(args.warmup, 5)):
@@ -244,8 +309,7 @@ def run_reference(args, world, rank, pg):
         line = {"impl": "reference", "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s",
                 "n_gpus": world, "steps": done, "warmup": args.warmup, "ms_per_step": 1000 * el / done,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic", "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
-                                                "particles": n},
+                "data": "synthetic", "config": workload_config(args, n),
                 "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": threads, "kind": "port",
                                  "sample": f"{done} of {args.steps} requested steps in {el:.1f} s after {min(args.warmup, 5)} "
                                            f"warm-up steps (C++ REAL*4 restatement of the reference, OpenMP "
@@ -254,19 +318,29 @@ def run_reference(args, world, rank, pg):
         print(json.dumps(line), flush=True)
 
 
-def run_serving(args, world, rank, local, pg, workdir):
-    """Served job stream: the first J jobs of a seeded stream (sizes log-uniform
-    in 500..50,000 beads, 1-3 types, chains of 10-100, per-job perturbed LJ
-    tables, Poisson arrivals at 20 jobs/s), replayed in wall-clock time against
-    the continuous-batching server; then the same jobs one after another on the
-    plain FP64 path, served in arrival order (computed from the measured
-    per-job times).  Jobs are split over ranks (no collective on the data
-    path); latencies and throughput are over all ranks."""
-    from ibisco_b200 import native, serving, synth
+def stream_jobs(args, workdir):
+    """The seeded served job stream (sizes log-uniform in 500..50,000 beads,
+    1-3 types, chains of 10-100, per-job perturbed LJ tables, Poisson arrivals
+    at 20 jobs/s), written once in the reference's input format; the batched
+    leg takes its first jobs, the serving leg all of them."""
+    from ibisco_b200 import serving, synth
 
-    stream = synth.job_stream(args.serve_jobs, seed=5)
-    base = os.path.join(workdir, "serve")
-    jobs = serving.stream_dirs(base, stream, args.serve_steps)
+    njobs = max(args.serve_jobs, args.batch_jobs)
+    stream = synth.job_stream(njobs, seed=5)
+    return serving.stream_dirs(os.path.join(workdir, "stream"), stream, args.serve_steps)
+
+
+def run_serving(args, world, rank, local, pg, jobs):
+    """Served job stream: the first J jobs of the seeded stream, replayed in
+    wall-clock time against the continuous-batching server; then the same jobs
+    one after another on the plain FP64 path, served in arrival order (computed
+    from the measured per-job times).  Both latencies run from a job's
+    scheduled arrival and include reading its input files.  Jobs are split over
+    ranks (no collective on the data path); latencies and throughput are over
+    all ranks."""
+    from ibisco_b200 import native, serving
+
+    jobs = jobs[: args.serve_jobs]
     mine = serving.partition(jobs, rank, world)
     barrier(pg)
     srv = native.Server(device=local, tick_steps=args.serve_tick, max_jobs=256)
@@ -289,8 +363,11 @@ def run_serving(args, world, rank, local, pg, workdir):
     all_served = serving.merge(pg, records)
     all_serial = serving.merge(pg, serial)
     total_as = reduce_sum(pg, atom_steps)
-    out = {"jobs": len(all_served), "stream": f"first {args.serve_jobs} jobs of the seeded 20 jobs/s stream",
+    out = {"jobs": len(all_served),
+           "stream": f"{'all' if args.serve_jobs >= 512 else 'first ' + str(args.serve_jobs) + ' of the'} "
+                     f"{len(jobs) if args.serve_jobs >= 512 else 512} jobs of the seeded 20 jobs/s stream",
            "steps_per_job": args.serve_steps, "tick_steps": args.serve_tick,
+           "latency": "from the scheduled arrival to completion, including ibg_setup_read of the job's files",
            "served": serving.summarize(all_served, total_as),
            "serial_fp64_plain": serving.summarize(all_serial, total_as),
            "server": {k: st[k] for k in ("peak_jobs", "peak_bytes", "budget_bytes", "ticks", "batch_builds", "gpu_s")}}
@@ -299,6 +376,81 @@ def run_serving(args, world, rank, local, pg, workdir):
         out["jobs_per_s_ratio"] = s_["jobs_per_s"] / p_["jobs_per_s"]
         out["p99_ratio"] = p_["p99_s"] / s_["p99_s"]
     return out
+
+
+BATCH_CANDIDATES = [dict(nb_tables_smem=0, nb_blocks_per_sm=0, nb_chunk=ch, nb_rows=rows)
+                    for rows in (8, 16) for ch in (0, 24, 48)]
+
+
+def run_batched_mixed(args, world, local, pg, jobs):
+    """The batched form on systems of mixed size: the first B jobs of the
+    served stream stepped together (FP32/fixed point, one launch per stage over
+    all systems, one CUDA graph per batch step, tuned by timing short batch
+    runs), against the same systems run one after another on the plain FP64
+    single-system path and on the FP32/fixed-point single-system path.  Device
+    time (CUDA events on each path's stream), state resident, K steps after W
+    warm-up steps on every path; the L2 is not flushed (the batch's working set
+    exceeds it; a small system alone fits in it, which favours the
+    single-system paths)."""
+    from ibisco_b200 import native
+
+    sel = jobs[: args.batch_jobs]
+    setups = [native.Setup(j.directory) for j in sel]
+    n_tot = sum(j.particles for j in sel)
+    K, W = args.batch_steps, args.warmup
+
+    def make_systems():
+        out = []
+        for st in setups:
+            g = native.System(st, native.IBG_PREC_FP32_FIXED)
+            g.set_state()
+            out.append(g)
+        return out
+
+    btuned, btimes = native.tune_batch(make_systems, BATCH_CANDIDATES, steps=50)
+    systems = make_systems()
+    for g in systems:
+        g.set_tuning(**btuned)
+    bat = native.Batch(systems)
+    with Clocks(local) as clk:
+        bat.run(W)
+        barrier(pg)
+        clk.mark(True)
+        bat.run(K)
+        clk.mark(False)
+    bms = reduce_max(pg, bat.timing()["run_ms"])
+    launches = bat.timing()["launches"]
+    bat.close()
+    for g in systems:
+        g.close()
+    bval = world * n_tot * K / (bms / 1000.0)
+
+    def single(prec):
+        total = 0.0
+        for st in setups:
+            g = native.System(st, prec)
+            g.set_state()
+            g.run(1, W)
+            g.run(1 + W, K)
+            total += g.timing()["run_ms"]
+            g.close()
+        total = reduce_max(pg, total)
+        return world * n_tot * K / (total / 1000.0), total / K
+
+    v64, ms64 = single(native.IBG_PREC_FP64_PLAIN)
+    v32, ms32 = single(native.IBG_PREC_FP32_FIXED)
+    sizes = [j.particles for j in sel]
+    return {"systems": len(sel), "particles": n_tot, "sizes": {"min": min(sizes), "max": max(sizes),
+                                                               "median": float(np.median(sizes))},
+            "workload": "first jobs of the seeded served stream (sizes log-uniform in 500..50,000 beads, 1-3 types, "
+                        "chains of 10-100, per-job perturbed LJ tables, dt 10 fs)",
+            "steps": K, "warmup": W, "value": bval, "unit": "atom-steps/s", "ms_per_batch_step": bms / K,
+            "tuning": btuned, "candidates_us_per_batch_step": [[t, u] for t, u in btimes],
+            "fp64_plain_single": {"value": v64, "ms_per_step_all_systems": ms64},
+            "fp32_fixed_single": {"value": v32, "ms_per_step_all_systems": ms32},
+            "ratio_over_fp64_plain_single": bval / v64, "ratio_over_fp32_fixed_single": bval / v32,
+            "gpu_launches": launches, "clocks": clk.summary(),
+            "l2": "not flushed (the batch's working set exceeds the 126 MB L2; single small systems fit in it)"}
 
 
 def reduce_sum(pg, x: float) -> float:
@@ -312,6 +464,16 @@ def reduce_sum(pg, x: float) -> float:
 
 
 TUNING_KEYS = ("nb_tables_smem", "nb_blocks_per_sm", "nb_chunk", "nb_rows")
+VS_COM = {"form": "fixed"}  # --vs-com
+
+
+def new_system(native, setup, prec):
+    """A system of the benchmark workload, with the centre-of-mass form of its
+    virtual sites as --vs-com selects."""
+    g = native.System(setup, prec)
+    if VS_COM["form"] == "reference":
+        g.set_vsite_com(native.IBG_VS_COM_REFERENCE)
+    return g
 
 
 def precision_report(native, setup, state):
@@ -321,7 +483,7 @@ def precision_report(native, setup, state):
     relative error of each nonzero energy and virial term."""
     out = {}
     for name, prec in (("fp32", native.IBG_PREC_FP32_FIXED), ("fp64", native.IBG_PREC_FP64_PLAIN)):
-        g = native.System(setup, prec)
+        g = new_system(native, setup, prec)
         g.set_state(*state)
         obs = g.forces(1)
         out[name] = (obs, g.state64()["fxyz"])
@@ -357,7 +519,7 @@ def pick_tuning(native, g, setup, prec, state, flush, reps=20, top=6):
     best = [dict(zip(TUNING_KEYS, c)) for c, _ in sorted(cands, key=lambda t: t[1])[:top]]
 
     def make_one():
-        x = native.System(setup, prec)
+        x = new_system(native, setup, prec)
         x.set_state(*state)
         return x
 
@@ -382,7 +544,7 @@ def run_b200(args, world, rank, local, pg):
         nitems = len(setup.array("ITYPE"))
         dt_ps = next(float(l.split()[1]) for l in open(os.path.join(d, "control")) if l.split()[0] == "time_step")
         prec = native.IBG_PREC_FP64_PLAIN if args.precision == "fp64" else native.IBG_PREC_FP32_FIXED
-        g = native.System(setup, prec)
+        g = new_system(native, setup, prec)
         g.set_state(s0, v0, b0)
         # launch tuning of the nonbonded kernel, picked by timing (state
         # unchanged), or fixed by --tuning (profiling runs)
@@ -394,12 +556,15 @@ def run_b200(args, world, rank, local, pg):
             tuned, tune_cands, tune_steps = g.tuning(), [], []
         else:
             tuned, tune_cands, tune_steps = pick_tuning(native, g, setup, prec, (s0, v0, b0), flush)
-        # ---- warm-up (captures the CUDA graphs) and device-timed region
-        g.run(1, args.warmup)
-        barrier(pg)
-        l0 = g.timing()["launches"]
+        # ---- warm-up (captures the CUDA graphs) and device-timed region, with
+        # the clock sampler running over both
         with Clocks(local) as clk:
+            g.run(1, args.warmup)
+            barrier(pg)
+            l0 = g.timing()["launches"]
+            clk.mark(True)
             g.run(1 + args.warmup, args.steps)
+            clk.mark(False)
         tm = g.timing()
         launches = tm["launches"] - l0
         ms = reduce_max(pg, tm["run_ms"])
@@ -478,7 +643,7 @@ def run_b200(args, world, rank, local, pg):
         # ---- plain FP64 path, same workload and timing
         fp64 = None
         if prec == native.IBG_PREC_FP32_FIXED and not args.no_fp64:
-            g64 = native.System(setup, native.IBG_PREC_FP64_PLAIN)
+            g64 = new_system(native, setup, native.IBG_PREC_FP64_PLAIN)
             g64.set_state(s0, v0, b0)
             g64.set_l2_flush(flush)
             if not args.tuning:  # the comparison path gets its own best launch tuning
@@ -489,48 +654,16 @@ def run_b200(args, world, rank, local, pg):
             fp64 = {"value": world * n * args.steps / (ms64 / 1000.0), "ms_per_step": ms64 / args.steps,
                     "ratio_fp32_fixed_over_fp64": ms64 / ms}
             g64.close()
-        # ---- batched form: B independent copies of the workload, one launch per
-        # stage over all of them (ibg_batch); device time, state resident
+        # ---- batched form on a mix of system sizes, and the served job stream
+        jobs = None
+        if prec == native.IBG_PREC_FP32_FIXED and (args.batch_jobs > 1 or args.serve_jobs > 0):
+            jobs = stream_jobs(args, d)
         batched = None
-        if prec == native.IBG_PREC_FP32_FIXED and args.batch > 1:
-            def make_systems():
-                out = []
-                for _ in range(args.batch):
-                    gb = native.System(setup, native.IBG_PREC_FP32_FIXED)
-                    gb.set_state(s0, v0, b0)
-                    out.append(gb)
-                return out
-
-            # the batch's own launch tuning (it can differ from one system's)
-            cands = []
-            for cand in [tuned] + [dict(nb_tables_smem=0, nb_blocks_per_sm=0, nb_chunk=ch, nb_rows=rows)
-                                   for rows in (8, 16) for ch in (0, 24, 48)]:
-                if cand not in cands:
-                    cands.append(cand)
-            btuned, btimes = native.tune_batch(make_systems, cands, steps=100)
-            systems = make_systems()
-            for gb in systems:
-                gb.set_tuning(**btuned)
-            bat = native.Batch(systems)
-            bat.run(args.warmup)
-            barrier(pg)
-            with Clocks(local) as clk_b:
-                bat.run(args.steps)
-            bms = reduce_max(pg, bat.timing()["run_ms"])
-            bval = world * args.batch * n * args.steps / (bms / 1000.0)
-            batched = {"systems": args.batch, "value": bval, "unit": "atom-steps/s", "tuning": btuned,
-                       "candidates_us_per_batch_step": [[t, u] for t, u in btimes],
-                       "ms_per_step": bms / args.steps, "particles_per_step": args.batch * n,
-                       "l2": "not flushed; the batch's working set exceeds the 126 MB L2",
-                       "clocks": clk_b.summary()}
-            if fp64:
-                batched["ratio_over_fp64_plain_single"] = bval / fp64["value"]
-            bat.close()
-            for gb in systems:
-                gb.close()
+        if jobs is not None and args.batch_jobs > 1:
+            batched = run_batched_mixed(args, world, local, pg, jobs)
         serving = None
-        if args.serve_jobs > 0 and prec == native.IBG_PREC_FP32_FIXED:
-            serving = run_serving(args, world, rank, local, pg, d)
+        if jobs is not None and args.serve_jobs > 0:
+            serving = run_serving(args, world, rank, local, pg, jobs)
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu:
             cpu = cpu_baseline(d, n)
@@ -542,11 +675,11 @@ def run_b200(args, world, rank, local, pg):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32" if prec == native.IBG_PREC_FP32_FIXED else "f64",
                 "data": "synthetic",
-                "config": {"workload": args.workload, "description": WORKLOADS[args.workload], "particles": n,
-                           "precision": "FP32 pair math, int64 fixed-point force sums, FP64 integration"
-                           if prec == native.IBG_PREC_FP32_FIXED else "FP64 throughout",
-                           "parallelism": f"{world} independent replica(s), one per GPU",
-                           "l2": "flushed before every step (256 MiB write, outside the timed interval)"},
+                "config": workload_config(args, n),
+                "precision": "FP32 pair math, int64 fixed-point force sums, FP64 integration"
+                if prec == native.IBG_PREC_FP32_FIXED else "FP64 throughout",
+                "parallelism": f"{world} independent replica(s), one per GPU",
+                "l2": "flushed before every step (256 MiB write, outside the timed interval)",
                 "ns_per_day": steps_per_s * dt_ps * 1e-3 * 86400.0,
                 "roofline": roof, "stage_ms_per_step": stage,
                 "tuning": {"nonbonded": tuned, "candidates_us": [[list(c), u] for c, u in tune_cands],
@@ -563,21 +696,28 @@ def run_b200(args, world, rank, local, pg):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10000)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="melt40k")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="melt2m")
+    ap.add_argument("--vs-com", choices=["fixed", "reference"], default="fixed",
+                    help="centre-of-mass virtual sites: each at its centre of mass, or the reference's form "
+                         "(VIRTUAL_DEF.f90:31 resets only the x sum)")
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--batch", type=int, default=16, help="systems in the batched leg (0 or 1: no batched leg)")
-    ap.add_argument("--serve-jobs", type=int, default=48, help="jobs of the served stream (0: no serving leg)")
+    ap.add_argument("--batch-jobs", type=int, default=64,
+                    help="systems of mixed size in the batched leg (0 or 1: no batched leg)")
+    ap.add_argument("--batch", dest="batch_jobs", type=int, help="same as --batch-jobs")
+    ap.add_argument("--batch-steps", type=int, default=200, help="steps of the batched leg and its comparisons")
+    ap.add_argument("--serve-jobs", type=int, default=512, help="jobs of the served stream (0: no serving leg)")
     ap.add_argument("--tuning", default="", help="fixed nonbonded tuning 'tables_smem,blocks_per_sm,chunk[,rows]' "
                                                   "instead of the autotuner (for profiling)")
     ap.add_argument("--serve-steps", type=int, default=2000)
     ap.add_argument("--serve-tick", type=int, default=100)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    VS_COM["form"] = args.vs_com
     world, rank, local, pg = dist_setup()
     try:
         if args.impl == "reference":

@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import time
 
 import numpy as np
 
@@ -465,6 +466,7 @@ class Server:
             raise IbiscoError(rc, "ibg_server_create failed")
         self._h = h
         self._shapes = {}
+        self._submitted = {}  # job -> time.perf_counter() at ibg_server_submit
 
     def submit(self, directory: str, nsteps: int) -> int:
         """Read a system directory (the reference's input files) and queue it."""
@@ -476,11 +478,13 @@ class Server:
         d = IbgDesc.from_address(lib().ibg_setup_desc(h))
         shape = (d.nitems, d.natoms)
         job = ctypes.c_longlong()
+        t = time.perf_counter()
         rc = lib().ibg_server_submit(self._h, h, int(nsteps), ctypes.byref(job))
         if rc != 0:
             lib().ibg_setup_free(h)
             raise IbiscoError(rc, "ibg_server_submit failed")
         self._shapes[job.value] = shape
+        self._submitted[job.value] = t
         return job.value
 
     def wait(self, job: int, timeout_s: float = -1.0) -> int:
@@ -498,7 +502,8 @@ class Server:
         rc = lib().ibg_server_result(self._h, int(job), _fp(s), _fp(v), ctypes.byref(o), t)
         if rc != 0:
             raise IbiscoError(rc, lib().ibg_server_job_error(self._h, int(job)).decode())
-        return {"sxyz": s, "vxyz": v, "obs": o.as_dict(), "queued_s": t[0], "run_s": t[1], "latency_s": t[2]}
+        return {"sxyz": s, "vxyz": v, "obs": o.as_dict(), "queued_s": t[0], "run_s": t[1], "latency_s": t[2],
+                "submitted_at": self._submitted[job]}
 
     def stats(self) -> dict:
         st = ServerStats()

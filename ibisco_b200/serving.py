@@ -73,7 +73,11 @@ def serial_schedule(arrivals, service_s):
 
 def replay(server, jobs, time_scale: float = 1.0):
     """Submit each job at its arrival time (scaled), wait for all; returns
-    [(arrival_s, done_s)] in submission-clock seconds and the job ids."""
+    [(arrival_s, done_s)] in stream-clock seconds and the job ids.  A job's
+    latency runs from its scheduled arrival to its completion, so it includes
+    reading its input files (ibg_setup_read, on this thread before the
+    submission) and any lag of the submission behind the schedule, as the
+    serial baseline's service time includes its setup."""
     t0 = time.perf_counter()
     ids = []
     for j in sorted(jobs, key=lambda j: j.arrival_s):
@@ -85,8 +89,7 @@ def replay(server, jobs, time_scale: float = 1.0):
     records = []
     for j, jid in ids:
         r = server.result(jid)
-        arrival = j.arrival_s * time_scale
-        records.append((arrival, arrival + r["latency_s"]))
+        records.append((j.arrival_s * time_scale, r["submitted_at"] - t0 + r["latency_s"]))
     return records, ids
 
 

@@ -105,16 +105,20 @@ def write_system(spec: SystemSpec, directory: str) -> str:
              " ********** Vx Vy Vz (in nm/ps) Indices_of_bonded_atoms         *******",
              " " + "*" * 70,
              f" num_of_molecules: {len(spec.molecules)}"]
+    # REAL*4 values to 9 significant digits, which read back to the same REAL*4
+    pos = spec.pos.astype(np.float32).astype(np.float64).tolist()
+    vel = spec.vel.astype(np.float32).astype(np.float64).tolist()
+    itype = [int(t) for t in spec.itype]
+    labels = [t[2] for t in spec.types]
     i = 0
     out = []
     for m, (name, cnt) in enumerate(spec.molecules, 1):
         out.append(f" {cnt} atoms_in_molecule_no. {m} {name}")
         for _ in range(cnt):
             b = spec.bonds[i]
-            lab = spec.types[spec.itype[i] - 1][2]
-            out.append(f" {i + 1} {spec.itype[i]} {len(b)} {_fmt(spec.pos[i, 0])} {_fmt(spec.pos[i, 1])} "
-                       f"{_fmt(spec.pos[i, 2])} {lab}")
-            out.append("   " + " ".join(_fmt(x) for x in spec.vel[i]) + "  " + " ".join(str(x) for x in b))
+            p, v, t = pos[i], vel[i], itype[i]
+            out.append(" %d %d %d %.9g %.9g %.9g %s" % (i + 1, t, len(b), p[0], p[1], p[2], labels[t - 1]))
+            out.append("   %.9g %.9g %.9g  " % (v[0], v[1], v[2]) + " ".join(map(str, b)))
             i += 1
     assert i == n
     with open(os.path.join(directory, "coordinate"), "w") as f:
