@@ -34,15 +34,28 @@
 namespace {
 
 // ------------------------------------------------------------ text records
+// Input files of the reader chain held in memory (ibg_setup_read_mem): file
+// name -> contents.  While set on the calling thread, every file the readers
+// open is looked up here by its name instead of on disk.
+thread_local const std::map<std::string, std::string>* t_files = nullptr;
+
 struct Records {
   std::vector<std::string> line;
   size_t at = 0;
   bool load(const std::string& path) {
-    std::ifstream f(path, std::ios::binary);
-    if (!f) return false;
-    std::stringstream ss;
-    ss << f.rdbuf();
-    std::string all = ss.str();
+    std::string all;
+    if (t_files) {
+      const size_t k = path.find_last_of('/');
+      auto it = t_files->find(k == std::string::npos ? path : path.substr(k + 1));
+      if (it == t_files->end()) return false;
+      all = it->second;
+    } else {
+      std::ifstream f(path, std::ios::binary);
+      if (!f) return false;
+      std::stringstream ss;
+      ss << f.rdbuf();
+      all = ss.str();
+    }
     line.clear();
     size_t b = 0;
     for (size_t i = 0; i <= all.size(); ++i) {
@@ -309,6 +322,31 @@ bool table_file(const std::string& path, XY* t) {
   return true;
 }
 
+// One nonbonded table into column i of s->tn (RDINTERACT.f90:504-533): the
+// potential converted from kJ/mol to reduced units, and a row at r = 0
+// inserted (row 1 then holds r = bin with row 0's potential) when the file's
+// first r is not 0.  The column must be zero and at least rows + 4 long.
+bool nb_table(ibg_setup* s, int i, const XY& t) {
+  auto energy = [&](float v) { return v * 1000.0f / s->NA / s->ESCALE; };  // RDINTERACT.f90:506-507,526
+  if (t.x.size() < 2) return false;
+  const float x0 = t.x[0], x1 = t.x[1], bin = x1 - x0;
+  s->tn.bin[i - 1] = bin;
+  int K;
+  if (x0 != 0.0f) {
+    s->tn.X(i, 0) = 0.0f; s->tn.P(i, 0) = energy(t.y[0]);
+    s->tn.X(i, 1) = bin;  s->tn.P(i, 1) = energy(t.y[0]);
+    s->tn.X(i, 2) = x1;   s->tn.P(i, 2) = energy(t.y[1]);
+    K = 3;
+  } else {
+    s->tn.X(i, 0) = x0; s->tn.P(i, 0) = energy(t.y[0]);
+    s->tn.X(i, 1) = x1; s->tn.P(i, 1) = energy(t.y[1]);
+    K = 2;
+  }
+  for (size_t k = 2; k < t.x.size(); ++k, ++K) { s->tn.X(i, K) = t.x[k]; s->tn.P(i, K) = energy(t.y[k]); }
+  s->tn.ndat[i - 1] = K - 1;
+  return true;
+}
+
 bool interaction(ibg_setup* s, const std::string& dir) {
   Records r;
   if (!r.load(dir + "/interaction")) return fail(s, "File interaction does not exist");
@@ -467,25 +505,8 @@ bool interaction(ibg_setup* s, const std::string& dir) {
     size_t maxn = 2;
     for (auto& t : nx) maxn = std::max(maxn, t.x.size());
     s->tn.init(nn, (int)maxn + 4, true);
-    for (int i = 1; i <= nn; ++i) {
-      auto& t = nx[i - 1];
-      if (t.x.size() < 2) return fail(s, "interaction: nonbonded table too short");
-      float x0 = t.x[0], x1 = t.x[1], bin = x1 - x0;
-      s->tn.bin[i - 1] = bin;
-      int K;
-      if (x0 != 0.0f) {
-        s->tn.X(i, 0) = 0.0f; s->tn.P(i, 0) = energy(t.y[0]);
-        s->tn.X(i, 1) = bin;  s->tn.P(i, 1) = energy(t.y[0]);
-        s->tn.X(i, 2) = x1;   s->tn.P(i, 2) = energy(t.y[1]);
-        K = 3;
-      } else {
-        s->tn.X(i, 0) = x0; s->tn.P(i, 0) = energy(t.y[0]);
-        s->tn.X(i, 1) = x1; s->tn.P(i, 1) = energy(t.y[1]);
-        K = 2;
-      }
-      for (size_t k = 2; k < t.x.size(); ++k, ++K) { s->tn.X(i, K) = t.x[k]; s->tn.P(i, K) = energy(t.y[k]); }
-      s->tn.ndat[i - 1] = K - 1;
-    }
+    for (int i = 1; i <= nn; ++i)
+      if (!nb_table(s, i, nx[i - 1])) return fail(s, "interaction: nonbonded table too short");
   }
   // out of planes (:543-666); the map is not symmetrised (:608-616)
   int no;
@@ -509,6 +530,16 @@ bool interaction(ibg_setup* s, const std::string& dir) {
 }
 
 // ---------------------------------------------------------------- FTABLE.f90
+// Nonbonded table i (FTABLE.f90:59-75); the last row uses the zero potential
+// past the table.
+void ftable_nb(ibg_setup* s, int i) {
+  Table& n = s->tn;
+  int nd = n.ndat[i - 1];
+  for (int j = 1; j <= nd; ++j)
+    n.F(i, j) = (float)((double)(-(n.P(i, j + 1) - n.P(i, j - 1)) / n.bin[i - 1] / n.X(i, j)) / 2.0);
+  n.F(i, 0) = n.F(i, 1);
+}
+
 void ftable(ibg_setup* s) {
   const float D2R = s->D2R;
   Table& b = s->tb;  // bonds :26-32, F/r; the end store at :31 indexes with the
@@ -532,13 +563,7 @@ void ftable(ibg_setup* s) {
   ang(s->ta, false);  // :35-43
   ang(s->tt, true);   // :47-55
   ang(s->to, true);   // :78-86
-  Table& n = s->tn;   // :59-75; the last row uses the zero potential past the table
-  for (int i = 1; i <= n.n; ++i) {
-    int nd = n.ndat[i - 1];
-    for (int j = 1; j <= nd; ++j)
-      n.F(i, j) = (float)((double)(-(n.P(i, j + 1) - n.P(i, j - 1)) / n.bin[i - 1] / n.X(i, j)) / 2.0);
-    n.F(i, 0) = n.F(i, 1);
-  }
+  for (int i = 1; i <= s->tn.n; ++i) ftable_nb(s, i);
 }
 
 // ---------------------------------------------------------------- SCALEV.f90
@@ -884,6 +909,52 @@ int ibg_setup_read(const char* dir, ibg_setup** out, char* err, int errlen) {
     return IBG_E_IO;
   }
   *out = s;
+  return IBG_OK;
+}
+
+int ibg_setup_read_mem(int nfiles, const char* const* names, const char* const* data, const long* sizes,
+                       ibg_setup** out, char* err, int errlen) {
+  if (!out || nfiles < 0 || (nfiles > 0 && (!names || !data || !sizes))) return IBG_E_INVALID;
+  *out = nullptr;
+  std::map<std::string, std::string> files;
+  for (int k = 0; k < nfiles; ++k) {
+    if (!names[k] || sizes[k] < 0 || (sizes[k] > 0 && !data[k])) return IBG_E_INVALID;
+    files[names[k]] = std::string(data[k] ? data[k] : "", (size_t)sizes[k]);
+  }
+  auto* s = new ibg_setup();
+  t_files = &files;
+  const bool ok = read_all(s, "");
+  t_files = nullptr;
+  if (!ok) {
+    if (err && errlen > 0) std::snprintf(err, errlen, "%s", s->err.c_str());
+    delete s;
+    return IBG_E_IO;
+  }
+  *out = s;
+  return IBG_OK;
+}
+
+int ibg_setup_set_nb_table(ibg_setup* s, int table, int nrows, const float* r, const float* v) {
+  if (!s || !r || !v || nrows < 2 || table < 1 || table > s->tn.n) return IBG_E_INVALID;
+  Table& n = s->tn;
+  const int need = nrows + 4;  // a possible inserted row 0, rows up to NDATNB+1 and the zero row past it
+  if (need > n.ld) {           // a longer table: widen every column
+    Table w;
+    w.init(n.n, need, true);
+    for (int i = 1; i <= n.n; ++i) {
+      for (int k = 0; k < n.ld; ++k) { w.X(i, k) = n.X(i, k); w.P(i, k) = n.P(i, k); w.F(i, k) = n.F(i, k); }
+      w.bin[i - 1] = n.bin[i - 1];
+      w.ndat[i - 1] = n.ndat[i - 1];
+    }
+    n = std::move(w);
+  }
+  for (int k = 0; k < n.ld; ++k) n.X(table, k) = n.P(table, k) = n.F(table, k) = 0.0f;
+  XY t;
+  t.x.assign(r, r + nrows);
+  t.y.assign(v, v + nrows);
+  nb_table(s, table, t);
+  ftable_nb(s, table);
+  fill_desc(s);
   return IBG_OK;
 }
 

@@ -42,6 +42,7 @@ EXPORTS = [
     "ibg_server_create", "ibg_server_submit", "ibg_server_wait", "ibg_server_drain", "ibg_server_result",
     "ibg_server_job_error", "ibg_server_get_stats", "ibg_server_destroy",
     "ibg_get_tuning", "ibg_set_tuning", "ibg_autotune", "ibg_set_vsite_com",
+    "ibg_setup_read_mem", "ibg_setup_set_nb_table",
 ]
 
 IBG_JOB_QUEUED, IBG_JOB_RUNNING, IBG_JOB_DONE, IBG_JOB_FAILED = 0, 1, 2, 3
@@ -143,6 +144,10 @@ def lib(build_if_missing: bool = True):
     sig = {
         "ibg_setup_read": (ctypes.c_int, [cp, pvp, cp, ctypes.c_int]),
         "ibg_setup_desc": (vp, [vp]),
+        "ibg_setup_read_mem": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
+                                              ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_long), pvp,
+                                              cp, ctypes.c_int]),
+        "ibg_setup_set_nb_table": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, fp, fp]),
         "ibg_setup_initial_state": (ctypes.c_int, [vp, fp, fp, fp]),
         "ibg_setup_control": (ctypes.c_int, [vp, ip, ctypes.c_int]),
         "ibg_setup_array_i": (ctypes.c_long, [vp, cp, ip, ctypes.c_long]),
@@ -218,13 +223,22 @@ def _dp(a):
 
 
 class Setup:
-    """The reference's setup phase run on the host from an input directory."""
+    """The reference's setup phase run on the host from an input directory,
+    or (files=) from the input files held in memory, {name: bytes or str}."""
 
-    def __init__(self, directory: str):
+    def __init__(self, directory: str = None, files: dict = None):
         L = lib()
         h = ctypes.c_void_p()
         err = ctypes.create_string_buffer(512)
-        rc = L.ibg_setup_read(directory.encode(), ctypes.byref(h), err, 512)
+        if files is not None:
+            items = [(k.encode(), v.encode() if isinstance(v, str) else bytes(v)) for k, v in files.items()]
+            n = len(items)
+            names = (ctypes.c_char_p * n)(*[k for k, _ in items])
+            data = (ctypes.c_char_p * n)(*[v for _, v in items])
+            sizes = (ctypes.c_long * n)(*[len(v) for _, v in items])
+            rc = L.ibg_setup_read_mem(n, names, data, sizes, ctypes.byref(h), err, 512)
+        else:
+            rc = L.ibg_setup_read(directory.encode(), ctypes.byref(h), err, 512)
         if rc != 0:
             raise IbiscoError(rc, err.value.decode())
         self._h = h
@@ -252,6 +266,19 @@ class Setup:
         a = np.zeros(max(n, 1), np.float32)
         L.ibg_setup_array_f(self._h, name.encode(), _fp(a), n)
         return a[:n]
+
+    def set_nb_table(self, table: int, r, v):
+        """Replace nonbonded table `table` (1-based) by rows r (nm), V (kJ/mol)."""
+        r = np.ascontiguousarray(r, np.float32)
+        v = np.ascontiguousarray(v, np.float32)
+        rc = lib().ibg_setup_set_nb_table(self._h, int(table), len(r), _fp(r), _fp(v))
+        if rc != 0:
+            raise IbiscoError(rc, "ibg_setup_set_nb_table failed")
+
+    def release(self):
+        """Hand the setup over (to ibg_server_submit, which frees it)."""
+        h, self._h = self._h, None
+        return h
 
     def initial_state(self):
         itype = self.array("ITYPE")
@@ -468,13 +495,18 @@ class Server:
         self._shapes = {}
         self._submitted = {}  # job -> time.perf_counter() at ibg_server_submit
 
-    def submit(self, directory: str, nsteps: int) -> int:
-        """Read a system directory (the reference's input files) and queue it."""
-        h = ctypes.c_void_p()
-        err = ctypes.create_string_buffer(512)
-        rc = lib().ibg_setup_read(directory.encode(), ctypes.byref(h), err, 512)
-        if rc != 0:
-            raise IbiscoError(rc, err.value.decode())
+    def submit(self, system, nsteps: int) -> int:
+        """Queue a job: a system directory (the reference's input files, read
+        here) or a Setup (made from files in memory, say), which the server
+        takes over."""
+        if isinstance(system, Setup):
+            h = ctypes.c_void_p(system.release())
+        else:
+            h = ctypes.c_void_p()
+            err = ctypes.create_string_buffer(512)
+            rc = lib().ibg_setup_read(system.encode(), ctypes.byref(h), err, 512)
+            if rc != 0:
+                raise IbiscoError(rc, err.value.decode())
         d = IbgDesc.from_address(lib().ibg_setup_desc(h))
         shape = (d.nitems, d.natoms)
         job = ctypes.c_longlong()

@@ -142,6 +142,23 @@ typedef struct ibg_setup ibg_setup;
  * initial_state receives SXYZ(3,NATOMS), VXYZ(3,NATOMS) (reduced units) and BOX.
  */
 int ibg_setup_read(const char* dir, ibg_setup** out, char* err, int errlen);
+/* The same reader chain on input files held in memory: nfiles buffers, each
+   with the file name the control and interaction files refer to ("control",
+   "interaction", "coordinate", "virtual", "virtbonds", "virtangles" and every
+   table file), data[k] of sizes[k] bytes.  A host that builds its inputs in
+   memory, such as an iterative Boltzmann inversion loop writing new trial
+   potentials, sets systems up without touching the file system
+   (RDINTERACT.f90, RDCOOR.f90 and RDVIRTUAL.f90 read those files). */
+int ibg_setup_read_mem(int nfiles, const char* const* names, const char* const* data, const long* sizes,
+                       ibg_setup** out, char* err, int errlen);
+/* Replace nonbonded table `table` (1..NNBTYPE) of a setup by nrows rows
+   r(nm), V(kJ/mol): the two columns of a table file, as REAL*4.  The rows go
+   through RDINTERACT.f90:504-533 (unit conversion, a row at r = 0 inserted
+   when r(1) is not 0) and FTABLE.f90:59-75, exactly as a file with those values
+   would; the setup's descriptor points to the new tables afterwards.  The
+   interaction of an IBI iteration changes its potentials this way between
+   trial runs. */
+int ibg_setup_set_nb_table(ibg_setup* s, int table, int nrows, const float* r, const float* v);
 const ibg_desc* ibg_setup_desc(const ibg_setup* s);
 int ibg_setup_initial_state(const ibg_setup* s, float* sxyz, float* vxyz, float* box);
 /* Integer/float scalars of the control file not carried by the descriptor:

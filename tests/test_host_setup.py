@@ -2,6 +2,8 @@
 phase bit for bit: type maps, SETLIS angle/torsion/out-of-plane lists,
 exclusions (BUILD_CONNECTIVITY + RDVIRTBONDS), virtual-site maps (RDVIRTUAL)
 and the FTABLE force tables, checked against the oracle's restatement."""
+import os
+
 import numpy as np
 import pytest
 
@@ -119,3 +121,65 @@ def test_exclusions_rows_are_sorted_and_bounded(sysdir):
     for i in range(natoms):
         row = to[: conn[i], i]
         assert (conn[i] <= 20) and np.all(row[:-1] < row[1:]) if len(row) > 1 else True
+
+
+def read_files(d):
+    return {f: open(os.path.join(d, f), "rb").read() for f in os.listdir(d)}
+
+
+def same_setup(a, b):
+    """Every array of two setups bit for bit; tables over the rows a step can
+    read (0..NDAT+1), whatever their leading dimension."""
+    for name in INT_ARRAYS + FLOAT_ARRAYS + ["SXYZ", "NDATNB", "BINNB"]:
+        np.testing.assert_array_equal(a.array(name), b.array(name), err_msg=name)
+    nd = a.array("NDATNB")
+    for name in ("RNBOND", "NBOND_POT", "NBOND_FORCE"):
+        xa, xb = a.array(name), b.array(name)
+        wa, wb = len(xa) // len(nd), len(xb) // len(nd)
+        for t in range(len(nd)):
+            rows = nd[t] + 2
+            np.testing.assert_array_equal(xa[wa * t + np.arange(rows)], xb[wb * t + np.arange(rows)],
+                                          err_msg=f"{name} table {t + 1}")
+
+
+@pytest.mark.parametrize("name", ["mix4", "hybrid", "mix5_mts"])
+def test_setup_from_files_in_memory_equals_directory(sysdir, name):
+    """ibg_setup_read_mem runs the same readers on buffers as ibg_setup_read
+    on the directory's files."""
+    d = sysdir(name)
+    same_setup(native.Setup(d), native.Setup(files=read_files(d)))
+
+
+def test_setup_from_memory_reports_a_missing_file(sysdir):
+    files = read_files(sysdir("mix4"))
+    del files["coordinate"]
+    with pytest.raises(native.IbiscoError, match="coordinate"):
+        native.Setup(files=files)
+
+
+@pytest.mark.parametrize("case", ["same_length", "longer", "offset_start"])
+def test_nonbonded_table_replacement_equals_reading_that_table(sysdir, tmp_path, case):
+    """ibg_setup_set_nb_table gives the arrays of a setup read from files whose
+    table holds the same rows (RDINTERACT.f90:504-533 and FTABLE.f90:59-75):
+    a perturbed table of the same length, a longer one (the table columns
+    widen), and one that does not start at r = 0 (a row 0 is inserted)."""
+    import shutil
+
+    from ibisco_b200 import synth
+
+    src = sysdir("fluid")
+    rmax, dr = {"same_length": (1.2, 0.002), "longer": (1.6, 0.002), "offset_start": (1.2, 0.002)}[case]
+    t = synth.perturbed_lj_table("nb11", 0.47, 3.5, rmax, dr, [0.3, -0.2, 0.1, 0.05, -0.05])
+    r, v = np.asarray(t.x, np.float32), np.asarray(t.v, np.float32)
+    if case == "offset_start":
+        r, v = r[5:], v[5:]
+    d2 = str(tmp_path / "replaced")
+    shutil.copytree(src, d2)
+    with open(os.path.join(d2, "nb11"), "w") as f:
+        for a, b in zip(r.astype(np.float64), v.astype(np.float64)):
+            f.write("%.9g  %.9g\n" % (a, b))
+    s = native.Setup(src)
+    s.set_nb_table(1, r, v)
+    same_setup(native.Setup(d2), s)
+    with pytest.raises(native.IbiscoError):
+        s.set_nb_table(2, r, v)

@@ -94,3 +94,33 @@ def test_failed_job_does_not_stop_the_others(jobdirs, tmp_path):
         srv.result(badj)
     assert e.value.code == -6
     srv.close()
+
+
+def test_served_job_from_memory_with_a_replaced_table(jobdirs, tmp_path):
+    """An iterative Boltzmann inversion trial without files: the job's inputs
+    are read from memory (ibg_setup_read_mem), its nonbonded table is replaced
+    (ibg_setup_set_nb_table) and the setup is submitted.  Its result is bitwise
+    that of the same system read from a directory whose table file holds the
+    new rows, run alone."""
+    import shutil
+
+    src = jobdirs[1]
+    files = {f: open(os.path.join(src, f), "rb").read() for f in os.listdir(src)}
+    s = native.Setup(files=files)
+    name = "nb11"  # table 1: the (1, 1) type pair of synth.serving_job
+    t = synth.perturbed_lj_table(name, 0.47, 3.5, 1.2, 0.002, [0.2, 0.1, -0.1, 0.05, 0.02])
+    r, v = np.asarray(t.x, np.float32), np.asarray(t.v, np.float32)
+    s.set_nb_table(1, r, v)
+    d2 = str(tmp_path / "trial")
+    shutil.copytree(src, d2)
+    with open(os.path.join(d2, name), "w") as f:
+        for a, b in zip(r.astype(np.float64), v.astype(np.float64)):
+            f.write("%.9g  %.9g\n" % (a, b))
+    srv = native.Server(tick_steps=20, max_jobs=4)
+    jid = srv.submit(s, 40)
+    assert srv.drain(120.0)
+    res = srv.result(jid)
+    srv.close()
+    ref, robs = alone(d2, 40)
+    assert np.array_equal(res["sxyz"], ref["sxyz"]) and np.array_equal(res["vxyz"], ref["vxyz"])
+    assert res["obs"]["V_NB1"] == robs["V_NB1"]
