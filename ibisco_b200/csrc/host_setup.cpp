@@ -169,7 +169,12 @@ struct ibg_setup {
   ibg_desc d;
   std::string err;
   // UNIT.f90 constants (REAL*4)
-  float NA = 0, MASSSCALE = 0, ESCALE = 0, TEMPSCALE = 0, PSCALE = 0, TIMESCALE = 0, VSCALE = 0, R2D = 0, D2R = 0;
+  float NA = 0, MASSSCALE = 0, ESCALE = 0, TEMPSCALE = 0, PSCALE = 0, TIMESCALE = 0, VSCALE = 0, R2D = 0, D2R = 0,
+        CONV = 0;
+  // coordinate file header (RDCOOR.f90:55-65) and molecule names, for the output files
+  std::string title;
+  float initime = 0;
+  std::vector<std::string> molname;
   // control values not in the descriptor
   int nstep = 0, ntrj = 0, restart = 0, nonbexc_atom = 4, nonbexc_bead = 4;
   float taut = 0, taup = 0, beta = 0;
@@ -217,6 +222,7 @@ void units(ibg_setup* s) {  // UNIT.f90:9-23, all REAL*4
   s->VSCALE = RSCALE / s->TIMESCALE;
   s->R2D = 180.0f / PI;
   s->D2R = PI / 180.0f;
+  s->CONV = (float)((double)(s->NA * s->ESCALE) / 1000.0);
 }
 
 // ---------------------------------------------------------- RDCONTROL.f90
@@ -593,6 +599,13 @@ bool coordinate(ibg_setup* s, const std::string& dir) {
   if (!r.load(dir + "/coordinate")) return fail(s, "File coordinate does not exist");
   ibg_desc& d = s->d;
   if (r.line.size() < 11) return fail(s, "coordinate: header too short");
+  {  // RDCOOR.f90:55-65: TITLE is the first word of line 1; INITIME follows 'Time' on line 2
+    auto w0 = words80(r.line[0]);
+    s->title = w0.empty() ? "" : w0[0].substr(0, 72);
+    auto w1 = words80(r.line[1]);
+    s->initime = 0.0f;
+    if (w1.size() >= 2 && w1[0] == "Time") to_f32(w1[1], &s->initime);
+  }
   r.at = 3;
   std::vector<std::string> v;
   if (!read_ld(r, 3, &v)) return fail(s, "coordinate: box");
@@ -602,12 +615,14 @@ bool coordinate(ibg_setup* s, const std::string& dir) {
   if (!read_ld(r, 2, &v) || !to_i32(v[1], &s->nmol)) return fail(s, "coordinate: num_of_molecules");
   const int N = d.nitems, NA = d.natoms;
   s->natm.assign(s->nmol, 0);
+  s->molname.assign(s->nmol, "");
   s->itype.assign(N, 0); s->type_label.assign(N, 1); s->nbonds.assign(N, 0);
   s->jbond.assign((size_t)N * 4, 0);
   s->sxyz.assign((size_t)3 * NA, 0.f); s->vxyz.assign((size_t)3 * NA, 0.f);
   int L = 0;
   for (int m = 0; m < s->nmol; ++m) {
     if (!read_ld(r, 4, &v) || !to_i32(v[0], &s->natm[m])) return fail(s, "coordinate: molecule name missing");
+    s->molname[m] = v[3];
     for (int k = 0; k < s->natm[m]; ++k) {
       if (L >= NA) return fail(s, "coordinate: number of atoms differs from NATOMS");
       if (!read_ld(r, 6, &v)) return fail(s, "coordinate: record");
@@ -1021,5 +1036,173 @@ long ibg_setup_array_f(const ibg_setup* s, const char* name, float* out, long n)
 }
 
 void ibg_setup_free(ibg_setup* s) { delete s; }
+
+}  // extern "C"
+
+// ------------------------------------------------------------ WRITETRJ.F90
+namespace {
+
+// One Fortran unformatted sequential record as gfortran writes it: the
+// payload between two 4-byte length markers.
+bool record(std::FILE* f, const void* p, size_t n) {
+  const unsigned m = (unsigned)n;
+  return std::fwrite(&m, 4, 1, f) == 1 && (n == 0 || std::fwrite(p, 1, n, f) == n) && std::fwrite(&m, 4, 1, f) == 1;
+}
+
+// Fortran Gw.d output editing: F(w-4).(d-k) and four blanks when the value
+// rounded to d digits has decimal exponent k in 0..d (0.1 <= |x| < 10^d),
+// Ew.d (0.ddd...E+ee) otherwise; zero as F(w-4).(d-1).
+std::string fortran_g(double x, int w, int d) {
+  char buf[96];
+  const double a = std::fabs(x);
+  if (a == 0.0) {
+    std::snprintf(buf, sizeof buf, "%*.*f    ", w - 4, d - 1, 0.0);
+    return buf;
+  }
+  std::snprintf(buf, sizeof buf, "%.*e", d - 1, a);  // m.mmm...e+XX, d digits
+  const char* e = std::strchr(buf, 'e');
+  const int k = std::atoi(e + 1) + 1;  // 10^(k-1) <= |x| < 10^k after rounding
+  if (k >= 0 && k <= d) {
+    char out[96];
+    std::snprintf(out, sizeof out, "%*.*f    ", w - 4, d - k, x);
+    return out;
+  }
+  std::string digits;
+  for (const char* c = buf; c < e; ++c)
+    if (*c >= '0' && *c <= '9') digits.push_back(*c);
+  char tail[16];
+  std::snprintf(tail, sizeof tail, "E%c%02d", k < 0 ? '-' : '+', std::abs(k));
+  std::string v = std::string(x < 0 ? "-" : "") + "0." + digits + tail;
+  return std::string(v.size() < (size_t)w ? w - v.size() : 0, ' ') + v;
+}
+
+}  // namespace
+
+struct ibg_trz {
+  const ibg_setup* s;
+  std::FILE* f;
+  int nframe;
+};
+
+extern "C" {
+
+int ibg_trz_open(const ibg_setup* s, const char* path, ibg_trz** out) {
+  if (!s || !path || !out) return IBG_E_INVALID;
+  std::FILE* f = std::fopen(path, "wb");
+  if (!f) return IBG_E_IO;
+  *out = new ibg_trz{s, f, 0};
+  return IBG_OK;
+}
+
+int ibg_trz_write(ibg_trz* t, int step, const ibg_obs* obs, const float* sxyz, const float* vxyz) {
+  if (!t || !obs || !sxyz || !vxyz) return IBG_E_INVALID;
+  const ibg_setup* s = t->s;
+  const ibg_desc& d = s->d;
+  const int NA = d.natoms;
+  const double small = 1.0 / 1.0e12 / (double)s->TIMESCALE;  // WRITETRJ.F90:31
+  std::vector<float> col((size_t)NA);
+  bool ok = true;
+  t->nframe += 1;
+  if (t->nframe == 1) {  // :51-55, header with the first frame
+    char title[80];
+    std::memset(title, ' ', sizeof title);
+    std::memcpy(title, s->title.data(), std::min<size_t>(s->title.size(), 72));
+    const int nrec = 10;
+    ok = ok && record(t->f, title, 80) && record(t->f, &nrec, 4);
+  }
+  // :56-58: frame number, its step index, NATOMS and the time in ps
+  const double treal = (double)((float)step * d.dt * s->TIMESCALE) * 1.0e12 + (double)s->initime;
+  unsigned char hdr[20];
+  const int hi[3] = {t->nframe, s->ntrj * t->nframe, NA};
+  std::memcpy(hdr, hi, 12);
+  std::memcpy(hdr + 12, &treal, 8);
+  ok = ok && record(t->f, hdr, 20);
+  const double boxr[9] = {(double)(float)obs->box[0], 0.0, 0.0, 0.0, (double)(float)obs->box[1], 0.0,
+                          0.0, 0.0, (double)(float)obs->box[2]};  // :60-66
+  ok = ok && record(t->f, boxr, sizeof boxr);
+  // :68-79, the pressure tensor of the step in REAL*4 as the host holds it
+  float pt[6];
+  for (int k = 0; k < 6; ++k) pt[k] = (float)obs->pt[k];  // PT11, PT22, PT33, PT12, PT13, PT23
+  const double pr[7] = {(double)(((pt[0] + pt[1]) + pt[2]) * s->PSCALE) / 3.0, (double)(pt[0] * s->PSCALE),
+                        (double)(pt[3] * s->PSCALE), (double)(pt[1] * s->PSCALE), (double)(pt[4] * s->PSCALE),
+                        (double)(pt[5] * s->PSCALE), (double)(pt[2] * s->PSCALE)};
+  ok = ok && record(t->f, pr, sizeof pr);
+  // :81-85, energies
+  auto sum3 = [](const double* v) { return (v[0] + v[1]) + v[2]; };
+  const double ptot = (((sum3(obs->v_bond) + sum3(obs->v_angle)) + sum3(obs->v_torsion)) + sum3(obs->v_oop)) +
+                      sum3(obs->v_nb);
+  const double ek = obs->ek[0] + obs->ek[1];
+  const double etot = ptot + ek;
+  const double temp = ek * (double)d.mktemp;
+  unsigned char en[52];
+  const int six = 6;
+  const double ev[6] = {etot * (double)s->CONV, ptot * (double)s->CONV, ek * (double)s->CONV, temp, 0.0, 0.0};
+  std::memcpy(en, &six, 4);
+  std::memcpy(en + 4, ev, 48);
+  ok = ok && record(t->f, en, 52);
+  for (int c = 0; c < 3 && ok; ++c) {  // :87-90
+    for (int j = 0; j < NA; ++j) col[j] = sxyz[3 * (size_t)j + c];
+    ok = record(t->f, col.data(), sizeof(float) * NA);
+  }
+  for (int c = 0; c < 3 && ok; ++c) {  // :39-47, :92-95
+    for (int j = 0; j < NA; ++j) col[j] = (float)((double)vxyz[3 * (size_t)j + c] * small);
+    ok = record(t->f, col.data(), sizeof(float) * NA);
+  }
+  ok = ok && std::fflush(t->f) == 0;
+  return ok ? IBG_OK : IBG_E_IO;
+}
+
+void ibg_trz_close(ibg_trz* t) {
+  if (!t) return;
+  if (t->f) std::fclose(t->f);
+  delete t;
+}
+
+int ibg_write_restart(const ibg_setup* s, const char* path, int step, const float* box, const float* sxyz,
+                      const float* vxyz) {
+  if (!s || !path || !box || !sxyz || !vxyz) return IBG_E_INVALID;
+  const ibg_desc& d = s->d;
+  std::FILE* f = std::fopen(path, "w");
+  if (!f) return IBG_E_IO;
+  // WRITETRJ.F90:129-143: title, time, box, a five-line header, molecule count
+  const float treal = (float)((double)((float)step * d.dt * s->TIMESCALE) * 1.0e12 + (double)s->initime);
+  std::fprintf(f, " %s\n Time\t%.9g\t(ps)\n *** box lengths X, Y, Z in nm ***\n %.9g %.9g %.9g\n", s->title.c_str(),
+               (double)treal, (double)box[0], (double)box[1], (double)box[2]);
+  std::fprintf(f, "%s\n", std::string(70, '*').c_str());
+  std::fprintf(f, "*** per atom: index, type, number of bonds, x y z (nm)\n");
+  std::fprintf(f, "*** then vx vy vz (nm/ps) and the bonded atoms\n");
+  std::fprintf(f, "*** written as WRITE_RESTART writes them\n");
+  std::fprintf(f, "%s\n", std::string(70, '*').c_str());
+  std::fprintf(f, " num_of_molecules  %d\n", s->nmol);
+  const int N = d.nitems;
+  int L = 0;
+  for (int m = 0; m < s->nmol; ++m) {  // :144-173
+    std::fprintf(f, " %d  Atoms_in_Molecule_No. %d %s\n", s->natm[m], m + 1, s->molname[m].c_str());
+    for (int j = 0; j < s->natm[m]; ++j, ++L) {
+      const int nb = s->nbonds[L];
+      std::string line = " ";
+      char buf[64];
+      std::snprintf(buf, sizeof buf, "%6d %2d %1d ", L + 1, s->itype[L], nb);
+      line += buf;
+      for (int c = 0; c < 3; ++c) line += fortran_g((double)sxyz[3 * (size_t)L + c], 21, 14) + " ";
+      std::fprintf(f, "%s\n", line.c_str());
+      line.clear();
+      const char* sep = nb == 2 ? "  " : " ";  // FORMAT 9060 spaces its velocities by two
+      for (int c = 0; c < 3; ++c) {
+        const double v = (double)(vxyz[3 * (size_t)L + c] * s->VSCALE) * 1.0e-3;
+        std::snprintf(buf, sizeof buf, "%16.10f%s", v, sep);
+        line += buf;
+      }
+      for (int b = 0; b < nb; ++b) {
+        std::snprintf(buf, sizeof buf, nb == 1 ? "%5d" : "%5d  ", s->jbond[(size_t)b * N + L]);
+        line += buf;
+      }
+      std::fprintf(f, "%s\n", line.c_str());
+    }
+  }
+  const bool ok = std::ferror(f) == 0;
+  std::fclose(f);
+  return ok ? IBG_OK : IBG_E_IO;
+}
 
 }  // extern "C"

@@ -43,6 +43,7 @@ EXPORTS = [
     "ibg_server_job_error", "ibg_server_get_stats", "ibg_server_destroy",
     "ibg_get_tuning", "ibg_set_tuning", "ibg_autotune", "ibg_set_vsite_com",
     "ibg_setup_read_mem", "ibg_setup_set_nb_table",
+    "ibg_trz_open", "ibg_trz_write", "ibg_trz_close", "ibg_write_restart",
 ]
 
 IBG_JOB_QUEUED, IBG_JOB_RUNNING, IBG_JOB_DONE, IBG_JOB_FAILED = 0, 1, 2, 3
@@ -148,6 +149,10 @@ def lib(build_if_missing: bool = True):
                                               ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_long), pvp,
                                               cp, ctypes.c_int]),
         "ibg_setup_set_nb_table": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, fp, fp]),
+        "ibg_trz_open": (ctypes.c_int, [vp, cp, pvp]),
+        "ibg_trz_write": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(IbgObs), fp, fp]),
+        "ibg_trz_close": (None, [vp]),
+        "ibg_write_restart": (ctypes.c_int, [vp, cp, ctypes.c_int, fp, fp, fp]),
         "ibg_setup_initial_state": (ctypes.c_int, [vp, fp, fp, fp]),
         "ibg_setup_control": (ctypes.c_int, [vp, ip, ctypes.c_int]),
         "ibg_setup_array_i": (ctypes.c_long, [vp, cp, ip, ctypes.c_long]),
@@ -549,6 +554,72 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+class Trajectory:
+    """A TRZ trajectory file written as WRITETRJ.F90 writes it (ibg_trz_*)."""
+
+    def __init__(self, setup: Setup, path: str):
+        h = ctypes.c_void_p()
+        rc = lib().ibg_trz_open(setup.handle, path.encode(), ctypes.byref(h))
+        if rc != 0:
+            raise IbiscoError(rc, f"cannot open {path}")
+        self._h = h
+        self.setup = setup
+
+    def write(self, step: int, obs: "IbgObs", sxyz, vxyz):
+        s = np.ascontiguousarray(sxyz, np.float32)
+        v = np.ascontiguousarray(vxyz, np.float32)
+        rc = lib().ibg_trz_write(self._h, int(step), ctypes.byref(obs), _fp(s), _fp(v))
+        if rc != 0:
+            raise IbiscoError(rc, "ibg_trz_write failed")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ibg_trz_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def write_restart(setup: Setup, path: str, step: int, box, sxyz, vxyz):
+    """The restart file of WRITE_RESTART (coordinate format) for this state."""
+    b = np.ascontiguousarray(box, np.float32)
+    s = np.ascontiguousarray(sxyz, np.float32)
+    v = np.ascontiguousarray(vxyz, np.float32)
+    rc = lib().ibg_write_restart(setup.handle, path.encode(), int(step), _fp(b), _fp(s), _fp(v))
+    if rc != 0:
+        raise IbiscoError(rc, f"cannot write {path}")
+
+
+def run_with_output(g: "System", first: int, nsteps: int, trz_path: str, restart_path: str = None,
+                    ntrj: int = None):
+    """Steps first..first+nsteps-1 in runs of NTRJ steps (the control file's
+    trajectory interval unless given); after each run a TRZ frame of its last
+    step and, when restart_path is given, the restart file, as NEW_LOOP.F90
+    calls WRITETRJ every NTRJ steps.  Each run's observables come from the
+    device's per-step ring (ibg_run) and its state from ibg_get_state.
+    Returns the observables of every step."""
+    ntrj = ntrj or g.setup.ntrj
+    trz = Trajectory(g.setup, trz_path)
+    out = []
+    st = first
+    last = first + nsteps - 1
+    while st <= last:
+        end = min(last, -(-st // ntrj) * ntrj)  # the next step that writes output
+        arr = (IbgObs * (end - st + 1))()
+        g._check(lib().ibg_run(g._h, int(st), int(end - st + 1), arr))
+        out += [arr[k].as_dict() for k in range(end - st + 1)]
+        if end % ntrj == 0:
+            x = g.state()
+            trz.write(end, arr[end - st], x["sxyz"][: g.natoms], x["vxyz"])
+            if restart_path:
+                write_restart(g.setup, restart_path, end, [arr[end - st].box[k] for k in range(3)],
+                              x["sxyz"][: g.natoms], x["vxyz"])
+        st = end + 1
+    trz.close()
+    return out
 
 
 def tune_steps(make_system, candidates, steps: int = 100, l2_flush: int = 0):

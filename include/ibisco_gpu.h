@@ -273,6 +273,25 @@ void ibg_destroy(ibg_ctx* c);
 /* Library version string. */
 const char* ibg_version(void);
 
+/* --------------------------------------------------------------- output --
+ * The trajectory and restart files of WRITETRJ.F90, for hosts that are not the
+ * Fortran program (the Fortran host keeps its own WRITETRJ).  A host runs
+ * NTRJ steps with ibg_run, reads the state with ibg_get_state and writes:
+ * ibg_trz_write: one TRZ frame after step `step` (WRITETRJ.F90:28-97): Fortran
+ *   unformatted sequential records with 4-byte length markers, as gfortran
+ *   writes them; the title and record count precede the first frame; obs of
+ *   that step (box, pressure tensor, energies), SXYZ(3,NATOMS) and
+ *   VXYZ(3,NATOMS) in reduced units as ibg_get_state returns them.
+ * ibg_write_restart: the restart file in the coordinate file's format
+ *   (WRITETRJ.F90:119-178): positions as G21.14, velocities as F16.10 nm/ps,
+ *   the setup's molecules, types and bonds; RDCOOR.f90 reads it back. */
+typedef struct ibg_trz ibg_trz;
+int ibg_trz_open(const ibg_setup* s, const char* path, ibg_trz** out);
+int ibg_trz_write(ibg_trz* t, int step, const ibg_obs* obs, const float* sxyz, const float* vxyz);
+void ibg_trz_close(ibg_trz* t);
+int ibg_write_restart(const ibg_setup* s, const char* path, int step, const float* box, const float* sxyz,
+                      const float* vxyz);
+
 /* ---------------------------------------------------------------- batch --
  * Many independent systems stepped together on one GPU.  A batch packs its
  * systems into one kernel launch per stage (blocks are mapped to systems) and
