@@ -1,13 +1,13 @@
 #!/usr/bin/env python
 """Benchmark of the B200 force-and-integrate step (one JSON line on rank 0).
 
-Workload (default): the bead-spring polymer melt of the headline metric —
-400 chains x 100 beads (40,000 beads, 3 types), tabulated harmonic bond,
-angle (112 deg) and 3-fold torsion, six Lorentz-Berthelot LJ tables to a
-1.0 nm cutoff (list 1.2 nm, rebuilt every 10 steps), Berendsen NVT at 500 K,
-dt 1 fs; seeded synthetic input written in the reference's file formats.
-A step is one loop body of NEW_LOOP.F90 (SHIFT, list rebuild when due,
-nonbonded + bonded forces, MOVE, Berendsen scaling).
+Workload (default): the CG melt of the roofline study (melt2m) -- 10,000
+chains x 200 beads (2,000,000 beads, 4 types), tabulated bond and angle
+terms, ten LJ tables to 1.4 nm (list 1.6 nm, rebuilt every 10 steps), NVT at
+300 K, dt 10 fs; seeded synthetic input written in the reference's file
+formats.  A step is one loop body of NEW_LOOP.F90 (SHIFT, list rebuild when
+due, nonbonded + bonded forces, MOVE, Berendsen scaling).  --workload picks
+the other configurations (melt40k, fluid4k, hybrid3a, hybrid3b).
 
 Legs:
   value      device time (CUDA events on the library's stream) of K steps
@@ -18,18 +18,22 @@ Legs:
              each step, ibg_get_state at the end (the L2 flush before each
              step stays outside the timed intervals);
   fp64_plain the same K steps on the plain FP64 path (comparison path);
-  batched    B independent copies of the workload stepped as one batch
-             (ibg_batch: one launch per stage over all systems, one CUDA graph
-             per batch step), against the single-system FP64 path;
-  serving    a seeded stream of jobs of mixed sizes with Poisson arrivals,
-             replayed against the continuous-batching server (ibg_server),
-             p50/p99 latency and jobs/s, against the same jobs run one after
-             another on the plain FP64 path;
+  batched    the first B jobs of the served stream (mixed sizes) stepped as
+             one batch (ibg_batch: one launch per stage over all systems, one
+             CUDA graph per batch step), against the same systems run one
+             after another on the plain FP64 and FP32 single-system paths;
+  serving    the seeded stream of 512 jobs of mixed sizes with Poisson
+             arrivals, replayed against the continuous-batching server
+             (ibg_server), p50/p99 latency and jobs/s, against the same jobs
+             run one after another on the plain FP64 path; latencies run
+             from the scheduled arrival and include reading the job's files;
   roofline   nonbonded kernel, the dominant launch: algorithmic bytes per
              launch (16 B position + 4 B per listed pair, per particle) over its
              event-timed average duration, against the measured HBM copy peak;
   cpu_baseline  the oracle (C++ restatement of the reference, OpenMP) on this
-             host's cores over a bounded sample of the same workload.
+             host's cores over a bounded sample of the same workload;
+  clocks     SM clock and clock-event reasons polled through NVML over the
+             warm-up and the timed region.
 
 --impl reference times that CPU restatement alone (the reference itself is
 Fortran and no Fortran compiler is available here or on the GPU host).
