@@ -68,6 +68,14 @@ MODULE IBISCO_GPU
        TYPE(C_PTR), INTENT(OUT) :: ctx
      END FUNCTION ibg_create
 
+     !> Centre-of-mass virtual sites as VIRTUAL_DEF.f90 computes them (1) or
+     !> each at its centre of mass (0, the default); before ibg_set_state.
+     INTEGER(C_INT) FUNCTION ibg_set_vsite_com(ctx, form) BIND(C, NAME='ibg_set_vsite_com')
+       IMPORT :: C_INT, C_PTR
+       TYPE(C_PTR), VALUE :: ctx
+       INTEGER(C_INT), VALUE :: form
+     END FUNCTION ibg_set_vsite_com
+
      INTEGER(C_INT) FUNCTION ibg_set_state(ctx, sxyz, vxyz, box) BIND(C, NAME='ibg_set_state')
        IMPORT :: C_INT, C_PTR, C_FLOAT
        TYPE(C_PTR), VALUE :: ctx
