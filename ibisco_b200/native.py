@@ -505,7 +505,7 @@ class Server:
         here) or a Setup (made from files in memory, say), which the server
         takes over."""
         if isinstance(system, Setup):
-            h = ctypes.c_void_p(system.release())
+            h = system.release()
         else:
             h = ctypes.c_void_p()
             err = ctypes.create_string_buffer(512)

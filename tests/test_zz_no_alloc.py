@@ -134,8 +134,8 @@ def call_static(torch, n, index_list, lst, nnebs, rxyz, arrays, box, rcutsq):
 def test_static_nonbonded_matches_oracle_on_hybrid_lists(sysdir, which):
     """The hybrid melt's atom list and bead list, each through the entry point
     and through the oracle's REAL*4 NONBONDED_FORCE of that list alone, on the
-    oracle's positions and lists: forces within 1e-5 (max-norm relative), and
-    V_NB(1..3) and the virial within 1e-5.  On the bead list both V_NB(2)
+    oracle's positions and lists: forces and V_NB(1..3) within 1e-5 (max-norm
+    relative), and the virial within 1e-5 of the FP64 restatement's.  On the bead list both V_NB(2)
     (bead-bead) and V_NB(3) (pairs with a site) are nonzero."""
     from oracle.oracle import Oracle
 
@@ -159,12 +159,18 @@ def test_static_nonbonded_matches_oracle_on_hybrid_lists(sysdir, which):
     box = np.array([o.finfo["BOX1"], o.finfo["BOX2"], o.finfo["BOX3"]], np.float32)
     rc_name = "RCUTSQ_ATOM" if which == 0 else "RCUTSQ_BEAD"
     f_ref, s_ref = o.nonbonded_list(which, 0)
+    # the reference sums the virial in REAL*4 (PT11... are REAL*4), which on
+    # the atom list loses ~1e-3 of it to rounding; the entry point sums it in
+    # double, so its virial is checked against the FP64 restatement
+    o64 = Oracle(d)
+    o64.init(1)
+    _, s64 = o64.nonbonded_list(which, 1)
     rc, msg, f, s = call_static(torch, len(index_list), index_list, lst, nnebs, rxyz, arrays, box,
                                 float(o.finfo[rc_name]))
     assert rc == 0, msg
     assert np.abs(f - f_ref).max() / np.abs(f_ref).max() < TOL
     assert np.abs(s[:3] - s_ref[:3]).max() <= TOL * np.abs(s_ref[:3]).max()
-    assert np.abs(s[3:] - s_ref[3:]).max() <= TOL * np.abs(s_ref[3:]).max()
+    assert np.abs(s[3:] - s64[3:]).max() <= TOL * np.abs(s64[3:]).max()
     if which == 1:
         assert abs(s_ref[1]) > 0 and abs(s_ref[2]) > 0 and s_ref[0] == 0
     # a pair type without a table: INBONDT zeroed for every pair
