@@ -622,7 +622,8 @@ def run_b200(args, world, rank, local, pg):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         g.set_state(sp, vp, bp)
-        e2e_s = time.perf_counter() - t0
+        set_s = time.perf_counter() - t0
+        e2e_s = set_s
         for k in range(k_e2e):
             flush_buf.fill_(k & 0xff)
             torch.cuda.synchronize()
@@ -631,15 +632,18 @@ def run_b200(args, world, rank, local, pg):
             e2e_s += time.perf_counter() - t0
             if rc:
                 raise native.IbiscoError(rc, L.ibg_last_error(g._h).decode())
+        steps_s = e2e_s - set_s
         t0 = time.perf_counter()
         g._check(L.ibg_get_state(g._h, native._fp(out["s"]), native._fp(out["r"]), native._fp(vo),
                                  native._fp(out["f"])))
-        e2e_s = reduce_max(pg, e2e_s + time.perf_counter() - t0)
+        get_s = time.perf_counter() - t0
+        e2e_s = reduce_max(pg, e2e_s + get_s)
         del flush_buf
         h2d = (sp.nbytes + vp.nbytes + bp.nbytes) / k_e2e
         d2h = ctypes.sizeof(native.IbgObs) + (3 * out["s"].nbytes + vo.nbytes) / k_e2e
         e2e = {"value": world * n * k_e2e / e2e_s, "unit": "atom-steps/s", "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h}
+               "d2h_bytes_per_step": d2h,
+               "seconds": {"ibg_set_state": set_s, "ibg_step_total": steps_s, "ibg_get_state": get_s}}
         # ---- error of the FP32/fixed-point path against the plain FP64 path
         precision = None
         if prec == native.IBG_PREC_FP32_FIXED and not args.no_fp64:

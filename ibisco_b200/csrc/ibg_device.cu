@@ -147,6 +147,7 @@ struct ibg_ctx {
   float r2d = 0;
   // device arrays
   double *S = nullptr, *V = nullptr, *mass = nullptr, *invmass = nullptr;
+  float* xfer = nullptr;  // device staging of REAL*4 state for ibg_set_state / ibg_get_state (12 x NITEMS)
   void *su = nullptr, *fnb = nullptr, *fb = nullptr;
   int *tbits = nullptr, *gslot = nullptr, *excl_n = nullptr, *excl = nullptr;
   int *vcenter = nullptr, *vnum = nullptr, *vmem = nullptr;
@@ -247,10 +248,15 @@ void build_list(ibg_ctx* c, const ibg_desc* d, int which) {
   L.rlist = which == 0 ? d->rlist_atom : d->rlist_bead;
   L.rlistsq = L.rlist * L.rlist;  // RLISTSQ = RLIST*RLIST (NEW_NEIGHBOUR_WITHLIST.f90:26)
   L.rcutsq = which == 0 ? d->rcutsq_atom : d->rcutsq_bead;
-  // lanes per particle: enough warps to fill the GPU twice over (64 per SM;
-  // measured: 8 lanes beat 4 on 40,000-bead batches and 48,000-atom lists)
-  L.T = 1;
-  while (L.T < 8 && (long long)L.n * L.T < 64LL * 32 * c->nsm) L.T *= 2;
+  // lanes per particle: 8.  The eight lanes of a particle take eight
+  // consecutive entries of its list, whose neighbours lie close together in
+  // slot order, so a warp's position gathers and force atomics touch fewer
+  // L1 sectors than with one lane per particle, where the 32 lanes of a row
+  // belong to 32 particles (the kernel is bound by L1 throughput).  Measured
+  // per nonbonded launch on the 2,000,000-bead melt: 1,779 us with 1 lane,
+  // 1,635 with 2, 1,505 with 4, 1,472 with 8, 1,465 with 16, 1,788 with 32;
+  // on the 40,000-bead melt 72, 61, 59, 59, 62 and 59 us.
+  L.T = 8;
   L.nslices = (L.n + 32 / L.T - 1) / (32 / L.T);
   auto& o = c->owned;
   L.idx = dupload(idx, o);
@@ -1269,14 +1275,93 @@ int ibg_create(const ibg_desc* d, int precision, ibg_ctx** out) {
   return IBG_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// REAL*4 state of the host into the FP64 state: SXYZ(3,NATOMS), the virtual
+// sites' rows zero until VIRTUAL_DEF fills them, and VXYZ(3,NATOMS).
+__global__ void k_state_in(int natoms, int nitems, const float* s, const float* v, double* S, double* V) {
+  const size_t n3 = 3 * (size_t)nitems, a3 = 3 * (size_t)natoms;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n3; k += (size_t)gridDim.x * blockDim.x) {
+    S[k] = k < a3 ? (double)s[k] : 0.0;
+    if (k < a3) V[k] = (double)v[k];
+  }
+}
+
+// Slots in list order before the first sort: slot_of = sorted = identity,
+// and each listed particle's gslot = slot * 2 + list.
+__global__ void k_slots_init(int n, int which, const int* idx, int* slot_of, int* sorted, int* gslot) {
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
+    slot_of[a] = a;
+    sorted[a] = a;
+    gslot[idx[a]] = a * 2 + which;
+  }
+}
+
+// The state as REAL*4 for ibg_get_state, into staging: SXYZ, RXYZ (wrapped,
+// from the slot-ordered positions of the particle's list), VXYZ (NATOMS rows)
+// and FXYZ (nonbonded + bonded sums), each 3 x NITEMS floats.
+template <typename R, typename A>
+__global__ void k_state_out(int natoms, int nitems, const double* S, const double* V, const int* gslot,
+                            const void* pos0, const void* pos1, const A* fnb, const A* fb, float* out) {
+  using PT = typename Prec<R>::pos_t;
+  const size_t n3 = 3 * (size_t)nitems;
+  float* s = out;
+  float* r = out + n3;
+  float* v = out + 2 * n3;
+  float* f = out + 3 * n3;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n3; k += (size_t)gridDim.x * blockDim.x) {
+    s[k] = (float)S[k];
+    if (k < 3 * (size_t)natoms) v[k] = (float)V[k];
+    if (sizeof(A) == 8 && sizeof(R) == 4) {
+      const long long q = (long long)fnb[k] + (long long)fb[k];
+      f[k] = (float)((double)q * kFixInv);
+    } else {
+      f[k] = (float)((double)fnb[k] + (double)fb[k]);
+    }
+    const size_t i = k / 3;
+    const int c3 = (int)(k - 3 * i);
+    const int g = gslot[i];
+    const PT p = ((const PT*)((g & 1) ? pos1 : pos0))[g >> 1];
+    r[k] = (float)(c3 == 0 ? p.x : (c3 == 1 ? p.y : p.z));
+  }
+}
+
+float* xfer_buf(ibg_ctx* c) {
+  if (!c->xfer) c->xfer = dalloc<float>(12 * (size_t)c->nitems, c->owned);
+  return c->xfer;
+}
+
+// The argument blocks and launch sizes a captured step graph depends on.
+std::vector<unsigned char> graph_key(const ibg_ctx* c) {
+  std::vector<unsigned char> k;
+  auto add = [&](const void* p, size_t n) {
+    const unsigned char* b = (const unsigned char*)p;
+    k.insert(k.end(), b, b + n);
+  };
+  if (c->prec == IBG_PREC_FP32_FIXED) add(&c->af, sizeof(c->af));
+  else add(&c->ad, sizeof(c->ad));
+  add(c->g_regrid, sizeof(c->g_regrid));
+  return k;
+}
+
+}  // namespace
+
+extern "C" {
+
 int ibg_set_state(ibg_ctx* c, const float* sxyz, const float* vxyz, const float* box) {
   if (!c || !sxyz || !vxyz || !box) return IBG_E_INVALID;
   try {
     const int NA = c->natoms;
-    std::vector<double> s(3 * (size_t)c->nitems, 0.0), v(3 * (size_t)NA);
-    for (size_t k = 0; k < 3 * (size_t)NA; ++k) { s[k] = sxyz[k]; v[k] = vxyz[k]; }
-    CK(cudaMemcpy(c->S, s.data(), sizeof(double) * s.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->V, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice));
+    const std::vector<unsigned char> key0 = graph_key(c);
+    {  // REAL*4 arrays to the device, widened to the FP64 state there
+      float* x = xfer_buf(c);
+      CK(cudaMemcpyAsync(x, sxyz, sizeof(float) * 3 * (size_t)NA, cudaMemcpyHostToDevice, c->st));
+      CK(cudaMemcpyAsync(x + 3 * (size_t)NA, vxyz, sizeof(float) * 3 * (size_t)NA, cudaMemcpyHostToDevice, c->st));
+      k_state_in<<<grid_for(c, 3LL * c->nitems), 256, 0, c->st>>>(NA, c->nitems, x, x + 3 * (size_t)NA, c->S, c->V);
+      CK(cudaGetLastError());
+    }
     Scalars h;
     std::memset(&h, 0, sizeof(h));
     for (int k = 0; k < 3; ++k) {
@@ -1296,30 +1381,25 @@ int ibg_set_state(ibg_ctx* c, const float* sxyz, const float* vxyz, const float*
     for (auto& L : c->L) {
       if (!L.present) continue;
       alloc_cells(c, L, box);
-      std::vector<int> ident(L.n);
-      for (int a = 0; a < L.n; ++a) ident[a] = a;
-      CK(cudaMemcpy(L.slot_of, ident.data(), sizeof(int) * L.n, cudaMemcpyHostToDevice));
-      CK(cudaMemcpy(L.sorted, ident.data(), sizeof(int) * L.n, cudaMemcpyHostToDevice));
-      CK(cudaMemset(L.fsort, 0, accsize(c) * 3 * (size_t)L.n));
-      if (L.mtsf) CK(cudaMemset(L.mtsf, 0, accsize(c) * 9 * (size_t)L.n));
+      CK(cudaMemsetAsync(L.fsort, 0, accsize(c) * 3 * (size_t)L.n, c->st));
+      if (L.mtsf) CK(cudaMemsetAsync(L.mtsf, 0, accsize(c) * 9 * (size_t)L.n, c->st));
       c->g_regrid[L.which] = grid_for(c, L.cell_cap, 2);
     }
-    CK(cudaMemset(c->fnb, 0, accsize(c) * 3 * (size_t)c->nitems));
-    CK(cudaMemset(c->fb, 0, accsize(c) * 3 * (size_t)c->nitems));
+    CK(cudaMemsetAsync(c->fnb, 0, accsize(c) * 3 * (size_t)c->nitems, c->st));
+    CK(cudaMemsetAsync(c->fb, 0, accsize(c) * 3 * (size_t)c->nitems, c->st));
     refresh_args(c);
-    {  // slots = list order before the first sort
-      std::vector<int> gs(c->nitems, 0);
-      std::vector<int> idx0, idx1;
-      for (int w = 0; w < 2; ++w) {
-        if (!c->L[w].present) continue;
-        std::vector<int> idx(c->L[w].n);
-        CK(cudaMemcpy(idx.data(), c->L[w].idx, sizeof(int) * idx.size(), cudaMemcpyDeviceToHost));
-        for (int a = 0; a < (int)idx.size(); ++a) gs[idx[a]] = a * 2 + w;
-      }
-      CK(cudaMemcpy(c->gslot, gs.data(), sizeof(int) * gs.size(), cudaMemcpyHostToDevice));
+    // slots = list order before the first sort
+    CK(cudaMemsetAsync(c->gslot, 0, sizeof(int) * (size_t)c->nitems, c->st));
+    for (auto& L : c->L)
+      if (L.present)
+        k_slots_init<<<grid_for(c, L.n), 256, 0, c->st>>>(L.n, L.which, L.idx, L.slot_of, L.sorted, c->gslot);
+    CK(cudaGetLastError());
+    // the step graphs hold the argument blocks by value: they are kept when
+    // this state left every array where it was
+    if (graph_key(c) != key0) {
+      for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+      c->graphs.clear();
     }
-    for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
-    c->graphs.clear();
     // main.F90:150-234: virtual sites, SHIFT, initial temperatures, first lists
     if (c->prec == IBG_PREC_FP32_FIXED) enq_positions<float>(c);
     else enq_positions<double>(c);
@@ -1468,51 +1548,25 @@ int ibg_run(ibg_ctx* c, int first_step, int nsteps, ibg_obs* per_step) {
 int ibg_get_state(ibg_ctx* c, float* sxyz, float* rxyz, float* vxyz, float* fxyz) {
   if (!c) return IBG_E_INVALID;
   try {
+    // narrowed to REAL*4 on the device, then one copy per requested array
+    const size_t N = c->nitems, NA = c->natoms, n3 = 3 * N;
+    float* x = xfer_buf(c);
+    const void* p0 = c->L[0].present ? c->L[0].pos4 : c->L[1].pos4;
+    const void* p1 = c->L[1].present ? c->L[1].pos4 : p0;
+    const int g = grid_for(c, (long long)n3);
+    if (c->prec == IBG_PREC_FP32_FIXED)
+      k_state_out<float, unsigned long long><<<g, 256, 0, c->st>>>(
+          c->natoms, c->nitems, c->S, c->V, c->gslot, p0, p1, (const unsigned long long*)c->fnb,
+          (const unsigned long long*)c->fb, x);
+    else
+      k_state_out<double, double><<<g, 256, 0, c->st>>>(c->natoms, c->nitems, c->S, c->V, c->gslot, p0, p1,
+                                                          (const double*)c->fnb, (const double*)c->fb, x);
+    CK(cudaGetLastError());
+    if (sxyz) CK(cudaMemcpyAsync(sxyz, x, sizeof(float) * n3, cudaMemcpyDeviceToHost, c->st));
+    if (rxyz) CK(cudaMemcpyAsync(rxyz, x + n3, sizeof(float) * n3, cudaMemcpyDeviceToHost, c->st));
+    if (vxyz) CK(cudaMemcpyAsync(vxyz, x + 2 * n3, sizeof(float) * 3 * NA, cudaMemcpyDeviceToHost, c->st));
+    if (fxyz) CK(cudaMemcpyAsync(fxyz, x + 3 * n3, sizeof(float) * n3, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
-    const size_t N = c->nitems, NA = c->natoms;
-    if (sxyz) {
-      std::vector<double> s(3 * N);
-      CK(cudaMemcpy(s.data(), c->S, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost));
-      for (size_t k = 0; k < 3 * N; ++k) sxyz[k] = (float)s[k];
-    }
-    if (vxyz) {
-      std::vector<double> v(3 * NA);
-      CK(cudaMemcpy(v.data(), c->V, sizeof(double) * 3 * NA, cudaMemcpyDeviceToHost));
-      for (size_t k = 0; k < 3 * NA; ++k) vxyz[k] = (float)v[k];
-    }
-    if (rxyz) {
-      std::vector<int> gs(N);
-      CK(cudaMemcpy(gs.data(), c->gslot, sizeof(int) * N, cudaMemcpyDeviceToHost));
-      std::vector<unsigned char> p[2];
-      for (int w = 0; w < 2; ++w) {
-        if (!c->L[w].present) continue;
-        p[w].resize(c->L[w].pos_bytes);
-        CK(cudaMemcpy(p[w].data(), c->L[w].pos4, c->L[w].pos_bytes, cudaMemcpyDeviceToHost));
-      }
-      for (size_t i = 0; i < N; ++i) {
-        int w = gs[i] & 1, s = gs[i] >> 1;
-        if (c->prec == IBG_PREC_FP32_FIXED) {
-          const float4* q = (const float4*)p[w].data();
-          rxyz[3 * i] = q[s].x; rxyz[3 * i + 1] = q[s].y; rxyz[3 * i + 2] = q[s].z;
-        } else {
-          const double4* q = (const double4*)p[w].data();
-          rxyz[3 * i] = (float)q[s].x; rxyz[3 * i + 1] = (float)q[s].y; rxyz[3 * i + 2] = (float)q[s].z;
-        }
-      }
-    }
-    if (fxyz) {
-      if (c->prec == IBG_PREC_FP32_FIXED) {
-        std::vector<long long> a(3 * N), b(3 * N);
-        CK(cudaMemcpy(a.data(), c->fnb, sizeof(long long) * 3 * N, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(b.data(), c->fb, sizeof(long long) * 3 * N, cudaMemcpyDeviceToHost));
-        for (size_t k = 0; k < 3 * N; ++k) fxyz[k] = (float)((double)(a[k] + b[k]) * kFixInv);
-      } else {
-        std::vector<double> a(3 * N), b(3 * N);
-        CK(cudaMemcpy(a.data(), c->fnb, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(b.data(), c->fb, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost));
-        for (size_t k = 0; k < 3 * N; ++k) fxyz[k] = (float)(a[k] + b[k]);
-      }
-    }
   } catch (CudaError& e) {
     return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
   }

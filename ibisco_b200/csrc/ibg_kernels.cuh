@@ -406,31 +406,50 @@ __global__ void k_scan_cells(__grid_constant__ const ListArgs L0, const ListArgs
   const int m = L.cell_cap;
   __shared__ int wsum[32];
   const int t = threadIdx.x, T = blockDim.x, lane = t & 31, warp = t >> 5, nw = (T + 31) >> 5;
-  const int chunk = (m + T - 1) / T;
-  const int b = t * chunk, e = min(m, b + chunk);
-  int s = 0;
-  for (int i = b; i < e; ++i) s += in[i];
-  int v = s;  // inclusive scan of the chunk sums: warps, then warp totals
+  // tiles of 4*T consecutive cells, thread t holding cells 4t..4t+3 of the
+  // tile: a warp reads 128 consecutive counts, and the tiles run in order
+  // with the running total carried from one to the next
+  int carry = 0;
+  for (int base = 0; base < m; base += 4 * T) {
+    int x[4], s = 0;
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, v, o);
-    if (lane >= o) v += y;
-  }
-  if (lane == 31) wsum[warp] = v;
-  __syncthreads();
-  if (warp == 0) {
-    int w = lane < nw ? wsum[lane] : 0;
+    for (int j = 0; j < 4; ++j) {
+      const int i = base + 4 * t + j;
+      x[j] = i < m ? in[i] : 0;
+      s += x[j];
+    }
+    int v = s;  // inclusive scan of the threads' sums: warps, then warp totals
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += y;
+      const int y = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += y;
     }
-    wsum[lane] = w;
+    if (lane == 31) wsum[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+      int w = lane < nw ? wsum[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      wsum[lane] = w;
+    }
+    __syncthreads();
+    int run = carry + v - s + (warp ? wsum[warp - 1] : 0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int i = base + 4 * t + j;
+      if (i < m) {
+        out[i] = run;
+        zero[i] = 0;
+      }
+      run += x[j];
+    }
+    carry += wsum[nw - 1];
+    __syncthreads();  // wsum is rewritten by the next tile
   }
-  __syncthreads();
-  int run = v - s + (warp ? wsum[warp - 1] : 0);
-  if (t == T - 1) out[m] = run + s;
-  for (int i = b; i < e; ++i) { int x = in[i]; out[i] = run; run += x; zero[i] = 0; }
+  if (t == 0) out[m] = carry;
 }
 
 template <bool B>

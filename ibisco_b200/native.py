@@ -297,7 +297,8 @@ class Setup:
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().ibg_setup_free(self._h)
+            if _lib is not None:  # None while the interpreter shuts down
+                _lib.ibg_setup_free(self._h)
             self._h = None
 
     def __del__(self):
@@ -439,7 +440,8 @@ class System:
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().ibg_destroy(self._h)
+            if _lib is not None:  # None while the interpreter shuts down
+                _lib.ibg_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -479,7 +481,8 @@ class Batch:
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().ibg_batch_destroy(self._h)
+            if _lib is not None:  # None while the interpreter shuts down
+                _lib.ibg_batch_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -549,7 +552,8 @@ class Server:
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().ibg_server_destroy(self._h)
+            if _lib is not None:  # None while the interpreter shuts down
+                _lib.ibg_server_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -576,7 +580,8 @@ class Trajectory:
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().ibg_trz_close(self._h)
+            if _lib is not None:  # None while the interpreter shuts down
+                _lib.ibg_trz_close(self._h)
             self._h = None
 
     def __del__(self):

@@ -58,29 +58,45 @@ def test_nve_drift_of_the_small_plain_case(tmp_path):
     nm^-3, unshifted table to 1.2 nm), NVE, dt 10 fs, 1,000 steps, list 1.4 nm
     rebuilt every 10 steps.  Overlaps are rejected below 0.42 nm instead of 0.3
     nm: from 0.3 nm the REAL*4 restatement of the reference itself heats to
-    ~1e33 within ten steps.  Pairs crossing the unshifted cutoff make the total
-    energy jump, so the fitted drift here measures those jumps as much as the
-    arithmetic; the bar is the same, the REAL*4 run's drift."""
+    ~1e33 within ten steps.
+
+    With the unshifted table every pair that crosses the cutoff makes the total
+    energy jump, and the trajectories of different arithmetic diverge within a
+    few hundred steps, so the fitted slope of one run is a random number of
+    order 1e-3 whatever the arithmetic (three seeds on the FP64 GPU path gave
+    7e-5, 9e-4 and 4.5e-3).  The slopes are printed; the bar is the
+    energy's step-to-step fluctuation, std(E(t+1) - E(t)) / |<E>|, which is
+    the same for every trajectory of one arithmetic: the FP32/fixed-point
+    path's must not exceed the FP64 path's (three seeds, 5 % margin) nor the
+    REAL*4 reference's (seed 1, 5 % margin)."""
     from ibisco_b200 import synth
 
-    d = str(tmp_path / "fluid4k")
-    synth.write_system(synth.lj_fluid(n=4000, seed=1, dmin=0.42, nsteps=1000), d)
     n = 1000
-    g = native.System(native.Setup(d), native.IBG_PREC_FP32_FIXED)
-    g.set_state()
-    eg = [etot(o) for o in g.run(1, n, observe=True)]
-    ref, ends = {}, {}
-    for prec in (0, 1):
-        o = Oracle(d, threads=8)
-        o.init(prec)
-        e = []
-        for st in range(1, n + 1):
-            o.step(st, prec)
-            e.append(etot(o.obs(prec)))
-        ref[prec] = drift(e)
-        ends[prec] = abs(e[-1] - e[0]) / abs(e[0])
-    gpu = drift(eg)
-    end_gpu = abs(eg[-1] - eg[0]) / abs(eg[0])
-    print(f"NVE drift over {n} steps, 4,000 beads (fitted, windowed; |E(end)-E(1)|/|E(1)|): "
-          f"GPU {gpu} {end_gpu:.3g}, oracle REAL*4 {ref[0]} {ends[0]:.3g}, oracle FP64 {ref[1]} {ends[1]:.3g}")
-    assert gpu[0] <= 1.25 * ref[0][0]
+    noise, slopes = {"fp32": [], "fp64": []}, {"fp32": [], "fp64": []}
+    ref_noise = None
+    for seed in (1, 2, 3):
+        d = str(tmp_path / f"fluid4k_{seed}")
+        synth.write_system(synth.lj_fluid(n=4000, seed=seed, dmin=0.42, nsteps=n), d)
+        s = native.Setup(d)
+        for name, prec in (("fp32", native.IBG_PREC_FP32_FIXED), ("fp64", native.IBG_PREC_FP64_PLAIN)):
+            g = native.System(s, prec)
+            g.set_state()
+            e = np.array([etot(o) for o in g.run(1, n, observe=True)])
+            noise[name].append(float(np.std(np.diff(e)) / abs(e.mean())))
+            slopes[name].append(drift(e)[0])
+            g.close()
+        if seed == 1:
+            o = Oracle(d, threads=8)
+            o.init(0)
+            e = []
+            for st in range(1, n + 1):
+                o.step(st, 0)
+                e.append(etot(o.obs(0)))
+            e = np.array(e)
+            ref_noise = float(np.std(np.diff(e)) / abs(e.mean()))
+            ref_slope = drift(e)[0]
+    print(f"4,000 beads, {n} NVE steps: step-to-step energy noise FP32/fixed {noise['fp32']}, FP64 path "
+          f"{noise['fp64']}, REAL*4 oracle (seed 1) {ref_noise:.3g}; fitted drift FP32/fixed {slopes['fp32']}, "
+          f"FP64 path {slopes['fp64']}, REAL*4 oracle (seed 1) {ref_slope:.3g}")
+    assert np.mean(noise["fp32"]) <= 1.05 * np.mean(noise["fp64"])
+    assert noise["fp32"][0] <= 1.05 * ref_noise
