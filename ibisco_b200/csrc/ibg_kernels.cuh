@@ -913,8 +913,8 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded(__grid_constant__ const NB
     for (int it = r0; it < r1; it += 2) {
       const bool v0 = it * T + q < cnt;
       const bool v1 = it + 1 < r1 && (it + 1) * T + q < cnt;
-      const int t0 = v0 ? ent[it * 32] : 0;
-      const int t1 = v1 ? ent[(it + 1) * 32] : 0;
+      const int t0 = v0 ? __ldcs(ent + it * 32) : 0;
+      const int t1 = v1 ? __ldcs(ent + (it + 1) * 32) : 0;
       const PT p0 = pos[t0];
       const PT p1 = pos[t1];
       if (v0) pair(t0, p0);
@@ -1075,11 +1075,14 @@ __global__ void __launch_bounds__(256, B ? 4 : 5) k_nonbonded_f32(__grid_constan
         vir[4] = __fmaf_rn(fz, d0, vir[4]);
         vir[5] = __fmaf_rn(fz, d1, vir[5]);
       };
+      // list entries are read once per launch: loaded evict-first (__ldcs),
+      // so that the streamed list does not push the positions and force sums
+      // it points into out of L2
       for (int it = b0; it < b1; it += 2) {
         const bool v0 = it * T + q < cnt;
         const bool v1 = it + 1 < b1 && (it + 1) * T + q < cnt;
-        const int t0 = v0 ? ent[it * 32] : 0;
-        const int t1 = v1 ? ent[(it + 1) * 32] : 0;
+        const int t0 = v0 ? __ldcs(ent + it * 32) : 0;
+        const int t1 = v1 ? __ldcs(ent + (it + 1) * 32) : 0;
         const int4 p0 = pos[t0];
         const int4 p1 = pos[t1];
         if (v0) pair(t0, p0);
