@@ -406,18 +406,27 @@ __global__ void k_scan_cells(__grid_constant__ const ListArgs L0, const ListArgs
   const int m = L.cell_cap;
   __shared__ int wsum[32];
   const int t = threadIdx.x, T = blockDim.x, lane = t & 31, warp = t >> 5, nw = (T + 31) >> 5;
-  // tiles of 4*T consecutive cells, thread t holding cells 4t..4t+3 of the
-  // tile: a warp reads 128 consecutive counts, and the tiles run in order
-  // with the running total carried from one to the next
+  // tiles of V*T consecutive cells, thread t holding cells V*t..V*t+V-1 of
+  // the tile (read and written as int4 where the tile is whole), the tiles in
+  // order with the running total carried from one to the next
+  constexpr int V = 16;
   int carry = 0;
-  for (int base = 0; base < m; base += 4 * T) {
-    int x[4], s = 0;
+  for (int base = 0; base < m; base += V * T) {
+    const int i0 = base + V * t;
+    const bool whole = i0 + V <= m;
+    int x[V], s = 0;
+    if (whole) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int i = base + 4 * t + j;
-      x[j] = i < m ? in[i] : 0;
-      s += x[j];
+      for (int j = 0; j < V / 4; ++j) {
+        const int4 q = ((const int4*)(in + i0))[j];
+        x[4 * j] = q.x; x[4 * j + 1] = q.y; x[4 * j + 2] = q.z; x[4 * j + 3] = q.w;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < V; ++j) x[j] = i0 + j < m ? in[i0 + j] : 0;
     }
+#pragma unroll
+    for (int j = 0; j < V; ++j) s += x[j];
     int v = s;  // inclusive scan of the threads' sums: warps, then warp totals
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -438,13 +447,24 @@ __global__ void k_scan_cells(__grid_constant__ const ListArgs L0, const ListArgs
     __syncthreads();
     int run = carry + v - s + (warp ? wsum[warp - 1] : 0);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int i = base + 4 * t + j;
-      if (i < m) {
-        out[i] = run;
-        zero[i] = 0;
-      }
+    for (int j = 0; j < V; ++j) {
+      const int e = run;
       run += x[j];
+      x[j] = e;
+    }
+    if (whole) {
+#pragma unroll
+      for (int j = 0; j < V / 4; ++j) {
+        ((int4*)(out + i0))[j] = make_int4(x[4 * j], x[4 * j + 1], x[4 * j + 2], x[4 * j + 3]);
+        ((int4*)(zero + i0))[j] = make_int4(0, 0, 0, 0);
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < V; ++j)
+        if (i0 + j < m) {
+          out[i0 + j] = x[j];
+          zero[i0 + j] = 0;
+        }
     }
     carry += wsum[nw - 1];
     __syncthreads();  // wsum is rewritten by the next tile
@@ -528,7 +548,8 @@ __global__ void k_slot_of(__grid_constant__ const ListArgs L0, const ListArgs* c
   }
 }
 
-// NEW_NEIGHBOUR_WITHLIST.f90:34-123.  A block builds the lists of one cell's
+// NEW_NEIGHBOUR_WITHLIST.f90:34-123 for lists of up to a few hundred
+// thousand particles.  A block builds the lists of one cell's
 // particles at a time (cells taken dynamically).  The candidates of the cell --
 // its own slots, then the slots of the 13 cells of the MAPS.f90:39-51
 // stencil, each run by decreasing A -- are staged once in shared memory, in
@@ -562,7 +583,7 @@ struct ListStage {
 };
 
 template <typename R, int T, bool B>
-__global__ void __launch_bounds__(256, 4) k_list_build(__grid_constant__ const ListArgs L0, const ListArgs* const* tab,
+__global__ void __launch_bounds__(256, 4) k_list_build_warp(__grid_constant__ const ListArgs L0, const ListArgs* const* tab,
                                                        const BlockMap bm, int always) {
   pdl_wait();
   pdl_trigger();
@@ -727,6 +748,133 @@ __global__ void __launch_bounds__(256, 4) k_list_build(__grid_constant__ const L
         }
       }
       __syncwarp();  // exs is rewritten for the next particle
+    }
+  }
+}
+
+// NEW_NEIGHBOUR_WITHLIST.f90:34-123 for large lists: a thread builds one
+// particle's list (k_list_build_warp, above, gives a warp to each particle and
+// suits lists too short to fill the GPU with one thread per particle).
+// A warp takes 32 consecutive slots at a time (dynamically), so its lanes
+// mostly share a cell and walk the same candidates in step: a candidate's
+// position is one load that the lanes share, and each lane appends what it
+// accepts to its own list in the order it visits the candidates.  That order
+// is the reference's: the particle's own cell below it by decreasing A (slots
+// keep increasing A within a cell), then the 13 cells of the MAPS.f90:39-51
+// stencil, each by decreasing A.  The distance test runs first and the
+// exclusion test only for candidates inside RLIST (the accepted set is the
+// same); exclusions are compared as slots of this list (the first four in
+// registers, the rest in shared memory), and a virtual site is recognised by
+// its label in the position's w, so no candidate's global id is loaded.
+//
+// The minimum image needs no per-candidate test: each stencil cell carries
+// its periodic shift s (0 or +-L per axis, from whether it wrapped around the
+// box), and a candidate's displacement is (x_i - x_j) - s.  For a pair inside
+// RLIST <= L/3 that shift is the nearest image, so s = ANINT(d/L)*L exactly
+// and d - s is the reference's d - ANINT(d*BOXINV)*BOX
+// (NEW_NEIGHBOUR_WITHLIST.f90:65) bit for bit; with any other shift the
+// distance is above RLIST either way.
+//
+// The list is stored in the nonbonded kernel's layout: T lanes per slot,
+// slices of P = 32/T slots, entry k of slot s (slice g) at
+// (g*w_cap + k/T)*32 + (s%P)*T + k%T.  A slot that needs more than w_cap rows
+// records its need and raises the abort flag (the host enlarges the storage
+// and repeats the step).
+template <typename R, int T, bool B>
+__global__ void __launch_bounds__(256) k_list_build_thread(__grid_constant__ const ListArgs L0, const ListArgs* const* tab,
+                                                    const BlockMap bm, int always) {
+  pdl_wait();
+  pdl_trigger();
+  using PT = typename Prec<R>::pos_t;
+  const Blk bk = blk<B>(bm);
+  __shared__ ListArgs s_args;
+  if (B) stage_args(&s_args, tab[bk.sys]);
+  const ListArgs& L = B ? s_args : L0;
+  Scalars* sc = L.sc;
+  if (sc->skip || !(always || sc->rebuild)) return;
+  constexpr int P = 32 / T;
+  __shared__ int s_ex[16][256];  // exclusions 5..20 of each thread's particle, as slots of this list
+  const int nx = sc->ncell[L.which][0], ny = sc->ncell[L.which][1], nz = sc->ncell[L.which][2];
+  const int nc[3] = {nx, ny, nz};
+  R b[3], bi[3], b2[3];
+  box_of<R>(sc, b, bi, b2);
+  const R rlsq = sizeof(R) == 4 ? (R)L.rlistsq : (R)L.rlistsqd;
+  const PT* pos = (const PT*)L.pos4;
+  const int lane = threadIdx.x & 31;
+  const int cap = L.w_cap * T;  // entries a slot may hold
+  const int nchunks = (L.n + 31) / 32;
+  for (;;) {
+    int ch = 0;
+    if (lane == 0) ch = (int)atomicAdd(&sc->work[2 + L.which], 1u);
+    ch = __shfl_sync(0xffffffffu, ch, 0);
+    if (ch >= nchunks) break;
+    const int s = ch * 32 + lane;
+    if (s >= L.n) continue;
+    const int a = L.sorted[s];
+    const int i = L.idx[a];
+    const int c0 = L.cell_of[a];
+    const PT pi = pos[s];
+    const int ne = min(L.excl_n[i], 20);
+    int e0 = -1, e1 = -1, e2 = -1, e3 = -1;
+    for (int e = 0; e < ne; ++e) {
+      const int gs = L.gslot[L.excl[(size_t)i * 20 + e]];
+      const int t = (gs & 1) == L.which ? gs >> 1 : -1;
+      if (e == 0) e0 = t;
+      else if (e == 1) e1 = t;
+      else if (e == 2) e2 = t;
+      else if (e == 3) e3 = t;
+      else s_ex[e - 4][threadIdx.x] = t;
+    }
+    const bool i_vs = L.hybrid && i >= L.natoms;
+    const int g = s / P;
+    int* row = L.entries + (long long)g * L.w_cap * 32 + (s % P) * T;
+    int cnt = 0;
+    // candidates slot hi down to lo, displaced by the run's image shift
+    auto scan = [&](int hi, int lo, R sh0, R sh1, R sh2) {
+#pragma unroll 4
+      for (int t = hi; t >= lo; --t) {
+        const PT pj = pos[t];
+        R d0 = pi.x - pj.x, d1 = pi.y - pj.y, d2 = pi.z - pj.z;
+        d0 = d0 - sh0;
+        d1 = d1 - sh1;
+        d2 = d2 - sh2;
+        R r2 = d0 * d0;
+        r2 = r2 + d1 * d1;
+        r2 = r2 + d2 * d2;
+        if (r2 < rlsq) {
+          bool ok = !(i_vs && (Prec<R>::bits(pj.w) >> 16) == 3) && t != e0 && t != e1 && t != e2 && t != e3;
+          if (ok && ne > 4)
+            for (int e = 4; e < ne; ++e) ok &= s_ex[e - 4][threadIdx.x] != t;
+          if (ok) {
+            if (cnt < cap) row[(cnt / T) * 32 + cnt % T] = t;
+            ++cnt;
+          }
+        }
+      }
+    };
+    scan(s - 1, L.cell_start[c0], (R)0, (R)0, (R)0);  // the own cell below this particle
+    const int ic[3] = {c0 / (nz * ny), (c0 / nz) % ny, c0 % nz};
+    for (int u = 0; u < 13; ++u) {
+      int jc[3];
+      R sh[3];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const int j = ic[q] + kStencil[u][q];
+        const int w = j >= nc[q] ? 1 : (j < 0 ? -1 : 0);
+        jc[q] = j - w * nc[q];
+        sh[q] = w > 0 ? b[q] : (w < 0 ? -b[q] : (R)0);
+      }
+      const int c = jc[0] * nz * ny + jc[1] * nz + jc[2];
+      scan(L.cell_start[c + 1] - 1, L.cell_start[c], sh[0], sh[1], sh[2]);
+    }
+    L.counts[s] = cnt;
+    if (cnt >= L.maxnab) atomicOr(&sc->err, EB_LIST_OVERFLOW);
+    const int rows = (cnt + T - 1) / T;
+    atomicMax(&L.slice_w[g], rows);
+    if (rows > L.w_cap) {
+      atomicMax(&sc->need_rows[L.which], rows);
+      sc->abort = 1;
+      sc->skip = 1;
     }
   }
 }
