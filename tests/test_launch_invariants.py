@@ -49,7 +49,8 @@ def test_every_programmatic_launch_waits_first():
     kernels = _read("ibg_kernels.cuh")
     names = _pdl_launched_kernels(host)
     # the chain of one step and of a batch step
-    assert {"k_nonbonded_f32", "k_nb_near", "k_nb_collect", "k_finalize", "k_list_build"} <= names
+    assert {"k_nonbonded_f32", "k_nb_near", "k_nb_collect", "k_finalize", "k_list_build_warp",
+            "k_list_build_thread"} <= names
     for name in sorted(names):
         opening = _body_opening(kernels, name)
         assert opening and opening[-1] == "pdl_wait();", (name, opening)
