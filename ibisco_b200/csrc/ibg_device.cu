@@ -520,7 +520,10 @@ void launch_pdl(ibg_ctx* c, void (*k)(KArgs...), int grid, int block, size_t sme
 
 template <typename R>
 void enq_positions(ibg_ctx* c, int begin = 0) {
-  k_positions<R, false><<<c->g_pos, 256, 0, c->st>>>(args<R>(c).pos, nullptr, kOne, begin);
+  const PosArgs& a = args<R>(c).pos;
+  // the reference's centre-of-mass chain works in dynamic shared memory
+  const size_t smem = a.com_carry ? sizeof(ComChunk<R>) : 0;
+  k_positions<R, false><<<c->g_pos, 256, smem, c->st>>>(a, nullptr, kOne, begin);
   ++c->launches;
 }
 
@@ -1737,6 +1740,7 @@ struct ibg_batch {
   std::vector<NBGroup> lb[2];  // list build, by T (smem unused)
   std::vector<NBGroup> nb[2];  // nonbonded, by (T, smem)
   bool any_vs = false, any_list[2] = {false, false};
+  bool any_com_carry = false;  // a system with the reference's centre-of-mass chain
   std::map<unsigned, cudaGraphExec_t> graphs;
   long long launches = 0, launches_per_variant[8] = {0};
   double run_ms = 0.0;
@@ -1792,6 +1796,7 @@ void batch_layout(ibg_batch* b) {
   for (size_t s = 0; s < n; ++s) g[s] = b->sys[s]->nvirta ? b->sys[s]->g_dist : 0;
   b->m_dist = make_map(b, g);
   for (size_t s = 0; s < n; ++s) b->any_vs |= b->sys[s]->nvirta > 0;
+  for (size_t s = 0; s < n; ++s) b->any_com_carry |= b->sys[s]->vs_com_form == IBG_VS_COM_REFERENCE;
   for (size_t s = 0; s < n; ++s) g[s] = b->sys[s]->g_b;
   b->m_bond = make_map(b, g);
   for (size_t s = 0; s < n; ++s) g[s] = b->sys[s]->g_mv;
@@ -1863,7 +1868,8 @@ template <typename R>
 void batch_enqueue(ibg_batch* b, unsigned v) {
   cudaStream_t st = b->st, st2 = b->st2;
   long long& n = b->launches;
-  k_positions<R, true><<<b->m_pos.grid, 256, 0, st>>>(PosArgs{}, (const PosArgs* const*)b->t_pos, b->m_pos.m(), 1);
+  const size_t smem = b->any_com_carry ? sizeof(ComChunk<R>) : 0;
+  k_positions<R, true><<<b->m_pos.grid, 256, smem, st>>>(PosArgs{}, (const PosArgs* const*)b->t_pos, b->m_pos.m(), 1);
   ++n;
   // bonded branch
   CK(cudaEventRecord(b->fork_ev[0], st));

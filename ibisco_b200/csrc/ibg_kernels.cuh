@@ -140,6 +140,18 @@ struct PosArgs {
 // counter and sets this step's flags, or marks the step skipped when the run
 // aborted.  A system that has run its last step (done) is left as it is, so
 // its virtual-site rows keep the values of its last step.
+// Shared storage of one chunk of the reference's centre-of-mass chain
+// (k_positions with com_carry): each site's mass-weighted member terms for y
+// and z, its member count (0 for a centre-atom site), and the running sums
+// after it.
+template <typename R>
+struct ComChunk {
+  static constexpr int kSites = sizeof(R) == 4 ? 256 : 128;
+  R ty[kSites][15], tz[kSites][15];
+  R cy[kSites], cz[kSites];
+  int nm[kSites];
+};
+
 template <typename R, bool B>
 __global__ void k_positions(__grid_constant__ const PosArgs a0, const PosArgs* const* tab, const BlockMap bm,
                             int begin) {
@@ -196,54 +208,99 @@ __global__ void k_positions(__grid_constant__ const PosArgs a0, const PosArgs* c
     // VIRTUAL_DEF.f90:30-39 as the reference runs it: only SUMTOTXYZ(1) is
     // reset before a centre-of-mass site (:31), so the y and z sums run on
     // from one such site to the next, from zero at the start of the pass.
-    // The chain is sequential, so one warp of block 0 walks the sites in
-    // order, two at a time: lanes 0-15 hold the members of the first site,
-    // lanes 16-31 those of the second, and every lane adds the broadcast
-    // terms in the reference's order.
-    if (bk.b != 0 || threadIdx.x >= 32) return;
-    R cy = 0, cz = 0;
-    for (int v0 = 0; v0 < a.nvirta; v0 += 2) {
-      const int v = v0 + (threadIdx.x >> 4);
-      const bool valid = v < a.nvirta;
-      const int ctr = valid ? a.vcenter[v] : 0;
-      const int nm = valid && ctr < 0 ? a.vnum[v] : 0;
-      R pm[3] = {0, 0, 0};
-      if (hl < nm) {
-        const int m = a.vmem[v * 15 + hl];
-        const R mm = (R)a.vmass[v * 15 + hl];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) pm[c] = mm * (R)a.S[3 * (size_t)m + c];
+    // Block 0 takes the sites in chunks: each thread forms its site's
+    // mass-weighted member terms and x sum, then one thread adds the chunk's
+    // y and z terms in the reference's order (the only sequential part),
+    // and each thread finishes its site.  The chunk lives in dynamic shared
+    // memory, which the host requests only for this form.
+    using CS = ComChunk<R>;
+    if (bk.b != 0) return;
+    unsigned dyn;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+    if (dyn < sizeof(CS)) {  // launched without the chunk's storage: nothing is written
+      if (threadIdx.x == 0) atomicOr(&sc->err, EB_CAPACITY);
+      return;
+    }
+    extern __shared__ __align__(16) unsigned char pos_smem[];
+    CS& ch = *reinterpret_cast<CS*>(pos_smem);
+    constexpr int kC = CS::kSites;
+    R cy = 0, cz = 0;  // the running sums, held by thread 0
+    for (int c0 = 0; c0 < a.nvirta; c0 += kC) {
+      const int v = c0 + (int)threadIdx.x;
+      const bool mine = threadIdx.x < kC && v < a.nvirta;
+      int ctr = 0;
+      R sx = 0;
+      if (mine) {
+        ctr = a.vcenter[v];
+        const int nm = ctr < 0 ? a.vnum[v] : 0;
+        for (int k = 0; k < nm; ++k) {
+          const int m = a.vmem[v * 15 + k];
+          const R mm = (R)a.vmass[v * 15 + k];
+          sx = sx + mm * (R)a.S[3 * (size_t)m + 0];
+          ch.ty[threadIdx.x][k] = mm * (R)a.S[3 * (size_t)m + 1];
+          ch.tz[threadIdx.x][k] = mm * (R)a.S[3 * (size_t)m + 2];
+        }
+        ch.nm[threadIdx.x] = nm;
       }
-      for (int h = 0; h < 2 && v0 + h < a.nvirta; ++h) {
-        const int vh = v0 + h;
-        const int ch = __shfl_sync(0xffffffffu, ctr, 16 * h);
-        const int nh = __shfl_sync(0xffffffffu, nm, 16 * h);
-        R s[3];
-        if (ch >= 0) {
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        // the next site's terms are loaded while this site's are added, so
+        // the chain waits only on its own additions
+        const int nc = min(kC, a.nvirta - c0);
+        R y[15], z[15];
+        int n = ch.nm[0];
 #pragma unroll
-          for (int c = 0; c < 3; ++c) s[c] = (R)a.S[3 * (size_t)ch + c];
+        for (int k = 0; k < 15; ++k) {
+          y[k] = k < n ? ch.ty[0][k] : (R)0;
+          z[k] = k < n ? ch.tz[0][k] : (R)0;
+        }
+        for (int u = 0; u < nc; ++u) {
+          const int un = u + 1 < nc ? u + 1 : u;
+          const int n1 = ch.nm[un];
+          R y1[15], z1[15];
+#pragma unroll
+          for (int k = 0; k < 15; ++k) {
+            y1[k] = k < n1 ? ch.ty[un][k] : (R)0;
+            z1[k] = k < n1 ? ch.tz[un][k] : (R)0;
+          }
+#pragma unroll
+          for (int k = 0; k < 15; ++k) {
+            if (k < n) {
+              cy = cy + y[k];
+              cz = cz + z[k];
+            }
+          }
+          ch.cy[u] = cy;
+          ch.cz[u] = cz;
+          n = n1;
+#pragma unroll
+          for (int k = 0; k < 15; ++k) {
+            y[k] = y1[k];
+            z[k] = z1[k];
+          }
+        }
+      }
+      __syncthreads();
+      if (mine) {
+        R sv[3];
+        if (ctr >= 0) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) sv[c] = (R)a.S[3 * (size_t)ctr + c];
         } else {
-          R sx = 0;
-#pragma unroll
-          for (int q = 0; q < 15; ++q) {
-            const R x = __shfl_sync(0xffffffffu, pm[0], 16 * h + q);
-            const R y = __shfl_sync(0xffffffffu, pm[1], 16 * h + q);
-            const R z = __shfl_sync(0xffffffffu, pm[2], 16 * h + q);
-            if (q < nh) { sx = sx + x; cy = cy + y; cz = cz + z; }
-          }
-          const R inv = (R)a.vinv[vh];
-          s[0] = sx * inv; s[1] = cy * inv; s[2] = cz * inv;
+          const R inv = (R)a.vinv[v];
+          sv[0] = sx * inv;
+          sv[1] = ch.cy[threadIdx.x] * inv;
+          sv[2] = ch.cz[threadIdx.x] * inv;
         }
-        if (threadIdx.x == 0) {
-          double sd[3];
+        double sd[3];
 #pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            sd[c] = (double)s[c];
-            a.Svs[3 * (size_t)vh + c] = sd[c];
-          }
-          store(a.natoms + vh, s, sd);
+        for (int c = 0; c < 3; ++c) {
+          sd[c] = (double)sv[c];
+          a.Svs[3 * (size_t)v + c] = sd[c];
         }
+        store(a.natoms + v, sv, sd);
       }
+      __syncthreads();  // the chunk's terms are rewritten by the next
     }
     return;
   }

@@ -334,7 +334,8 @@ class System:
             raise IbiscoError(rc, lib().ibg_last_error(self._h).decode())
 
     def set_state(self, sxyz=None, vxyz=None, box=None):
-        s0, v0, b0 = self.setup.initial_state()
+        if sxyz is None or vxyz is None or box is None:
+            s0, v0, b0 = self.setup.initial_state()
         s = np.ascontiguousarray(s0 if sxyz is None else sxyz, np.float32)
         v = np.ascontiguousarray(v0 if vxyz is None else vxyz, np.float32)
         b = np.ascontiguousarray(b0 if box is None else box, np.float32)
