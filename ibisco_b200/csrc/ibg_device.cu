@@ -7,7 +7,7 @@
 //                   point (FP32 path) or double (FP64 path)
 //   per list (atom list, bead list):
 //     pos4          wrapped positions in cell order, type|label in .w
-//     fsort         nonbonded forces per slot (cell order)
+//     fsort         nonbonded forces per slot (cell order), component-major
 //     cells         counting-sorted cell index (LINKS.f90 grid)
 //     entries       Verlet list as slot indices, sliced-ELL: slice g of 32
 //                   slots stores entry k of slot s at off[g] + 32 k + (s & 31)
@@ -177,6 +177,7 @@ struct ibg_ctx {
   int nb_chunk = 0;          // tuning (FP32): 256ths of the units taken dynamically after the block ranges (0: all, per warp)
   int nb_rows = 16;          // tuning: list rows per nonbonded work unit (8 or 16)
   int vs_com_form = IBG_VS_COM_FIXED;  // centre-of-mass virtual sites: fixed or the reference's form
+  void* vchain = nullptr;              // the reference form's per-site terms (k_vsite_chain)
   ObsD* ring = nullptr;
   int ring_cap = 0;
   double *p_b = nullptr, *p_mv = nullptr, *p_mom = nullptr;
@@ -415,6 +416,7 @@ void make_args(ibg_ctx* c) {
   p.posq[0] = c->L[0].posq; p.posq[1] = c->L[1].posq;
   p.vcenter = c->vcenter; p.vnum = c->vnum; p.vmem = c->vmem; p.vmass = c->vmass; p.vinv = c->vinv;
   p.com_carry = c->vs_com_form == IBG_VS_COM_REFERENCE;
+  p.chain = c->vchain;
   for (int w = 0; w < 2; ++w) {
     DevList& L = c->L[w];
     ListArgs& a = A.list[w];
@@ -521,9 +523,11 @@ void launch_pdl(ibg_ctx* c, void (*k)(KArgs...), int grid, int block, size_t sme
 template <typename R>
 void enq_positions(ibg_ctx* c, int begin = 0) {
   const PosArgs& a = args<R>(c).pos;
-  // the reference's centre-of-mass chain works in dynamic shared memory
-  const size_t smem = a.com_carry ? sizeof(ComChunk<R>) : 0;
-  k_positions<R, false><<<c->g_pos, 256, smem, c->st>>>(a, nullptr, kOne, begin);
+  k_positions<R, false><<<c->g_pos, 256, 0, c->st>>>(a, nullptr, kOne, begin);
+  if (a.com_carry && c->nvirta > 0) {  // the reference's centre-of-mass sums
+    k_vsite_chain<R, false><<<1, 256, 0, c->st>>>(a, nullptr, kOne);
+    ++c->launches;
+  }
   ++c->launches;
 }
 
@@ -904,6 +908,10 @@ int ibg_set_vsite_com(ibg_ctx* c, int form) {
   try {
     CK(cudaStreamSynchronize(c->st));
     c->vs_com_form = form;
+    if (form == IBG_VS_COM_REFERENCE && c->nvirta > 0 && !c->vchain) {
+      const size_t nb = c->prec == IBG_PREC_FP32_FIXED ? chain_bytes<float>(c->nvirta) : chain_bytes<double>(c->nvirta);
+      c->vchain = dalloc<unsigned char>(nb, c->owned);
+    }
     refresh_args(c);
     for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
     c->graphs.clear();
@@ -1868,9 +1876,12 @@ template <typename R>
 void batch_enqueue(ibg_batch* b, unsigned v) {
   cudaStream_t st = b->st, st2 = b->st2;
   long long& n = b->launches;
-  const size_t smem = b->any_com_carry ? sizeof(ComChunk<R>) : 0;
-  k_positions<R, true><<<b->m_pos.grid, 256, smem, st>>>(PosArgs{}, (const PosArgs* const*)b->t_pos, b->m_pos.m(), 1);
+  k_positions<R, true><<<b->m_pos.grid, 256, 0, st>>>(PosArgs{}, (const PosArgs* const*)b->t_pos, b->m_pos.m(), 1);
   ++n;
+  if (b->any_com_carry) {
+    k_vsite_chain<R, true><<<b->m_fin.grid, 256, 0, st>>>(PosArgs{}, (const PosArgs* const*)b->t_pos, b->m_fin.m());
+    ++n;
+  }
   // bonded branch
   CK(cudaEventRecord(b->fork_ev[0], st));
   CK(cudaStreamWaitEvent(st2, b->fork_ev[0], 0));

@@ -131,7 +131,44 @@ struct PosArgs {
   const float* vmass;  // member masses per [v*15 + k]
   const float* vinv;   // VIRT_INVMASS per VS
   int com_carry;       // 1: the reference's centre-of-mass form (VIRTUAL_DEF.f90:31)
+  // com_carry: per site the mass-weighted y and z member terms (R[32]: y at
+  // 0..14, z at 16..30), then the x coordinates (R[nvirta]), then the member
+  // counts (int[nvirta], -1 for a centre-atom site), for k_vsite_chain
+  void* chain;
 };
+
+template <typename R>
+struct ChainView {
+  R* terms;
+  R* xs;
+  int* n;
+  __device__ ChainView(const PosArgs& a)
+      : terms((R*)a.chain), xs((R*)a.chain + 32 * (size_t)a.nvirta), n((int*)(xs + a.nvirta)) {}
+};
+
+// Bytes of the com_carry scratch for nvirta sites.
+template <typename R>
+constexpr size_t chain_bytes(long long nvirta) {
+  return (size_t)nvirta * (33 * sizeof(R) + sizeof(int));
+}
+
+// A particle's wrapped position into its list's slot: the FP32/FP64 record
+// with its type/label word, and on the FP32 path the 32-bit box fractions
+// from the FP64 value sd.
+template <typename R>
+__device__ __forceinline__ void store_position(const PosArgs& a, const R* b2, const double* boxinv, int i, const R* s,
+                                               const double* sd) {
+  using PT = typename Prec<R>::pos_t;
+  const int g = a.gslot[i];
+  const int tb = a.tbits[i];
+  R r[3] = {s[0], s[1], s[2]};
+  fold3<R>(r, b2);
+  PT p;
+  p.x = r[0]; p.y = r[1]; p.z = r[2];
+  p.w = Prec<R>::tbits(tb);
+  ((PT*)a.pos4[g & 1])[g >> 1] = p;
+  if (a.posq[g & 1]) a.posq[g & 1][g >> 1] = box_fraction(sd, boxinv, tb);
+}
 
 // SHIFT.f90:33-45 for atoms and VIRTUAL_DEF.f90:19-47 for virtual sites
 // (centre-of-mass sums with all three components reset per site, or the
@@ -140,18 +177,6 @@ struct PosArgs {
 // counter and sets this step's flags, or marks the step skipped when the run
 // aborted.  A system that has run its last step (done) is left as it is, so
 // its virtual-site rows keep the values of its last step.
-// Shared storage of one chunk of the reference's centre-of-mass chain
-// (k_positions with com_carry): each site's mass-weighted member terms for y
-// and z, its member count (0 for a centre-atom site), and the running sums
-// after it.
-template <typename R>
-struct ComChunk {
-  static constexpr int kSites = sizeof(R) == 4 ? 256 : 128;
-  R ty[kSites][15], tz[kSites][15];
-  R cy[kSites], cz[kSites];
-  int nm[kSites];
-};
-
 template <typename R, bool B>
 __global__ void k_positions(__grid_constant__ const PosArgs a0, const PosArgs* const* tab, const BlockMap bm,
                             int begin) {
@@ -182,17 +207,7 @@ __global__ void k_positions(__grid_constant__ const PosArgs a0, const PosArgs* c
   // sd: the position in FP64 for the fixed-point copy (FP32 path).  The slot
   // and label are loaded before the first store (the arrays may alias as far
   // as the compiler knows, and a load after a store would wait for it).
-  auto store = [&](int i, const R* s, const double* sd) {
-    const int g = a.gslot[i];
-    const int tb = a.tbits[i];
-    R r[3] = {s[0], s[1], s[2]};
-    fold3<R>(r, b2);
-    PT p;
-    p.x = r[0]; p.y = r[1]; p.z = r[2];
-    p.w = Prec<R>::tbits(tb);
-    ((PT*)a.pos4[g & 1])[g >> 1] = p;
-    if (a.posq[g & 1]) a.posq[g & 1][g >> 1] = box_fraction(sd, boxinv, tb);
-  };
+  auto store = [&](int i, const R* s, const double* sd) { store_position<R>(a, b2, boxinv, i, s, sd); };
   for (int i = bk.b * blockDim.x + threadIdx.x; i < a.natoms; i += bk.g * blockDim.x) {
     R s[3];
     double sd[3];
@@ -204,111 +219,15 @@ __global__ void k_positions(__grid_constant__ const PosArgs a0, const PosArgs* c
     store(i, s, sd);
   }
   const int hl = threadIdx.x & 15;
-  if (a.com_carry) {
-    // VIRTUAL_DEF.f90:30-39 as the reference runs it: only SUMTOTXYZ(1) is
-    // reset before a centre-of-mass site (:31), so the y and z sums run on
-    // from one such site to the next, from zero at the start of the pass.
-    // Block 0 takes the sites in chunks: each thread forms its site's
-    // mass-weighted member terms and x sum, then one thread adds the chunk's
-    // y and z terms in the reference's order (the only sequential part),
-    // and each thread finishes its site.  The chunk lives in dynamic shared
-    // memory, which the host requests only for this form.
-    using CS = ComChunk<R>;
-    if (bk.b != 0) return;
-    unsigned dyn;
-    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
-    if (dyn < sizeof(CS)) {  // launched without the chunk's storage: nothing is written
-      if (threadIdx.x == 0) atomicOr(&sc->err, EB_CAPACITY);
-      return;
-    }
-    extern __shared__ __align__(16) unsigned char pos_smem[];
-    CS& ch = *reinterpret_cast<CS*>(pos_smem);
-    constexpr int kC = CS::kSites;
-    R cy = 0, cz = 0;  // the running sums, held by thread 0
-    for (int c0 = 0; c0 < a.nvirta; c0 += kC) {
-      const int v = c0 + (int)threadIdx.x;
-      const bool mine = threadIdx.x < kC && v < a.nvirta;
-      int ctr = 0;
-      R sx = 0;
-      if (mine) {
-        ctr = a.vcenter[v];
-        const int nm = ctr < 0 ? a.vnum[v] : 0;
-        for (int k = 0; k < nm; ++k) {
-          const int m = a.vmem[v * 15 + k];
-          const R mm = (R)a.vmass[v * 15 + k];
-          sx = sx + mm * (R)a.S[3 * (size_t)m + 0];
-          ch.ty[threadIdx.x][k] = mm * (R)a.S[3 * (size_t)m + 1];
-          ch.tz[threadIdx.x][k] = mm * (R)a.S[3 * (size_t)m + 2];
-        }
-        ch.nm[threadIdx.x] = nm;
-      }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        // the next site's terms are loaded while this site's are added, so
-        // the chain waits only on its own additions
-        const int nc = min(kC, a.nvirta - c0);
-        R y[15], z[15];
-        int n = ch.nm[0];
-#pragma unroll
-        for (int k = 0; k < 15; ++k) {
-          y[k] = k < n ? ch.ty[0][k] : (R)0;
-          z[k] = k < n ? ch.tz[0][k] : (R)0;
-        }
-        for (int u = 0; u < nc; ++u) {
-          const int un = u + 1 < nc ? u + 1 : u;
-          const int n1 = ch.nm[un];
-          R y1[15], z1[15];
-#pragma unroll
-          for (int k = 0; k < 15; ++k) {
-            y1[k] = k < n1 ? ch.ty[un][k] : (R)0;
-            z1[k] = k < n1 ? ch.tz[un][k] : (R)0;
-          }
-#pragma unroll
-          for (int k = 0; k < 15; ++k) {
-            if (k < n) {
-              cy = cy + y[k];
-              cz = cz + z[k];
-            }
-          }
-          ch.cy[u] = cy;
-          ch.cz[u] = cz;
-          n = n1;
-#pragma unroll
-          for (int k = 0; k < 15; ++k) {
-            y[k] = y1[k];
-            z[k] = z1[k];
-          }
-        }
-      }
-      __syncthreads();
-      if (mine) {
-        R sv[3];
-        if (ctr >= 0) {
-#pragma unroll
-          for (int c = 0; c < 3; ++c) sv[c] = (R)a.S[3 * (size_t)ctr + c];
-        } else {
-          const R inv = (R)a.vinv[v];
-          sv[0] = sx * inv;
-          sv[1] = ch.cy[threadIdx.x] * inv;
-          sv[2] = ch.cz[threadIdx.x] * inv;
-        }
-        double sd[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          sd[c] = (double)sv[c];
-          a.Svs[3 * (size_t)v + c] = sd[c];
-        }
-        store(a.natoms + v, sv, sd);
-      }
-      __syncthreads();  // the chunk's terms are rewritten by the next
-    }
-    return;
-  }
   // VIRTUAL_DEF.f90:30-39 with all three sums reset per site: 16 lanes per
   // site (half a warp), lane k holding member k's mass-weighted position; the
   // sum runs over the members in order (0 + p0 + p1 + ...), as the
   // reference's loop does.  The loop over sites is uniform within a warp, so
-  // its shuffles see all 32 lanes.
+  // its shuffles see all 32 lanes.  In the reference's form (com_carry) only
+  // the x sum is reset per site (:31): the x coordinate is formed here, and
+  // the y and z member terms go to the chain scratch, whose sums
+  // k_vsite_chain runs on from site to site.
+  const ChainView<R> cv(a);
   const int w0 = (bk.b * blockDim.x + threadIdx.x) >> 5, nw = (bk.g * blockDim.x) >> 5;
   for (int w = w0; 2 * w < a.nvirta; w += nw) {
     const int v = 2 * w + ((threadIdx.x >> 4) & 1);
@@ -322,6 +241,10 @@ __global__ void k_positions(__grid_constant__ const PosArgs a0, const PosArgs* c
 #pragma unroll
       for (int c = 0; c < 3; ++c) pm[c] = mm * (R)a.S[3 * (size_t)m + c];
     }
+    if (a.com_carry && hl < nm) {
+      cv.terms[32 * (size_t)v + hl] = pm[1];
+      cv.terms[32 * (size_t)v + 16 + hl] = pm[2];
+    }
     R acc[3] = {0, 0, 0};
 #pragma unroll
     for (int q = 0; q < 15; ++q) {
@@ -332,6 +255,13 @@ __global__ void k_positions(__grid_constant__ const PosArgs a0, const PosArgs* c
       }
     }
     if (!valid || hl != 0) continue;
+    if (a.com_carry) {
+      cv.n[v] = ctr >= 0 ? -1 : nm;  // -1: a centre-atom site, outside the sums
+      if (ctr < 0) {  // finished by k_vsite_chain
+        cv.xs[v] = acc[0] * (R)a.vinv[v];
+        continue;
+      }
+    }
     R s[3];
     if (ctr >= 0) {
 #pragma unroll
@@ -349,6 +279,121 @@ __global__ void k_positions(__grid_constant__ const PosArgs a0, const PosArgs* c
     }
     store(a.natoms + v, s, sd);
   }
+}
+
+// VIRTUAL_DEF.f90:30-39 as the reference runs it (com_carry): SUMTOTXYZ(2)
+// and (3) are not reset before a centre-of-mass site (only (1) is, :31), so
+// the y and z sums run on from one such site to the next, from zero at the
+// start of the pass.  k_positions has formed each site's x coordinate and its
+// mass-weighted y and z member terms; one block per system adds the terms in
+// the reference's order.  The sites go through shared memory in chunks, two
+// buffers: thread 0 runs the sums over one chunk while warps 1..7 load the
+// next and finish the one before (the sums times VIRT_INVMASS, the FP64 row
+// and the list record).
+// A row of 32 values from shared memory in 16-byte loads issued back to back
+// (asm volatile keeps them together, ahead of the arithmetic that uses them).
+__device__ __forceinline__ void lds_row(float* t, const float* row) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(row);
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(t[4 * k]), "=f"(t[4 * k + 1]), "=f"(t[4 * k + 2]), "=f"(t[4 * k + 3])
+                 : "r"(a + 16 * k));
+}
+__device__ __forceinline__ void lds_row(double* t, const double* row) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(row);
+#pragma unroll
+  for (int k = 0; k < 16; ++k)
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(t[2 * k]), "=d"(t[2 * k + 1]) : "r"(a + 16 * k));
+}
+
+template <typename R, bool B>
+__global__ void __launch_bounds__(256) k_vsite_chain(__grid_constant__ const PosArgs a0, const PosArgs* const* tab,
+                                                     const BlockMap bm) {
+  constexpr int kC = sizeof(R) == 4 ? 128 : 64;  // sites per chunk
+  __shared__ __align__(16) R s_t[2][kC][32];
+  __shared__ int s_n[2][kC];
+  __shared__ R s_c[2][kC][2];
+  const Blk bk = blk<B>(bm);
+  const PosArgs& a = B ? *tab[bk.sys] : a0;
+  Scalars* sc = a.sc;
+  if (!a.com_carry || bk.b != 0 || sc->done) return;
+  const ChainView<R> cv(a);
+  R b[3], bi[3], b2[3];
+  box_of<R>(sc, b, bi, b2);
+  const double boxinv[3] = {sc->boxinv[0], sc->boxinv[1], sc->boxinv[2]};
+  const int nv = a.nvirta;
+  // chunk c0 into buffer q, by the threads from t0 on
+  auto load = [&](int c0, int q, int t0) {
+    const int nc = min(kC, nv - c0);
+    for (int k = (int)threadIdx.x - t0; k < nc * 32; k += (int)blockDim.x - t0)
+      s_t[q][k >> 5][k & 31] = cv.terms[32 * (size_t)c0 + k];
+    for (int k = (int)threadIdx.x - t0; k < nc; k += (int)blockDim.x - t0) s_n[q][k] = cv.n[c0 + k];
+  };
+  // the sites of chunk c0 from the sums in s_c[q], by the threads from t0 on:
+  // the sums times VIRT_INVMASS, the FP64 row and the list record
+  auto finish = [&](int c0, int q, int t0) {
+    const int nc = min(kC, nv - c0);
+    for (int u = (int)threadIdx.x - t0; u < nc; u += (int)blockDim.x - t0) {
+      const int v = c0 + u;
+      if (cv.n[v] < 0) continue;  // a centre-atom site: k_positions placed it
+      const R inv = (R)a.vinv[v];
+      R sv[3] = {cv.xs[v], s_c[q][u][0] * inv, s_c[q][u][1] * inv};
+      double sd[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        sd[c] = (double)sv[c];
+        a.Svs[3 * (size_t)v + c] = sd[c];
+      }
+      store_position<R>(a, b2, boxinv, a.natoms + v, sv, sd);
+    }
+  };
+  if (nv > 0) load(0, 0, 0);
+  __syncthreads();
+  // step j: thread 0 sums chunk j (buffer j&1) while warps 1..7 load chunk
+  // j+1 into the other buffer and finish chunk j-1 from its sums
+  R cy = 0, cz = 0;  // the running sums, held by thread 0
+  int last = -1;     // the chunk summed last, still to be finished
+  for (int c0 = 0, q = 0; c0 < nv; c0 += kC, q ^= 1) {
+    const int nc = min(kC, nv - c0);
+    if (threadIdx.x == 0) {
+      // two sites at a time: both sites' terms are loaded (whole rows, the
+      // unused slots included) before the first addition, so the additions
+      // wait on one another only
+      for (int u = 0; u < nc; u += 2) {
+        const int u1 = min(u + 1, nc - 1);
+        R t0[32], t1[32];
+        lds_row(t0, s_t[q][u]);
+        lds_row(t1, s_t[q][u1]);
+        const int n0 = s_n[q][u], n1 = s_n[q][u1];
+#pragma unroll
+        for (int k = 0; k < 15; ++k) {
+          if (k < n0) {
+            cy = cy + t0[k];
+            cz = cz + t0[16 + k];
+          }
+        }
+        s_c[q][u][0] = cy;
+        s_c[q][u][1] = cz;
+        if (u1 == u) break;
+#pragma unroll
+        for (int k = 0; k < 15; ++k) {
+          if (k < n1) {
+            cy = cy + t1[k];
+            cz = cz + t1[16 + k];
+          }
+        }
+        s_c[q][u1][0] = cy;
+        s_c[q][u1][1] = cz;
+      }
+    } else if (threadIdx.x >= 32) {
+      if (c0 + kC < nv) load(c0 + kC, q ^ 1, 32);
+      if (last >= 0) finish(last, q ^ 1, 32);
+    }
+    __syncthreads();  // buffer q is summed, q^1 loaded and its sums used
+    last = c0;
+  }
+  if (last >= 0) finish(last, ((last / kC) & 1), 0);
 }
 
 // ------------------------------------------------------------ cell lists
@@ -953,7 +998,7 @@ struct NBArgs {
   const int* entries;
   int w_cap;                       // rows of 32 entries per slice
   int work;                        // index of this launch's work counter
-  typename Prec<R>::acc_t* fsort;  // [3n] per slot
+  typename Prec<R>::acc_t* fsort;  // [3][n]: the x, y and z sums of every slot in turn
   // tables of this list: ltab[ti*ntype+tj] = local table or -1; rows of table
   // t are [toff[t], toff[t+1]); fp = {F,P} per row, x = RNBOND per row
   const int* ltab;
@@ -1103,9 +1148,9 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded(__grid_constant__ const NB
       const R fx = fij * d0, fy = fij * d1, fz = fij * d2;
       const reg_t qx = P::q(fx, &sc->err), qy = P::q(fy, &sc->err), qz = P::q(fz, &sc->err);
       fi0 += qx; fi1 += qy; fi2 += qz;
-      P::add(&A.fsort[3 * (size_t)t + 0], -qx);
-      P::add(&A.fsort[3 * (size_t)t + 1], -qy);
-      P::add(&A.fsort[3 * (size_t)t + 2], -qz);
+      P::add(&A.fsort[t], -qx);
+      P::add(&A.fsort[(size_t)A.n + t], -qy);
+      P::add(&A.fsort[2 * (size_t)A.n + t], -qz);
       acc[3] += (double)(fx * d0);
       acc[4] += (double)(fy * d1);
       acc[5] += (double)(fz * d2);
@@ -1132,9 +1177,9 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded(__grid_constant__ const NB
       fi2 += __shfl_down_sync(0xffffffffu, fi2, o, T);
     }
     if (q == 0 && valid && r0 * T < cnt) {
-      P::add(&A.fsort[3 * (size_t)s + 0], fi0);
-      P::add(&A.fsort[3 * (size_t)s + 1], fi1);
-      P::add(&A.fsort[3 * (size_t)s + 2], fi2);
+      P::add(&A.fsort[s], fi0);
+      P::add(&A.fsort[(size_t)A.n + s], fi1);
+      P::add(&A.fsort[2 * (size_t)A.n + s], fi2);
     }
   }
   if (err) atomicOr(&sc->err, err);
@@ -1270,9 +1315,9 @@ __global__ void __launch_bounds__(256, B ? 4 : 5) k_nonbonded_f32(__grid_constan
         const long long qx = __float2ll_rn(fx * -kFixScale), qy = __float2ll_rn(fy * -kFixScale),
                         qz = __float2ll_rn(fz * -kFixScale);
         fi0 -= qx; fi1 -= qy; fi2 -= qz;
-        atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 0], (unsigned long long)qx);
-        atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 1], (unsigned long long)qy);
-        atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)t + 2], (unsigned long long)qz);
+        atomicAdd((unsigned long long*)&A.fsort[t], (unsigned long long)qx);
+        atomicAdd((unsigned long long*)&A.fsort[(size_t)A.n + t], (unsigned long long)qy);
+        atomicAdd((unsigned long long*)&A.fsort[2 * (size_t)A.n + t], (unsigned long long)qz);
         vir[0] = __fmaf_rn(fx, d0, vir[0]);
         vir[1] = __fmaf_rn(fy, d1, vir[1]);
         vir[2] = __fmaf_rn(fz, d2, vir[2]);
@@ -1305,9 +1350,9 @@ __global__ void __launch_bounds__(256, B ? 4 : 5) k_nonbonded_f32(__grid_constan
       fi2 += __shfl_down_sync(0xffffffffu, fi2, o, T);
     }
     if (q == 0 && valid && r0 * T < cnt) {
-      atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)s + 0], (unsigned long long)fi0);
-      atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)s + 1], (unsigned long long)fi1);
-      atomicAdd((unsigned long long*)&A.fsort[3 * (size_t)s + 2], (unsigned long long)fi2);
+      atomicAdd((unsigned long long*)&A.fsort[s], (unsigned long long)fi0);
+      atomicAdd((unsigned long long*)&A.fsort[(size_t)A.n + s], (unsigned long long)fi1);
+      atomicAdd((unsigned long long*)&A.fsort[2 * (size_t)A.n + s], (unsigned long long)fi2);
     }
   };
   if (A.chunk > 0) {
@@ -1444,12 +1489,12 @@ __global__ void __launch_bounds__(256) k_nb_near(__grid_constant__ const NBArgs<
     const long long qx = __float2ll_rn(fx * kFixScale), qy = __float2ll_rn(fy * kFixScale),
                     qz = __float2ll_rn(fz * kFixScale);
     unsigned long long* fs = (unsigned long long*)A.fsort;
-    atomicAdd(fs + 3 * (size_t)s + 0, (unsigned long long)qx);
-    atomicAdd(fs + 3 * (size_t)s + 1, (unsigned long long)qy);
-    atomicAdd(fs + 3 * (size_t)s + 2, (unsigned long long)qz);
-    atomicAdd(fs + 3 * (size_t)t + 0, (unsigned long long)(-qx));
-    atomicAdd(fs + 3 * (size_t)t + 1, (unsigned long long)(-qy));
-    atomicAdd(fs + 3 * (size_t)t + 2, (unsigned long long)(-qz));
+    atomicAdd(fs + s, (unsigned long long)qx);
+    atomicAdd(fs + (size_t)A.n + s, (unsigned long long)qy);
+    atomicAdd(fs + 2 * (size_t)A.n + s, (unsigned long long)qz);
+    atomicAdd(fs + t, (unsigned long long)(-qx));
+    atomicAdd(fs + (size_t)A.n + t, (unsigned long long)(-qy));
+    atomicAdd(fs + 2 * (size_t)A.n + t, (unsigned long long)(-qz));
     const bool lab3 = li == 3 || lj == 3;
     const long long qe = fixq<24>(vij, err);
     if (li == 1) acc[0] += qe;
@@ -1505,12 +1550,12 @@ __global__ void k_nb_collect(__grid_constant__ const CollectArgs<R> C0, const Co
       // as the compiler knows)
       typename P::acc_t v[3];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) v[c] = C.fsort[3 * (size_t)s + c];
+      for (int c = 0; c < 3; ++c) v[c] = C.fsort[c * (size_t)C.n + s];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         C.fnb[3 * (size_t)gi + c] = v[c];
         if (C.mts) C.mtsf[((size_t)(m - 1) * C.n + a) * 3 + c] = v[c];
-        C.fsort[3 * (size_t)s + c] = 0;
+        C.fsort[c * (size_t)C.n + s] = 0;
       }
     } else {
       const double coef = (double)(m - 3) * 0.5;
