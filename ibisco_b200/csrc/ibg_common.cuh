@@ -27,6 +27,14 @@ constexpr float kFixScale = 4294967296.0f;        // 2^32
 constexpr double kFixInv = 1.0 / 4294967296.0;   // 2^-32
 constexpr float kFixMax = 2147483520.0f;          // largest float below 2^31
 
+// Slot-ordered nonbonded force sums, in blocks of 32 slots: a block's 32 x
+// sums, then its 32 y sums and its 32 z sums.  A slot's three sums lie 256
+// bytes apart (one address and two fixed offsets per particle), and the sums
+// of neighbouring slots share sectors.  fs_at(t) is slot t's x sum; its y and
+// z sums follow at +32 and +64.
+__host__ __device__ __forceinline__ size_t fs_at(int t) { return (size_t)(t >> 5) * 96 + (t & 31); }
+__host__ __device__ __forceinline__ size_t fs_len(int n) { return (size_t)((n + 31) >> 5) * 96; }
+
 // Observables in the order of ibg_obs (ek[2] .. pt[6], box[3]).
 struct ObsD {
   double ek[2], temp, temp_atom, temp_bead;

@@ -7,7 +7,7 @@
 //                   point (FP32 path) or double (FP64 path)
 //   per list (atom list, bead list):
 //     pos4          wrapped positions in cell order, type|label in .w
-//     fsort         nonbonded forces per slot (cell order), component-major
+//     fsort         nonbonded forces per slot (cell order), in blocks of 32 slots: x, y, z sums (fs_at)
 //     cells         counting-sorted cell index (LINKS.f90 grid)
 //     entries       Verlet list as slot indices, sliced-ELL: slice g of 32
 //                   slots stores entry k of slot s at off[g] + 32 k + (s & 31)
@@ -118,6 +118,7 @@ struct DevList {
   size_t smem = 0;
   bool use_smem = false;
   float rlist = 0, rlistsq = 0, rcutsq = 0;
+  float rgroupsq = 0;  // FP32 path: outer group of the stored lists (ListArgs::rgroupsq); 0: reference order
   int grid_nb = 0;
 };
 
@@ -176,6 +177,7 @@ struct ibg_ctx {
   int nb_blocks_per_sm = 0;  // tuning: resident nonbonded blocks per SM (0: all that fit)
   int nb_chunk = 0;          // tuning (FP32): 256ths of the units taken dynamically after the block ranges (0: all, per warp)
   int nb_rows = 16;          // tuning: list rows per nonbonded work unit (8 or 16)
+  int nb_window = 0;         // tuning (FP32, nb_chunk > 0): units per run dealt to the blocks in turn (0: one range per block)
   int vs_com_form = IBG_VS_COM_FIXED;  // centre-of-mass virtual sites: fixed or the reference's form
   void* vchain = nullptr;              // the reference form's per-site terms (k_vsite_chain)
   ObsD* ring = nullptr;
@@ -255,6 +257,14 @@ void build_list(ibg_ctx* c, const ibg_desc* d, int which) {
   L.rlist = which == 0 ? d->rlist_atom : d->rlist_bead;
   L.rlistsq = L.rlist * L.rlist;  // RLISTSQ = RLIST*RLIST (NEW_NEIGHBOUR_WITHLIST.f90:26)
   L.rcutsq = which == 0 ? d->rcutsq_atom : d->rcutsq_bead;
+  // FP32 path: pairs beyond rc + skin/4 at the rebuild are stored after the
+  // rest of each list (the nonbonded kernel then skips most of their rows);
+  // ibg_get_neighbour_list restores the reference's order
+  if (c->prec == IBG_PREC_FP32_FIXED && L.rcutsq > 0.f && L.rlist * L.rlist > L.rcutsq) {
+    const double rc = std::sqrt((double)L.rcutsq);
+    const double rg = rc + 0.25 * ((double)L.rlist - rc);
+    L.rgroupsq = (float)(rg * rg);
+  }
   // lanes per particle: 8 (the list-build and nonbonded launches assume it).  The eight lanes of a particle take eight
   // consecutive entries of its list, whose neighbours lie close together in
   // slot order, so a warp's position gathers and force atomics touch fewer
@@ -287,7 +297,7 @@ void build_list(ibg_ctx* c, const ibg_desc* d, int which) {
     L.near_cap = std::max(4096, L.n / 32);
     L.near = dalloc<int4>(L.near_cap, o);
   }
-  L.fsort = dalloc<unsigned char>(accsize(c) * 3 * L.n, o);
+  L.fsort = dalloc<unsigned char>(accsize(c) * fs_len(L.n), o);
   if (which == 1 && c->nmts > 0) L.mtsf = dalloc<unsigned char>(accsize(c) * 9 * L.n, o);
   L.cell_cap = 0;  // sized in ibg_set_state once the box is known
   // nonbonded tables of the type pairs present in this list
@@ -323,6 +333,9 @@ void build_list(ibg_ctx* c, const ibg_desc* d, int which) {
     for (int k = rows; k < nd + 2; ++k) { fp.push_back(0); fp.push_back(0); xx.push_back(0); }
   }
   toff[L.ntab] = (int)xx.size();
+  // at least two rows: the FP32 kernel reads a row pair even for a type pair
+  // without a table (it then stops the step with an error)
+  while (xx.size() < 2) { fp.push_back(0); fp.push_back(0); xx.push_back(0); }
   L.nrows = (int)xx.size();
   L.ltab = dupload(ltab, o);
   L.toff = dupload(toff, o);
@@ -431,6 +444,7 @@ void make_args(ibg_ctx* c) {
     a.gslot = c->gslot; a.pos4 = L.pos4; a.pos4_new = L.pos4_new;
     a.posq = L.posq; a.posq_new = L.posq_new;
     a.counts = L.counts; a.slice_w = L.slice_w; a.entries = L.entries; a.w_cap = L.w_cap;
+    a.rgroupsq = L.rgroupsq;
     a.excl_n = c->excl_n; a.excl = c->excl;
     NBArgs<R>& n = A.nb[w];
     n.sc = sc; n.mts = (w == 1 && c->nmts > 0);
@@ -441,6 +455,7 @@ void make_args(ibg_ctx* c) {
     n.ltab = L.ltab; n.toff = L.toff; n.tndat = L.tndat; n.tbin = (const R*)L.tbin; n.tinv = (const R*)L.tinv;
     n.tfp = (const R*)L.tfp; n.tx = (const R*)L.tx; n.ptab = L.ptab; n.chunk = c->nb_chunk;
     n.rows = c->nb_rows;
+    n.window = c->nb_window;
     n.ntab = L.ntab; n.nrows = L.nrows; n.rcutsq = (R)L.rcutsq;
     n.rcut_lo = L.rcutsq * (1.0f - 1e-6f);
     n.rcut_hi = L.rcutsq * (1.0f + 1e-6f);
@@ -857,7 +872,7 @@ int grow_lists(ibg_ctx* c) {
   // the cutoff): their sums are recomputed when the step is repeated
   CK(cudaMemset(c->fb, 0, accsize(c) * 3 * (size_t)c->nitems));
   for (auto& L : c->L)
-    if (L.present) CK(cudaMemset(L.fsort, 0, accsize(c) * 3 * (size_t)L.n));
+    if (L.present) CK(cudaMemset(L.fsort, 0, accsize(c) * fs_len(L.n)));
   CK(cudaMemset(c->sc->nbacc, 0, sizeof(c->sc->nbacc)));
   refresh_args(c);
   for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);  // they bake the old pointers
@@ -928,17 +943,19 @@ int ibg_get_tuning(const ibg_ctx* c, ibg_tuning* t) {
   t->nb_blocks_per_sm = c->nb_blocks_per_sm;
   t->nb_chunk = c->nb_chunk;
   t->nb_rows = c->nb_rows;
+  t->nb_window = c->nb_window;
   return IBG_OK;
 }
 
 int ibg_set_tuning(ibg_ctx* c, const ibg_tuning* t) {
-  if (!c || !t || t->nb_blocks_per_sm < 0 || t->nb_chunk < 0) return IBG_E_INVALID;
+  if (!c || !t || t->nb_blocks_per_sm < 0 || t->nb_chunk < 0 || t->nb_window < 0) return IBG_E_INVALID;
   if (t->nb_rows != 0 && t->nb_rows != 8 && t->nb_rows != 16) return IBG_E_INVALID;
   if (c->in_batch) return fail(c, IBG_E_INVALID, "the context is in a batch");
   try {
     c->nb_blocks_per_sm = t->nb_blocks_per_sm;
     c->nb_chunk = c->prec == IBG_PREC_FP32_FIXED ? t->nb_chunk : 0;
     c->nb_rows = t->nb_rows ? t->nb_rows : 16;
+    c->nb_window = c->prec == IBG_PREC_FP32_FIXED ? t->nb_window : 0;
     for (auto& L : c->L) {
       if (!L.present) continue;
       L.use_smem = t->nb_tables_smem != 0 && L.smem <= 200 * 1024;
@@ -962,12 +979,14 @@ int ibg_autotune(ibg_ctx* c, int reps, ibg_tuning* best, ibg_tuning* cand_out, d
   if (c->prec == IBG_PREC_FP32_FIXED) {
     for (int rows : {8, 16})
       for (int chunk : {0, 12, 24, 48, 96})
-        for (int smem : {0, 1})
-          for (int per : {0, 4, 3}) cand.push_back(ibg_tuning{smem, per, chunk, rows});
+        for (int window : {0, 8})
+          for (int smem : {0, 1})
+            for (int per : {0, 4, 3})
+              if (chunk > 0 || window == 0) cand.push_back(ibg_tuning{smem, per, chunk, rows, window});
   } else {
     for (int rows : {8, 16})
       for (int smem : {0, 1})
-        for (int per : {0, 3, 2}) cand.push_back(ibg_tuning{smem, per, 0, rows});
+        for (int per : {0, 3, 2}) cand.push_back(ibg_tuning{smem, per, 0, rows, 0});
   }
   ibg_tuning keep;
   ibg_get_tuning(c, &keep);
@@ -1028,7 +1047,7 @@ int ibg_autotune(ibg_ctx* c, int reps, ibg_tuning* best, ibg_tuning* cand_out, d
     drop_events();
     // the timing launches summed forces and energies: clear them
     for (auto& L : c->L)
-      if (L.present) CK(cudaMemset(L.fsort, 0, accsize(c) * 3 * (size_t)L.n));
+      if (L.present) CK(cudaMemset(L.fsort, 0, accsize(c) * fs_len(L.n)));
     CK(cudaMemset(c->sc->nbacc, 0, sizeof(c->sc->nbacc)));
     CK(cudaMemset(c->sc->work, 0, sizeof(c->sc->work)));
     unsigned bits = 0;
@@ -1399,7 +1418,7 @@ int ibg_set_state(ibg_ctx* c, const float* sxyz, const float* vxyz, const float*
     for (auto& L : c->L) {
       if (!L.present) continue;
       alloc_cells(c, L, box);
-      CK(cudaMemsetAsync(L.fsort, 0, accsize(c) * 3 * (size_t)L.n, c->st));
+      CK(cudaMemsetAsync(L.fsort, 0, accsize(c) * fs_len(L.n), c->st));
       if (L.mtsf) CK(cudaMemsetAsync(L.mtsf, 0, accsize(c) * 9 * (size_t)L.n, c->st));
       c->g_regrid[L.which] = grid_for(c, L.cell_cap, 2);
     }
@@ -1629,7 +1648,33 @@ int ibg_get_neighbour_list(ibg_ctx* c, int which, int* list, int maxnab, int* nn
     CK(cudaMemcpy(idx.data(), L.idx, sizeof(int) * L.n, cudaMemcpyDeviceToHost));
     std::vector<int> e(list ? (size_t)L.nslices * 32 * L.w_cap : 0);
     if (!e.empty()) CK(cudaMemcpy(e.data(), L.entries, sizeof(int) * e.size(), cudaMemcpyDeviceToHost));
+    // lists stored in two groups (rgroupsq) are put back in the reference's
+    // order: the own cell, then the 13 stencil cells, each by decreasing slot
+    const bool regroup = list && L.rgroupsq > 0.f;
+    std::vector<int> cell_of;
+    int nc[3] = {0, 0, 0};
+    if (regroup) {
+      cell_of.resize(L.n);
+      CK(cudaMemcpy(cell_of.data(), L.cell_of, sizeof(int) * L.n, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(nc, c->sc->ncell[which], sizeof(nc), cudaMemcpyDeviceToHost));
+    }
+    auto run_of = [&](int s, int t) {
+      const int ci = cell_of[sorted[s]], cj = cell_of[sorted[t]];
+      if (ci == cj) return 0;
+      const int a[3] = {ci / (nc[2] * nc[1]), (ci / nc[2]) % nc[1], ci % nc[2]};
+      const int b[3] = {cj / (nc[2] * nc[1]), (cj / nc[2]) % nc[1], cj % nc[2]};
+      int d[3];
+      for (int q = 0; q < 3; ++q) {
+        d[q] = b[q] - a[q];
+        if (d[q] > 1) d[q] -= nc[q];
+        if (d[q] < -1) d[q] += nc[q];
+      }
+      for (int u = 0; u < 13; ++u)
+        if (d[0] == kStencilHost[u][0] && d[1] == kStencilHost[u][1] && d[2] == kStencilHost[u][2]) return u + 1;
+      return 14;  // not a stencil cell: cannot happen for a list built on this grid
+    };
     const int T = L.T, P = 32 / L.T;
+    std::vector<std::pair<int, int>> keyed;
     for (int s = 0; s < L.n; ++s) {
       const int a = sorted[s];
       const int g = s / P, lane0 = (s % P) * T;
@@ -1637,9 +1682,16 @@ int ibg_get_neighbour_list(ibg_ctx* c, int which, int* list, int maxnab, int* nn
       if (!list) continue;
       if (counts[s] >= maxnab) return fail(c, IBG_E_INVALID, "maxnab smaller than a list");
       int* col = list + (size_t)a * maxnab;
+      keyed.clear();
+      for (int k = 0; k < counts[s]; ++k) {
+        const int t = e[((size_t)g * L.w_cap + (size_t)(k / T)) * 32 + lane0 + (k % T)];
+        keyed.emplace_back(regroup ? run_of(s, t) : 0, regroup ? -t : k);
+      }
+      if (regroup) std::sort(keyed.begin(), keyed.end());
       for (int k = 0; k < maxnab; ++k) {
         if (k < counts[s]) {
-          int t = e[((size_t)g * L.w_cap + (size_t)(k / T)) * 32 + lane0 + (k % T)];
+          const int t = regroup ? -keyed[k].second
+                                : e[((size_t)g * L.w_cap + (size_t)(k / T)) * 32 + lane0 + (k % T)];
           col[k] = idx[sorted[t]] + 1;
         } else {
           col[k] = 0;

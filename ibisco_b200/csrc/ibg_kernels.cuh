@@ -408,6 +408,11 @@ struct ListArgs {
   int nslices;       // slices of the list storage
   float rlist, rlistsq;
   double rlistd, rlistsqd;
+  // FP32 path: accepted pairs at r^2 >= rgroupsq (rc + skin/4, squared) are
+  // stored after the others, each group in the reference's order, so that
+  // list rows far beyond the cutoff are mostly skipped whole by the
+  // nonbonded kernel's warps; 0 keeps the reference's order throughout
+  float rgroupsq;
   const int* idx;    // INDEX_LIST, 0-based global ids
   int* cell_of;      // [n] cell of list entry A
   int* cell_count;   // [cell_cap]
@@ -671,14 +676,22 @@ __global__ void k_slot_of(__grid_constant__ const ListArgs L0, const ListArgs* c
 // needs more than w_cap rows records its need and raises the abort flag (the
 // host enlarges the storage and repeats the step).
 // The 13 neighbour cells of the half stencil in MAPS.f90:39-51 order.
-__constant__ int kStencil[13][3] = {{1, 0, 0}, {1, 1, 0},  {0, 1, 0},  {-1, 1, 0}, {1, 0, -1}, {1, 1, -1}, {0, 1, -1},
-                                    {-1, 1, -1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}, {-1, 1, 1}, {0, 0, 1}};
+#define IBG_HALF_STENCIL                                                                                    \
+  {{1, 0, 0}, {1, 1, 0},  {0, 1, 0},  {-1, 1, 0}, {1, 0, -1}, {1, 1, -1}, {0, 1, -1},                        \
+   {-1, 1, -1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}, {-1, 1, 1}, {0, 0, 1}}
+__constant__ int kStencil[13][3] = IBG_HALF_STENCIL;
+static const int kStencilHost[13][3] = IBG_HALF_STENCIL;  // the same, for host code
 
 // Candidates one block stages (positions and slots): 2,304 in FP32 (about 160
 // particles per cell), 1,152 in FP64, within 48 KB of static shared memory.
 // A staged slot carries its run (0..13) in bits 27..30, so lists hold fewer
 // than 2^27 particles.
 constexpr int kSlotMask = (1 << 27) - 1;
+// Entries of the outer group (ListArgs::rgroupsq) a list build holds back to
+// append after the others: per warp in the warp-per-particle build, per
+// thread in the thread-per-particle build.
+constexpr int kLateWarp = 48;
+constexpr int kLateThread = 24;
 template <typename R>
 struct ListStage {
   static constexpr int cap = sizeof(R) == 4 ? 2304 : 1152;
@@ -704,15 +717,18 @@ __global__ void __launch_bounds__(256, 4) k_list_build_warp(__grid_constant__ co
   __shared__ int s_hi[14], s_pre[15];  // run u: slots s_hi[u] down, staged from s_pre[u]
   __shared__ R s_sh[14][3];            // run u: periodic image shift, 0 or +-L per axis
   __shared__ int s_exs[kWarps][20];    // each warp's particle's exclusions, as slots of this list
+  __shared__ int s_late[kWarps][kLateWarp];  // each warp's entries of the outer group (rgroupsq), in order
   __shared__ int s_cell;
   const int nx = sc->ncell[L.which][0], ny = sc->ncell[L.which][1], nz = sc->ncell[L.which][2];
   const int ncells = nx * ny * nz;
   R b[3], bi[3], b2[3];
   box_of<R>(sc, b, bi, b2);
   const R rlsq = sizeof(R) == 4 ? (R)L.rlistsq : (R)L.rlistsqd;
+  const R rg = L.rgroupsq > 0.f ? (R)L.rgroupsq : rlsq;
   const PT* pos = (const PT*)L.pos4;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned below = (1u << lane) - 1u;
+  int* late = s_late[warp];
   const int cap = L.w_cap * T;  // entries a slot may hold
   int* exs = s_exs[warp];
   for (;;) {
@@ -798,7 +814,7 @@ __global__ void __launch_bounds__(256, 4) k_list_build_warp(__grid_constant__ co
       const int e0 = ne > 0 ? exs[0] : -1, e1 = ne > 1 ? exs[1] : -1, e2 = ne > 2 ? exs[2] : -1,
                 e3 = ne > 3 ? exs[3] : -1;
       const bool i_vs = L.hybrid && i >= L.natoms;
-      int cnt = 0;
+      int cnt = 0, nlate = 0;
       // minimum image: d - s with s the run's image shift.  For a pair inside
       // RLIST <= L/3 that shift is the nearest image, so s = ANINT(d/L)*L
       // exactly and d - s is the reference's d - ANINT(d/L)*L bit for bit;
@@ -807,6 +823,7 @@ __global__ void __launch_bounds__(256, 4) k_list_build_warp(__grid_constant__ co
         const int v = v0 + lane;
         bool ok = false;
         int t = -1;
+        R r2 = (R)0;
         if (v < total) {
           PT pj;
           int tu;
@@ -823,7 +840,7 @@ __global__ void __launch_bounds__(256, 4) k_list_build_warp(__grid_constant__ co
           d0 = d0 - sh[0];
           d1 = d1 - sh[1];
           d2 = d2 - sh[2];
-          R r2 = d0 * d0;
+          r2 = d0 * d0;
           r2 = r2 + d1 * d1;
           r2 = r2 + d2 * d2;
           ok = r2 < rlsq && !(i_vs && (Prec<R>::bits(pj.w) >> 16) == 3) && t != e0 && t != e1 && t != e2 &&
@@ -831,13 +848,28 @@ __global__ void __launch_bounds__(256, 4) k_list_build_warp(__grid_constant__ co
           if (ok && ne > 4)
             for (int e = 4; e < ne; ++e) ok &= exs[e] != t;
         }
-        const unsigned m = __ballot_sync(0xffffffffu, ok);
-        if (ok) {
+        // entries of the outer group go to the warp's stage while it has
+        // room (the rest are written in place, which only mixes the groups)
+        const bool outer = ok && r2 >= rg;
+        const unsigned mo = __ballot_sync(0xffffffffu, outer);
+        const int po = __popc(mo & below), room = kLateWarp - nlate;
+        const bool staged_late = outer && po < room;
+        const bool now = ok && !staged_late;
+        const unsigned m = __ballot_sync(0xffffffffu, now);
+        if (now) {
           const int k = cnt + __popc(m & below);
           if (k < cap) ((int*)L.entries)[base + (long long)(k / T) * 32 + (k % T)] = t;
         }
+        if (staged_late) late[nlate + po] = t;
         cnt += __popc(m);
+        nlate += min(__popc(mo), room);
       }
+      __syncwarp();
+      for (int q = lane; q < nlate; q += 32) {
+        const int k = cnt + q;
+        if (k < cap) ((int*)L.entries)[base + (long long)(k / T) * 32 + (k % T)] = late[q];
+      }
+      cnt += nlate;
       if (lane == 0) {
         L.counts[s] = cnt;
         if (cnt >= L.maxnab) atomicOr(&sc->err, EB_LIST_OVERFLOW);
@@ -896,11 +928,13 @@ __global__ void __launch_bounds__(256) k_list_build_thread(__grid_constant__ con
   if (sc->skip || !(always || sc->rebuild)) return;
   constexpr int P = 32 / T;
   __shared__ int s_ex[16][256];  // exclusions 5..20 of each thread's particle, as slots of this list
+  __shared__ int s_late[kLateThread][256];  // each thread's entries of the outer group (rgroupsq), in order
   const int nx = sc->ncell[L.which][0], ny = sc->ncell[L.which][1], nz = sc->ncell[L.which][2];
   const int nc[3] = {nx, ny, nz};
   R b[3], bi[3], b2[3];
   box_of<R>(sc, b, bi, b2);
   const R rlsq = sizeof(R) == 4 ? (R)L.rlistsq : (R)L.rlistsqd;
+  const R rg = L.rgroupsq > 0.f ? (R)L.rgroupsq : rlsq;
   const PT* pos = (const PT*)L.pos4;
   const int lane = threadIdx.x & 31;
   const int cap = L.w_cap * T;  // entries a slot may hold
@@ -930,7 +964,7 @@ __global__ void __launch_bounds__(256) k_list_build_thread(__grid_constant__ con
     const bool i_vs = L.hybrid && i >= L.natoms;
     const int g = s / P;
     int* row = L.entries + (long long)g * L.w_cap * 32 + (s % P) * T;
-    int cnt = 0;
+    int cnt = 0, nlate = 0;
     // candidates slot hi down to lo, displaced by the run's image shift
     auto scan = [&](int hi, int lo, R sh0, R sh1, R sh2) {
 #pragma unroll 4
@@ -948,8 +982,12 @@ __global__ void __launch_bounds__(256) k_list_build_thread(__grid_constant__ con
           if (ok && ne > 4)
             for (int e = 4; e < ne; ++e) ok &= s_ex[e - 4][threadIdx.x] != t;
           if (ok) {
-            if (cnt < cap) row[(cnt / T) * 32 + cnt % T] = t;
-            ++cnt;
+            if (r2 >= rg && nlate < kLateThread) {
+              s_late[nlate++][threadIdx.x] = t;  // the outer group, appended below
+            } else {
+              if (cnt < cap) row[(cnt / T) * 32 + cnt % T] = t;
+              ++cnt;
+            }
           }
         }
       }
@@ -969,6 +1007,8 @@ __global__ void __launch_bounds__(256) k_list_build_thread(__grid_constant__ con
       const int c = jc[0] * nz * ny + jc[1] * nz + jc[2];
       scan(L.cell_start[c + 1] - 1, L.cell_start[c], sh[0], sh[1], sh[2]);
     }
+    for (int q = 0; q < nlate; ++q, ++cnt)
+      if (cnt < cap) row[(cnt / T) * 32 + cnt % T] = s_late[q][threadIdx.x];
     L.counts[s] = cnt;
     if (cnt >= L.maxnab) atomicOr(&sc->err, EB_LIST_OVERFLOW);
     const int rows = (cnt + T - 1) / T;
@@ -998,7 +1038,7 @@ struct NBArgs {
   const int* entries;
   int w_cap;                       // rows of 32 entries per slice
   int work;                        // index of this launch's work counter
-  typename Prec<R>::acc_t* fsort;  // [3][n]: the x, y and z sums of every slot in turn
+  typename Prec<R>::acc_t* fsort;  // per slot, in blocks of 32 slots (fs_at)
   // tables of this list: ltab[ti*ntype+tj] = local table or -1; rows of table
   // t are [toff[t], toff[t+1]); fp = {F,P} per row, x = RNBOND per row
   const int* ltab;
@@ -1008,6 +1048,8 @@ struct NBArgs {
   const R* tinv; // 1/bin per table (FP32 force kernel)
   const int4* ptab;  // FP32 kernel: per type pair {first row, NDAT, 1/bin bits, 1 if a table}
   int chunk;         // FP32 kernel: 256ths of the units taken dynamically after the blocks' own ranges (0: all, per warp)
+  int window;        // FP32 kernel, chunk > 0: 0 = each block one contiguous range of units; W > 0 = runs of W
+                     // consecutive units dealt to the blocks in turn (block b takes runs b, b + G, b + 2G, ...)
   int rows;          // list rows per work unit, a multiple of kEnergyRows
   // FP32 kernel: pairs whose r^2 lies within a relative 1e-6 of the cutoff
   // are left to k_nb_near, which decides them as the FP64 path does from the
@@ -1148,9 +1190,10 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded(__grid_constant__ const NB
       const R fx = fij * d0, fy = fij * d1, fz = fij * d2;
       const reg_t qx = P::q(fx, &sc->err), qy = P::q(fy, &sc->err), qz = P::q(fz, &sc->err);
       fi0 += qx; fi1 += qy; fi2 += qz;
-      P::add(&A.fsort[t], -qx);
-      P::add(&A.fsort[(size_t)A.n + t], -qy);
-      P::add(&A.fsort[2 * (size_t)A.n + t], -qz);
+      typename P::acc_t* fj = A.fsort + fs_at(t);
+      P::add(fj, -qx);
+      P::add(fj + 32, -qy);
+      P::add(fj + 64, -qz);
       acc[3] += (double)(fx * d0);
       acc[4] += (double)(fy * d1);
       acc[5] += (double)(fz * d2);
@@ -1177,9 +1220,10 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded(__grid_constant__ const NB
       fi2 += __shfl_down_sync(0xffffffffu, fi2, o, T);
     }
     if (q == 0 && valid && r0 * T < cnt) {
-      P::add(&A.fsort[s], fi0);
-      P::add(&A.fsort[(size_t)A.n + s], fi1);
-      P::add(&A.fsort[2 * (size_t)A.n + s], fi2);
+      typename P::acc_t* fo = A.fsort + fs_at(s);
+      P::add(fo, fi0);
+      P::add(fo + 32, fi1);
+      P::add(fo + 64, fi2);
     }
   }
   if (err) atomicOr(&sc->err, err);
@@ -1193,6 +1237,9 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded(__grid_constant__ const NB
 // round(v * 2^S) to the nearest 64-bit integer: the scaling by a power of two
 // is exact and the conversion rounds to nearest.  Values of magnitude
 // 2^(63-S) and above (and Inf/NaN) raise EB_FIXED and count as 0.
+// fabsf(fij) r below 0.99 kFixMax, tested on the force scaled by 2^32
+constexpr float kFixLimScaled = 0.99f * kFixMax * kFixScale;
+
 template <int S>
 __device__ __forceinline__ long long fixq(float v, unsigned& err) {
   const float s = v * (float)(1ull << S);
@@ -1214,7 +1261,7 @@ __device__ __forceinline__ long long fixq(float v, unsigned& err) {
 // integer sums depend neither on which warp took which unit nor on the rows
 // per unit, so they are reproducible and the same alone or in a batch.
 template <bool SMEM, int T, bool B>
-__global__ void __launch_bounds__(256, B ? 4 : 5) k_nonbonded_f32(__grid_constant__ const NBArgs<float> A0,
+__global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ const NBArgs<float> A0,
                                                           const NBArgs<float>* const* tab, const BlockMap bm) {
   constexpr int PS = 32 / T;
   pdl_wait();
@@ -1268,13 +1315,20 @@ __global__ void __launch_bounds__(256, B ? 4 : 5) k_nonbonded_f32(__grid_constan
     const int4 pi = valid ? pos[s] : make_int4(0, 0, 0, 0);
     const int wi = pi.w;
     const int ti = wi & 0xffff, li = wi >> 16;
+    const int4* pti = ptab + ti * A.ntype;  // descriptors of (ti, tj) for every tj
+    // the energy term of a pair follows from j's label once i's is fixed:
+    // V_NB(1) when i is an atom, V_NB(3) when i is a virtual site; when i is
+    // a bead, V_NB(2) for a bead j and V_NB(3) for a site j
+    const bool i_bead = li == 2;
     long long fi0 = 0, fi1 = 0, fi2 = 0;
     // energies and virials: FP32 over kEnergyRows rows (aligned to multiples of
     // kEnergyRows), then fixed point, so that their sums depend neither on the
     // rows per unit nor on which warp took which unit
     for (int b0 = r0; b0 < r1; b0 += kEnergyRows) {
       const int b1 = min(r1, b0 + kEnergyRows);
-      float e[3] = {0.f, 0.f, 0.f}, vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      // em: the term of i's label (and bead-bead); e3: bead i with site j.
+      // The virials are summed scaled by -2^32 (exact: a power of two).
+      float em = 0.f, e3 = 0.f, vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       auto pair = [&](int t, const int4& pj) {
         // nearest image: the wrapped difference of the box fractions (it and
         // ANINT could choose differently only at |d| = L/2, beyond the cutoff)
@@ -1290,40 +1344,43 @@ __global__ void __launch_bounds__(256, B ? 4 : 5) k_nonbonded_f32(__grid_constan
         }
         const int wj = pj.w;
         const int tj = wj & 0xffff, lj = wj >> 16;
-        const int4 pt = ptab[ti * A.ntype + tj];
-        if (!pt.w) { err |= EB_MISSING_TABLE; return; }
+        const int4 pt = pti[tj];
         const float r = r2 * rsqrtf(r2);
         const float ib = __int_as_float(pt.z);
-        const int ni = (int)(r * ib);
-        if (ni > pt.y) { err |= EB_TABLE_RANGE; return; }
+        int ni = (int)(r * ib);
+        // a missing table (all-zero descriptor) or a distance beyond the table
+        // stops the step with an error; the rows read stay inside the arrays
+        // (they hold at least two rows), so no branch is needed here
+        err |= pt.w ? 0u : (unsigned)EB_MISSING_TABLE;
+        err |= ni > pt.y ? (unsigned)EB_TABLE_RANGE : 0u;
+        ni = min(ni, pt.y);
         const int row = pt.x + ni;
         const float alpha = (r - tx[row]) * ib;
         const float2 a0 = tfp[row], a1 = tfp[row + 1];
         const float fij = __fmaf_rn(a1.x - a0.x, alpha, a0.x);
         const float vij = __fmaf_rn(a1.y - a0.y, alpha, a0.y);
-        // V_NB(1) atom pairs, V_NB(2) bead-bead, V_NB(3) pairs with a virtual site
-        const bool lab3 = li == 3 || lj == 3;
-        e[0] += li == 1 ? vij : 0.f;
-        e[1] += (li == 2 && lj == 2) ? vij : 0.f;
-        e[2] += (li != 1 && lab3) ? vij : 0.f;
+        em += (!i_bead || lj == 2) ? vij : 0.f;
+        e3 += (i_bead && lj == 3) ? vij : 0.f;
+        // j's share in fixed point, round(-f * 2^32): fs * d equals the
+        // product f_c * -2^32 exactly (scaling by a power of two), and
+        // round-to-nearest is symmetric, so i's share is exactly its negation.
         // |f component| <= |fij| r (to rounding): one test keeps every
         // component in range
-        if (!(fabsf(fij) * r < 0.99f * kFixMax)) { err |= EB_FIXED; return; }
-        const float fx = fij * d0, fy = fij * d1, fz = fij * d2;
-        // j's share, round(-f * 2^32): the scaling is exact and round-to-nearest
-        // is symmetric, so i's share is exactly its negation (subtracted below)
-        const long long qx = __float2ll_rn(fx * -kFixScale), qy = __float2ll_rn(fy * -kFixScale),
-                        qz = __float2ll_rn(fz * -kFixScale);
+        const float fs = fij * -kFixScale;
+        err |= fabsf(fs) * r < kFixLimScaled ? 0u : (unsigned)EB_FIXED;
+        const float sx = fs * d0, sy = fs * d1, sz = fs * d2;
+        const long long qx = __float2ll_rn(sx), qy = __float2ll_rn(sy), qz = __float2ll_rn(sz);
         fi0 -= qx; fi1 -= qy; fi2 -= qz;
-        atomicAdd((unsigned long long*)&A.fsort[t], (unsigned long long)qx);
-        atomicAdd((unsigned long long*)&A.fsort[(size_t)A.n + t], (unsigned long long)qy);
-        atomicAdd((unsigned long long*)&A.fsort[2 * (size_t)A.n + t], (unsigned long long)qz);
-        vir[0] = __fmaf_rn(fx, d0, vir[0]);
-        vir[1] = __fmaf_rn(fy, d1, vir[1]);
-        vir[2] = __fmaf_rn(fz, d2, vir[2]);
-        vir[3] = __fmaf_rn(fy, d0, vir[3]);
-        vir[4] = __fmaf_rn(fz, d0, vir[4]);
-        vir[5] = __fmaf_rn(fz, d1, vir[5]);
+        unsigned long long* fj = (unsigned long long*)A.fsort + fs_at(t);
+        atomicAdd(fj, (unsigned long long)qx);
+        atomicAdd(fj + 32, (unsigned long long)qy);
+        atomicAdd(fj + 64, (unsigned long long)qz);
+        vir[0] = __fmaf_rn(sx, d0, vir[0]);
+        vir[1] = __fmaf_rn(sy, d1, vir[1]);
+        vir[2] = __fmaf_rn(sz, d2, vir[2]);
+        vir[3] = __fmaf_rn(sy, d0, vir[3]);
+        vir[4] = __fmaf_rn(sz, d0, vir[4]);
+        vir[5] = __fmaf_rn(sz, d1, vir[5]);
       };
       // list entries are read once per launch: loaded evict-first (__ldcs),
       // so that the streamed list does not push the positions and force sums
@@ -1338,10 +1395,10 @@ __global__ void __launch_bounds__(256, B ? 4 : 5) k_nonbonded_f32(__grid_constan
         if (v0) pair(t0, p0);
         if (v1) pair(t1, p1);
       }
+      la[(li == 1 ? 0 : (i_bead ? 1 : 2)) * blockDim.x] += fixq<24>(em, err);
+      la[2 * blockDim.x] += fixq<24>(e3, err);
 #pragma unroll
-      for (int k = 0; k < 3; ++k) la[k * blockDim.x] += fixq<24>(e[k], err);
-#pragma unroll
-      for (int k = 0; k < 6; ++k) la[(3 + k) * blockDim.x] += fixq<24>(vir[k], err);
+      for (int k = 0; k < 6; ++k) la[(3 + k) * blockDim.x] += fixq<24>(vir[k] * -0x1p-32f, err);
     }
 #pragma unroll
     for (int o = T / 2; o > 0; o >>= 1) {
@@ -1350,9 +1407,10 @@ __global__ void __launch_bounds__(256, B ? 4 : 5) k_nonbonded_f32(__grid_constan
       fi2 += __shfl_down_sync(0xffffffffu, fi2, o, T);
     }
     if (q == 0 && valid && r0 * T < cnt) {
-      atomicAdd((unsigned long long*)&A.fsort[s], (unsigned long long)fi0);
-      atomicAdd((unsigned long long*)&A.fsort[(size_t)A.n + s], (unsigned long long)fi1);
-      atomicAdd((unsigned long long*)&A.fsort[2 * (size_t)A.n + s], (unsigned long long)fi2);
+      unsigned long long* fo = (unsigned long long*)A.fsort + fs_at(s);
+      atomicAdd(fo, (unsigned long long)fi0);
+      atomicAdd(fo + 32, (unsigned long long)fi1);
+      atomicAdd(fo + 64, (unsigned long long)fi2);
     }
   };
   if (A.chunk > 0) {
@@ -1366,13 +1424,28 @@ __global__ void __launch_bounds__(256, B ? 4 : 5) k_nonbonded_f32(__grid_constan
     __syncthreads();
     const int tail = (int)((long long)nunits * min(A.chunk, 256) / 256);
     const int nstat = nunits - tail;
-    const int lo = (int)((long long)nstat * bk.b / bk.g), hi = (int)((long long)nstat * (bk.b + 1) / bk.g);
-    for (;;) {
-      int k = 0;
-      if (lane == 0) k = atomicAdd(&s_next, 1);
-      k = __shfl_sync(0xffffffffu, k, 0);
-      if (lo + k >= hi) break;
-      unit(lo + k);
+    if (A.window > 0) {
+      // runs of W consecutive units dealt to the blocks in turn: the blocks
+      // advance together through one window of space, whose positions and
+      // force sums then stay in L2, while a block's warps still share a run
+      const int W = A.window;
+      for (;;) {
+        int k = 0;
+        if (lane == 0) k = atomicAdd(&s_next, 1);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        const long long u = ((long long)(k / W) * bk.g + bk.b) * W + k % W;
+        if (u >= nstat) break;
+        unit((int)u);
+      }
+    } else {
+      const int lo = (int)((long long)nstat * bk.b / bk.g), hi = (int)((long long)nstat * (bk.b + 1) / bk.g);
+      for (;;) {
+        int k = 0;
+        if (lane == 0) k = atomicAdd(&s_next, 1);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        if (lo + k >= hi) break;
+        unit(lo + k);
+      }
     }
     for (;;) {
       int u = 0;
@@ -1488,13 +1561,14 @@ __global__ void __launch_bounds__(256) k_nb_near(__grid_constant__ const NBArgs<
     const float fx = fij * d0, fy = fij * d1, fz = fij * d2;
     const long long qx = __float2ll_rn(fx * kFixScale), qy = __float2ll_rn(fy * kFixScale),
                     qz = __float2ll_rn(fz * kFixScale);
-    unsigned long long* fs = (unsigned long long*)A.fsort;
-    atomicAdd(fs + s, (unsigned long long)qx);
-    atomicAdd(fs + (size_t)A.n + s, (unsigned long long)qy);
-    atomicAdd(fs + 2 * (size_t)A.n + s, (unsigned long long)qz);
-    atomicAdd(fs + t, (unsigned long long)(-qx));
-    atomicAdd(fs + (size_t)A.n + t, (unsigned long long)(-qy));
-    atomicAdd(fs + 2 * (size_t)A.n + t, (unsigned long long)(-qz));
+    unsigned long long* fsi = (unsigned long long*)A.fsort + fs_at(s);
+    unsigned long long* fsj = (unsigned long long*)A.fsort + fs_at(t);
+    atomicAdd(fsi, (unsigned long long)qx);
+    atomicAdd(fsi + 32, (unsigned long long)qy);
+    atomicAdd(fsi + 64, (unsigned long long)qz);
+    atomicAdd(fsj, (unsigned long long)(-qx));
+    atomicAdd(fsj + 32, (unsigned long long)(-qy));
+    atomicAdd(fsj + 64, (unsigned long long)(-qz));
     const bool lab3 = li == 3 || lj == 3;
     const long long qe = fixq<24>(vij, err);
     if (li == 1) acc[0] += qe;
@@ -1550,12 +1624,12 @@ __global__ void k_nb_collect(__grid_constant__ const CollectArgs<R> C0, const Co
       // as the compiler knows)
       typename P::acc_t v[3];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) v[c] = C.fsort[c * (size_t)C.n + s];
+      for (int c = 0; c < 3; ++c) v[c] = C.fsort[fs_at(s) + 32 * c];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         C.fnb[3 * (size_t)gi + c] = v[c];
         if (C.mts) C.mtsf[((size_t)(m - 1) * C.n + a) * 3 + c] = v[c];
-        C.fsort[c * (size_t)C.n + s] = 0;
+        C.fsort[fs_at(s) + 32 * c] = 0;
       }
     } else {
       const double coef = (double)(m - 3) * 0.5;

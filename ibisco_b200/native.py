@@ -80,7 +80,7 @@ class IbgDesc(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("nb_tables_smem", ctypes.c_int), ("nb_blocks_per_sm", ctypes.c_int), ("nb_chunk", ctypes.c_int),
-                ("nb_rows", ctypes.c_int)]
+                ("nb_rows", ctypes.c_int), ("nb_window", ctypes.c_int)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -416,8 +416,9 @@ class System:
         sum).  Call before set_state."""
         self._check(lib().ibg_set_vsite_com(self._h, int(form)))
 
-    def set_tuning(self, nb_tables_smem: int = 0, nb_blocks_per_sm: int = 0, nb_chunk: int = 0, nb_rows: int = 0):
-        t = Tuning(nb_tables_smem, nb_blocks_per_sm, nb_chunk, nb_rows)
+    def set_tuning(self, nb_tables_smem: int = 0, nb_blocks_per_sm: int = 0, nb_chunk: int = 0, nb_rows: int = 0,
+                   nb_window: int = 0):
+        t = Tuning(nb_tables_smem, nb_blocks_per_sm, nb_chunk, nb_rows, nb_window)
         self._check(lib().ibg_set_tuning(self._h, ctypes.byref(t)))
 
     def autotune(self, reps: int = 20):
@@ -430,7 +431,7 @@ class System:
         n = lib().ibg_autotune(self._h, int(reps), ctypes.byref(best), cand, us, cap)
         if n < 0:
             self._check(n)
-        return best.as_dict(), [((c.nb_tables_smem, c.nb_blocks_per_sm, c.nb_chunk, c.nb_rows), us[k])
+        return best.as_dict(), [((c.nb_tables_smem, c.nb_blocks_per_sm, c.nb_chunk, c.nb_rows, c.nb_window), us[k])
                                 for k, c in enumerate(cand[:min(n, cap)])]
 
     def set_timing(self, on: bool):

@@ -228,7 +228,9 @@ int ibg_set_list_rows(ibg_ctx* c, int rows);
    gather from one region of space, and the last nb_chunk/256 of the units are
    taken dynamically by whichever warps finish first (0: every warp takes
    units alone, dynamically); nb_rows: list rows per work unit, 8 or 16 (0:
-   16).  Forces and trajectories do not depend on the tuning (integer force
+   16); nb_window (FP32 path, nb_chunk > 0): 0 gives each block one contiguous
+   range of units, W > 0 deals runs of W consecutive units to the blocks in
+   turn, so that all blocks work through one region of space at a time.  Forces and trajectories do not depend on the tuning (integer force
    sums); on the FP32 path nonbonded energies and virials are summed in groups
    of 8 list rows before their exact fixed-point sum, so they do not depend on
    it either.  Set it before a batch is made of the context.
@@ -243,6 +245,7 @@ typedef struct ibg_tuning {
   int nb_blocks_per_sm;
   int nb_chunk;
   int nb_rows;
+  int nb_window;
 } ibg_tuning;
 int ibg_get_tuning(const ibg_ctx* c, ibg_tuning* t);
 int ibg_set_tuning(ibg_ctx* c, const ibg_tuning* t);

@@ -305,13 +305,17 @@ def test_tuning_changes_no_trajectory(sysdir):
     _, a = make(d, native.IBG_PREC_FP32_FIXED)
     _, b = make(d, native.IBG_PREC_FP32_FIXED)
     _, c = make(d, native.IBG_PREC_FP32_FIXED)
+    _, w = make(d, native.IBG_PREC_FP32_FIXED)
     best, cands = a.autotune(reps=3)
     assert len(cands) >= 2 and all(us > 0 for _, us in cands)
     assert a.tuning() == best
     c.set_tuning(nb_tables_smem=1 - best["nb_tables_smem"], nb_blocks_per_sm=2,
                  nb_chunk=16 if best["nb_chunk"] == 0 else 0, nb_rows=8 if best["nb_rows"] == 16 else 16)
+    # runs of two units dealt to the blocks in turn
+    w.set_tuning(nb_tables_smem=0, nb_blocks_per_sm=0, nb_chunk=24, nb_rows=8, nb_window=2)
     oa, ob, oc = a.run(1, 20, observe=True), b.run(1, 20, observe=True), c.run(1, 20, observe=True)
-    sa, sb, sc = a.state64(), b.state64(), c.state64()
+    ow = w.run(1, 20, observe=True)
+    sa, sb, sc, sw = a.state64(), b.state64(), c.state64(), w.state64()
     for k in ("sxyz", "vxyz", "fxyz"):
-        assert np.array_equal(sa[k], sb[k]) and np.array_equal(sb[k], sc[k])
-    assert oa == ob == oc
+        assert np.array_equal(sa[k], sb[k]) and np.array_equal(sb[k], sc[k]) and np.array_equal(sa[k], sw[k])
+    assert oa == ob == oc == ow
