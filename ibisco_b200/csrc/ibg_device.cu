@@ -358,7 +358,7 @@ void build_list(ibg_ctx* c, const ibg_desc* d, int which) {
   }
   const size_t rs = rsize(c);
   L.smem = c->prec == IBG_PREC_FP32_FIXED
-               ? 9 * 256 * sizeof(double) + sizeof(int4) * (size_t)NT * NT + 12 * (size_t)L.nrows + 64
+               ? kNbAccBytes + sizeof(int4) * (size_t)NT * NT + 12 * (size_t)L.nrows + 64
                : 9 * 256 * sizeof(double) + rs * 3 * (size_t)L.nrows + 2 * rs * L.ntab +
                      sizeof(int) * ((size_t)NT * NT + 2 * L.ntab + 1) + 64;
   // launch defaults (ibg_set_tuning / ibg_autotune change them): the FP32
@@ -624,7 +624,7 @@ NBKernel<double, true> nb_kernel<double, true>(bool smem, int T) { return nb_ker
 
 // Dynamic shared memory of a nonbonded launch over list L.
 size_t nb_smem(const ibg_ctx* c, const DevList& L) {
-  const size_t base = c->prec == IBG_PREC_FP32_FIXED ? 9 * 256 * sizeof(long long) : 9 * 8 * sizeof(double);
+  const size_t base = c->prec == IBG_PREC_FP32_FIXED ? (size_t)kNbAccBytes : 9 * 8 * sizeof(double);
   return L.use_smem ? L.smem : base;
 }
 
@@ -636,7 +636,21 @@ int nb_occupancy(const ibg_ctx* c, const DevList& L, size_t sm) {
   if (sm > 48 * 1024) CK(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   int per = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k, 256, sm));
-  return std::max(1, per);
+  per = std::max(1, per);
+  // L1 and shared memory share each SM's 256 KB: ask for the smallest
+  // shared-memory carveout that holds `per` blocks and leave the rest to L1,
+  // which caches the position gathers and the table rows (the driver rounds
+  // the request up to a configuration the SM supports)
+  cudaFuncAttributes fa;
+  CK(cudaFuncGetAttributes(&fa, (const void*)k));
+  int dev = 0, maxsm = 0, resv = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+  CK(cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+  const size_t need = (size_t)per * (sm + fa.sharedSizeBytes + (size_t)resv);
+  const int pct = maxsm > 0 ? (int)std::min<size_t>(100, (need * 100 + (size_t)maxsm - 1) / (size_t)maxsm) : 100;
+  CK(cudaFuncSetAttribute((const void*)k, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+  return per;
 }
 
 template <typename R>

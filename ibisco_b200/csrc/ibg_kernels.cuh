@@ -1239,6 +1239,10 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded(__grid_constant__ const NB
 // 2^(63-S) and above (and Inf/NaN) raise EB_FIXED and count as 0.
 // fabsf(fij) r below 0.99 kFixMax, tested on the force scaled by 2^32
 constexpr float kFixLimScaled = 0.99f * kFixMax * kFixScale;
+// The FP32 nonbonded kernel's energy and virial sums: 9 per pair of lanes of
+// its 256-thread blocks, at the start of its dynamic shared memory.
+constexpr int kNbPairs = 128;
+constexpr int kNbAccBytes = 9 * kNbPairs * (int)sizeof(long long);
 
 template <int S>
 __device__ __forceinline__ long long fixq(float v, unsigned& err) {
@@ -1273,13 +1277,16 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
   Scalars* sc = A.sc;
   if (nb_idle(A)) return;
   extern __shared__ unsigned char smem_raw[];
-  long long* lacc = (long long*)smem_raw;  // [9][blockDim.x] per-lane sums
+  // [9][kNbPairs] sums of each pair of lanes (the two lanes of a pair serve
+  // the same particle): half the shared memory of per-lane sums, which leaves
+  // more of the SM's 256 KB to L1
+  long long* lacc = (long long*)smem_raw;
   // per type pair {first row, last row index, 1/bin bits, has a table}
   const int4* ptab = A.ptab;
   const float2* tfp = (const float2*)A.tfp;
   const float* tx = A.tx;
   {
-    unsigned char* p = smem_raw + 9 * 256 * sizeof(double);
+    unsigned char* p = smem_raw + kNbAccBytes;
     if (SMEM) {
       int4* s_ptab = (int4*)p;       p += sizeof(int4) * A.ntype * A.ntype;
       float2* s_fp = (float2*)p;     p += sizeof(float2) * A.nrows;
@@ -1289,7 +1296,8 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
       ptab = s_ptab; tfp = s_fp; tx = s_x;
     }
   }
-  for (int k = 0; k < 9; ++k) lacc[k * blockDim.x + threadIdx.x] = 0;
+  if (!(threadIdx.x & 1))
+    for (int k = 0; k < 9; ++k) lacc[k * kNbPairs + (threadIdx.x >> 1)] = 0;
   __syncthreads();
   // displacement unit per axis: L / 2^32
   const float ux = (float)(sc->box[0] * 0x1p-32), uy = (float)(sc->box[1] * 0x1p-32), uz = (float)(sc->box[2] * 0x1p-32);
@@ -1301,7 +1309,7 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
   const int rows = A.rows;
   const int U = (A.w_cap + rows - 1) / rows;
   const int nunits = A.nslices * U;
-  long long* la = lacc + threadIdx.x;
+  long long* la = lacc + (threadIdx.x >> 1);
   auto unit = [&](int u) {
     const int g = u / U;
     const int r0 = (u - g * U) * rows;
@@ -1395,10 +1403,19 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
         if (v0) pair(t0, p0);
         if (v1) pair(t1, p1);
       }
-      la[(li == 1 ? 0 : (i_bead ? 1 : 2)) * blockDim.x] += fixq<24>(em, err);
-      la[2 * blockDim.x] += fixq<24>(e3, err);
+      long long v[8];
+      v[0] = fixq<24>(em, err);
+      v[1] = fixq<24>(e3, err);
 #pragma unroll
-      for (int k = 0; k < 6; ++k) la[(3 + k) * blockDim.x] += fixq<24>(vir[k] * -0x1p-32f, err);
+      for (int k = 0; k < 6; ++k) v[2 + k] = fixq<24>(vir[k] * -0x1p-32f, err);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], 1);
+      if (!(lane & 1)) {
+        la[(li == 1 ? 0 : (i_bead ? 1 : 2)) * kNbPairs] += v[0];
+        la[2 * kNbPairs] += v[1];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) la[(3 + k) * kNbPairs] += v[2 + k];
+      }
     }
 #pragma unroll
     for (int o = T / 2; o > 0; o >>= 1) {
@@ -1465,7 +1482,7 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
   }
   if (err) atomicOr(&sc->err, err);
   long long acc[9];
-  for (int k = 0; k < 9; ++k) acc[k] = lacc[k * blockDim.x + threadIdx.x];
+  for (int k = 0; k < 9; ++k) acc[k] = (threadIdx.x & 1) ? 0 : lacc[k * kNbPairs + (threadIdx.x >> 1)];
   __syncthreads();
   block_sum_i64<9>(acc, lacc);
   if (threadIdx.x < 9 && lacc[threadIdx.x] != 0)
