@@ -114,6 +114,7 @@ struct DevList {
   int *ltab = nullptr, *toff = nullptr, *tndat = nullptr;
   int4* ptab = nullptr;  // per type pair: first row, NDAT, 1/bin bits, table present
   void *tbin = nullptr, *tinv = nullptr, *tfp = nullptr, *tx = nullptr;
+  float4* tcoef = nullptr;  // FP32 path: per row {F - dF e, dF, P - dP e, dP} (NBArgs::tcoef)
   int ntab = 0, nrows = 0;
   size_t smem = 0;
   bool use_smem = false;
@@ -344,6 +345,22 @@ void build_list(ibg_ctx* c, const ibg_desc* d, int which) {
     std::vector<float> f1(fp.begin(), fp.end()), x1(xx.begin(), xx.end()), b1(bin.begin(), bin.end()), i1(bin.size());
     for (size_t k = 0; k < bin.size(); ++k) i1[k] = (float)(1.0 / (double)(float)bin[k]);
     L.tfp = dupload(f1, o); L.tx = dupload(x1, o); L.tbin = dupload(b1, o); L.tinv = dupload(i1, o);
+    // interpolation coefficients of every row k of table t (local index n =
+    // k - toff[t]): with u = r/bin - n, the kernel's alpha = (r - X_k)/bin
+    // is u - e_k, e_k = X_k/bin - n, so F = F_k + (F_k+1 - F_k) alpha is
+    // (F_k - dF e_k) + dF u, and the same for P; computed in FP64 from the
+    // FP32 rows the kernel would otherwise read
+    std::vector<float4> co(L.nrows, make_float4(0.f, 0.f, 0.f, 0.f));
+    for (int t = 0; t < L.ntab; ++t)
+      for (int k = toff[t]; k < toff[t + 1]; ++k) {
+        const bool last = k + 1 >= toff[t + 1];
+        const double fk = f1[2 * (size_t)k], pk = f1[2 * (size_t)k + 1];
+        const double df = last ? 0.0 : (double)f1[2 * (size_t)k + 2] - fk;
+        const double dp = last ? 0.0 : (double)f1[2 * (size_t)k + 3] - pk;
+        const double e = (double)x1[k] * (double)i1[t] - (double)(k - toff[t]);
+        co[k] = make_float4((float)(fk - df * e), (float)df, (float)(pk - dp * e), (float)dp);
+      }
+    L.tcoef = dupload(co, o);
     std::vector<int4> pt((size_t)NT * NT);
     for (size_t k = 0; k < pt.size(); ++k) {
       const int t = ltab[k];
@@ -358,7 +375,7 @@ void build_list(ibg_ctx* c, const ibg_desc* d, int which) {
   }
   const size_t rs = rsize(c);
   L.smem = c->prec == IBG_PREC_FP32_FIXED
-               ? kNbAccBytes + sizeof(int4) * (size_t)NT * NT + 12 * (size_t)L.nrows + 64
+               ? kNbAccBytes + sizeof(int4) * (size_t)NT * NT + sizeof(float4) * (size_t)L.nrows + 64
                : 9 * 256 * sizeof(double) + rs * 3 * (size_t)L.nrows + 2 * rs * L.ntab +
                      sizeof(int) * ((size_t)NT * NT + 2 * L.ntab + 1) + 64;
   // launch defaults (ibg_set_tuning / ibg_autotune change them): the FP32
@@ -454,6 +471,7 @@ void make_args(ibg_ctx* c) {
     n.fsort = (acc_t*)L.fsort;
     n.ltab = L.ltab; n.toff = L.toff; n.tndat = L.tndat; n.tbin = (const R*)L.tbin; n.tinv = (const R*)L.tinv;
     n.tfp = (const R*)L.tfp; n.tx = (const R*)L.tx; n.ptab = L.ptab; n.chunk = c->nb_chunk;
+    n.tcoef = L.tcoef;
     n.rows = c->nb_rows;
     n.window = c->nb_window;
     n.ntab = L.ntab; n.nrows = L.nrows; n.rcutsq = (R)L.rcutsq;

@@ -1062,6 +1062,9 @@ struct NBArgs {
   const double* S;
   int natoms;
   const R* tfp;  // 2 per row
+  // FP32 kernel: per row {A, B, C, D}, F = A + B u and P = C + D u with
+  // u = r/bin - (row within the table); one 16-byte read per pair
+  const float4* tcoef;
   const R* tx;
   int ntab, nrows;
   R rcutsq;
@@ -1283,17 +1286,15 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
   long long* lacc = (long long*)smem_raw;
   // per type pair {first row, last row index, 1/bin bits, has a table}
   const int4* ptab = A.ptab;
-  const float2* tfp = (const float2*)A.tfp;
-  const float* tx = A.tx;
+  const float4* tco = A.tcoef;
   {
     unsigned char* p = smem_raw + kNbAccBytes;
     if (SMEM) {
       int4* s_ptab = (int4*)p;       p += sizeof(int4) * A.ntype * A.ntype;
-      float2* s_fp = (float2*)p;     p += sizeof(float2) * A.nrows;
-      float* s_x = (float*)p;
-      for (int k = threadIdx.x; k < A.nrows; k += blockDim.x) { s_fp[k] = ((const float2*)A.tfp)[k]; s_x[k] = A.tx[k]; }
+      float4* s_co = (float4*)p;
+      for (int k = threadIdx.x; k < A.nrows; k += blockDim.x) s_co[k] = A.tcoef[k];
       for (int k = threadIdx.x; k < A.ntype * A.ntype; k += blockDim.x) s_ptab[k] = A.ptab[k];
-      ptab = s_ptab; tfp = s_fp; tx = s_x;
+      ptab = s_ptab; tco = s_co;
     }
   }
   if (!(threadIdx.x & 1))
@@ -1354,19 +1355,19 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
         const int tj = wj & 0xffff, lj = wj >> 16;
         const int4 pt = pti[tj];
         const float r = r2 * rsqrtf(r2);
-        const float ib = __int_as_float(pt.z);
-        int ni = (int)(r * ib);
+        const float rb = r * __int_as_float(pt.z);  // r / bin
+        int ni = (int)rb;
         // a missing table (all-zero descriptor) or a distance beyond the table
-        // stops the step with an error; the rows read stay inside the arrays
-        // (they hold at least two rows), so no branch is needed here
+        // stops the step with an error; the row read stays inside the array
+        // (it holds at least two rows), so no branch is needed here
         err |= pt.w ? 0u : (unsigned)EB_MISSING_TABLE;
         err |= ni > pt.y ? (unsigned)EB_TABLE_RANGE : 0u;
         ni = min(ni, pt.y);
-        const int row = pt.x + ni;
-        const float alpha = (r - tx[row]) * ib;
-        const float2 a0 = tfp[row], a1 = tfp[row + 1];
-        const float fij = __fmaf_rn(a1.x - a0.x, alpha, a0.x);
-        const float vij = __fmaf_rn(a1.y - a0.y, alpha, a0.y);
+        // linear interpolation between rows ni and ni + 1 (NONBONDED_FORCE.F90:66-74)
+        const float u = rb - (float)ni;
+        const float4 co = tco[pt.x + ni];
+        const float fij = __fmaf_rn(co.y, u, co.x);
+        const float vij = __fmaf_rn(co.w, u, co.z);
         em += (!i_bead || lj == 2) ? vij : 0.f;
         e3 += (i_bead && lj == 3) ? vij : 0.f;
         // j's share in fixed point, round(-f * 2^32): fs * d equals the
