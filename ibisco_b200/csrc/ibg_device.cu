@@ -114,12 +114,13 @@ struct DevList {
   int *ltab = nullptr, *toff = nullptr, *tndat = nullptr;
   int4* ptab = nullptr;  // per type pair: first row, NDAT, 1/bin bits, table present
   void *tbin = nullptr, *tinv = nullptr, *tfp = nullptr, *tx = nullptr;
-  float4* tcoef = nullptr;  // FP32 path: per row {F - dF e, dF, P - dP e, dP} (NBArgs::tcoef)
+  float4* tcoef = nullptr;  // FP32 path: per row {F - dF e, P - dP e, dF, dP} (NBArgs::tcoef)
   int ntab = 0, nrows = 0;
   size_t smem = 0;
   bool use_smem = false;
   float rlist = 0, rlistsq = 0, rcutsq = 0;
   float rgroupsq = 0;  // FP32 path: outer group of the stored lists (ListArgs::rgroupsq); 0: reference order
+  bool mixed = true;   // the list holds particles of more than one label (k_nonbonded_f32's MIXED)
   int grid_nb = 0;
 };
 
@@ -276,6 +277,13 @@ void build_list(ibg_ctx* c, const ibg_desc* d, int which) {
   // on the 40,000-bead melt 72, 61, 59, 59, 62 and 59 us.
   L.T = 8;
   L.nslices = (L.n + 32 / L.T - 1) / (32 / L.T);
+  // one label throughout (an atom list, or a CG list without virtual sites):
+  // every pair adds to that label's energy term
+  {
+    auto lab = [&](int i) { return i < d->natoms ? d->type_label[i] : 3; };
+    L.mixed = false;
+    for (int i : idx) L.mixed = L.mixed || lab(i) != lab(idx[0]);
+  }
   auto& o = c->owned;
   L.idx = dupload(idx, o);
   L.cell_of = dalloc<int>(L.n, o);
@@ -358,7 +366,7 @@ void build_list(ibg_ctx* c, const ibg_desc* d, int which) {
         const double df = last ? 0.0 : (double)f1[2 * (size_t)k + 2] - fk;
         const double dp = last ? 0.0 : (double)f1[2 * (size_t)k + 3] - pk;
         const double e = (double)x1[k] * (double)i1[t] - (double)(k - toff[t]);
-        co[k] = make_float4((float)(fk - df * e), (float)df, (float)(pk - dp * e), (float)dp);
+        co[k] = make_float4((float)(fk - df * e), (float)(pk - dp * e), (float)df, (float)dp);
       }
     L.tcoef = dupload(co, o);
     std::vector<int4> pt((size_t)NT * NT);
@@ -594,51 +602,29 @@ void enq_rebuild(ibg_ctx* c, DevList& L, int always) {
 template <typename R, bool B>
 using NBKernel = void (*)(const NBArgs<R>, const NBArgs<R>* const*, const BlockMap);
 
+// The nonbonded kernel of a list: tables staged in shared memory or read
+// through L1 (smem), and on the FP32 path whether the list mixes labels.
+// Lists are built for eight lanes per particle.
 template <typename R, bool B>
-NBKernel<R, B> nb_kernel(bool smem, int T);
+NBKernel<R, B> nb_kernel(bool smem, bool mixed);
 
 template <bool B>
-NBKernel<float, B> nb_kernel_f(bool smem, int T) {
-  if (smem) {
-    switch (T) {
-      case 1: return k_nonbonded_f32<true, 1, B>;
-      case 2: return k_nonbonded_f32<true, 2, B>;
-      case 4: return k_nonbonded_f32<true, 4, B>;
-      default: return k_nonbonded_f32<true, 8, B>;
-    }
-  }
-  switch (T) {
-    case 1: return k_nonbonded_f32<false, 1, B>;
-    case 2: return k_nonbonded_f32<false, 2, B>;
-    case 4: return k_nonbonded_f32<false, 4, B>;
-    default: return k_nonbonded_f32<false, 8, B>;
-  }
-}
-template <bool B>
-NBKernel<double, B> nb_kernel_d(bool smem, int T) {
-  if (smem) {
-    switch (T) {
-      case 1: return k_nonbonded<double, true, 1, B>;
-      case 2: return k_nonbonded<double, true, 2, B>;
-      case 4: return k_nonbonded<double, true, 4, B>;
-      default: return k_nonbonded<double, true, 8, B>;
-    }
-  }
-  switch (T) {
-    case 1: return k_nonbonded<double, false, 1, B>;
-    case 2: return k_nonbonded<double, false, 2, B>;
-    case 4: return k_nonbonded<double, false, 4, B>;
-    default: return k_nonbonded<double, false, 8, B>;
-  }
+NBKernel<float, B> nb_kernel_f(bool smem, bool mixed) {
+  if (smem) return mixed ? k_nonbonded_f32<true, true, B> : k_nonbonded_f32<true, false, B>;
+  return mixed ? k_nonbonded_f32<false, true, B> : k_nonbonded_f32<false, false, B>;
 }
 template <>
-NBKernel<float, false> nb_kernel<float, false>(bool smem, int T) { return nb_kernel_f<false>(smem, T); }
+NBKernel<float, false> nb_kernel<float, false>(bool smem, bool mixed) { return nb_kernel_f<false>(smem, mixed); }
 template <>
-NBKernel<float, true> nb_kernel<float, true>(bool smem, int T) { return nb_kernel_f<true>(smem, T); }
+NBKernel<float, true> nb_kernel<float, true>(bool smem, bool mixed) { return nb_kernel_f<true>(smem, mixed); }
 template <>
-NBKernel<double, false> nb_kernel<double, false>(bool smem, int T) { return nb_kernel_d<false>(smem, T); }
+NBKernel<double, false> nb_kernel<double, false>(bool smem, bool) {
+  return smem ? k_nonbonded<double, true, 8, false> : k_nonbonded<double, false, 8, false>;
+}
 template <>
-NBKernel<double, true> nb_kernel<double, true>(bool smem, int T) { return nb_kernel_d<true>(smem, T); }
+NBKernel<double, true> nb_kernel<double, true>(bool smem, bool) {
+  return smem ? k_nonbonded<double, true, 8, true> : k_nonbonded<double, false, 8, true>;
+}
 
 // Dynamic shared memory of a nonbonded launch over list L.
 size_t nb_smem(const ibg_ctx* c, const DevList& L) {
@@ -650,7 +636,7 @@ size_t nb_smem(const ibg_ctx* c, const DevList& L) {
 // dynamic shared-memory limit when needed).
 template <typename R, bool B>
 int nb_occupancy(const ibg_ctx* c, const DevList& L, size_t sm) {
-  NBKernel<R, B> k = nb_kernel<R, B>(L.use_smem, L.T);
+  NBKernel<R, B> k = nb_kernel<R, B>(L.use_smem, L.mixed);
   if (sm > 48 * 1024) CK(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   int per = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k, 256, sm));
@@ -682,7 +668,7 @@ void nb_configure(ibg_ctx* c, DevList& L) {
 
 template <typename R>
 void enq_nonbonded(ibg_ctx* c, DevList& L) {
-  launch_pdl(c, nb_kernel<R, false>(L.use_smem, L.T), L.grid_nb, 256, nb_smem(c, L), args<R>(c).nb[L.which],
+  launch_pdl(c, nb_kernel<R, false>(L.use_smem, L.mixed), L.grid_nb, 256, nb_smem(c, L), args<R>(c).nb[L.which],
              (const NBArgs<R>* const*)nullptr, kOne);
   if (c->prec == IBG_PREC_FP32_FIXED)
     launch_pdl(c, k_nb_near<false>, 1, 256, 0, args<float>(c).nb[L.which], (const NBArgs<float>* const*)nullptr, kOne);
@@ -1808,6 +1794,7 @@ struct BMap {
 struct NBGroup {
   int T = 1;
   bool smem = false;
+  bool mixed = true;  // nonbonded groups: lists of more than one label
   size_t sm = 0;
   BMap map;
 };
@@ -1917,26 +1904,26 @@ void batch_layout(ibg_batch* b) {
       grp.map = make_map(b, g);
       b->lb[w].push_back(grp);
     }
-    // nonbonded: one group per (T, smem); the group's resident blocks are
-    // shared among its systems in proportion to their work units
+    // nonbonded: one group per (labels mixed, smem); the group's resident
+    // blocks are shared among its systems in proportion to their work units
     std::set<std::pair<int, int>> keys;
     for (size_t s = 0; s < n; ++s)
-      if (b->sys[s]->L[w].present) keys.insert({b->sys[s]->L[w].T, (int)b->sys[s]->L[w].use_smem});
+      if (b->sys[s]->L[w].present) keys.insert({(int)b->sys[s]->L[w].mixed, (int)b->sys[s]->L[w].use_smem});
     for (auto key : keys) {
       NBGroup grp;
-      grp.T = key.first;
+      grp.mixed = key.first != 0;
       grp.smem = key.second != 0;
       double units = 0;
       for (size_t s = 0; s < n; ++s) {
         const DevList& L = b->sys[s]->L[w];
-        if (!(L.present && L.T == grp.T && (int)L.use_smem == key.second)) continue;
+        if (!(L.present && (int)L.mixed == key.first && (int)L.use_smem == key.second)) continue;
         grp.sm = std::max(grp.sm, nb_smem(b->sys[s], L));
         units += (double)L.nslices * ((L.w_cap + 7) / 8);
       }
       int per = 1;
       for (size_t s = 0; s < n; ++s) {
         const DevList& L = b->sys[s]->L[w];
-        if (L.present && L.T == grp.T && (int)L.use_smem == key.second) {
+        if (L.present && (int)L.mixed == key.first && (int)L.use_smem == key.second) {
           per = nb_occupancy<R, true>(b->sys[s], L, grp.sm);
           break;
         }
@@ -1944,7 +1931,7 @@ void batch_layout(ibg_batch* b) {
       const double resident = (double)b->nsm * per;
       for (size_t s = 0; s < n; ++s) {
         const DevList& L = b->sys[s]->L[w];
-        if (!(L.present && L.T == grp.T && (int)L.use_smem == key.second)) { g[s] = 0; continue; }
+        if (!(L.present && (int)L.mixed == key.first && (int)L.use_smem == key.second)) { g[s] = 0; continue; }
         const double u = (double)L.nslices * ((L.w_cap + 7) / 8);
         g[s] = std::max(1, std::min(L.grid_nb, (int)std::lround(resident * u / std::max(units, 1.0))));
       }
@@ -2005,7 +1992,7 @@ void batch_enqueue(ibg_batch* b, unsigned v) {
   // each list (one block per system with the list, as the cell scan)
   for (int w : {1, 0}) {
     for (const NBGroup& grp : b->nb[w]) {
-      launch_on(st, true, nb_kernel<R, true>(grp.smem, grp.T), grp.map.grid, 256, grp.sm, NBArgs<R>{},
+      launch_on(st, true, nb_kernel<R, true>(grp.smem, grp.mixed), grp.map.grid, 256, grp.sm, NBArgs<R>{},
                 (const NBArgs<R>* const*)b->t_nb[w], grp.map.m());
       ++n;
     }

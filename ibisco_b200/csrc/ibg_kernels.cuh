@@ -1062,7 +1062,7 @@ struct NBArgs {
   const double* S;
   int natoms;
   const R* tfp;  // 2 per row
-  // FP32 kernel: per row {A, B, C, D}, F = A + B u and P = C + D u with
+  // FP32 kernel: per row {A, C, B, D}, F = A + B u and P = C + D u with
   // u = r/bin - (row within the table); one 16-byte read per pair
   const float4* tcoef;
   const R* tx;
@@ -1267,9 +1267,13 @@ __device__ __forceinline__ long long fixq(float v, unsigned& err) {
 // (2^-24) per lane and per block, and added to the system's accumulators:
 // integer sums depend neither on which warp took which unit nor on the rows
 // per unit, so they are reproducible and the same alone or in a batch.
-template <bool SMEM, int T, bool B>
+// MIXED: the list holds particles of more than one label, so each pair's
+// energy term depends on j's label; otherwise every pair adds to the term of
+// the list's one label.
+template <bool SMEM, bool MIXED, bool B>
 __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ const NBArgs<float> A0,
                                                           const NBArgs<float>* const* tab, const BlockMap bm) {
+  constexpr int T = 8;  // lanes per particle (the lists are built for eight)
   constexpr int PS = 32 / T;
   pdl_wait();
   pdl_trigger();
@@ -1302,6 +1306,7 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
   __syncthreads();
   // displacement unit per axis: L / 2^32
   const float ux = (float)(sc->box[0] * 0x1p-32), uy = (float)(sc->box[1] * 0x1p-32), uz = (float)(sc->box[2] * 0x1p-32);
+  const float2 uxy = make_float2(ux, uy);
   const int4* pos = A.posq;
   const int lane = threadIdx.x & 31, grp = lane / T, q = lane % T;
   unsigned err = 0;
@@ -1337,12 +1342,17 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
       const int b1 = min(r1, b0 + kEnergyRows);
       // em: the term of i's label (and bead-bead); e3: bead i with site j.
       // The virials are summed scaled by -2^32 (exact: a power of two).
-      float em = 0.f, e3 = 0.f, vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      float em = 0.f, e3 = 0.f;
+      float2 v03 = make_float2(0.f, 0.f), v15 = v03, v24 = v03;  // virial pairs (0,3), (1,5), (2,4)
       auto pair = [&](int t, const int4& pj) {
         // nearest image: the wrapped difference of the box fractions (it and
         // ANINT could choose differently only at |d| = L/2, beyond the cutoff)
-        const float d0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * ux;
-        const float d1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * uy;
+        // packed FP32 pairs (fmul/ffma .f32x2) round each element as the
+        // scalar instructions do
+        const float2 d01 = __fmul2_rn(make_float2((float)(int)((unsigned)pi.x - (unsigned)pj.x),
+                                                  (float)(int)((unsigned)pi.y - (unsigned)pj.y)),
+                                      uxy);
+        const float d0 = d01.x, d1 = d01.y;
         const float d2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * uz;
         const float r2 = __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, d0 * d0));
         if (!(r2 < A.rcut_hi)) return;
@@ -1365,11 +1375,15 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
         ni = min(ni, pt.y);
         // linear interpolation between rows ni and ni + 1 (NONBONDED_FORCE.F90:66-74)
         const float u = rb - (float)ni;
-        const float4 co = tco[pt.x + ni];
-        const float fij = __fmaf_rn(co.y, u, co.x);
-        const float vij = __fmaf_rn(co.w, u, co.z);
-        em += (!i_bead || lj == 2) ? vij : 0.f;
-        e3 += (i_bead && lj == 3) ? vij : 0.f;
+        const float4 co = tco[pt.x + ni];  // {F base, P base, dF, dP}
+        const float2 fv = __ffma2_rn(make_float2(co.z, co.w), make_float2(u, u), make_float2(co.x, co.y));
+        const float fij = fv.x, vij = fv.y;
+        if (MIXED) {
+          em += (!i_bead || lj == 2) ? vij : 0.f;
+          e3 += (i_bead && lj == 3) ? vij : 0.f;
+        } else {
+          em += vij;
+        }
         // j's share in fixed point, round(-f * 2^32): fs * d equals the
         // product f_c * -2^32 exactly (scaling by a power of two), and
         // round-to-nearest is symmetric, so i's share is exactly its negation.
@@ -1377,19 +1391,18 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
         // component in range
         const float fs = fij * -kFixScale;
         err |= fabsf(fs) * r < kFixLimScaled ? 0u : (unsigned)EB_FIXED;
-        const float sx = fs * d0, sy = fs * d1, sz = fs * d2;
+        const float2 sxy = __fmul2_rn(make_float2(fs, fs), d01);
+        const float sx = sxy.x, sy = sxy.y, sz = fs * d2;
         const long long qx = __float2ll_rn(sx), qy = __float2ll_rn(sy), qz = __float2ll_rn(sz);
         fi0 -= qx; fi1 -= qy; fi2 -= qz;
         unsigned long long* fj = (unsigned long long*)A.fsort + fs_at(t);
         atomicAdd(fj, (unsigned long long)qx);
         atomicAdd(fj + 32, (unsigned long long)qy);
         atomicAdd(fj + 64, (unsigned long long)qz);
-        vir[0] = __fmaf_rn(sx, d0, vir[0]);
-        vir[1] = __fmaf_rn(sy, d1, vir[1]);
-        vir[2] = __fmaf_rn(sz, d2, vir[2]);
-        vir[3] = __fmaf_rn(sy, d0, vir[3]);
-        vir[4] = __fmaf_rn(sz, d0, vir[4]);
-        vir[5] = __fmaf_rn(sz, d1, vir[5]);
+        // (xx, yx) += (sx, sy) d0; (yy, zy) += (sy, sz) d1; (zz, zx) += sz (d2, d0)
+        v03 = __ffma2_rn(sxy, make_float2(d0, d0), v03);
+        v15 = __ffma2_rn(make_float2(sy, sz), make_float2(d1, d1), v15);
+        v24 = __ffma2_rn(make_float2(sz, sz), make_float2(d2, d0), v24);
       };
       // list entries are read once per launch: loaded evict-first (__ldcs),
       // so that the streamed list does not push the positions and force sums
@@ -1407,8 +1420,11 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
       long long v[8];
       v[0] = fixq<24>(em, err);
       v[1] = fixq<24>(e3, err);
+      {
+        const float vir[6] = {v03.x, v15.x, v24.x, v03.y, v24.y, v15.y};
 #pragma unroll
-      for (int k = 0; k < 6; ++k) v[2 + k] = fixq<24>(vir[k] * -0x1p-32f, err);
+        for (int k = 0; k < 6; ++k) v[2 + k] = fixq<24>(vir[k] * -0x1p-32f, err);
+      }
 #pragma unroll
       for (int k = 0; k < 8; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], 1);
       if (!(lane & 1)) {
