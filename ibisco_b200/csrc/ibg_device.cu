@@ -997,7 +997,7 @@ int ibg_autotune(ibg_ctx* c, int reps, ibg_tuning* best, ibg_tuning* cand_out, d
   if (c->prec == IBG_PREC_FP32_FIXED) {
     for (int rows : {8, 16})
       for (int chunk : {0, 12, 24, 48, 96})
-        for (int window : {0, 8})
+        for (int window : {0, 64})
           for (int smem : {0, 1})
             for (int per : {0, 4, 3})
               if (chunk > 0 || window == 0) cand.push_back(ibg_tuning{smem, per, chunk, rows, window});
