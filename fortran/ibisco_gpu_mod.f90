@@ -68,6 +68,14 @@ MODULE IBISCO_GPU
        TYPE(C_PTR), INTENT(OUT) :: ctx
      END FUNCTION ibg_create
 
+     !> Verlet-list form of the FP32 path: a list per particle (0, the
+     !> default) or per slice of four slots (1); before ibg_set_state.
+     INTEGER(C_INT) FUNCTION ibg_set_list_form(ctx, form) BIND(C, NAME='ibg_set_list_form')
+       IMPORT :: C_PTR, C_INT
+       TYPE(C_PTR), VALUE :: ctx
+       INTEGER(C_INT), VALUE :: form
+     END FUNCTION ibg_set_list_form
+
      !> Centre-of-mass virtual sites as VIRTUAL_DEF.f90 computes them (1) or
      !> each at its centre of mass (0, the default); before ibg_set_state.
      INTEGER(C_INT) FUNCTION ibg_set_vsite_com(ctx, form) BIND(C, NAME='ibg_set_vsite_com')

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -100,6 +101,11 @@ enum Variant : unsigned {
 struct DevList {
   int n = 0, which = 0, present = 0;
   int T = 1;  // lanes per particle in the list build and the nonbonded kernel (1, 2, 4 or 8)
+  // list form: 0 = a list per particle, T lanes per particle (k_list_build_*,
+  // k_nonbonded_f32 / k_nonbonded); 1 = a list per slice of four slots, each
+  // neighbour once with a mask of its pairs (k_list_build_slices,
+  // k_nonbonded_slices; FP32 path only)
+  int form = 0;
   int cell_cap = 0, nslices = 0;
   int w_cap = 0;  // rows of 32 list entries per slice
   int *idx = nullptr, *cell_of = nullptr, *cell_count = nullptr, *cell_start = nullptr, *cell_fill = nullptr;
@@ -181,6 +187,7 @@ struct ibg_ctx {
   int nb_rows = 16;          // tuning: list rows per nonbonded work unit (8 or 16)
   int nb_window = 0;         // tuning (FP32, nb_chunk > 0): units per run dealt to the blocks in turn (0: one range per block)
   int vs_com_form = IBG_VS_COM_FIXED;  // centre-of-mass virtual sites: fixed or the reference's form
+  int list_form = 0;                   // FP32 path: list form of new lists (DevList::form)
   void* vchain = nullptr;              // the reference form's per-site terms (k_vsite_chain)
   ObsD* ring = nullptr;
   int ring_cap = 0;
@@ -277,6 +284,7 @@ void build_list(ibg_ctx* c, const ibg_desc* d, int which) {
   // on the 40,000-bead melt 72, 61, 59, 59, 62 and 59 us.
   L.T = 8;
   L.nslices = (L.n + 32 / L.T - 1) / (32 / L.T);
+  L.form = c->prec == IBG_PREC_FP32_FIXED && c->list_form == 1 && L.n < (1 << 28) ? 1 : 0;
   // one label throughout (an atom list, or a CG list without virtual sites):
   // every pair adds to that label's energy term
   {
@@ -593,7 +601,9 @@ void enq_rebuild(ibg_ctx* c, DevList& L, int always) {
   // a thread per particle once the list has enough particles to fill the GPU
   // that way (twice the resident warps), a warp per particle below that;
   // both give the same lists
-  if (L.n >= kThreadBuildMin * c->nsm)
+  if (L.form == 1)
+    launch_pdl(c, k_list_build_slices<false>, gl, 256, 0, a, (LA)nullptr, kOne, always);
+  else if (L.n >= kThreadBuildMin * c->nsm)
     launch_pdl(c, k_list_build_thread<R, 8, false>, gl, 256, 0, a, (LA)nullptr, kOne, always);
   else
     launch_pdl(c, k_list_build_warp<R, 8, false>, gl, 256, 0, a, (LA)nullptr, kOne, always);
@@ -603,26 +613,35 @@ template <typename R, bool B>
 using NBKernel = void (*)(const NBArgs<R>, const NBArgs<R>* const*, const BlockMap);
 
 // The nonbonded kernel of a list: tables staged in shared memory or read
-// through L1 (smem), and on the FP32 path whether the list mixes labels.
-// Lists are built for eight lanes per particle.
+// through L1 (smem), on the FP32 path whether the list mixes labels, and the
+// list form (DevList::form).  Per-particle lists are built for eight lanes
+// per particle.
 template <typename R, bool B>
-NBKernel<R, B> nb_kernel(bool smem, bool mixed);
+NBKernel<R, B> nb_kernel(bool smem, bool mixed, int form);
 
 template <bool B>
-NBKernel<float, B> nb_kernel_f(bool smem, bool mixed) {
+NBKernel<float, B> nb_kernel_f(bool smem, bool mixed, int form) {
+  if (form == 1) {
+    if (smem) return mixed ? k_nonbonded_slices<true, true, B> : k_nonbonded_slices<true, false, B>;
+    return mixed ? k_nonbonded_slices<false, true, B> : k_nonbonded_slices<false, false, B>;
+  }
   if (smem) return mixed ? k_nonbonded_f32<true, true, B> : k_nonbonded_f32<true, false, B>;
   return mixed ? k_nonbonded_f32<false, true, B> : k_nonbonded_f32<false, false, B>;
 }
 template <>
-NBKernel<float, false> nb_kernel<float, false>(bool smem, bool mixed) { return nb_kernel_f<false>(smem, mixed); }
+NBKernel<float, false> nb_kernel<float, false>(bool smem, bool mixed, int form) {
+  return nb_kernel_f<false>(smem, mixed, form);
+}
 template <>
-NBKernel<float, true> nb_kernel<float, true>(bool smem, bool mixed) { return nb_kernel_f<true>(smem, mixed); }
+NBKernel<float, true> nb_kernel<float, true>(bool smem, bool mixed, int form) {
+  return nb_kernel_f<true>(smem, mixed, form);
+}
 template <>
-NBKernel<double, false> nb_kernel<double, false>(bool smem, bool) {
+NBKernel<double, false> nb_kernel<double, false>(bool smem, bool, int) {
   return smem ? k_nonbonded<double, true, 8, false> : k_nonbonded<double, false, 8, false>;
 }
 template <>
-NBKernel<double, true> nb_kernel<double, true>(bool smem, bool) {
+NBKernel<double, true> nb_kernel<double, true>(bool smem, bool, int) {
   return smem ? k_nonbonded<double, true, 8, true> : k_nonbonded<double, false, 8, true>;
 }
 
@@ -636,7 +655,7 @@ size_t nb_smem(const ibg_ctx* c, const DevList& L) {
 // dynamic shared-memory limit when needed).
 template <typename R, bool B>
 int nb_occupancy(const ibg_ctx* c, const DevList& L, size_t sm) {
-  NBKernel<R, B> k = nb_kernel<R, B>(L.use_smem, L.mixed);
+  NBKernel<R, B> k = nb_kernel<R, B>(L.use_smem, L.mixed, L.form);
   if (sm > 48 * 1024) CK(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   int per = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k, 256, sm));
@@ -668,7 +687,7 @@ void nb_configure(ibg_ctx* c, DevList& L) {
 
 template <typename R>
 void enq_nonbonded(ibg_ctx* c, DevList& L) {
-  launch_pdl(c, nb_kernel<R, false>(L.use_smem, L.mixed), L.grid_nb, 256, nb_smem(c, L), args<R>(c).nb[L.which],
+  launch_pdl(c, nb_kernel<R, false>(L.use_smem, L.mixed, L.form), L.grid_nb, 256, nb_smem(c, L), args<R>(c).nb[L.which],
              (const NBArgs<R>* const*)nullptr, kOne);
   if (c->prec == IBG_PREC_FP32_FIXED)
     launch_pdl(c, k_nb_near<false>, 1, 256, 0, args<float>(c).nb[L.which], (const NBArgs<float>* const*)nullptr, kOne);
@@ -987,6 +1006,45 @@ int ibg_set_tuning(ibg_ctx* c, const ibg_tuning* t) {
     return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
   }
   return IBG_OK;
+}
+
+int ibg_set_list_form(ibg_ctx* c, int form) {
+  if (!c || form < 0 || form > 1) return IBG_E_INVALID;
+  if (form == 1 && c->prec != IBG_PREC_FP32_FIXED) return fail(c, IBG_E_INVALID, "slice lists are an FP32-path form");
+  if (c->in_batch) return fail(c, IBG_E_INVALID, "the context is in a batch");
+  try {
+    CK(cudaStreamSynchronize(c->st));
+    c->list_form = form;
+    bool changed = false;
+    for (auto& L : c->L) {
+      if (!L.present) continue;
+      const int f = form == 1 && L.n < (1 << 28) ? 1 : 0;
+      if (f == L.form) continue;
+      if (L.entries) c->owned.release(L.entries);
+      L.entries = nullptr;
+      L.w_cap = 0;  // sized by the next build
+      L.form = f;
+      if (c->prec == IBG_PREC_FP32_FIXED) nb_configure<float>(c, L);
+      else nb_configure<double>(c, L);
+      changed = true;
+    }
+    if (changed) {
+      refresh_args(c);
+      for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+      c->graphs.clear();
+      c->state_set = false;  // the lists are rebuilt by the next ibg_set_state
+    }
+  } catch (CudaError& e) {
+    return fail(c, IBG_E_CUDA, cudaGetErrorString(e.e));
+  }
+  return IBG_OK;
+}
+
+int ibg_get_list_form(const ibg_ctx* c) {
+  if (!c) return IBG_E_INVALID;
+  for (const auto& L : c->L)
+    if (L.present) return L.form;
+  return c->prec == IBG_PREC_FP32_FIXED ? c->list_form : 0;
 }
 
 int ibg_autotune(ibg_ctx* c, int reps, ibg_tuning* best, ibg_tuning* cand_out, double* us, int ncand) {
@@ -1666,9 +1724,10 @@ int ibg_get_neighbour_list(ibg_ctx* c, int which, int* list, int maxnab, int* nn
     CK(cudaMemcpy(idx.data(), L.idx, sizeof(int) * L.n, cudaMemcpyDeviceToHost));
     std::vector<int> e(list ? (size_t)L.nslices * 32 * L.w_cap : 0);
     if (!e.empty()) CK(cudaMemcpy(e.data(), L.entries, sizeof(int) * e.size(), cudaMemcpyDeviceToHost));
-    // lists stored in two groups (rgroupsq) are put back in the reference's
-    // order: the own cell, then the 13 stencil cells, each by decreasing slot
-    const bool regroup = list && L.rgroupsq > 0.f;
+    // lists stored in two groups (rgroupsq), and slice lists, are put back in
+    // the reference's order: the own cell, then the 13 stencil cells, each by
+    // decreasing slot
+    const bool regroup = list && (L.rgroupsq > 0.f || L.form == 1);
     std::vector<int> cell_of;
     int nc[3] = {0, 0, 0};
     if (regroup) {
@@ -1692,6 +1751,11 @@ int ibg_get_neighbour_list(ibg_ctx* c, int which, int* list, int maxnab, int* nn
       return 14;  // not a stencil cell: cannot happen for a list built on this grid
     };
     const int T = L.T, P = 32 / L.T;
+    std::vector<int> slice_w;
+    if (list && L.form == 1) {
+      slice_w.resize(L.nslices);
+      CK(cudaMemcpy(slice_w.data(), L.slice_w, sizeof(int) * L.nslices, cudaMemcpyDeviceToHost));
+    }
     std::vector<std::pair<int, int>> keyed;
     for (int s = 0; s < L.n; ++s) {
       const int a = sorted[s];
@@ -1701,9 +1765,22 @@ int ibg_get_neighbour_list(ibg_ctx* c, int which, int* list, int maxnab, int* nn
       if (counts[s] >= maxnab) return fail(c, IBG_E_INVALID, "maxnab smaller than a list");
       int* col = list + (size_t)a * maxnab;
       keyed.clear();
-      for (int k = 0; k < counts[s]; ++k) {
-        const int t = e[((size_t)g * L.w_cap + (size_t)(k / T)) * 32 + lane0 + (k % T)];
-        keyed.emplace_back(regroup ? run_of(s, t) : 0, regroup ? -t : k);
+      if (L.form == 1) {  // the entries of slot s's slice whose mask holds s
+        const unsigned bit = 1u << (s % kUSlots);
+        const size_t base = (size_t)(s / kUSlots) * L.w_cap * 32;
+        const int ne = std::min(slice_w[s / kUSlots], L.w_cap) * 32;
+        for (int k = 0; k < ne; ++k) {
+          const unsigned u = (unsigned)e[base + k];
+          if (((u >> 28) & bit) == 0) continue;
+          const int t = (int)(u & kUSlotMask);
+          keyed.emplace_back(run_of(s, t), -t);
+        }
+        if ((int)keyed.size() != counts[s]) return fail(c, IBG_E_INVALID, "slice list and pair count disagree");
+      } else {
+        for (int k = 0; k < counts[s]; ++k) {
+          const int t = e[((size_t)g * L.w_cap + (size_t)(k / T)) * 32 + lane0 + (k % T)];
+          keyed.emplace_back(regroup ? run_of(s, t) : 0, regroup ? -t : k);
+        }
       }
       if (regroup) std::sort(keyed.begin(), keyed.end());
       for (int k = 0; k < maxnab; ++k) {
@@ -1793,6 +1870,7 @@ struct BMap {
 
 struct NBGroup {
   int T = 1;
+  int form = 0;  // list form (DevList::form)
   bool smem = false;
   bool mixed = true;  // nonbonded groups: lists of more than one label
   size_t sm = 0;
@@ -1890,40 +1968,44 @@ void batch_layout(ibg_batch* b) {
     b->m_list[w] = make_map(b, g);
     for (size_t s = 0; s < n; ++s) g[s] = b->sys[s]->L[w].present ? 1 : 0;
     b->m_scan[w] = make_map(b, g);
-    // list build: one group per T, each system with its own grid
-    std::set<int> Ts;
+    // list build: one group per list form, each system with its own grid
+    std::set<int> forms;
     for (size_t s = 0; s < n; ++s)
-      if (b->sys[s]->L[w].present) Ts.insert(b->sys[s]->L[w].T);
-    for (int T : Ts) {
+      if (b->sys[s]->L[w].present) forms.insert(b->sys[s]->L[w].form);
+    for (int f : forms) {
       NBGroup grp;
-      grp.T = T;
+      grp.T = 8;
+      grp.form = f;
       for (size_t s = 0; s < n; ++s) {
         const DevList& L = b->sys[s]->L[w];
-        g[s] = (L.present && L.T == T) ? b->sys[s]->g_build[w] : 0;
+        g[s] = (L.present && L.form == f) ? b->sys[s]->g_build[w] : 0;
       }
       grp.map = make_map(b, g);
       b->lb[w].push_back(grp);
     }
-    // nonbonded: one group per (labels mixed, smem); the group's resident
-    // blocks are shared among its systems in proportion to their work units
-    std::set<std::pair<int, int>> keys;
+    // nonbonded: one group per (labels mixed, smem, list form); the group's
+    // resident blocks are shared among its systems in proportion to their
+    // work units
+    std::set<std::array<int, 3>> keys;
+    auto key_of = [](const DevList& L) { return std::array<int, 3>{(int)L.mixed, (int)L.use_smem, L.form}; };
     for (size_t s = 0; s < n; ++s)
-      if (b->sys[s]->L[w].present) keys.insert({(int)b->sys[s]->L[w].mixed, (int)b->sys[s]->L[w].use_smem});
+      if (b->sys[s]->L[w].present) keys.insert(key_of(b->sys[s]->L[w]));
     for (auto key : keys) {
       NBGroup grp;
-      grp.mixed = key.first != 0;
-      grp.smem = key.second != 0;
+      grp.mixed = key[0] != 0;
+      grp.smem = key[1] != 0;
+      grp.form = key[2];
       double units = 0;
       for (size_t s = 0; s < n; ++s) {
         const DevList& L = b->sys[s]->L[w];
-        if (!(L.present && (int)L.mixed == key.first && (int)L.use_smem == key.second)) continue;
+        if (!(L.present && key_of(L) == key)) continue;
         grp.sm = std::max(grp.sm, nb_smem(b->sys[s], L));
         units += (double)L.nslices * ((L.w_cap + 7) / 8);
       }
       int per = 1;
       for (size_t s = 0; s < n; ++s) {
         const DevList& L = b->sys[s]->L[w];
-        if (L.present && (int)L.mixed == key.first && (int)L.use_smem == key.second) {
+        if (L.present && key_of(L) == key) {
           per = nb_occupancy<R, true>(b->sys[s], L, grp.sm);
           break;
         }
@@ -1931,7 +2013,7 @@ void batch_layout(ibg_batch* b) {
       const double resident = (double)b->nsm * per;
       for (size_t s = 0; s < n; ++s) {
         const DevList& L = b->sys[s]->L[w];
-        if (!(L.present && (int)L.mixed == key.first && (int)L.use_smem == key.second)) { g[s] = 0; continue; }
+        if (!(L.present && key_of(L) == key)) { g[s] = 0; continue; }
         const double u = (double)L.nslices * ((L.w_cap + 7) / 8);
         g[s] = std::max(1, std::min(L.grid_nb, (int)std::lround(resident * u / std::max(units, 1.0))));
       }
@@ -1983,7 +2065,10 @@ void batch_enqueue(ibg_batch* b, unsigned v) {
       n += 7;
       for (const NBGroup& grp : b->lb[w]) {
         const BlockMap bm = grp.map.m();
-        launch_on(st, true, k_list_build_warp<R, 8, true>, grp.map.grid, 256, 0, ListArgs{}, t, bm, 0);
+        if (grp.form == 1)
+          launch_on(st, true, k_list_build_slices<true>, grp.map.grid, 256, 0, ListArgs{}, t, bm, 0);
+        else
+          launch_on(st, true, k_list_build_warp<R, 8, true>, grp.map.grid, 256, 0, ListArgs{}, t, bm, 0);
         ++n;
       }
     }
@@ -1992,7 +2077,7 @@ void batch_enqueue(ibg_batch* b, unsigned v) {
   // each list (one block per system with the list, as the cell scan)
   for (int w : {1, 0}) {
     for (const NBGroup& grp : b->nb[w]) {
-      launch_on(st, true, nb_kernel<R, true>(grp.smem, grp.mixed), grp.map.grid, 256, grp.sm, NBArgs<R>{},
+      launch_on(st, true, nb_kernel<R, true>(grp.smem, grp.mixed, grp.form), grp.map.grid, 256, grp.sm, NBArgs<R>{},
                 (const NBArgs<R>* const*)b->t_nb[w], grp.map.m());
       ++n;
     }

@@ -1021,6 +1021,234 @@ __global__ void __launch_bounds__(256) k_list_build_thread(__grid_constant__ con
   }
 }
 
+// Slice lists (FP32 path, ListArgs/NBArgs form 1).  Slice g is the four
+// slots 4g..4g+3.  Its list holds each neighbour once, as the entry
+// slot | mask << 28, where bit k of the mask says that slot 4g+k pairs with
+// it: the union of the four half lists, with no pair added or lost.  The
+// four slots are consecutive in the cell order, so their lists share most of
+// their neighbours (a stored entry stands for ~1.9 pairs on the melts), and
+// the nonbonded kernel gathers each neighbour's position and adds its force
+// once per slice instead of once per pair.  Entry e of slice g lives at
+// g*w_cap*32 + e; the last row is filled up with empty entries (mask 0).
+constexpr int kUSlots = 4;
+constexpr unsigned kUSlotMask = (1u << 28) - 1u;
+constexpr int kUBuf = 256;  // entries of a slice each warp sorts in shared memory
+
+// NEW_NEIGHBOUR_WITHLIST.f90:34-123 in the slice form: a warp builds one
+// slice's list.  For each cell that holds particles of the slice (one, or two
+// when the slice straddles a cell boundary) it walks that cell's candidates,
+// 32 at a time, one per lane: the own cell below the slice's last particle
+// there, then the 13 stencil cells of MAPS.f90:39-51, each by decreasing slot.
+// A lane tests its candidate against each particle of the slice in that cell
+// with the reference's REAL*4 distance (the run's image shift gives the
+// nearest image, as in k_list_build_thread), the own-cell rule (only slots
+// below the particle), the virtual-site rule and the particle's exclusions.
+// A candidate that two cells of a slice both reach is stored once per cell,
+// with disjoint masks, so every pair is stored exactly once.
+//
+// The accepted entries are gathered in shared memory and stored sorted by
+// the key (outer group, mask), stably: first the entries with a pair inside
+// rgroupsq, by mask, then the rest, by mask.  So a row of 32 entries mostly
+// shares one mask, and the nonbonded kernel's warp runs the pair arithmetic
+// once per bit of that mask with all its lanes busy, instead of once per
+// particle of the slice with the lanes whose masks hold it.  Entries beyond
+// the first kUBuf of a slice are stored unsorted after them.  counts[s] is the
+// number of pairs of slot s (its reference NNEBS).
+template <bool B>
+__global__ void __launch_bounds__(256) k_list_build_slices(__grid_constant__ const ListArgs L0,
+                                                          const ListArgs* const* tab, const BlockMap bm, int always) {
+  pdl_wait();
+  pdl_trigger();
+  const Blk bk = blk<B>(bm);
+  __shared__ ListArgs s_args;
+  if (B) stage_args(&s_args, tab[bk.sys]);
+  const ListArgs& L = B ? s_args : L0;
+  Scalars* sc = L.sc;
+  if (sc->skip || !(always || sc->rebuild)) return;
+  constexpr int kWarps = 8;
+  __shared__ int s_ex[kWarps][kUSlots][20];  // each particle's exclusions as slots of this list
+  __shared__ int s_buf[kWarps][kUBuf];       // the slice's entries, in the order accepted
+  __shared__ unsigned char s_key[kWarps][kUBuf];  // their keys: mask | 16 for the outer group
+  __shared__ int s_off[kWarps][32];          // per key: count, then next position
+  const int nx = sc->ncell[L.which][0], ny = sc->ncell[L.which][1], nz = sc->ncell[L.which][2];
+  const int nc[3] = {nx, ny, nz};
+  float b[3], bi[3], b2[3];
+  box_of<float>(sc, b, bi, b2);
+  const float rlsq = L.rlistsq;
+  const float rg = L.rgroupsq > 0.f ? L.rgroupsq : rlsq;
+  const float4* pos = (const float4*)L.pos4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned below = (1u << lane) - 1u;
+  int* buf = s_buf[warp];
+  unsigned char* keys = s_key[warp];
+  int* off = s_off[warp];
+  const int cap = L.w_cap * 32;  // entries a slice may hold
+  for (;;) {
+    int g = 0;
+    if (lane == 0) g = (int)atomicAdd(&sc->work[2 + L.which], 1u);
+    g = __shfl_sync(0xffffffffu, g, 0);
+    if (g >= L.nslices) break;
+    // the slice's particles: slot, cell, position, exclusions, site flag
+    int my_cell = INT_MAX, my_ne = 0, my_vs = 0;
+    float4 my_pos = make_float4(0.f, 0.f, 0.f, 0.f);
+    int my_i = 0;
+    if (lane < kUSlots && kUSlots * g + lane < L.n) {
+      const int s = kUSlots * g + lane;
+      const int a = L.sorted[s];
+      my_i = L.idx[a];
+      my_cell = L.cell_of[a];
+      my_pos = pos[s];
+      my_ne = min(L.excl_n[my_i], 20);
+      my_vs = L.hybrid && my_i >= L.natoms;
+    }
+    float4 pi[kUSlots];
+    int ci[kUSlots], ne[kUSlots];
+    unsigned vsm = 0;
+#pragma unroll
+    for (int k = 0; k < kUSlots; ++k) {
+      pi[k].x = __shfl_sync(0xffffffffu, my_pos.x, k);
+      pi[k].y = __shfl_sync(0xffffffffu, my_pos.y, k);
+      pi[k].z = __shfl_sync(0xffffffffu, my_pos.z, k);
+      ci[k] = __shfl_sync(0xffffffffu, my_cell, k);
+      ne[k] = __shfl_sync(0xffffffffu, my_ne, k);
+      vsm |= (unsigned)__shfl_sync(0xffffffffu, my_vs, k) << k;
+      const int ik = __shfl_sync(0xffffffffu, my_i, k);
+      if (lane < ne[k]) {
+        const int gs = L.gslot[L.excl[(size_t)ik * 20 + lane]];
+        s_ex[warp][k][lane] = (gs & 1) == L.which ? gs >> 1 : -1;
+      }
+    }
+    __syncwarp();
+    const long long base = (long long)g * cap;
+    int cnt = 0;
+    int npair[kUSlots] = {0, 0, 0, 0};
+    // candidates slot hi down to lo, displaced by the run's image shift; gm:
+    // the slice's particles in the walked cell; own: the run is that cell
+    auto scan = [&](int hi, int lo, float sh0, float sh1, float sh2, unsigned gm, bool own) {
+      for (int t0 = hi; t0 >= lo; t0 -= 32) {
+        const int t = t0 - lane;
+        unsigned m = 0;
+        bool inner = false;
+        if (t >= lo) {
+          const float4 pj = pos[t];
+          const bool j_vs = (__float_as_int(pj.w) >> 16) == 3;
+#pragma unroll
+          for (int k = 0; k < kUSlots; ++k) {
+            if (!((gm >> k) & 1u)) continue;
+            float d0 = pi[k].x - pj.x, d1 = pi[k].y - pj.y, d2 = pi[k].z - pj.z;
+            d0 = d0 - sh0;
+            d1 = d1 - sh1;
+            d2 = d2 - sh2;
+            float r2 = d0 * d0;
+            r2 = r2 + d1 * d1;
+            r2 = r2 + d2 * d2;
+            if (!(r2 < rlsq)) continue;
+            if (own && t >= kUSlots * g + k) continue;  // the own cell: only slots below the particle
+            if (((vsm >> k) & 1u) && j_vs) continue;    // no site-site pair
+            bool ok = true;
+            for (int e = 0; e < ne[k]; ++e) ok &= s_ex[warp][k][e] != t;
+            if (!ok) continue;
+            m |= 1u << k;
+            inner |= r2 < rg;
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < kUSlots; ++k) npair[k] += __popc(__ballot_sync(0xffffffffu, (m >> k) & 1u));
+        const unsigned ma = __ballot_sync(0xffffffffu, m != 0);
+        if (m != 0) {
+          const int k = cnt + __popc(ma & below);
+          const int entry = t | (int)(m << 28);
+          if (k < kUBuf) {
+            buf[k] = entry;
+            keys[k] = (unsigned char)(m | (inner ? 0u : 16u));
+          } else if (k < cap) {
+            L.entries[base + k] = entry;  // beyond the sort buffer: stored as found
+          }
+        }
+        cnt += __popc(ma);
+      }
+    };
+    // each cell of the slice in turn (slots are in cell order, so the
+    // particles of one cell are consecutive)
+    for (int k0 = 0; k0 < kUSlots && ci[k0] != INT_MAX;) {
+      const int c0 = ci[k0];
+      unsigned gm = 0;
+      int k1 = k0;
+      while (k1 < kUSlots && ci[k1] == c0) gm |= 1u << k1++;
+      scan(kUSlots * g + k1 - 2, L.cell_start[c0], 0.f, 0.f, 0.f, gm, true);
+      const int ic[3] = {c0 / (nz * ny), (c0 / nz) % ny, c0 % nz};
+      for (int u = 0; u < 13; ++u) {
+        int jc[3];
+        float sh[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const int j = ic[q] + kStencil[u][q];
+          const int w = j >= nc[q] ? 1 : (j < 0 ? -1 : 0);
+          jc[q] = j - w * nc[q];
+          sh[q] = w > 0 ? b[q] : (w < 0 ? -b[q] : 0.f);
+        }
+        const int c = jc[0] * nz * ny + jc[1] * nz + jc[2];
+        scan(L.cell_start[c + 1] - 1, L.cell_start[c], sh[0], sh[1], sh[2], gm, false);
+      }
+      k0 = k1;
+    }
+    // stable counting sort of the buffered entries by key
+    __syncwarp();
+    const int nb = min(cnt, kUBuf);
+    off[lane] = 0;
+    __syncwarp();
+    for (int c = 0; c < nb; c += 32) {
+      const int q = c + lane;
+      const int key = q < nb ? keys[q] : 32 + lane;  // unique keys for the idle lanes
+      const unsigned same = __match_any_sync(0xffffffffu, key);
+      if (q < nb && (same & below) == 0) off[key] += __popc(same);
+      __syncwarp();
+    }
+    {
+      const int n_key = off[lane];
+      int incl = n_key;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      __syncwarp();
+      off[lane] = incl - n_key;  // first position of key `lane`
+      __syncwarp();
+    }
+    for (int c = 0; c < nb; c += 32) {
+      const int q = c + lane;
+      const int key = q < nb ? keys[q] : 32 + lane;
+      const unsigned same = __match_any_sync(0xffffffffu, key);
+      int at = 0;
+      if (q < nb) at = off[key] + __popc(same & below);
+      __syncwarp();
+      if (q < nb && (same & below) == 0) off[key] += __popc(same);
+      if (q < nb && at < cap) L.entries[base + at] = buf[q];
+      __syncwarp();
+    }
+    // empty entries up to the end of the last row
+    const int rows = (cnt + 31) / 32;
+    if (cnt + lane < rows * 32 && cnt + lane < cap) L.entries[base + cnt + lane] = 0;
+    if (lane < kUSlots && kUSlots * g + lane < L.n) {
+      int np = npair[0];
+#pragma unroll
+      for (int k = 1; k < kUSlots; ++k) np = lane == k ? npair[k] : np;
+      L.counts[kUSlots * g + lane] = np;
+      if (np >= L.maxnab) atomicOr(&sc->err, EB_LIST_OVERFLOW);
+    }
+    if (lane == 0) {
+      L.slice_w[g] = rows;
+      if (rows > L.w_cap) {
+        atomicMax(&sc->need_rows[L.which], rows);
+        sc->abort = 1;
+        sc->skip = 1;
+      }
+    }
+    __syncwarp();  // s_ex, buf and keys are rewritten for the next slice
+  }
+}
+
 // ------------------------------------------------------------- nonbonded
 // FP32 nonbonded energies and virials are summed in FP32 over this many list
 // rows of a slice, then in fixed point.
@@ -1254,6 +1482,63 @@ __device__ __forceinline__ long long fixq(float v, unsigned& err) {
   return __float2ll_rn(s);
 }
 
+// The work units of an FP32 nonbonded launch handed to the warps of a block
+// (NBArgs::chunk, NBArgs::window); unit(u) is called for each of them.
+template <typename F>
+__device__ __forceinline__ void nb_schedule(const NBArgs<float>& A, const Blk& bk, int nunits, F&& unit) {
+  const int lane = threadIdx.x & 31;
+  if (A.chunk > 0) {
+    // each block a contiguous range of units (neighbouring slices), its warps
+    // taking them through a shared counter, so they gather from one region of
+    // space and share it in L1, with no barrier between them; the last
+    // chunk/256 of the units are taken from the global counter by whichever
+    // warps finish their block's range first
+    __shared__ int s_next;
+    if (threadIdx.x == 0) s_next = 0;
+    __syncthreads();
+    const int tail = (int)((long long)nunits * min(A.chunk, 256) / 256);
+    const int nstat = nunits - tail;
+    if (A.window > 0) {
+      // runs of W consecutive units dealt to the blocks in turn: the blocks
+      // advance together through one window of space, whose positions and
+      // force sums then stay in L2, while a block's warps still share a run
+      const int W = A.window;
+      for (;;) {
+        int k = 0;
+        if (lane == 0) k = atomicAdd(&s_next, 1);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        const long long u = ((long long)(k / W) * bk.g + bk.b) * W + k % W;
+        if (u >= nstat) break;
+        unit((int)u);
+      }
+    } else {
+      const int lo = (int)((long long)nstat * bk.b / bk.g), hi = (int)((long long)nstat * (bk.b + 1) / bk.g);
+      for (;;) {
+        int k = 0;
+        if (lane == 0) k = atomicAdd(&s_next, 1);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        if (lo + k >= hi) break;
+        unit(lo + k);
+      }
+    }
+    for (;;) {
+      int u = 0;
+      if (lane == 0) u = nstat + (int)atomicAdd(&A.sc->work[A.work], 1u);
+      u = __shfl_sync(0xffffffffu, u, 0);
+      if (u >= nunits) break;
+      unit(u);
+    }
+  } else {
+    for (;;) {
+      int u = 0;
+      if (lane == 0) u = (int)atomicAdd(&A.sc->work[A.work], 1u);
+      u = __shfl_sync(0xffffffffu, u, 0);
+      if (u >= nunits) break;
+      unit(u);
+    }
+  }
+}
+
 // NONBONDED_FORCE.F90:45-104, FP32 force path.  Same structure as
 // k_nonbonded (slices of P = 32/T slots, T lanes per slot, dynamic units of
 // `rows` list rows).  The arithmetic is REAL*4 as in the reference, with
@@ -1310,7 +1595,6 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
   const int4* pos = A.posq;
   const int lane = threadIdx.x & 31, grp = lane / T, q = lane % T;
   unsigned err = 0;
-  const bool run = true;
   // a work unit is `rows` list rows of one slice (a multiple of kEnergyRows)
   const int rows = A.rows;
   const int U = (A.w_cap + rows - 1) / rows;
@@ -1447,56 +1731,220 @@ __global__ void __launch_bounds__(256, 4) k_nonbonded_f32(__grid_constant__ cons
       atomicAdd(fo + 64, (unsigned long long)fi2);
     }
   };
-  if (A.chunk > 0) {
-    // each block a contiguous range of units (neighbouring slices), its warps
-    // taking them through a shared counter, so they gather from one region of
-    // space and share it in L1, with no barrier between them; the last
-    // chunk/256 of the units are taken from the global counter by whichever
-    // warps finish their block's range first
-    __shared__ int s_next;
-    if (threadIdx.x == 0) s_next = 0;
-    __syncthreads();
-    const int tail = (int)((long long)nunits * min(A.chunk, 256) / 256);
-    const int nstat = nunits - tail;
-    if (A.window > 0) {
-      // runs of W consecutive units dealt to the blocks in turn: the blocks
-      // advance together through one window of space, whose positions and
-      // force sums then stay in L2, while a block's warps still share a run
-      const int W = A.window;
-      for (;;) {
-        int k = 0;
-        if (lane == 0) k = atomicAdd(&s_next, 1);
-        k = __shfl_sync(0xffffffffu, k, 0);
-        const long long u = ((long long)(k / W) * bk.g + bk.b) * W + k % W;
-        if (u >= nstat) break;
-        unit((int)u);
-      }
-    } else {
-      const int lo = (int)((long long)nstat * bk.b / bk.g), hi = (int)((long long)nstat * (bk.b + 1) / bk.g);
-      for (;;) {
-        int k = 0;
-        if (lane == 0) k = atomicAdd(&s_next, 1);
-        k = __shfl_sync(0xffffffffu, k, 0);
-        if (lo + k >= hi) break;
-        unit(lo + k);
-      }
-    }
-    for (;;) {
-      int u = 0;
-      if (lane == 0) u = nstat + (int)atomicAdd(&sc->work[A.work], 1u);
-      u = __shfl_sync(0xffffffffu, u, 0);
-      if (u >= nunits) break;
-      unit(u);
-    }
-  } else {
-    for (;;) {
-      int u = 0;
-      if (lane == 0) u = run ? (int)atomicAdd(&sc->work[A.work], 1u) : nunits;
-      u = __shfl_sync(0xffffffffu, u, 0);
-      if (u >= nunits) break;
-      unit(u);
+  nb_schedule(A, bk, nunits, unit);
+  if (err) atomicOr(&sc->err, err);
+  long long acc[9];
+  for (int k = 0; k < 9; ++k) acc[k] = (threadIdx.x & 1) ? 0 : lacc[k * kNbPairs + (threadIdx.x >> 1)];
+  __syncthreads();
+  block_sum_i64<9>(acc, lacc);
+  if (threadIdx.x < 9 && lacc[threadIdx.x] != 0)
+    atomicAdd(&sc->nbacc[A.work][threadIdx.x], (unsigned long long)lacc[threadIdx.x]);
+}
+
+// NONBONDED_FORCE.F90:45-104 over slice lists (k_list_build_slices), FP32
+// force path.  A warp takes a unit of `rows` rows of one slice: its 32 lanes
+// take 32 entries of the slice's list at a time, and each lane evaluates the
+// pairs of its entry's neighbour with the (up to four) particles of its mask,
+// holding the four particles' positions in registers.  The pair arithmetic,
+// cutoff handling, error bits, fixed-point conversion and energy/virial
+// grouping are those of k_nonbonded_f32, so every pair's force
+// contribution is the same integer and the force sums are bit for bit those
+// of the per-particle form.  What changes is what a pair costs in memory
+// traffic: one list entry, one position gather and one set of three j-force
+// atomics serve all the pairs of an entry, and the slice's i-forces are
+// summed over the warp once per unit (a butterfly that leaves each of the
+// twelve sums on one pair of lanes) before one atomic each.
+template <bool SMEM, bool MIXED, bool B>
+__global__ void __launch_bounds__(256, 3) k_nonbonded_slices(__grid_constant__ const NBArgs<float> A0,
+                                                             const NBArgs<float>* const* tab, const BlockMap bm) {
+  pdl_wait();
+  pdl_trigger();
+  const Blk bk = blk<B>(bm);
+  __shared__ NBArgs<float> s_args;
+  if (B) stage_args(&s_args, tab[bk.sys]);
+  const NBArgs<float>& A = B ? s_args : A0;
+  Scalars* sc = A.sc;
+  if (nb_idle(A)) return;
+  extern __shared__ unsigned char smem_raw[];
+  long long* lacc = (long long*)smem_raw;  // [9][kNbPairs] sums of each pair of lanes
+  const int4* ptab = A.ptab;
+  const float4* tco = A.tcoef;
+  {
+    unsigned char* p = smem_raw + kNbAccBytes;
+    if (SMEM) {
+      int4* s_ptab = (int4*)p;       p += sizeof(int4) * A.ntype * A.ntype;
+      float4* s_co = (float4*)p;
+      for (int k = threadIdx.x; k < A.nrows; k += blockDim.x) s_co[k] = A.tcoef[k];
+      for (int k = threadIdx.x; k < A.ntype * A.ntype; k += blockDim.x) s_ptab[k] = A.ptab[k];
+      ptab = s_ptab; tco = s_co;
     }
   }
+  if (!(threadIdx.x & 1))
+    for (int k = 0; k < 9; ++k) lacc[k * kNbPairs + (threadIdx.x >> 1)] = 0;
+  __syncthreads();
+  const float ux = (float)(sc->box[0] * 0x1p-32), uy = (float)(sc->box[1] * 0x1p-32), uz = (float)(sc->box[2] * 0x1p-32);
+  const float2 uxy = make_float2(ux, uy);
+  const int4* pos = A.posq;
+  const int lane = threadIdx.x & 31;
+  unsigned err = 0;
+  const int rows = A.rows;
+  const int U = (A.w_cap + rows - 1) / rows;
+  const int nunits = A.nslices * U;
+  long long* la = lacc + (threadIdx.x >> 1);
+  // each warp's slice: the positions of its four particles, read from shared
+  // memory by the pair passes (held in registers they push the kernel past
+  // its 80-register bound into spills)
+  __shared__ int4 s_pi[8][kUSlots];
+  auto unit = [&](int u) {
+    const int g = u / U;
+    const int r0 = (u - g * U) * rows;
+    const int w = min(A.slice_w[g], A.w_cap);
+    if (r0 >= w) return;
+    const int r1 = min(w, r0 + rows);
+    const int s0 = kUSlots * g;
+    int4* pi = s_pi[threadIdx.x >> 5];
+    if (lane < kUSlots) pi[lane] = s0 + lane < A.n ? pos[s0 + lane] : make_int4(0, 0, 0, 0);
+    __syncwarp();
+    const int* ent = A.entries + (long long)g * A.w_cap * 32 + lane;
+    long long fi[kUSlots][3];
+#pragma unroll
+    for (int k = 0; k < kUSlots; ++k) fi[k][0] = fi[k][1] = fi[k][2] = 0;
+    // energies and virials: FP32 over kEnergyRows rows, then fixed point
+    for (int b0 = r0; b0 < r1; b0 += kEnergyRows) {
+      const int b1 = min(r1, b0 + kEnergyRows);
+      // V_NB(1), V_NB(2), V_NB(3) terms (MIXED); e1 alone otherwise.  The
+      // virials are summed scaled by -2^32 (exact: a power of two).
+      float e1 = 0.f, e2 = 0.f, e3 = 0.f;
+      float2 v03 = make_float2(0.f, 0.f), v15 = v03, v24 = v03;
+      auto entry = [&](int e, const int4& pj) {
+        const int t = (int)((unsigned)e & kUSlotMask);
+        const unsigned m = (unsigned)e >> 28;
+        const int wj = pj.w;
+        const int tj = wj & 0xffff, lj = wj >> 16;
+        long long qj0 = 0, qj1 = 0, qj2 = 0;
+        bool hit = false;
+#pragma unroll
+        for (int k = 0; k < kUSlots; ++k) {
+          if (!((m >> k) & 1u)) continue;
+          const int4 pik = pi[k];
+          const float2 d01 = __fmul2_rn(make_float2((float)(int)((unsigned)pik.x - (unsigned)pj.x),
+                                                    (float)(int)((unsigned)pik.y - (unsigned)pj.y)),
+                                        uxy);
+          const float d0 = d01.x, d1 = d01.y;
+          const float d2 = (float)(int)((unsigned)pik.z - (unsigned)pj.z) * uz;
+          const float r2 = __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, d0 * d0));
+          if (!(r2 < A.rcut_hi)) continue;
+          if (r2 > A.rcut_lo) {  // at the cutoff: k_nb_near decides and computes it
+            const unsigned kk = atomicAdd(&sc->near_n[A.work], 1u);
+            if (kk < (unsigned)A.near_cap)
+              A.near[kk] = make_int4(s0 + k, t, A.idx[A.sorted[s0 + k]], A.idx[A.sorted[t]]);
+            continue;  // beyond the buffer: k_nb_near has the step repeated with a larger one
+          }
+          const int wi = pik.w;
+          const int ti = wi & 0xffff, li = wi >> 16;
+          const int4 pt = ptab[ti * A.ntype + tj];
+          const float r = r2 * rsqrtf(r2);
+          const float rb = r * __int_as_float(pt.z);  // r / bin
+          int ni = (int)rb;
+          err |= pt.w ? 0u : (unsigned)EB_MISSING_TABLE;
+          err |= ni > pt.y ? (unsigned)EB_TABLE_RANGE : 0u;
+          ni = min(ni, pt.y);
+          const float uu = rb - (float)ni;
+          const float4 co = tco[pt.x + ni];  // {F base, P base, dF, dP}
+          const float2 fv = __ffma2_rn(make_float2(co.z, co.w), make_float2(uu, uu), make_float2(co.x, co.y));
+          const float fij = fv.x, vij = fv.y;
+          if (MIXED) {
+            // V_NB(1) for an atom i, V_NB(3) for a site i or a bead i with a
+            // site j, V_NB(2) for two beads
+            if (li == 1) e1 += vij;
+            else if (li == 3 || lj == 3) e3 += vij;
+            else if (lj == 2) e2 += vij;
+          } else {
+            e1 += vij;
+          }
+          const float fs = fij * -kFixScale;
+          err |= fabsf(fs) * r < kFixLimScaled ? 0u : (unsigned)EB_FIXED;
+          const float2 sxy = __fmul2_rn(make_float2(fs, fs), d01);
+          const float sx = sxy.x, sy = sxy.y, sz = fs * d2;
+          const long long qx = __float2ll_rn(sx), qy = __float2ll_rn(sy), qz = __float2ll_rn(sz);
+          fi[k][0] -= qx; fi[k][1] -= qy; fi[k][2] -= qz;
+          qj0 += qx; qj1 += qy; qj2 += qz;
+          hit = true;
+          v03 = __ffma2_rn(sxy, make_float2(d0, d0), v03);
+          v15 = __ffma2_rn(make_float2(sy, sz), make_float2(d1, d1), v15);
+          v24 = __ffma2_rn(make_float2(sz, sz), make_float2(d2, d0), v24);
+        }
+        if (hit) {
+          unsigned long long* fj = (unsigned long long*)A.fsort + fs_at(t);
+          atomicAdd(fj, (unsigned long long)qj0);
+          atomicAdd(fj + 32, (unsigned long long)qj1);
+          atomicAdd(fj + 64, (unsigned long long)qj2);
+        }
+      };
+      // two rows per iteration: both entry loads and both position gathers
+      // in flight before either is evaluated; entries are read once per
+      // launch (evict-first), empty ones (mask 0) point at slot 0
+      for (int it = b0; it < b1; it += 2) {
+        const bool has1 = it + 1 < b1;
+        const int ea = __ldcs(ent + it * 32);
+        const int eb = has1 ? __ldcs(ent + (it + 1) * 32) : 0;
+        const int4 pa = pos[(unsigned)ea & kUSlotMask];
+        const int4 pb = pos[(unsigned)eb & kUSlotMask];
+        entry(ea, pa);
+        if (has1) entry(eb, pb);
+      }
+      long long v[9];
+      v[0] = fixq<24>(e1, err);
+      v[1] = MIXED ? fixq<24>(e2, err) : 0;
+      v[2] = MIXED ? fixq<24>(e3, err) : 0;
+      {
+        const float vir[6] = {v03.x, v15.x, v24.x, v03.y, v24.y, v15.y};
+#pragma unroll
+        for (int k = 0; k < 6; ++k) v[3 + k] = fixq<24>(vir[k] * -0x1p-32f, err);
+      }
+#pragma unroll
+      for (int k = 0; k < 9; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], 1);
+      if (!(lane & 1)) {
+        if (MIXED) {
+#pragma unroll
+          for (int k = 0; k < 3; ++k) la[k * kNbPairs] += v[k];
+        } else {
+          const int li = pi[0].w >> 16;  // the list's one label
+          la[(li == 1 ? 0 : (li == 2 ? 1 : 2)) * kNbPairs] += v[0];
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) la[(3 + k) * kNbPairs] += v[3 + k];
+      }
+    }
+    // the twelve i-force sums over the warp: at each level a lane keeps one
+    // half of its values and adds the partner's share of that half, which
+    // leaves sum 8 b4 + 4 b3 + 2 b2 + b1 (b: the lane's bits) on lanes 2m, 2m+1
+    long long v[16];
+#pragma unroll
+    for (int k = 0; k < kUSlots; ++k)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) v[3 * k + c] = fi[k][c];
+#pragma unroll
+    for (int k = 12; k < 16; ++k) v[k] = 0;
+#pragma unroll
+    for (int h = 8, o = 16; h >= 1; h >>= 1, o >>= 1) {
+      const bool up = (lane & o) != 0;
+#pragma unroll
+      for (int j = 0; j < h; ++j) {
+        const long long send = up ? v[j] : v[j + h];
+        const long long keep = up ? v[j + h] : v[j];
+        v[j] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+      }
+    }
+    const long long tot = v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+    const int vi = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+    if (!(lane & 1) && vi < 3 * kUSlots && tot != 0) {
+      const int s = s0 + vi / 3;
+      if (s < A.n) atomicAdd((unsigned long long*)A.fsort + fs_at(s) + 32 * (vi % 3), (unsigned long long)tot);
+    }
+    __syncwarp();  // pi is rewritten by the next unit
+  };
+  nb_schedule(A, bk, nunits, unit);
   if (err) atomicOr(&sc->err, err);
   long long acc[9];
   for (int k = 0; k < 9; ++k) acc[k] = (threadIdx.x & 1) ? 0 : lacc[k * kNbPairs + (threadIdx.x >> 1)];

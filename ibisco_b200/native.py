@@ -36,7 +36,7 @@ EXPORTS = [
     "ibg_create", "ibg_set_state", "ibg_step", "ibg_forces", "ibg_run", "ibg_get_state",
     "ibg_get_state_f64", "ibg_get_neighbour_list", "ibg_get_exclusions", "ibg_set_timing",
     "ibg_get_timing", "ibg_last_error", "ibg_destroy", "ibg_version", "ibg_set_l2_flush", "ibg_set_device",
-    "ibg_set_list_rows", "ibg_nonbonded_static",
+    "ibg_set_list_rows", "ibg_set_list_form", "ibg_get_list_form", "ibg_nonbonded_static",
     "ibg_batch_create", "ibg_batch_run", "ibg_batch_size", "ibg_batch_get_timing", "ibg_batch_last_error",
     "ibg_batch_destroy", "ibg_device_bytes", "ibg_estimate_bytes",
     "ibg_server_create", "ibg_server_submit", "ibg_server_wait", "ibg_server_drain", "ibg_server_result",
@@ -48,6 +48,7 @@ EXPORTS = [
 
 IBG_JOB_QUEUED, IBG_JOB_RUNNING, IBG_JOB_DONE, IBG_JOB_FAILED = 0, 1, 2, 3
 IBG_VS_COM_FIXED, IBG_VS_COM_REFERENCE = 0, 1
+LIST_PER_PARTICLE, LIST_PER_SLICE = 0, 1  # ibg_set_list_form
 
 
 _I, _F, _PI, _PF = ctypes.c_int, ctypes.c_float, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)
@@ -175,6 +176,8 @@ def lib(build_if_missing: bool = True):
         "ibg_set_l2_flush": (ctypes.c_int, [vp, ctypes.c_longlong]),
         "ibg_set_device": (ctypes.c_int, [ctypes.c_int]),
         "ibg_set_list_rows": (ctypes.c_int, [vp, ctypes.c_int]),
+        "ibg_set_list_form": (ctypes.c_int, [vp, ctypes.c_int]),
+        "ibg_get_list_form": (ctypes.c_int, [vp]),
         "ibg_set_vsite_com": (ctypes.c_int, [vp, ctypes.c_int]),
         "ibg_nonbonded_static": (ctypes.c_int, [ctypes.c_int, ctypes.c_int] + [vp] * 5 + [ctypes.c_int, vp, ctypes.c_int, vp,
                                                 ctypes.c_int, ctypes.c_int] + [vp] * 5 + [vp, ctypes.c_float, vp, vp, vp,
@@ -436,6 +439,15 @@ class System:
 
     def set_timing(self, on: bool):
         self._check(lib().ibg_set_timing(self._h, 1 if on else 0))
+
+    def set_list_form(self, form: int):
+        """Verlet-list form of the FP32 path: LIST_PER_PARTICLE (0, the
+        default) or LIST_PER_SLICE (1).  The lists are rebuilt by the next
+        set_state, which must follow."""
+        self._check(lib().ibg_set_list_form(self._h, int(form)))
+
+    def list_form(self) -> int:
+        return int(lib().ibg_get_list_form(self._h))
 
     def set_l2_flush(self, nbytes: int):
         self._check(lib().ibg_set_l2_flush(self._h, int(nbytes)))

@@ -220,6 +220,25 @@ int ibg_set_l2_flush(ibg_ctx* c, long long bytes);
    (the same path a growing system takes).  stage_ms[7] of ibg_get_timing
    counts the growths. */
 int ibg_set_list_rows(ibg_ctx* c, int rows);
+/* Form of the stored Verlet lists (FP32 path; the FP64 path always keeps
+   IBG_LIST_PER_PARTICLE).  IBG_LIST_PER_PARTICLE (the default): a list per
+   particle, eight lanes of the nonbonded kernel per particle.
+   IBG_LIST_PER_SLICE: a list per slice of four consecutive
+   slots holding each neighbour once, with a mask of which of the four it
+   pairs with; the same pairs as the reference's half lists, so
+   ibg_get_neighbour_list returns the same LIST and NNEBS and every force sum
+   is bit for bit the same, but each stored neighbour's position is gathered
+   and its force added once per slice.  On the 2,000,000-bead melt that cuts
+   the nonbonded kernel's DRAM traffic from 1.06 GB to 0.45 GB a launch and
+   its time by 4 %, but the slice list build takes 3.1 ms against 2.2 ms, so
+   with lists rebuilt every 10 steps a step is 3 % slower; the slice form
+   pays where lists are rebuilt less often.  Changing the form discards the
+   stored lists: ibg_set_state must be called again before the next step.
+   ibg_get_list_form returns the form in use. */
+#define IBG_LIST_PER_PARTICLE 0
+#define IBG_LIST_PER_SLICE 1
+int ibg_set_list_form(ibg_ctx* c, int form);
+int ibg_get_list_form(const ibg_ctx* c);
 /* Launch tuning of the nonbonded kernel: nb_tables_smem stages the tables in
    shared memory per block (1) or reads them through L1 (0; the FP32 default,
    the FP64 path stages them); nb_blocks_per_sm limits the resident blocks per

@@ -86,3 +86,24 @@ def test_energies_are_bitwise_reproducible(sysdir):
     ob = b.run(1, 30, observe=True)
     assert oa == ob
     same_state(a, b)
+
+
+def test_batch_mixes_list_forms(sysdir):
+    """Systems with slice lists and systems with per-particle lists share a
+    batch (one launch per list form and stage); each system's trajectory is
+    bitwise the one it has alone in either form."""
+    names = ["melt", "mix5_mts", "fluid"]
+    dirs = [sysdir(n) for n in names]
+    alone = [system(d) for d in dirs]
+    for g in alone:
+        g.run(1, 23)
+    mixed = []
+    for k, d in enumerate(dirs):
+        g = native.System(native.Setup(d), native.IBG_PREC_FP32_FIXED)
+        g.set_list_form(native.LIST_PER_SLICE if k != 1 else native.LIST_PER_PARTICLE)
+        g.set_state()
+        mixed.append(g)
+    b = native.Batch(mixed)
+    b.run(23)
+    for g0, g1 in zip(alone, mixed):
+        same_state(g0, g1)

@@ -319,3 +319,57 @@ def test_tuning_changes_no_trajectory(sysdir):
     for k in ("sxyz", "vxyz", "fxyz"):
         assert np.array_equal(sa[k], sb[k]) and np.array_equal(sb[k], sc[k]) and np.array_equal(sa[k], sw[k])
     assert oa == ob == oc == ow
+
+
+def make_form(d, form):
+    s = native.Setup(d)
+    g = native.System(s, native.IBG_PREC_FP32_FIXED)
+    g.set_list_form(form)
+    g.set_state()
+    assert g.list_form() == form
+    return s, g
+
+
+@pytest.mark.parametrize("name", ["melt", "mix4", "mix5_mts", "mix_nve", "hybrid"])
+def test_list_forms_agree(sysdir, name):
+    """The slice lists (each neighbour once per slice of four slots, with a mask
+    of its pairs) hold exactly the per-particle lists' pairs: the exported
+    LIST and NNEBS are identical, every force sum is the same integer, so the
+    trajectory is the same bit for bit; only the order of the FP32 energy and
+    virial partial sums differs."""
+    d = sysdir(name)
+    _, a = make_form(d, native.LIST_PER_PARTICLE)
+    _, b = make_form(d, native.LIST_PER_SLICE)
+    for which in (0, 1):
+        la, na = a.neighbour_list(which)
+        lb, nb = b.neighbour_list(which)
+        np.testing.assert_array_equal(na, nb)
+        np.testing.assert_array_equal(la, lb)
+    fa, fb = a.forces(1), b.forces(1)
+    assert np.array_equal(a.state64()["fxyz"], b.state64()["fxyz"])
+    # FP32 partial sums in another order: within the energy tolerance
+    for k in ("V_NB1", "V_NB2", "V_NB3"):
+        assert fa[k] == pytest.approx(fb[k], rel=ENERGY_TOL, abs=1e-9), k
+    a.set_state()
+    b.set_state()
+    oa, ob = a.run(1, 25, observe=True), b.run(1, 25, observe=True)
+    sa, sb = a.state64(), b.state64()
+    for k in ("sxyz", "vxyz", "fxyz"):
+        assert np.array_equal(sa[k], sb[k]), k
+    for x, y in zip(oa, ob):
+        for k in ("V_NB1", "V_NB2", "V_NB3"):
+            assert x[k] == pytest.approx(y[k], rel=ENERGY_TOL, abs=1e-9), k
+
+
+def test_list_form_switch_needs_a_new_state(sysdir):
+    d = sysdir("melt")
+    _, g = make_form(d, native.LIST_PER_SLICE)
+    g.set_list_form(native.LIST_PER_PARTICLE)
+    with pytest.raises(native.IbiscoError):
+        g.run(1, 2)
+    g.set_state()
+    g.run(1, 2)
+    s64 = native.System(native.Setup(d), native.IBG_PREC_FP64_PLAIN)
+    assert s64.list_form() == native.LIST_PER_PARTICLE
+    with pytest.raises(native.IbiscoError):
+        s64.set_list_form(native.LIST_PER_SLICE)
