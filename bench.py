@@ -214,6 +214,8 @@ def workload_config(args, n: int) -> dict:
         cfg["virtual_sites"] = "reference centre-of-mass form (VIRTUAL_DEF.f90:31 resets only the x sum)"
     if args.list_form == "slice":
         cfg["verlet_lists"] = "FP32 path: one list per slice of four slots, a pair mask per neighbour"
+    elif args.list_form == "per-particle":
+        cfg["verlet_lists"] = "FP32 path: one list per particle"
     return cfg
 
 
@@ -225,11 +227,11 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(workload: str):
-    """DRAM bytes (read + write) per nonbonded launch of this workload, from
-    its committed ncu summary (a 'dram_bytes_per_launch: <n>' line), or None
-    where no capture of this workload exists."""
-    kernel = "nonbonded_slices" if LIST_FORM["form"] == "slice" else "nonbonded"
+def ncu_traffic(workload: str, slice_lists: bool):
+    """DRAM bytes (read + write) per nonbonded launch of this workload and
+    list form, from its committed ncu summary (a 'dram_bytes_per_launch: <n>'
+    line), or None where no capture of this workload exists."""
+    kernel = "nonbonded_slices" if slice_lists else "nonbonded"
     p = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
     if not os.path.exists(p):
         return None
@@ -474,7 +476,7 @@ def reduce_sum(pg, x: float) -> float:
 
 TUNING_KEYS = ("nb_tables_smem", "nb_blocks_per_sm", "nb_chunk", "nb_rows", "nb_window")
 VS_COM = {"form": "fixed"}  # --vs-com
-LIST_FORM = {"form": "per-particle"}  # --list-form
+LIST_FORM = {"form": "auto"}  # --list-form
 
 
 def new_system(native, setup, prec):
@@ -483,8 +485,8 @@ def new_system(native, setup, prec):
     g = native.System(setup, prec)
     if VS_COM["form"] == "reference":
         g.set_vsite_com(native.IBG_VS_COM_REFERENCE)
-    if LIST_FORM["form"] == "slice" and prec == native.IBG_PREC_FP32_FIXED:
-        g.set_list_form(native.LIST_PER_SLICE)
+    if LIST_FORM["form"] != "auto" and prec == native.IBG_PREC_FP32_FIXED:
+        g.set_list_form(native.LIST_PER_SLICE if LIST_FORM["form"] == "slice" else native.LIST_PER_PARTICLE)
     return g
 
 
@@ -604,9 +606,10 @@ def run_b200(args, world, rank, local, pg):
         bytes_launch = nb_bytes / nb_count
         peak, peak_kind = measured_peak()
         achieved = bytes_launch / nb_launch_s / 1e9
-        roof = {"bound": "hbm", "kernel": "k_nonbonded_slices" if args.list_form == "slice" else "k_nonbonded",
+        slice_lists = prec == native.IBG_PREC_FP32_FIXED and g.list_form() == native.LIST_PER_SLICE
+        roof = {"bound": "hbm", "kernel": "k_nonbonded_slices" if slice_lists else "k_nonbonded",
                 "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": ncu_traffic(args.workload),
+                "frac": achieved / peak, "traffic": ncu_traffic(args.workload, slice_lists),
                 "peak_kind": peak_kind, "launch_us": nb_launch_s * 1e6,
                 "algorithmic_bytes_per_launch": bytes_launch,
                 "mean_half_list": {("atom", "bead")[w]: pw / nw for w, (nw, pw) in lists.items()}}
@@ -727,9 +730,10 @@ def main():
     ap.add_argument("--vs-com", choices=["fixed", "reference"], default="fixed",
                     help="centre-of-mass virtual sites: each at its centre of mass, or the reference's form "
                          "(VIRTUAL_DEF.f90:31 resets only the x sum)")
-    ap.add_argument("--list-form", choices=["per-particle", "slice"], default="per-particle",
-                    help="Verlet lists of the FP32 single-system legs: a list per particle, or one per slice of "
-                         "four slots with a pair mask per neighbour (ibg_set_list_form)")
+    ap.add_argument("--list-form", choices=["auto", "per-particle", "slice"], default="auto",
+                    help="Verlet lists of the FP32 single-system legs: the library's choice by list size, a list "
+                         "per particle, or one per slice of four slots with a pair mask per neighbour "
+                         "(ibg_set_list_form)")
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")

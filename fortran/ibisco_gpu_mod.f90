@@ -68,8 +68,9 @@ MODULE IBISCO_GPU
        TYPE(C_PTR), INTENT(OUT) :: ctx
      END FUNCTION ibg_create
 
-     !> Verlet-list form of the FP32 path: a list per particle (0, the
-     !> default) or per slice of four slots (1); before ibg_set_state.
+     !> Verlet-list form of the FP32 path: automatic (-1, the default), a
+     !> list per particle (0) or per slice of four slots (1); before
+     !> ibg_set_state.
      INTEGER(C_INT) FUNCTION ibg_set_list_form(ctx, form) BIND(C, NAME='ibg_set_list_form')
        IMPORT :: C_PTR, C_INT
        TYPE(C_PTR), VALUE :: ctx

@@ -966,6 +966,20 @@ __global__ void __launch_bounds__(256) k_list_build_thread(__grid_constant__ con
     int* row = L.entries + (long long)g * L.w_cap * 32 + (s % P) * T;
     int cnt = 0, nlate = 0;
     // candidates slot hi down to lo, displaced by the run's image shift
+    // a candidate inside RLIST: exclusions, the site-site rule, then stored
+    auto accept = [&](int t, R r2, const PT& pj) {
+      bool ok = !(i_vs && (Prec<R>::bits(pj.w) >> 16) == 3) && t != e0 && t != e1 && t != e2 && t != e3;
+      if (ok && ne > 4)
+        for (int e = 4; e < ne; ++e) ok &= s_ex[e - 4][threadIdx.x] != t;
+      if (ok) {
+        if (r2 >= rg && nlate < kLateThread) {
+          s_late[nlate++][threadIdx.x] = t;  // the outer group, appended below
+        } else {
+          if (cnt < cap) row[(cnt / T) * 32 + cnt % T] = t;
+          ++cnt;
+        }
+      }
+    };
     auto scan = [&](int hi, int lo, R sh0, R sh1, R sh2) {
 #pragma unroll 4
       for (int t = hi; t >= lo; --t) {
@@ -977,19 +991,7 @@ __global__ void __launch_bounds__(256) k_list_build_thread(__grid_constant__ con
         R r2 = d0 * d0;
         r2 = r2 + d1 * d1;
         r2 = r2 + d2 * d2;
-        if (r2 < rlsq) {
-          bool ok = !(i_vs && (Prec<R>::bits(pj.w) >> 16) == 3) && t != e0 && t != e1 && t != e2 && t != e3;
-          if (ok && ne > 4)
-            for (int e = 4; e < ne; ++e) ok &= s_ex[e - 4][threadIdx.x] != t;
-          if (ok) {
-            if (r2 >= rg && nlate < kLateThread) {
-              s_late[nlate++][threadIdx.x] = t;  // the outer group, appended below
-            } else {
-              if (cnt < cap) row[(cnt / T) * 32 + cnt % T] = t;
-              ++cnt;
-            }
-          }
-        }
+        if (r2 < rlsq) accept(t, r2, pj);
       }
     };
     scan(s - 1, L.cell_start[c0], (R)0, (R)0, (R)0);  // the own cell below this particle
@@ -1070,6 +1072,8 @@ __global__ void __launch_bounds__(256) k_list_build_slices(__grid_constant__ con
   __shared__ int s_buf[kWarps][kUBuf];       // the slice's entries, in the order accepted
   __shared__ unsigned char s_key[kWarps][kUBuf];  // their keys: mask | 16 for the outer group
   __shared__ int s_off[kWarps][32];          // per key: count, then next position
+  __shared__ int2 s_run[kWarps][14];         // each candidate run: highest slot, first index
+  __shared__ float s_sh[kWarps][14][3];      // each candidate run: image shift
   const int nx = sc->ncell[L.which][0], ny = sc->ncell[L.which][1], nz = sc->ncell[L.which][2];
   const int nc[3] = {nx, ny, nz};
   float b[3], bi[3], b2[3];
@@ -1121,20 +1125,73 @@ __global__ void __launch_bounds__(256) k_list_build_slices(__grid_constant__ con
     __syncwarp();
     const long long base = (long long)g * cap;
     int cnt = 0;
-    int npair[kUSlots] = {0, 0, 0, 0};
-    // candidates slot hi down to lo, displaced by the run's image shift; gm:
-    // the slice's particles in the walked cell; own: the run is that cell
-    auto scan = [&](int hi, int lo, float sh0, float sh1, float sh2, unsigned gm, bool own) {
-      for (int t0 = hi; t0 >= lo; t0 -= 32) {
-        const int t = t0 - lane;
+    int npair[kUSlots] = {0, 0, 0, 0};  // this lane's accepted pairs of each particle
+    // each cell of the slice in turn (slots are in cell order, so the
+    // particles of one cell are consecutive).  Its 14 runs (the own cell
+    // below the group's last particle, then the 13 stencil cells) are walked
+    // as one sequence of candidates, 32 at a time: lane u < 14 describes run
+    // u (highest slot, image shift), a prefix sum gives each run's first index
+    for (int k0 = 0; k0 < kUSlots && ci[k0] != INT_MAX;) {
+      const int c0 = ci[k0];
+      unsigned gm = 0;
+      int k1 = k0;
+      while (k1 < kUSlots && ci[k1] == c0) gm |= 1u << k1++;
+      int hi = -1, len = 0;
+      float sh[3] = {0.f, 0.f, 0.f};
+      if (lane == 0) {
+        hi = kUSlots * g + k1 - 2;
+        len = max(0, hi - L.cell_start[c0] + 1);
+      } else if (lane < 14) {
+        const int ic[3] = {c0 / (nz * ny), (c0 / nz) % ny, c0 % nz};
+        int jc[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const int j = ic[q] + kStencil[lane - 1][q];
+          const int w = j >= nc[q] ? 1 : (j < 0 ? -1 : 0);
+          jc[q] = j - w * nc[q];
+          sh[q] = w > 0 ? b[q] : (w < 0 ? -b[q] : 0.f);
+        }
+        const int c = jc[0] * nz * ny + jc[1] * nz + jc[2];
+        hi = L.cell_start[c + 1] - 1;
+        len = hi - L.cell_start[c] + 1;
+      }
+      int incl = len;
+#pragma unroll
+      for (int o = 1; o < 16; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const int total = __shfl_sync(0xffffffffu, incl, 13);
+      __syncwarp();  // the previous cell's run table is no longer read
+      if (lane < 14) {
+        s_run[warp][lane] = make_int2(hi, incl - len);
+        s_sh[warp][lane][0] = sh[0];
+        s_sh[warp][lane][1] = sh[1];
+        s_sh[warp][lane][2] = sh[2];
+      }
+      __syncwarp();
+      for (int v0 = 0; v0 < total; v0 += 32) {
+        const int v = v0 + lane;
         unsigned m = 0;
         bool inner = false;
-        if (t >= lo) {
+        int t = 0;
+        if (v < total) {
+          // the run of candidate v: the last run that starts at or before v
+          // (empty runs start where the next one does, and are skipped)
+          int u = 0;
+#pragma unroll
+          for (int step = 8; step > 0; step >>= 1)
+            if (u + step < 14 && s_run[warp][u + step].y <= v) u += step;
+          const int2 run = s_run[warp][u];
+          t = run.x - (v - run.y);
+          const float sh0 = s_sh[warp][u][0], sh1 = s_sh[warp][u][1], sh2 = s_sh[warp][u][2];
+          const bool own = u == 0;
           const float4 pj = pos[t];
           const bool j_vs = (__float_as_int(pj.w) >> 16) == 3;
 #pragma unroll
           for (int k = 0; k < kUSlots; ++k) {
             if (!((gm >> k) & 1u)) continue;
+            // the reference's REAL*4 distance, scalar and uncontracted
             float d0 = pi[k].x - pj.x, d1 = pi[k].y - pj.y, d2 = pi[k].z - pj.z;
             d0 = d0 - sh0;
             d1 = d1 - sh1;
@@ -1149,11 +1206,10 @@ __global__ void __launch_bounds__(256) k_list_build_slices(__grid_constant__ con
             for (int e = 0; e < ne[k]; ++e) ok &= s_ex[warp][k][e] != t;
             if (!ok) continue;
             m |= 1u << k;
+            ++npair[k];
             inner |= r2 < rg;
           }
         }
-#pragma unroll
-        for (int k = 0; k < kUSlots; ++k) npair[k] += __popc(__ballot_sync(0xffffffffu, (m >> k) & 1u));
         const unsigned ma = __ballot_sync(0xffffffffu, m != 0);
         if (m != 0) {
           const int k = cnt + __popc(ma & below);
@@ -1167,31 +1223,12 @@ __global__ void __launch_bounds__(256) k_list_build_slices(__grid_constant__ con
         }
         cnt += __popc(ma);
       }
-    };
-    // each cell of the slice in turn (slots are in cell order, so the
-    // particles of one cell are consecutive)
-    for (int k0 = 0; k0 < kUSlots && ci[k0] != INT_MAX;) {
-      const int c0 = ci[k0];
-      unsigned gm = 0;
-      int k1 = k0;
-      while (k1 < kUSlots && ci[k1] == c0) gm |= 1u << k1++;
-      scan(kUSlots * g + k1 - 2, L.cell_start[c0], 0.f, 0.f, 0.f, gm, true);
-      const int ic[3] = {c0 / (nz * ny), (c0 / nz) % ny, c0 % nz};
-      for (int u = 0; u < 13; ++u) {
-        int jc[3];
-        float sh[3];
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-          const int j = ic[q] + kStencil[u][q];
-          const int w = j >= nc[q] ? 1 : (j < 0 ? -1 : 0);
-          jc[q] = j - w * nc[q];
-          sh[q] = w > 0 ? b[q] : (w < 0 ? -b[q] : 0.f);
-        }
-        const int c = jc[0] * nz * ny + jc[1] * nz + jc[2];
-        scan(L.cell_start[c + 1] - 1, L.cell_start[c], sh[0], sh[1], sh[2], gm, false);
-      }
       k0 = k1;
     }
+#pragma unroll
+    for (int k = 0; k < kUSlots; ++k)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) npair[k] += __shfl_xor_sync(0xffffffffu, npair[k], o);
     // stable counting sort of the buffered entries by key
     __syncwarp();
     const int nb = min(cnt, kUBuf);

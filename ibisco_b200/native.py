@@ -48,7 +48,7 @@ EXPORTS = [
 
 IBG_JOB_QUEUED, IBG_JOB_RUNNING, IBG_JOB_DONE, IBG_JOB_FAILED = 0, 1, 2, 3
 IBG_VS_COM_FIXED, IBG_VS_COM_REFERENCE = 0, 1
-LIST_PER_PARTICLE, LIST_PER_SLICE = 0, 1  # ibg_set_list_form
+LIST_AUTO, LIST_PER_PARTICLE, LIST_PER_SLICE = -1, 0, 1  # ibg_set_list_form
 
 
 _I, _F, _PI, _PF = ctypes.c_int, ctypes.c_float, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)
@@ -441,9 +441,10 @@ class System:
         self._check(lib().ibg_set_timing(self._h, 1 if on else 0))
 
     def set_list_form(self, form: int):
-        """Verlet-list form of the FP32 path: LIST_PER_PARTICLE (0, the
-        default) or LIST_PER_SLICE (1).  The lists are rebuilt by the next
-        set_state, which must follow."""
+        """Verlet-list form of the FP32 path: LIST_AUTO (-1, the default:
+        slice lists for lists of at least 2*64*32 particles per SM),
+        LIST_PER_PARTICLE (0) or LIST_PER_SLICE (1).  The lists are rebuilt by
+        the next set_state, which must follow."""
         self._check(lib().ibg_set_list_form(self._h, int(form)))
 
     def list_form(self) -> int:

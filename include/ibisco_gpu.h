@@ -221,20 +221,23 @@ int ibg_set_l2_flush(ibg_ctx* c, long long bytes);
    counts the growths. */
 int ibg_set_list_rows(ibg_ctx* c, int rows);
 /* Form of the stored Verlet lists (FP32 path; the FP64 path always keeps
-   IBG_LIST_PER_PARTICLE).  IBG_LIST_PER_PARTICLE (the default): a list per
-   particle, eight lanes of the nonbonded kernel per particle.
-   IBG_LIST_PER_SLICE: a list per slice of four consecutive
+   IBG_LIST_PER_PARTICLE).  IBG_LIST_PER_PARTICLE: a list per particle, eight
+   lanes of the nonbonded kernel per particle.  IBG_LIST_PER_SLICE: a list
+   per slice of four consecutive
    slots holding each neighbour once, with a mask of which of the four it
    pairs with; the same pairs as the reference's half lists, so
    ibg_get_neighbour_list returns the same LIST and NNEBS and every force sum
    is bit for bit the same, but each stored neighbour's position is gathered
    and its force added once per slice.  On the 2,000,000-bead melt that cuts
    the nonbonded kernel's DRAM traffic from 1.06 GB to 0.45 GB a launch and
-   its time by 4 %, but the slice list build takes 3.1 ms against 2.2 ms, so
-   with lists rebuilt every 10 steps a step is 3 % slower; the slice form
-   pays where lists are rebuilt less often.  Changing the form discards the
+   its time by 3 %; its list build is slower, and with lists rebuilt every 10
+   steps a step takes 1.656 ms against 1.669 ms.  IBG_LIST_AUTO (the
+   default): slice lists for lists of at least 2*64*32 particles per SM of the
+   device (606,208 on 148 SMs), per-particle lists below (unmeasured there
+   with slices).  Changing the form discards the
    stored lists: ibg_set_state must be called again before the next step.
    ibg_get_list_form returns the form in use. */
+#define IBG_LIST_AUTO (-1)
 #define IBG_LIST_PER_PARTICLE 0
 #define IBG_LIST_PER_SLICE 1
 int ibg_set_list_form(ibg_ctx* c, int form);
