@@ -37,3 +37,26 @@ def test_version_string_without_gpu():
 def test_create_rejects_null_descriptor():
     h = ctypes.c_void_p()
     assert native.lib().ibg_create(None, 0, ctypes.byref(h)) == -1
+
+
+def header_defines(prefix):
+    src = open(HEADER).read()
+    return {m.group(1): int(m.group(2)) for m in re.finditer(r"#define\s+(" + prefix + r"[A-Z0-9_]*)\s+\(?(-?\d+)\)?", src)}
+
+
+def test_constants_match_the_header():
+    """The binding's precision, centre-of-mass and list-form constants are the
+    header's."""
+    d = header_defines("IBG_")
+    assert d["IBG_PREC_FP32_FIXED"] == native.IBG_PREC_FP32_FIXED
+    assert d["IBG_PREC_FP64_PLAIN"] == native.IBG_PREC_FP64_PLAIN
+    assert d["IBG_VS_COM_FIXED"] == native.IBG_VS_COM_FIXED
+    assert d["IBG_VS_COM_REFERENCE"] == native.IBG_VS_COM_REFERENCE
+    assert d["IBG_LIST_AUTO"] == native.LIST_AUTO
+    assert d["IBG_LIST_PER_PARTICLE"] == native.LIST_PER_PARTICLE
+    assert d["IBG_LIST_PER_SLICE"] == native.LIST_PER_SLICE
+
+
+def test_list_form_rejects_bad_arguments_without_gpu():
+    assert native.lib().ibg_set_list_form(None, native.LIST_PER_SLICE) == -1
+    assert native.lib().ibg_get_list_form(None) == -1
