@@ -1055,7 +1055,10 @@ int ibg_get_list_form(const ibg_ctx* c) {
   if (!c) return IBG_E_INVALID;
   for (const auto& L : c->L)
     if (L.present) return L.form;
-  return c->prec == IBG_PREC_FP32_FIXED ? c->list_form : 0;
+  // no list: the form a list would get if it were explicitly chosen, else
+  // per particle (never IBG_LIST_AUTO, which equals IBG_E_INVALID)
+  return c->prec == IBG_PREC_FP32_FIXED && c->list_form == IBG_LIST_PER_SLICE ? IBG_LIST_PER_SLICE
+                                                                              : IBG_LIST_PER_PARTICLE;
 }
 
 int ibg_autotune(ibg_ctx* c, int reps, ibg_tuning* best, ibg_tuning* cand_out, double* us, int ncand) {

@@ -222,21 +222,22 @@ int ibg_set_l2_flush(ibg_ctx* c, long long bytes);
 int ibg_set_list_rows(ibg_ctx* c, int rows);
 /* Form of the stored Verlet lists (FP32 path; the FP64 path always keeps
    IBG_LIST_PER_PARTICLE).  IBG_LIST_PER_PARTICLE: a list per particle, eight
-   lanes of the nonbonded kernel per particle.  IBG_LIST_PER_SLICE: a list
-   per slice of four consecutive
-   slots holding each neighbour once, with a mask of which of the four it
-   pairs with; the same pairs as the reference's half lists, so
-   ibg_get_neighbour_list returns the same LIST and NNEBS and every force sum
-   is bit for bit the same, but each stored neighbour's position is gathered
-   and its force added once per slice.  On the 2,000,000-bead melt that cuts
-   the nonbonded kernel's DRAM traffic from 1.06 GB to 0.45 GB a launch and
-   its time by 3 %; its list build is slower, and with lists rebuilt every 10
-   steps a step takes 1.656 ms against 1.669 ms.  IBG_LIST_AUTO (the
-   default): slice lists for lists of at least 2*64*32 particles per SM of the
-   device (606,208 on 148 SMs), per-particle lists below (unmeasured there
-   with slices).  Changing the form discards the
-   stored lists: ibg_set_state must be called again before the next step.
-   ibg_get_list_form returns the form in use. */
+   lanes of the nonbonded kernel per particle.  IBG_LIST_PER_SLICE: a list per
+   slice of four consecutive slots holding each neighbour once, with a mask of
+   which of the four it pairs with.  Both hold the reference's half-list
+   pairs, so ibg_get_neighbour_list returns the same LIST and NNEBS and every
+   force sum is bit for bit the same; the slice form gathers each stored
+   neighbour's position and adds its force once per slice.  On the
+   2,000,000-bead melt that cuts the nonbonded kernel's DRAM traffic from
+   1.06 GB to 0.45 GB a launch and its time by 3 %; its list build is slower,
+   and with lists rebuilt every 10 steps a step takes 1.656 ms against
+   1.669 ms (0.0887 against 0.0941 ms on a 40,000-bead melt).  IBG_LIST_AUTO
+   (the default): slice lists for lists of at least 2*64*32 particles per SM
+   of the device (606,208 on 148 SMs), per-particle lists below.  Changing
+   the form discards the stored lists: ibg_set_state must be called again
+   before the next step.  ibg_get_list_form returns the form in use (of the
+   atom list, or of the bead list when there is no atom list):
+   IBG_LIST_PER_PARTICLE or IBG_LIST_PER_SLICE. */
 #define IBG_LIST_AUTO (-1)
 #define IBG_LIST_PER_PARTICLE 0
 #define IBG_LIST_PER_SLICE 1
