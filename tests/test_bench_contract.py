@@ -24,3 +24,21 @@ def test_reference_arm_prints_one_contract_line():
     cb = d["cpu_baseline"]
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_committed_traffic_follows_the_list_form():
+    """The roofline's traffic comes from the committed ncu summary of the
+    kernel that the list form runs, and the workload config names an explicit
+    list form (the same dict on both arms)."""
+    sys.path.insert(0, ROOT)
+    import argparse
+
+    import bench
+
+    per_particle = bench.ncu_traffic("melt2m", False)
+    slices = bench.ncu_traffic("melt2m", True)
+    assert per_particle and slices and slices < 0.5 * per_particle
+    base = dict(workload="melt2m", vs_com="fixed")
+    assert "verlet_lists" not in bench.workload_config(argparse.Namespace(list_form="auto", **base), 2000000)
+    cfg = bench.workload_config(argparse.Namespace(list_form="slice", **base), 2000000)
+    assert "slice" in cfg["verlet_lists"]
