@@ -18,6 +18,8 @@ MODULE IBISCO_GPU
   IMPLICIT NONE
 
   INTEGER(C_INT), PARAMETER :: IBG_PREC_FP32_FIXED = 0, IBG_PREC_FP64_PLAIN = 1
+  INTEGER(C_INT), PARAMETER :: IBG_VS_COM_FIXED = 0, IBG_VS_COM_REFERENCE = 1
+  INTEGER(C_INT), PARAMETER :: IBG_LIST_AUTO = -1, IBG_LIST_PER_PARTICLE = 0, IBG_LIST_PER_SLICE = 1
 
   TYPE, BIND(C) :: IBG_DESC_T
      INTEGER(C_INT) :: natoms, nvirta, nitems, ntype

@@ -60,3 +60,13 @@ def test_constants_match_the_header():
 def test_list_form_rejects_bad_arguments_without_gpu():
     assert native.lib().ibg_set_list_form(None, native.LIST_PER_SLICE) == -1
     assert native.lib().ibg_get_list_form(None) == -1
+
+
+def test_fortran_parameters_match_the_header():
+    """The Fortran module's named constants are the header's."""
+    src = open(os.path.join(os.path.dirname(HEADER), "..", "fortran", "ibisco_gpu_mod.f90")).read()
+    params = {m.group(1): int(m.group(2)) for m in re.finditer(r"\b(IBG_[A-Z0-9_]+)\s*=\s*(-?\d+)", src)}
+    d = header_defines("IBG_")
+    assert params, "no PARAMETER constants found"
+    for name, value in params.items():
+        assert d[name] == value, name
