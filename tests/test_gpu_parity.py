@@ -363,6 +363,9 @@ def test_list_forms_agree(sysdir, name):
 
 def test_list_form_switch_needs_a_new_state(sysdir):
     d = sysdir("melt")
+    # the automatic form takes slice lists only from 2*64*32 particles per SM
+    _, auto = make(d, native.IBG_PREC_FP32_FIXED)
+    assert auto.list_form() == native.LIST_PER_PARTICLE
     _, g = make_form(d, native.LIST_PER_SLICE)
     g.set_list_form(native.LIST_PER_PARTICLE)
     with pytest.raises(native.IbiscoError):
